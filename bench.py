@@ -1,0 +1,363 @@
+"""Benchmark of the SOD stage: halos/s on a synthetic clustered box.
+
+A step is one pass of the hot path over one box: the cell sort of the
+particles (the reference's linked list), CIC density, seed order and the SOD
+(spherover) through psod_run.  ``value`` is whole-job halos/s with the
+particles already in HBM; ``e2e`` is the same through the C-ABI from pinned
+host buffers, with the host-to-device copy of the particles and the
+device-to-host copy of the halo table inside the timed region.
+
+One process per GPU (torchrun for N > 1).  The SOD of one box does not
+shard, so every rank runs an independent replica on its own box (weak
+scaling); the ranks only meet at a barrier and a max-reduction of the
+timings.
+
+``--impl reference`` times the reference algorithm on the host cores: the
+CPU oracle (a C restatement of the Fortran, reference arithmetic) on a
+bounded sample of the workload, one sample box per core.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# synthetic workloads: the reference's box sizes with the NFW-mixture generator
+WORKLOADS = {
+    128: dict(nmax_halo=20000, box="128^3, 82.03125 Mpc/h, halo N in [20, 2e4]"),
+    256: dict(nmax_halo=50000, box="256^3, halo N in [20, 5e4]"),
+    512: dict(nmax_halo=200000, box="512^3, 656.25 Mpc/h, halo N in [20, 2e5]"),
+    1024: dict(nmax_halo=1000000, box="1024^3, 1312.5 Mpc/h, halo N in [20, 1e6]"),
+}
+
+
+def npu_for(nx):
+    return {128: 0, 256: 0, 512: 200000, 1024: 1000000}.get(nx, 0)
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(
+                    ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits"],
+                    capture_output=True, text=True, timeout=5,
+                ).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=6)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit())
+        mx = max(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if "Active" in s[3 + i]})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_setup():
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+
+    from psod_b200 import synth
+    from psod_b200.sod import SphericalOverdensity
+
+    world, rank, local = dist_setup()
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    nx = args.nx
+    wl = WORKLOADS.get(nx, dict(nmax_halo=20000, box=f"{nx}^3"))
+    box = synth.make_box(nx, nmax_halo=wl["nmax_halo"], seed=args.seed + rank, device=f"cuda:{dev}")
+    pos_d, ids_d = box.pos, box.ids
+    n = box.n
+    params = dict(npu=npu_for(nx), mode=args.mode_id)
+    if args.ndelta:
+        params["delta_extra"] = (500.0, 178.0)
+        params["nbins"] = 48
+    sod = SphericalOverdensity(nx, device=dev, **params)
+    # L2 flush buffer (used when the inputs are smaller than L2)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
+    inputs_bytes = n * (12 + 8)
+    need_flush = inputs_bytes < (126 << 20) * 2
+
+    def step_device():
+        if need_flush:
+            flush.zero_()
+        sod.load(pos_d, ids_d)
+        return sod.run()
+
+    for _ in range(args.warmup):
+        st = step_device()
+    torch.cuda.synchronize()
+    barrier(world)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats_list = []
+    with ClockSampler(dev) as clk:
+        torch.cuda.synchronize()
+        ev0.record()
+        for _ in range(args.steps):
+            stats_list.append(step_device())
+        ev1.record()
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    ms = max_over_ranks(ms, world)
+    nhalo = stats_list[-1]["nhalo"]
+
+    # e2e: pinned host buffers through the C-ABI, copies inside the timed region
+    pos_h = pos_d.cpu().pin_memory()
+    ids_h = ids_d.cpu().pin_memory()
+    t = sod.halos(members=True)
+    nm = t.member_index.shape[0]
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sod.load(pos_h, ids_h)
+        sod.run()
+        t = sod.halos(members=True)
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
+    e2e_ms = max_over_ranks(e2e_ms, world)
+    d2h = t.halo_id.nbytes + t.halo_mass.nbytes + t.halo_rank.nbytes + t.halo_center.nbytes + t.halo_rdelta.nbytes \
+        + t.halo_mass2.nbytes + t.halo_mextra.nbytes + t.halo_profile.nbytes + t.member_offset.nbytes \
+        + t.member_index.nbytes + t.member_id.nbytes
+
+    s = stats_list[-1]
+    peak, peak_kind = load_peaks()
+    # dominant kernel: the per-seed SOD kernel.  Algorithmic bytes: one
+    # 16-byte record per particle of each examined seed's preselect cube
+    # (count pass), plus the claim (4 B) and member (12 B) writes.
+    alg_bytes = 16.0 * s["touched"] + 4.0 * n * 0 + 16.0 * s["nmember"]
+    kern_s = s["ms_sod_kernel"] / 1000.0
+    achieved = alg_bytes / kern_s / 1e9 if kern_s > 0 else 0.0
+    value = world * nhalo / (ms / 1000.0)
+    line = {
+        "metric": "SOD halos/s (delta=200, N200 exact)",
+        "value": round(value, 2),
+        "unit": "halos/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms, 3),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic NFW-mixture box (seeded); inputs resident in HBM",
+        "config": {
+            "workload": wl["box"],
+            "nx": nx,
+            "particles": n,
+            "mode": args.mode,
+            "npu": params["npu"],
+            "halos": nhalo,
+            "members": s["nmember"],
+            "seeds": s["npart_new"],
+            "processed_seeds": s["nprocessed"],
+            "rounds": s["rounds"],
+            "l2": "flushed between steps" if need_flush else "inputs larger than L2",
+            "parallelism": f"replicas x{world}",
+        },
+        "e2e": {
+            "value": round(world * nhalo / (e2e_ms / 1000.0), 2),
+            "unit": "halos/s",
+            "h2d_bytes_per_step": int(n * (12 + 8)),
+            "d2h_bytes_per_step": int(d2h),
+            "ms_per_step": round(e2e_ms, 3),
+        },
+        "gpu_launches": int(s["kernel_launches"]),
+        "roofline": {
+            "bound": "hbm",
+            "kernel": "k_sod_seeds",
+            "achieved": round(achieved, 1),
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": round(achieved / peak, 4),
+            "peak_kind": peak_kind,
+            "traffic": None,
+            "sod_kernel_ms": round(s["ms_sod_kernel"], 3),
+            "sod_stage_ms": round(s["ms_total"], 3),
+        },
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, nx, wl, quick=True)
+    sod.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def _cpu_sample(seed, nx, nmax):
+    """One sample box through the oracle's reference arithmetic."""
+    from oracle import oracle as O
+    from psod_b200 import synth
+
+    b = synth.make_box(nx, nmax_halo=nmax, seed=seed)
+    t0 = time.perf_counter()
+    r = O.run(O.Params(nx=nx), b.pos, b.ids, O.REFERENCE)
+    return r.nhalo, time.perf_counter() - t0
+
+
+def cpu_baseline(args, nx, wl, quick=False, cores=None):
+    """The reference algorithm on host cores: one sample box per core."""
+    import multiprocessing as mp
+
+    from oracle import oracle as O
+
+    O.build()
+    snx = 64 if quick else 96
+    nmax = 5000 if quick else 10000
+    ncores = 1 if quick else (cores or os.cpu_count() or 1)
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(ncores) as pool:
+        res = pool.starmap(_cpu_sample, [(args.seed + 100 + i, snx, nmax) for i in range(ncores)])
+    wall = time.perf_counter() - t0
+    halos = sum(r[0] for r in res)
+    busy = max(r[1] for r in res)
+    return {
+        "value": round(halos / busy, 3),
+        "unit": "halos/s",
+        "cores": ncores,
+        "kind": "port",
+        "sample": f"{ncores} box(es) of {snx}^3 with the same generator (halo N in [20, {nmax}]), "
+                  f"full cic/cicm1/tri_cic/spherover, reference arithmetic; wall {wall:.1f}s",
+    }
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    nx = args.nx
+    wl = WORKLOADS.get(nx, dict(nmax_halo=20000, box=f"{nx}^3"))
+    vals = []
+    cb = None
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(args, nx, wl, quick=False)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = sum(vals) / len(vals)
+    line = {
+        "impl": "reference",
+        "metric": "SOD halos/s (delta=200, N200 exact)",
+        "value": round(v, 3),
+        "unit": "halos/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic NFW-mixture boxes (seeded)",
+        "config": {"workload": wl["box"], "nx": nx, "mode": "reference CPU oracle"},
+        "cpu_baseline": {"value": round(v, 3), "unit": "halos/s", "cores": cb["cores"], "kind": "port",
+                         "sample": cb["sample"]},
+        "e2e": {"value": round(v, 3), "unit": "halos/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nx", type=int, default=1024)
+    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "learned"])
+    ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--ndelta", action="store_true", help="Delta = 200, 500, 178 and 48 bins (config 3)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.mode_id = {"plain": 0, "batched": 1, "learned": 2}[args.mode]
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,171 @@
+/*
+ * psod.h -- C-ABI of the B200 SOD engine (libpsod.so).
+ *
+ * Drop-in for the hot path of the reference's SOD stage,
+ * sod/sod_profile_rdfof_parallel_hdf5.f90 ("main").  The reference calls
+ * four external Fortran subroutines with implicit interfaces, passing the
+ * particle arrays through module globals (modvar posf/idf/mpf, modcic
+ * cube/rho, main:1-24):
+ *
+ *   call cic(...)        main:673-674   ->  psod_cic
+ *   call cicm1(...)      main:679       ->  psod_cicm1
+ *   call tri_cic(...)    main:713       ->  psod_tri_cic
+ *   call spherover(...)  main:740-744   ->  psod_spherover (+ psod_get_halos)
+ *
+ * Here the module globals become a context that owns device copies of the
+ * particles (psod_load_particles).  Conventions:
+ *   - plain pointers and sizes; no torch or CUDA types in any signature;
+ *   - array pointers may be host (pageable or pinned) or device memory; the
+ *     library detects which and copies as needed;
+ *   - indices are 0-based (the reference's are 1-based);
+ *   - every entry point returns a psod_status; psod_last_error() gives the
+ *     message of the last failure on that context;
+ *   - one context per thread; contexts are independent.
+ * The library has no CPU fallback: without a usable CUDA device every
+ * compute entry point returns PSOD_ERR_CUDA.
+ */
+#ifndef PSOD_H
+#define PSOD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PSOD_ABI_VERSION 1
+#define PSOD_MAX_EXTRA_DELTA 4
+
+typedef enum psod_status {
+  PSOD_OK = 0,
+  PSOD_ERR_NSEL = 1,      /* preselection exceeded nsel (main:1681-1693):
+                             the whole zone's output is lost */
+  PSOD_ERR_SELRADIUS = 2, /* overdensity still above delta at the selection
+                             edge (main:2072-2089): zone output lost */
+  PSOD_ERR_TIMEOUT = 3,   /* a bounded device wait ran out */
+  PSOD_ERR_CUDA = 4,      /* CUDA runtime error or no device */
+  PSOD_ERR_ARG = 5,       /* invalid argument or parameter */
+  PSOD_ERR_STATE = 6,     /* entry point called out of order */
+  PSOD_ERR_NOMEM = 7      /* device allocation failed */
+} psod_status;
+
+typedef enum psod_mode {
+  PSOD_MODE_PLAIN = 0,   /* one launch per round, full-cube gather */
+  PSOD_MODE_BATCHED = 1, /* size-classed seeds, graph-captured rounds */
+  PSOD_MODE_LEARNED = 2  /* batched + learned radius bracket */
+} psod_mode;
+
+/* Parameters: the reference's CLI flags (read_params, main:767-906) and the
+ * hard-coded constants of spherover.  psod_params_default() fills the
+ * reference defaults (main:110-114, 1414, 1459, 1525-1530, 1558-1559). */
+typedef struct psod_params {
+  int32_t nx;          /* -nx : grid cells per side; CIC uses 2*nx */
+  int32_t nmin;        /* -min: minimum halo particle count Mmin (100) */
+  double delta;        /* -del: overdensity threshold seuil (200) */
+  double delta2;       /* -dl2: second threshold seuil2 (800) */
+  int32_t ncut;        /* -sel: preselect half-width in cells (4) */
+  int64_t nsel;        /* -nse: preselected-particle capacity (4000000) */
+  int32_t nxbuffer;    /* -nxb: buffer cells; 0 means nx/2 (main:380-381) */
+  int64_t npu;         /* -npu: halo-size upper bound; >0 derives ncut,
+                          nxbuffer and nsel as main:211-219 does */
+  int32_t nbins;       /* profile bins (60, main:1414) */
+  double rbin_lo;      /* inner profile edge as a fraction of R_delta (0.01) */
+  double rbin_hi;      /* outer profile edge as a fraction of R_delta (1.0) */
+  int32_t ndelta_extra;                     /* extra thresholds, <= 4 */
+  double delta_extra[PSOD_MAX_EXTRA_DELTA]; /* N and R for each, same rule */
+  int32_t mode;        /* psod_mode */
+  int32_t device;      /* CUDA device ordinal */
+} psod_params;
+
+/* Halo table.  The caller provides the arrays it wants (NULL = skip), sized
+ * from psod_halo_count(); host or device memory.  Halos are in the
+ * reference's order (seed processing order); members of halo h are
+ * member_*[member_offset[h] .. member_offset[h+1]) in ascending distance
+ * from the centre, as the reference writes them (main:2306-2315). */
+typedef struct psod_halo_table {
+  int64_t *halo_id;       /* [nhalo]  ID of the centre particle (iamas) */
+  int64_t *halo_mass;     /* [nhalo]  N_delta (particle count) */
+  int64_t *halo_rank;     /* [nhalo]  seed rank in density order */
+  float *halo_center;     /* [3*nhalo] centre, box units (xc/scale) */
+  double *halo_rdelta;    /* [nhalo]  R_delta in grid cells */
+  int64_t *halo_mass2;    /* [nhalo]  last step above delta2, 0 if none */
+  int64_t *halo_mextra;   /* [nhalo*ndelta_extra] N for extra thresholds,
+                             -1 when not crossed inside the selection */
+  int64_t *halo_profile;  /* [nhalo*nbins] cumulative counts below each
+                             log-spaced edge */
+  int64_t *member_offset; /* [nhalo+1] */
+  int64_t *member_index;  /* [nmember] 0-based input particle index */
+  int64_t *member_id;     /* [nmember] particle IDs */
+} psod_halo_table;
+
+/* Counters of the last psod_spherover call. */
+typedef struct psod_run_stats {
+  int64_t npart_new;     /* seeds examined (tri_cic's npart_new) */
+  int64_t nprocessed;    /* seeds that passed Mtotsel >= Mmin */
+  int64_t nhalo;         /* kept halos */
+  int64_t nmember;       /* members of kept halos */
+  int64_t rounds;        /* scheduler rounds */
+  int64_t fail_rank;     /* failing seed rank, -1 if none */
+  int64_t touched;       /* particle records read by the SOD kernels */
+  double ms_total;       /* device time of psod_spherover */
+  double ms_sod_kernel;  /* device time inside the per-seed kernels */
+  int64_t sod_launches;  /* per-seed kernel launches */
+  int64_t kernel_launches; /* all kernels launched by psod_spherover */
+} psod_run_stats;
+
+typedef struct psod_ctx psod_ctx;
+
+void psod_params_default(psod_params *p);
+
+/* Create a context on p->device.  Validates the parameters the way the
+ * reference driver does (main:386-397): nxbuffer >= ncut, nxbuffer <= nx. */
+int psod_ctx_create(const psod_params *p, psod_ctx **out);
+int psod_ctx_destroy(psod_ctx *ctx);
+
+/* Optional: run on the caller's stream (a cudaStream_t passed as void*).
+ * Default: a stream owned by the context. */
+int psod_set_stream(psod_ctx *ctx, void *stream);
+
+/* Load n particles: pos is xyz-interleaved float32 in box units [0,1]
+ * (posf(3,n), modvar main:9), id int64 (idf, main:8), vel optional
+ * (velf; copied for the member table only).  npart_total is the
+ * simulation's particle count (nparttotal, main:302-310); mpf = 1/that.
+ * Builds the cell-sorted cube (the linked list of main:1564-1604). */
+int psod_load_particles(psod_ctx *ctx, int64_t n, const float *pos,
+                        const float *vel, const int64_t *id,
+                        int64_t npart_total);
+
+/* cic (main:1077-1265): CIC density on the (2nx)^3 periodic grid,
+ * accumulated in int64 fixed point (2^-40 per unit weight) so the grid is
+ * the same on every run.  grid_out (optional, (2nx)^3 doubles, x fastest)
+ * receives the grid in units of the mean density. */
+int psod_cic(psod_ctx *ctx, double *grid_out);
+
+/* cicm1 (main:1268-1390): per-particle density.  rho_out (optional, n
+ * doubles) in input order. */
+int psod_cicm1(psod_ctx *ctx, double *rho_out);
+
+/* tri_cic (main:998-1037): seeds in ascending 1/rho, ties by input index.
+ * isort_out (optional, npart_new entries, 0-based input indices);
+ * *npart_new_out gets the reference's npart_new. */
+int psod_tri_cic(psod_ctx *ctx, int64_t *isort_out, int64_t *npart_new_out);
+
+/* spherover compute (main:1396-2201).  Returns PSOD_ERR_NSEL or
+ * PSOD_ERR_SELRADIUS with the reference's zone-abort meaning (no halos).
+ * stats optional. */
+int psod_spherover(psod_ctx *ctx, psod_run_stats *stats);
+
+int psod_halo_count(psod_ctx *ctx, int64_t *nhalo, int64_t *nmember);
+int psod_get_halos(psod_ctx *ctx, const psod_halo_table *t);
+
+/* Convenience: cic, cicm1, tri_cic and spherover in one call. */
+int psod_run(psod_ctx *ctx, psod_run_stats *stats);
+
+const char *psod_last_error(const psod_ctx *ctx);
+const char *psod_status_string(int status);
+int psod_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PSOD_H */

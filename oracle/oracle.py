@@ -1,0 +1,260 @@
+"""ctypes wrapper of the CPU oracle (test infrastructure only).
+
+TEST INFRASTRUCTURE: used by tests/, __graft_entry__.smoke() and bench.py's
+cpu_baseline leg as the checker; the product never imports it.
+
+The oracle restates the 1-rank SOD stage of
+sod/sod_profile_rdfof_parallel_hdf5.f90 (cic main:1077-1265, cicm1
+main:1268-1390, tri_cic main:998-1037, quick_sort main:2477-2571,
+spherover main:1396-2201). Parity unpinned: the reference has no golden
+vectors for this path.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libpsod_oracle.so")
+
+REFERENCE = 0
+CANONICAL = 1
+MAX_EXTRA = 4
+
+
+class _Params(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32),
+        ("nmin", C.c_int32),
+        ("delta", C.c_double),
+        ("delta2", C.c_double),
+        ("ncut", C.c_int32),
+        ("nsel", C.c_int64),
+        ("nxbuffer", C.c_int32),
+        ("nbins", C.c_int32),
+        ("rbin_lo", C.c_double),
+        ("rbin_hi", C.c_double),
+        ("ndelta_extra", C.c_int32),
+        ("delta_extra", C.c_double * MAX_EXTRA),
+        ("npart_total", C.c_int64),
+    ]
+
+
+class _Result(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("fail_rank", C.c_int64),
+        ("npart_new", C.c_int64),
+        ("nprocessed", C.c_int64),
+        ("nhalo", C.c_int64),
+        ("nmember", C.c_int64),
+        ("halo_id", C.POINTER(C.c_int64)),
+        ("halo_mass", C.POINTER(C.c_int64)),
+        ("halo_rank", C.POINTER(C.c_int64)),
+        ("halo_cidx", C.POINTER(C.c_int64)),
+        ("halo_center", C.POINTER(C.c_float)),
+        ("halo_rdelta", C.POINTER(C.c_double)),
+        ("halo_mass2", C.POINTER(C.c_int64)),
+        ("halo_mextra", C.POINTER(C.c_int64)),
+        ("halo_profile", C.POINTER(C.c_int64)),
+        ("member_offset", C.POINTER(C.c_int64)),
+        ("member_index", C.POINTER(C.c_int64)),
+    ]
+
+
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    """Compile the oracle with its Makefile (gcc, no GPU needed)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        L.psod_oracle_quick_sort.argtypes = [P(C.c_double), P(C.c_int64), C.c_int64]
+        L.psod_oracle_cic.argtypes = [P(_Params), C.c_int64, P(C.c_float), C.c_int, P(C.c_double)]
+        L.psod_oracle_cicm1.argtypes = [P(_Params), C.c_int64, P(C.c_float), P(C.c_double), P(C.c_double)]
+        L.psod_oracle_tri_cic.argtypes = [C.c_int64, P(C.c_double), C.c_int, P(C.c_int64), P(C.c_int64)]
+        L.psod_oracle_run.argtypes = [P(_Params), C.c_int64, P(C.c_float), P(C.c_int64), C.c_int, P(_Result)]
+        L.psod_oracle_spherover.argtypes = [
+            P(_Params), C.c_int64, P(C.c_float), P(C.c_int64), P(C.c_int64), C.c_int64, C.c_int, P(_Result)
+        ]
+        L.psod_oracle_free.argtypes = [P(_Result)]
+        _lib = L
+    return _lib
+
+
+@dataclass
+class Params:
+    """Same meaning and defaults as the reference CLI (main:110-114, 1414)."""
+
+    nx: int
+    nmin: int = 100
+    delta: float = 200.0
+    delta2: float = 800.0
+    ncut: int = 4
+    nsel: int = 4_000_000
+    nxbuffer: int = 0
+    nbins: int = 60
+    rbin_lo: float = 0.01
+    rbin_hi: float = 1.0
+    delta_extra: tuple = ()
+    npart_total: int = 0
+
+    def c(self, n: int) -> _Params:
+        p = _Params()
+        p.nx = self.nx
+        p.nmin = self.nmin
+        p.delta = self.delta
+        p.delta2 = self.delta2
+        p.ncut = self.ncut
+        p.nsel = self.nsel
+        p.nxbuffer = self.nxbuffer
+        p.nbins = self.nbins
+        p.rbin_lo = self.rbin_lo
+        p.rbin_hi = self.rbin_hi
+        p.ndelta_extra = len(self.delta_extra)
+        for i, d in enumerate(self.delta_extra):
+            p.delta_extra[i] = d
+        p.npart_total = self.npart_total if self.npart_total > 0 else n
+        return p
+
+
+@dataclass
+class Result:
+    status: int
+    fail_rank: int
+    npart_new: int
+    nprocessed: int
+    halo_id: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    halo_mass: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    halo_rank: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    halo_cidx: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    halo_center: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.float32))
+    halo_rdelta: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float64))
+    halo_mass2: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    halo_mextra: np.ndarray = field(default_factory=lambda: np.zeros((0, 0), np.int64))
+    halo_profile: np.ndarray = field(default_factory=lambda: np.zeros((0, 0), np.int64))
+    member_offset: np.ndarray = field(default_factory=lambda: np.zeros(1, np.int64))
+    member_index: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+
+    @property
+    def nhalo(self) -> int:
+        return int(self.halo_id.shape[0])
+
+
+def _ptr(a, ctype):
+    return a.ctypes.data_as(C.POINTER(ctype))
+
+
+def _as_pos(pos) -> np.ndarray:
+    a = pos.cpu().numpy() if hasattr(pos, "cpu") else np.asarray(pos)
+    return np.ascontiguousarray(a, dtype=np.float32).reshape(-1, 3)
+
+
+def _as_ids(ids) -> np.ndarray:
+    a = ids.cpu().numpy() if hasattr(ids, "cpu") else np.asarray(ids)
+    return np.ascontiguousarray(a, dtype=np.int64)
+
+
+def quick_sort(values) -> tuple[np.ndarray, np.ndarray]:
+    lst = np.ascontiguousarray(values, dtype=np.float64).copy()
+    order = np.zeros(lst.shape[0], np.int64)
+    lib().psod_oracle_quick_sort(_ptr(lst, C.c_double), _ptr(order, C.c_int64), lst.shape[0])
+    return lst, order
+
+
+def cic_grid(params: Params, pos, mode=REFERENCE) -> np.ndarray:
+    p = _as_pos(pos)
+    nc = 2 * params.nx
+    grid = np.zeros(nc**3, np.float64)
+    cp = params.c(p.shape[0])
+    st = lib().psod_oracle_cic(C.byref(cp), p.shape[0], _ptr(p, C.c_float), mode, _ptr(grid, C.c_double))
+    if st:
+        raise ValueError(f"oracle cic status {st}")
+    return grid.reshape(nc, nc, nc)  # [z, y, x]
+
+
+def rho(params: Params, pos, mode=REFERENCE, grid=None) -> np.ndarray:
+    p = _as_pos(pos)
+    if grid is None:
+        grid = cic_grid(params, p, mode)
+    g = np.ascontiguousarray(grid, dtype=np.float64).reshape(-1)
+    out = np.zeros(p.shape[0], np.float64)
+    cp = params.c(p.shape[0])
+    st = lib().psod_oracle_cicm1(C.byref(cp), p.shape[0], _ptr(p, C.c_float), _ptr(g, C.c_double), _ptr(out, C.c_double))
+    if st:
+        raise ValueError(f"oracle cicm1 status {st}")
+    return out
+
+
+def tri_cic(rho_values, mode=REFERENCE) -> tuple[np.ndarray, int]:
+    r = np.ascontiguousarray(rho_values, dtype=np.float64)
+    isort = np.zeros(r.shape[0], np.int64)
+    nn = C.c_int64(0)
+    lib().psod_oracle_tri_cic(r.shape[0], _ptr(r, C.c_double), mode, _ptr(isort, C.c_int64), C.byref(nn))
+    return isort, int(nn.value)
+
+
+def _collect(res: _Result, params: Params) -> Result:
+    out = Result(status=res.status, fail_rank=res.fail_rank, npart_new=res.npart_new, nprocessed=res.nprocessed)
+    h = int(res.nhalo)
+    if res.status == 0:
+        def arr(ptr, n, dt):
+            if n == 0:
+                return np.zeros(0, dt)
+            return np.ctypeslib.as_array(ptr, shape=(n,)).copy().astype(dt)
+
+        out.halo_id = arr(res.halo_id, h, np.int64)
+        out.halo_mass = arr(res.halo_mass, h, np.int64)
+        out.halo_rank = arr(res.halo_rank, h, np.int64)
+        out.halo_cidx = arr(res.halo_cidx, h, np.int64)
+        out.halo_center = arr(res.halo_center, 3 * h, np.float32).reshape(h, 3)
+        out.halo_rdelta = arr(res.halo_rdelta, h, np.float64)
+        out.halo_mass2 = arr(res.halo_mass2, h, np.int64)
+        ne = len(params.delta_extra)
+        out.halo_mextra = arr(res.halo_mextra, ne * h, np.int64).reshape(h, ne)
+        out.halo_profile = arr(res.halo_profile, params.nbins * h, np.int64).reshape(h, params.nbins)
+        out.member_offset = arr(res.member_offset, h + 1, np.int64)
+        out.member_index = arr(res.member_index, int(res.nmember), np.int64)
+    return out
+
+
+def run(params: Params, pos, ids, mode=REFERENCE) -> Result:
+    """cic -> cicm1 -> tri_cic -> spherover, one rank, one zone."""
+    p = _as_pos(pos)
+    i = _as_ids(ids)
+    cp = params.c(p.shape[0])
+    res = _Result()
+    lib().psod_oracle_run(C.byref(cp), p.shape[0], _ptr(p, C.c_float), _ptr(i, C.c_int64), mode, C.byref(res))
+    try:
+        return _collect(res, params)
+    finally:
+        lib().psod_oracle_free(C.byref(res))
+
+
+def spherover(params: Params, pos, ids, isort, npart_new, mode=REFERENCE) -> Result:
+    p = _as_pos(pos)
+    i = _as_ids(ids)
+    s = np.ascontiguousarray(isort, dtype=np.int64)
+    cp = params.c(p.shape[0])
+    res = _Result()
+    lib().psod_oracle_spherover(
+        C.byref(cp), p.shape[0], _ptr(p, C.c_float), _ptr(i, C.c_int64), _ptr(s, C.c_int64), npart_new, mode, C.byref(res)
+    )
+    try:
+        return _collect(res, params)
+    finally:
+        lib().psod_oracle_free(C.byref(res))

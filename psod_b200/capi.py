@@ -1,0 +1,158 @@
+"""ctypes binding of libpsod.so (include/psod.h).
+
+The product path: every call goes to the sm_100a kernels in the in-tree
+library. There is no CPU fallback; without the library or a CUDA device the
+calls raise.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import build as _build
+
+MAX_EXTRA = 4
+
+OK = 0
+ERR_NSEL = 1
+ERR_SELRADIUS = 2
+ERR_TIMEOUT = 3
+ERR_CUDA = 4
+ERR_ARG = 5
+ERR_STATE = 6
+ERR_NOMEM = 7
+
+MODE_PLAIN = 0
+MODE_BATCHED = 1
+MODE_LEARNED = 2
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int32),
+        ("nmin", C.c_int32),
+        ("delta", C.c_double),
+        ("delta2", C.c_double),
+        ("ncut", C.c_int32),
+        ("nsel", C.c_int64),
+        ("nxbuffer", C.c_int32),
+        ("npu", C.c_int64),
+        ("nbins", C.c_int32),
+        ("rbin_lo", C.c_double),
+        ("rbin_hi", C.c_double),
+        ("ndelta_extra", C.c_int32),
+        ("delta_extra", C.c_double * MAX_EXTRA),
+        ("mode", C.c_int32),
+        ("device", C.c_int32),
+    ]
+
+
+class HaloTable(C.Structure):
+    _fields_ = [
+        ("halo_id", C.c_void_p),
+        ("halo_mass", C.c_void_p),
+        ("halo_rank", C.c_void_p),
+        ("halo_center", C.c_void_p),
+        ("halo_rdelta", C.c_void_p),
+        ("halo_mass2", C.c_void_p),
+        ("halo_mextra", C.c_void_p),
+        ("halo_profile", C.c_void_p),
+        ("member_offset", C.c_void_p),
+        ("member_index", C.c_void_p),
+        ("member_id", C.c_void_p),
+    ]
+
+
+class RunStats(C.Structure):
+    _fields_ = [
+        ("npart_new", C.c_int64),
+        ("nprocessed", C.c_int64),
+        ("nhalo", C.c_int64),
+        ("nmember", C.c_int64),
+        ("rounds", C.c_int64),
+        ("fail_rank", C.c_int64),
+        ("touched", C.c_int64),
+        ("ms_total", C.c_double),
+        ("ms_sod_kernel", C.c_double),
+        ("sod_launches", C.c_int64),
+        ("kernel_launches", C.c_int64),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+EXPORTS = [
+    "psod_abi_version",
+    "psod_status_string",
+    "psod_params_default",
+    "psod_ctx_create",
+    "psod_ctx_destroy",
+    "psod_set_stream",
+    "psod_load_particles",
+    "psod_cic",
+    "psod_cicm1",
+    "psod_tri_cic",
+    "psod_spherover",
+    "psod_run",
+    "psod_halo_count",
+    "psod_get_halos",
+    "psod_last_error",
+]
+
+_lib = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True):
+    """Load the in-tree libpsod.so (building it first if asked and needed)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB
+    if build_if_missing and not os.path.exists(path):
+        _build.build()
+    if not os.path.exists(path):
+        raise RuntimeError(f"libpsod.so not built at {path}: run psod_b200/build.py")
+    L = C.CDLL(path)
+    P = C.POINTER
+    vp = C.c_void_p
+    L.psod_abi_version.restype = C.c_int
+    L.psod_status_string.restype = C.c_char_p
+    L.psod_status_string.argtypes = [C.c_int]
+    L.psod_params_default.argtypes = [P(Params)]
+    L.psod_params_default.restype = None
+    L.psod_ctx_create.argtypes = [P(Params), P(vp)]
+    L.psod_ctx_destroy.argtypes = [vp]
+    L.psod_set_stream.argtypes = [vp, vp]
+    L.psod_load_particles.argtypes = [vp, C.c_int64, vp, vp, vp, C.c_int64]
+    L.psod_cic.argtypes = [vp, vp]
+    L.psod_cicm1.argtypes = [vp, vp]
+    L.psod_tri_cic.argtypes = [vp, vp, P(C.c_int64)]
+    L.psod_spherover.argtypes = [vp, P(RunStats)]
+    L.psod_run.argtypes = [vp, P(RunStats)]
+    L.psod_halo_count.argtypes = [vp, P(C.c_int64), P(C.c_int64)]
+    L.psod_get_halos.argtypes = [vp, P(HaloTable)]
+    L.psod_last_error.argtypes = [vp]
+    L.psod_last_error.restype = C.c_char_p
+    for name in EXPORTS:
+        L[name].restype = L[name].restype if name in ("psod_status_string", "psod_last_error", "psod_params_default") else C.c_int
+    _lib = L
+    return L
+
+
+def default_params(nx: int, **kw) -> Params:
+    p = Params()
+    load().psod_params_default(C.byref(p))
+    p.nx = nx
+    extra = kw.pop("delta_extra", ())
+    for k, v in kw.items():
+        setattr(p, k, v)
+    p.ndelta_extra = len(extra)
+    for i, d in enumerate(extra):
+        p.delta_extra[i] = d
+    return p

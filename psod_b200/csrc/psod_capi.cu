@@ -1,0 +1,306 @@
+// psod_capi.cu -- the extern "C" boundary of libpsod.so (include/psod.h).
+#include <cmath>
+#include <cstring>
+
+#include "psod_internal.cuh"
+
+namespace psod {
+
+int set_err(psod_ctx *c, int code, const std::string &msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+int cuda_check(psod_ctx *c, cudaError_t e, const char *what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  cudaGetLastError();
+  return set_err(c, PSOD_ERR_CUDA, m);
+}
+
+bool is_device_ptr(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+int copy_out(psod_ctx *c, void *dst, const void *dsrc, size_t bytes) {
+  if (bytes == 0) return PSOD_OK;
+  PSOD_CUDA(c, cudaMemcpyAsync(dst, dsrc, bytes, cudaMemcpyDefault, c->stream));
+  PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PSOD_OK;
+}
+
+int copy_in(psod_ctx *c, void *ddst, const void *src, size_t bytes) {
+  if (bytes == 0) return PSOD_OK;
+  PSOD_CUDA(c, cudaMemcpyAsync(ddst, src, bytes, cudaMemcpyDefault, c->stream));
+  return PSOD_OK;
+}
+
+}  // namespace psod
+
+using namespace psod;
+
+static void free_all(psod_ctx *c) {
+  dfree(&c->d_pos);
+  dfree(&c->d_vel);
+  dfree(&c->d_ids);
+  dfree(&c->d_cube);
+  dfree(&c->d_cube_orig);
+  dfree(&c->d_cell_start);
+  dfree(&c->d_inv);
+  dfree(&c->d_rho);
+  dfree(&c->d_grid);
+  dfree(&c->d_seed_idx);
+  dfree(&c->d_h_id);
+  dfree(&c->d_h_mass);
+  dfree(&c->d_h_rank);
+  dfree(&c->d_h_mass2);
+  dfree(&c->d_h_mextra);
+  dfree(&c->d_h_profile);
+  dfree(&c->d_h_center);
+  dfree(&c->d_h_rdelta);
+  dfree(&c->d_m_offset);
+  dfree(&c->d_m_index);
+}
+
+extern "C" {
+
+int psod_abi_version(void) { return PSOD_ABI_VERSION; }
+
+const char *psod_status_string(int s) {
+  switch (s) {
+    case PSOD_OK: return "ok";
+    case PSOD_ERR_NSEL: return "preselection exceeded nsel (zone output lost)";
+    case PSOD_ERR_SELRADIUS: return "overdensity above delta at the selection radius (zone output lost)";
+    case PSOD_ERR_TIMEOUT: return "bounded device wait ran out";
+    case PSOD_ERR_CUDA: return "CUDA error";
+    case PSOD_ERR_ARG: return "invalid argument";
+    case PSOD_ERR_STATE: return "call out of order or internal check failed";
+    case PSOD_ERR_NOMEM: return "device allocation failed";
+    default: return "unknown status";
+  }
+}
+
+void psod_params_default(psod_params *p) {
+  if (!p) return;
+  memset(p, 0, sizeof(*p));
+  p->nx = 0;
+  p->nmin = 100;        // main:112
+  p->delta = 200.0;     // main:110
+  p->delta2 = 800.0;    // main:110
+  p->ncut = 4;          // main:114
+  p->nsel = 4000000;    // main:114
+  p->nxbuffer = 0;      // main:114 (0 -> nx/2 at main:380-381)
+  p->npu = 0;
+  p->nbins = 60;        // main:1414
+  p->rbin_lo = 0.01;    // main:2105
+  p->rbin_hi = 1.0;     // main:2105
+  p->ndelta_extra = 0;
+  p->mode = PSOD_MODE_PLAIN;
+  p->device = 0;
+}
+
+int psod_ctx_create(const psod_params *pin, psod_ctx **out) {
+  if (!pin || !out) return PSOD_ERR_ARG;
+  *out = nullptr;
+  psod_ctx *c = new psod_ctx();
+  c->p = *pin;
+  psod_params &p = c->p;
+  // -npu (main:211-219): derive ncut, nxbuffer and nsel from a halo-size bound
+  if (p.npu > 0) {
+    p.ncut = (int)std::ceil(std::pow(p.npu * 2.0 / p.delta, 1.0 / 3.0) / 2.0);
+    p.nxbuffer = 4 * p.ncut;
+    p.nsel = (int64_t)std::ceil(std::pow(2.0 * p.ncut + 1.0, 3) * p.delta * 4.0);
+  }
+  std::string why;
+  if (p.nx < 5) why = "nx must be >= 5";
+  else if (p.ncut < 1 || 2 * p.ncut + 1 > p.nx) why = "ncut must satisfy 1 <= ncut and 2*ncut+1 <= nx";
+  else if (p.nmin < 10) why = "nmin must be >= 10 (the crossing loop always takes 10 steps, main:2046)";
+  else if (p.nbins < 1 || p.nbins > PSOD_MAX_BINS) why = "nbins must be in [1, 128]";
+  else if (p.nsel < 1) why = "nsel must be positive";
+  else if (!(p.rbin_lo > 0.0) || !(p.rbin_hi > 0.0)) why = "profile edge factors must be positive";
+  else if (p.ndelta_extra < 0 || p.ndelta_extra > PSOD_MAX_EXTRA_DELTA) why = "at most 4 extra thresholds";
+  else if (!(p.delta > 0.0)) why = "delta must be positive";
+  int nxbuffer = p.nxbuffer == 0 ? p.nx / 2 : p.nxbuffer;  // main:380-381, nxzone = nx
+  if (why.empty() && nxbuffer < p.ncut) why = "nxbuffer must be >= ncut (main:386)";
+  if (why.empty() && nxbuffer > p.nx) why = "nxbuffer must be <= nx (main:392)";
+  if (!why.empty()) {
+    delete c;
+    return PSOD_ERR_ARG;
+  }
+  c->nx = p.nx;
+  c->nxbuffer = nxbuffer;
+  c->ncut = p.ncut;
+  c->nsel = p.nsel;
+  // zone with buffer for one rank (main:401-402): (0 - nxb/nxzone)/nxcpu
+  const double q = (double)nxbuffer / (double)p.nx;
+  c->xxmin = (0.0 - q) / 1.0;
+  c->scale = (double)p.nx;  // main:689
+  // profile edge factors with the host libm, as the reference evaluates
+  // exp(log(lo) + (j-1)*(log(hi)-log(lo))/(nbins-1)) (main:2105)
+  c->edge_fac.resize(p.nbins);
+  for (int j = 0; j < p.nbins; j++) {
+    const double denom = (double)p.nbins - 1.0;
+    c->edge_fac[j] = denom > 0.0 ? std::exp(std::log(p.rbin_lo) + ((double)j * (std::log(p.rbin_hi) - std::log(p.rbin_lo))) / denom)
+                                 : p.rbin_hi;
+  }
+  c->device = p.device;
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev <= p.device) {
+    cudaGetLastError();
+    delete c;
+    return PSOD_ERR_CUDA;
+  }
+  if (cudaSetDevice(p.device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    delete c;
+    return PSOD_ERR_CUDA;
+  }
+  c->own_stream = true;
+  *out = c;
+  return PSOD_OK;
+}
+
+int psod_ctx_destroy(psod_ctx *c) {
+  if (!c) return PSOD_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_all(c);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return PSOD_OK;
+}
+
+int psod_set_stream(psod_ctx *c, void *stream) {
+  if (!c) return PSOD_ERR_ARG;
+  cudaSetDevice(c->device);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  c->stream = (cudaStream_t)stream;
+  c->own_stream = false;
+  return PSOD_OK;
+}
+
+int psod_load_particles(psod_ctx *c, int64_t n, const float *pos, const float *vel, const int64_t *id,
+                        int64_t npart_total) {
+  if (!c) return PSOD_ERR_ARG;
+  if (n < 1 || !pos || !id) return set_err(c, PSOD_ERR_ARG, "need n >= 1, pos and id");
+  if (n >= (int64_t)PSOD_DEAD_BIT) return set_err(c, PSOD_ERR_ARG, "n must be below 2^31");
+  if (npart_total < 1) npart_total = n;
+  if (cudaSetDevice(c->device) != cudaSuccess) return cuda_check(c, cudaGetLastError(), "cudaSetDevice");
+  c->n = n;
+  c->npart_total = npart_total;
+  c->mpf = (float)(1.0 / (double)npart_total);                // main:662
+  c->munit = (float)((double)c->mpf * (double)npart_total);   // main:685
+  c->cic_done = c->rho_done = c->seeds_done = c->sod_done = false;
+  int st;
+  if ((st = dalloc(c, &c->d_pos, (size_t)n * 3))) return st;
+  if ((st = dalloc(c, &c->d_ids, (size_t)n))) return st;
+  if ((st = copy_in(c, c->d_pos, pos, sizeof(float) * 3 * n))) return st;
+  if ((st = copy_in(c, c->d_ids, id, sizeof(int64_t) * n))) return st;
+  if (vel) {
+    if ((st = dalloc(c, &c->d_vel, (size_t)n * 3))) return st;
+    if ((st = copy_in(c, c->d_vel, vel, sizeof(float) * 3 * n))) return st;
+  } else {
+    dfree(&c->d_vel);
+  }
+  return stage_cellsort(c);
+}
+
+int psod_cic(psod_ctx *c, double *grid_out) {
+  if (!c) return PSOD_ERR_ARG;
+  if (c->n == 0) return set_err(c, PSOD_ERR_STATE, "psod_cic needs psod_load_particles first");
+  cudaSetDevice(c->device);
+  return stage_cic(c, grid_out);
+}
+
+int psod_cicm1(psod_ctx *c, double *rho_out) {
+  if (!c) return PSOD_ERR_ARG;
+  cudaSetDevice(c->device);
+  return stage_cicm1(c, rho_out);
+}
+
+int psod_tri_cic(psod_ctx *c, int64_t *isort_out, int64_t *npart_new_out) {
+  if (!c) return PSOD_ERR_ARG;
+  cudaSetDevice(c->device);
+  int st = stage_tri_cic(c, isort_out);
+  if (!st && npart_new_out) *npart_new_out = c->npart_new;
+  return st;
+}
+
+int psod_spherover(psod_ctx *c, psod_run_stats *stats) {
+  if (!c) return PSOD_ERR_ARG;
+  cudaSetDevice(c->device);
+  return stage_spherover(c, stats);
+}
+
+int psod_run(psod_ctx *c, psod_run_stats *stats) {
+  int st;
+  if ((st = psod_cic(c, nullptr))) return st;
+  if ((st = psod_cicm1(c, nullptr))) return st;
+  if ((st = psod_tri_cic(c, nullptr, nullptr))) return st;
+  return psod_spherover(c, stats);
+}
+
+int psod_halo_count(psod_ctx *c, int64_t *nhalo, int64_t *nmember) {
+  if (!c) return PSOD_ERR_ARG;
+  if (!c->sod_done) return set_err(c, PSOD_ERR_STATE, "no halo table: call psod_spherover first");
+  if (nhalo) *nhalo = c->nhalo;
+  if (nmember) *nmember = c->nmember;
+  return PSOD_OK;
+}
+
+namespace {
+__global__ void k_member_ids(const unsigned *midx, long long n, const long long *ids, long long *out_idx,
+                             long long *out_id) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned k = midx[i];
+  if (out_idx) out_idx[i] = (long long)k;
+  if (out_id) out_id[i] = ids[k];
+}
+}  // namespace
+
+int psod_get_halos(psod_ctx *c, const psod_halo_table *t) {
+  if (!c || !t) return PSOD_ERR_ARG;
+  if (!c->sod_done) return set_err(c, PSOD_ERR_STATE, "no halo table: call psod_spherover first");
+  cudaSetDevice(c->device);
+  const long long nh = c->nhalo, nm = c->nmember;
+  int st;
+  if (t->halo_id && (st = copy_out(c, t->halo_id, c->d_h_id, sizeof(int64_t) * nh))) return st;
+  if (t->halo_mass && (st = copy_out(c, t->halo_mass, c->d_h_mass, sizeof(int64_t) * nh))) return st;
+  if (t->halo_rank && (st = copy_out(c, t->halo_rank, c->d_h_rank, sizeof(int64_t) * nh))) return st;
+  if (t->halo_center && (st = copy_out(c, t->halo_center, c->d_h_center, sizeof(float) * 3 * nh))) return st;
+  if (t->halo_rdelta && (st = copy_out(c, t->halo_rdelta, c->d_h_rdelta, sizeof(double) * nh))) return st;
+  if (t->halo_mass2 && (st = copy_out(c, t->halo_mass2, c->d_h_mass2, sizeof(int64_t) * nh))) return st;
+  if (t->halo_mextra && c->p.ndelta_extra > 0 &&
+      (st = copy_out(c, t->halo_mextra, c->d_h_mextra, sizeof(int64_t) * nh * c->p.ndelta_extra)))
+    return st;
+  if (t->halo_profile && (st = copy_out(c, t->halo_profile, c->d_h_profile, sizeof(int64_t) * nh * c->p.nbins)))
+    return st;
+  if (t->member_offset && (st = copy_out(c, t->member_offset, c->d_m_offset, sizeof(int64_t) * (nh + 1))))
+    return st;
+  if ((t->member_index || t->member_id) && nm > 0) {
+    long long *d_idx = nullptr, *d_id = nullptr;
+    if (t->member_index && (st = dalloc(c, &d_idx, (size_t)nm))) return st;
+    if (t->member_id && (st = dalloc(c, &d_id, (size_t)nm))) {
+      dfree(&d_idx);
+      return st;
+    }
+    k_member_ids<<<(unsigned)((nm + 255) / 256), 256, 0, c->stream>>>(c->d_m_index, nm, c->d_ids, d_idx, d_id);
+    st = PSOD_OK;
+    if (t->member_index) st = copy_out(c, t->member_index, d_idx, sizeof(int64_t) * nm);
+    if (!st && t->member_id) st = copy_out(c, t->member_id, d_id, sizeof(int64_t) * nm);
+    dfree(&d_idx);
+    dfree(&d_id);
+    if (st) return st;
+  }
+  return PSOD_OK;
+}
+
+const char *psod_last_error(const psod_ctx *c) { return c ? c->err.c_str() : "null context"; }
+
+}  // extern "C"

@@ -1,0 +1,225 @@
+// psod_internal.cuh -- shared definitions of the B200 SOD engine.
+//
+// Data layout in HBM (one context = one zone of the reference's 1-rank run):
+//   cube4[n]        float4, particles sorted by SOD cell (the reference's
+//                   linked list, main:1564-1604): x, y, z in box units and
+//                   w = input index | DEAD_BIT (bit 31 set once claimed).
+//   cell_start[nc+1] uint32 offsets of each cell's run in cube4, nc = nx^3,
+//                   cell index = i + nx*(j + nx*k).
+//   ids[n], vel[3n] input order.
+//   rho[n]          double, input order (cicm1 output).
+//   seeds           ranks 0..npart_new-1 -> cube4 position.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/psod.h"
+
+#define PSOD_DEAD_BIT 0x80000000u
+#define PSOD_IDX_MASK 0x7fffffffu
+#define PSOD_INF_RANK 0xffffffffu
+#define PSOD_MAX_BINS 128
+
+namespace psod {
+
+// ---------------------------------------------------------------------------
+// exact FP64 building blocks: explicit round-to-nearest intrinsics so that no
+// multiply-add is ever contracted (the reference is built at -O0)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double ddiv(double a, double b) { return __ddiv_rn(a, b); }
+__device__ __forceinline__ double dsqrt(double a) { return __dsqrt_rn(a); }
+
+// posf = posf*scale stored back to real(4) (main:690).  The double product
+// of a float and a float-exact nx is exact, so one correctly rounded float
+// multiply gives the same value.
+__device__ __forceinline__ float to_grid(float x, float nxf) { return __fmul_rn(x, nxf); }
+
+// SOD cell along one axis (main:1565-1576): floor(x_g - xxmin*scale), wrapped
+// once into [0, nx).
+__device__ __forceinline__ int sod_cell_axis(float xg, double xs, int nx) {
+  double d = dsub((double)xg, xs);
+  int i = (int)floor(d);
+  if (i < 0) i += nx;
+  if (i >= nx) i -= nx;
+  return i;
+}
+
+// minimum-image squared distance (main:2014-2020 and 1844-1850):
+// dx = |xx-xc|; dx = min(dx, nx-dx); d2 = (dx*dx + dy*dy) + dz*dz.
+__device__ __forceinline__ double min_image_d2(double xx, double yy, double zz, double xc, double yc,
+                                               double zc, double tx) {
+  double dx = fabs(dsub(xx, xc));
+  double t = dsub(tx, dx);
+  dx = dx < t ? dx : t;
+  double dy = fabs(dsub(yy, yc));
+  t = dsub(tx, dy);
+  dy = dy < t ? dy : t;
+  double dz = fabs(dsub(zz, zc));
+  t = dsub(tx, dz);
+  dz = dz < t ? dz : t;
+  return dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
+}
+
+__device__ __forceinline__ unsigned long long dbits(double d) {
+  return (unsigned long long)__double_as_longlong(d);
+}
+__device__ __forceinline__ double bitsd(unsigned long long b) {
+  return __longlong_as_double((long long)b);
+}
+
+// periodic signed offset a-b in (-nx/2, nx/2]
+__device__ __forceinline__ int pdiff(int a, int b, int nx) {
+  int d = a - b;
+  if (d > nx / 2) d -= nx;
+  if (d <= -((nx + 1) / 2)) d += nx;
+  return d;
+}
+
+// ---------------------------------------------------------------------------
+// parameters shared by the SOD kernels (passed by value)
+// ---------------------------------------------------------------------------
+struct SodConst {
+  int nx;
+  int ncut;
+  float nxf;
+  double xs;        // xxmin*scale (grid units)
+  double tx;        // taillex = nx (main:1517)
+  double scale;     // nx
+  double delta;     // seuil
+  double delta2;    // seuil2
+  double cvol;      // 2/3*twopi (main:2049)
+  double munit;     // per-particle mass after main:685
+  double mmin;      // Mmin
+  long long nsel;
+  double zmin, zmax; // utile zone in grid units (main:691-696)
+  double eps2;      // (scale/nx/2**6)**2 (main:1527)
+  double rmin2;     // (scale/nx)**2 (main:1526)
+  int nbins;
+  int ndx;
+  double dx_extra[PSOD_MAX_EXTRA_DELTA];
+  // the one particle the reference's run scan files under the previous cell
+  // (main:1596-1599): cube position, listed cell, own cell
+  unsigned quirk_pos;
+  unsigned quirk_listed;
+  unsigned quirk_phys;
+  int has_quirk;
+};
+
+}  // namespace psod
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+struct psod_ctx {
+  psod_params p;  // resolved parameters
+  int nx = 0, nxbuffer = 0, ncut = 0;
+  long long nsel = 0;
+  double xxmin = 0;  // zone-with-buffer lower edge, box units
+  double scale = 0;
+  float mpf = 0, munit = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  std::string err;
+
+  // particles
+  long long n = 0, npart_total = 0;
+  float *d_pos = nullptr;   // input order, 3n (box units)
+  float *d_vel = nullptr;   // input order, 3n (optional)
+  long long *d_ids = nullptr;
+  float4 *d_cube = nullptr;       // sorted
+  float4 *d_cube_orig = nullptr;  // pristine copy (alive flags reset)
+  unsigned *d_cell_start = nullptr;
+  unsigned *d_inv = nullptr;  // input index -> cube position
+  unsigned long long ncell = 0;
+  unsigned quirk_pos = 0xffffffffu, quirk_listed = 0, quirk_phys = 0;
+  int has_quirk = 0;
+
+  // cic
+  double *d_rho = nullptr;  // input order
+  bool cic_done = false, rho_done = false;
+  unsigned long long *d_grid = nullptr;  // fixed-point grid (tests only)
+
+  // seeds
+  long long npart_new = 0, nseed_dense = 0;
+  unsigned *d_seed_idx = nullptr;  // rank -> input index
+  bool seeds_done = false;
+
+  // halos
+  bool sod_done = false;
+  long long nhalo = 0, nmember = 0;
+  long long *d_h_id = nullptr, *d_h_mass = nullptr, *d_h_rank = nullptr, *d_h_mass2 = nullptr;
+  long long *d_h_mextra = nullptr, *d_h_profile = nullptr;
+  float *d_h_center = nullptr;
+  double *d_h_rdelta = nullptr;
+  long long *d_m_offset = nullptr;
+  unsigned *d_m_index = nullptr;
+  psod_run_stats last_stats{};
+
+  std::vector<double> edge_fac;  // profile edge factors (host libm)
+};
+
+namespace psod {
+
+// ---------------------------------------------------------------------------
+// host helpers
+// ---------------------------------------------------------------------------
+int set_err(psod_ctx *c, int code, const std::string &msg);
+int cuda_check(psod_ctx *c, cudaError_t e, const char *what);
+#define PSOD_CUDA(ctx, call)                               \
+  do {                                                     \
+    cudaError_t _e = (call);                               \
+    if (_e != cudaSuccess) return psod::cuda_check(ctx, _e, #call); \
+  } while (0)
+
+template <typename T>
+int dalloc(psod_ctx *c, T **p, size_t count) {
+  if (*p) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void **)p, count * sizeof(T));
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return set_err(c, PSOD_ERR_NOMEM,
+                   std::string("device allocation of ") + std::to_string(count * sizeof(T)) + " bytes failed");
+  }
+  return PSOD_OK;
+}
+template <typename T>
+void dfree(T **p) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+}
+
+bool is_device_ptr(const void *p);
+int copy_out(psod_ctx *c, void *dst, const void *dsrc, size_t bytes);
+int copy_in(psod_ctx *c, void *ddst, const void *src, size_t bytes);
+
+// device-wide exclusive scan of uint32 (values and total must fit 32 bits);
+// out may alias in; out[n] receives the total when with_total.
+int scan_u32(psod_ctx *c, const unsigned *in, unsigned *out, long long n, bool with_total);
+
+// stable LSD radix sort of (key, value) pairs on bits [0, end_bit); keys and
+// vals hold the input and receive the output.
+int radix_sort_u64(psod_ctx *c, unsigned long long *keys, unsigned *vals, long long n, int end_bit);
+int radix_sort_u32(psod_ctx *c, unsigned *keys, unsigned *vals, long long n, int end_bit);
+
+SodConst make_sod_const(const psod_ctx *c);
+
+int stage_cellsort(psod_ctx *c);
+int stage_cic(psod_ctx *c, double *grid_out);
+int stage_cicm1(psod_ctx *c, double *rho_out);
+int stage_tri_cic(psod_ctx *c, int64_t *isort_out);
+int stage_spherover(psod_ctx *c, psod_run_stats *st);
+
+}  // namespace psod

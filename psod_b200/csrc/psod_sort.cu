@@ -1,0 +1,278 @@
+// psod_sort.cu -- device-wide exclusive scan and stable LSD radix sort.
+//
+// Both are plain HBM-bound passes: the scan reads and writes 4 B per
+// element in three passes (tile reduce, tile-sum scan, tile scan + offset);
+// the radix sort makes one histogram pass and one stable scatter pass per
+// 8-bit digit, skipping digits that every key shares.
+#include "psod_internal.cuh"
+
+namespace psod {
+
+namespace {
+
+constexpr int SCAN_THREADS = 1024;
+constexpr int SCAN_ITEMS = 4;
+constexpr int SCAN_TILE = SCAN_THREADS * SCAN_ITEMS;
+
+__device__ __forceinline__ unsigned warp_incl_scan(unsigned v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    unsigned t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
+
+// block-wide exclusive scan for blockDim.x <= 1024 (multiple of 32)
+__device__ unsigned block_excl_scan(unsigned v, unsigned *total) {
+  __shared__ unsigned s_warp[33];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nw = blockDim.x >> 5;
+  unsigned inc = warp_incl_scan(v);
+  if (lane == 31) s_warp[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    unsigned x = lane < nw ? s_warp[lane] : 0u;
+    unsigned xi = warp_incl_scan(x);
+    if (lane < nw) s_warp[lane] = xi - x;
+    if (lane == 31) s_warp[32] = xi;  // lanes >= nw add 0, so this is the total
+  }
+  __syncthreads();
+  unsigned off = s_warp[w];
+  unsigned tot = s_warp[32];
+  __syncthreads();
+  if (total) *total = tot;
+  return off + inc - v;
+}
+
+__global__ void k_tile_reduce(const unsigned *in, long long n, unsigned *partial) {
+  long long base = (long long)blockIdx.x * SCAN_TILE;
+  unsigned s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    long long i = base + (long long)k * SCAN_THREADS + threadIdx.x;
+    if (i < n) s += in[i];
+  }
+  // reduce
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  __shared__ unsigned sw[32];
+  if ((threadIdx.x & 31) == 0) sw[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    unsigned v = threadIdx.x < (blockDim.x >> 5) ? sw[threadIdx.x] : 0u;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (threadIdx.x == 0) partial[blockIdx.x] = v;
+  }
+}
+
+// per-tile exclusive scan; blocked layout (thread t owns items t*ITEMS..)
+__global__ void k_tile_scan(const unsigned *in, unsigned *out, long long n, const unsigned *offsets,
+                            unsigned *total_out) {
+  long long base = (long long)blockIdx.x * SCAN_TILE + (long long)threadIdx.x * SCAN_ITEMS;
+  unsigned v[SCAN_ITEMS];
+  unsigned s = 0;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    long long i = base + k;
+    v[k] = (i < n) ? in[i] : 0u;
+    s += v[k];
+  }
+  unsigned tot;
+  unsigned ex = block_excl_scan(s, &tot);
+  unsigned off = (offsets ? offsets[blockIdx.x] : 0u) + ex;
+#pragma unroll
+  for (int k = 0; k < SCAN_ITEMS; k++) {
+    long long i = base + k;
+    if (i < n) out[i] = off;
+    off += v[k];
+  }
+  if (total_out && blockIdx.x == gridDim.x - 1 && threadIdx.x == blockDim.x - 1) {
+    // off now holds the inclusive sum through the last element of the tile
+    *total_out = off;
+  }
+}
+
+}  // namespace
+
+int scan_u32(psod_ctx *c, const unsigned *in, unsigned *out, long long n, bool with_total) {
+  if (n <= 0) {
+    if (with_total) PSOD_CUDA(c, cudaMemsetAsync(out, 0, sizeof(unsigned), c->stream));
+    return PSOD_OK;
+  }
+  long long ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
+  unsigned *partial = nullptr;
+  if (ntiles > 1) {
+    int st = dalloc(c, &partial, (size_t)ntiles + 1);
+    if (st) return st;
+    k_tile_reduce<<<(unsigned)ntiles, SCAN_THREADS, 0, c->stream>>>(in, n, partial);
+    st = scan_u32(c, partial, partial, ntiles, false);
+    if (st) {
+      dfree(&partial);
+      return st;
+    }
+  }
+  k_tile_scan<<<(unsigned)ntiles, SCAN_THREADS, 0, c->stream>>>(in, out, n, partial,
+                                                                 with_total ? out + n : nullptr);
+  cudaError_t e = cudaGetLastError();
+  if (partial) {
+    cudaStreamSynchronize(c->stream);
+    dfree(&partial);
+  }
+  if (e != cudaSuccess) return cuda_check(c, e, "scan_u32");
+  return PSOD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// radix sort
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_ITEMS = 16;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+constexpr int RS_RADIX = 256;
+
+template <typename K>
+__global__ void k_radix_hist(const K *keys, long long n, int shift, unsigned *hist, long long ntiles) {
+  __shared__ unsigned s_h[RS_RADIX];
+  s_h[threadIdx.x] = 0;
+  __syncthreads();
+  long long base = (long long)blockIdx.x * RS_TILE;
+#pragma unroll 4
+  for (int k = 0; k < RS_ITEMS; k++) {
+    long long i = base + (long long)k * RS_THREADS + threadIdx.x;
+    if (i < n) atomicAdd(&s_h[(unsigned)(keys[i] >> shift) & 0xffu], 1u);
+  }
+  __syncthreads();
+  hist[(long long)threadIdx.x * ntiles + blockIdx.x] = s_h[threadIdx.x];
+}
+
+// stable scatter: elements of a tile are ranked in order j*256 + t
+template <typename K>
+__global__ void k_radix_scatter(const K *keys, const unsigned *vals, K *okeys, unsigned *ovals, long long n,
+                                int shift, const unsigned *offsets, long long ntiles) {
+  __shared__ unsigned s_base[RS_RADIX];
+  __shared__ unsigned s_run[RS_RADIX];
+  __shared__ unsigned s_warp[RS_THREADS / 32][RS_RADIX];
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  s_base[t] = offsets[(long long)t * ntiles + blockIdx.x];
+  s_run[t] = 0;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  long long base = (long long)blockIdx.x * RS_TILE;
+  for (int j = 0; j < RS_ITEMS; j++) {
+#pragma unroll
+    for (int q = 0; q < RS_THREADS / 32; q++) s_warp[q][t] = 0;
+    __syncthreads();
+    long long i = base + (long long)j * RS_THREADS + t;
+    bool valid = i < n;
+    K key = valid ? keys[i] : (K)0;
+    unsigned val = valid ? vals[i] : 0u;
+    unsigned d = valid ? ((unsigned)(key >> shift) & 0xffu) : (RS_RADIX + lane);
+    unsigned peers = __match_any_sync(0xffffffffu, d);
+    unsigned rank_w = __popc(peers & lt_mask);
+    if (valid && rank_w == 0) s_warp[w][d] = __popc(peers);
+    __syncthreads();
+    {
+      unsigned run = s_run[t], acc = 0;
+#pragma unroll
+      for (int q = 0; q < RS_THREADS / 32; q++) {
+        unsigned cnt = s_warp[q][t];
+        s_warp[q][t] = run + acc;
+        acc += cnt;
+      }
+      s_run[t] = run + acc;
+    }
+    __syncthreads();
+    if (valid) {
+      unsigned pos = s_base[d] + s_warp[w][d] + rank_w;
+      okeys[pos] = key;
+      ovals[pos] = val;
+    }
+    __syncthreads();
+  }
+}
+
+template <typename K>
+__global__ void k_key_range(const K *keys, long long n, unsigned long long *mn_mx) {
+  unsigned long long mn = ~0ull, mx = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    unsigned long long k = (unsigned long long)keys[i];
+    mn = k < mn ? k : mn;
+    mx = k > mx ? k : mx;
+  }
+  atomicMin(&mn_mx[0], mn);
+  atomicMax(&mn_mx[1], mx);
+}
+
+template <typename K>
+int radix_sort_impl(psod_ctx *c, K *keys, unsigned *vals, long long n, int end_bit) {
+  if (n <= 1) return PSOD_OK;
+  // digits every key shares need no pass: find the highest differing bit
+  unsigned long long *d_rng = nullptr;
+  int st = dalloc(c, &d_rng, 2);
+  if (st) return st;
+  unsigned long long init[2] = {~0ull, 0ull};
+  PSOD_CUDA(c, cudaMemcpyAsync(d_rng, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+  k_key_range<K><<<592, 256, 0, c->stream>>>(keys, n, d_rng);
+  unsigned long long rng[2] = {0, ~0ull};
+  PSOD_CUDA(c, cudaMemcpyAsync(rng, d_rng, sizeof(rng), cudaMemcpyDeviceToHost, c->stream));
+  PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+  dfree(&d_rng);
+  unsigned long long diff = rng[0] ^ rng[1];
+  if (diff == 0) return PSOD_OK;  // all keys equal: a stable sort is the identity
+  int hi_bit = 64 - __builtin_clzll(diff);
+  if (hi_bit > end_bit) hi_bit = end_bit;
+  int ndigits = (hi_bit + 7) / 8;
+  long long ntiles = (n + RS_TILE - 1) / RS_TILE;
+  K *tk = nullptr;
+  unsigned *tv = nullptr, *hist = nullptr;
+  if ((st = dalloc(c, &tk, (size_t)n))) return st;
+  if ((st = dalloc(c, &tv, (size_t)n))) {
+    dfree(&tk);
+    return st;
+  }
+  if ((st = dalloc(c, &hist, (size_t)ntiles * RS_RADIX + 1))) {
+    dfree(&tk);
+    dfree(&tv);
+    return st;
+  }
+  K *ka = keys, *kb = tk;
+  unsigned *va = vals, *vb = tv;
+  for (int dgt = 0; dgt < ndigits; dgt++) {
+    int shift = dgt * 8;
+    k_radix_hist<K><<<(unsigned)ntiles, RS_THREADS, 0, c->stream>>>(ka, n, shift, hist, ntiles);
+    st = scan_u32(c, hist, hist, ntiles * RS_RADIX, false);
+    if (st) break;
+    k_radix_scatter<K><<<(unsigned)ntiles, RS_THREADS, 0, c->stream>>>(ka, va, kb, vb, n, shift, hist, ntiles);
+    K *tkk = ka;
+    ka = kb;
+    kb = tkk;
+    unsigned *tvv = va;
+    va = vb;
+    vb = tvv;
+  }
+  if (!st && ka != keys) {
+    cudaMemcpyAsync(keys, ka, sizeof(K) * n, cudaMemcpyDeviceToDevice, c->stream);
+    cudaMemcpyAsync(vals, va, sizeof(unsigned) * n, cudaMemcpyDeviceToDevice, c->stream);
+  }
+  cudaError_t e = cudaGetLastError();
+  cudaStreamSynchronize(c->stream);
+  dfree(&tk);
+  dfree(&tv);
+  dfree(&hist);
+  if (st) return st;
+  if (e != cudaSuccess) return cuda_check(c, e, "radix_sort");
+  return PSOD_OK;
+}
+
+}  // namespace
+
+int radix_sort_u64(psod_ctx *c, unsigned long long *keys, unsigned *vals, long long n, int end_bit) {
+  return radix_sort_impl<unsigned long long>(c, keys, vals, n, end_bit);
+}
+int radix_sort_u32(psod_ctx *c, unsigned *keys, unsigned *vals, long long n, int end_bit) {
+  return radix_sort_impl<unsigned>(c, keys, vals, n, end_bit);
+}
+
+}  // namespace psod

@@ -1,0 +1,367 @@
+// psod_stages.cu -- cell-sorted cube, CIC density and seed order.
+//
+//  stage_cellsort  the linked list of spherover (main:1564-1604) as a
+//                  counting sort of the particles into nx^3 SOD cells.
+//                  Each particle becomes one 16-byte float4 record, so every
+//                  later gather is a coalesced stream of whole cells.
+//  stage_cic       cic (main:1077-1265) on the 2nx-per-side periodic grid,
+//                  deposited as int64 fixed point (integer atomics are
+//                  associative, so the grid is the same on every run).
+//  stage_cicm1     cicm1 (main:1268-1390): 8-node gather per particle in the
+//                  reference's term order, FP64 without contraction.
+//  stage_tri_cic   tri_cic (main:998-1037): 1/rho < 0.01 compaction and a
+//                  stable radix sort of the seeds, ties by input index.
+#include <cmath>
+
+#include "psod_internal.cuh"
+
+namespace psod {
+
+namespace {
+
+constexpr double FIX_ONE = 1099511627776.0;  // 2^40
+
+// ---------------------------------------------------------------------------
+// cell sort
+// ---------------------------------------------------------------------------
+__global__ void k_cell_count(const float *pos, long long n, float nxf, double xs, int nx, unsigned *cell,
+                             unsigned *count, int *bad) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+  if (!(x >= 0.f && x <= 1.f && y >= 0.f && y <= 1.f && z >= 0.f && z <= 1.f)) {
+    atomicOr(bad, 1);
+    cell[i] = 0;
+    return;
+  }
+  int ci = sod_cell_axis(to_grid(x, nxf), xs, nx);
+  int cj = sod_cell_axis(to_grid(y, nxf), xs, nx);
+  int ck = sod_cell_axis(to_grid(z, nxf), xs, nx);
+  unsigned c = (unsigned)ci + (unsigned)nx * ((unsigned)cj + (unsigned)nx * (unsigned)ck);
+  cell[i] = c;
+  atomicAdd(&count[c], 1u);
+}
+
+__global__ void k_cell_scatter(const float *pos, long long n, const unsigned *cell, const unsigned *start,
+                               unsigned *fill, float4 *cube, unsigned *inv) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  unsigned c = cell[i];
+  unsigned slot = start[c] + atomicAdd(&fill[c], 1u);
+  cube[slot] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], __uint_as_float((unsigned)i));
+  inv[i] = slot;
+}
+
+__global__ void k_set_range(unsigned *a, unsigned long long lo, unsigned long long hi, unsigned v) {
+  unsigned long long i = lo + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < hi) a[i] = v;
+}
+
+// ---------------------------------------------------------------------------
+// CIC along one axis (main:1154-1190): returns the two node indices and the
+// weights ddx (upper node) and dex (lower node).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void cic_axis(float xf, double xxmin, double dx, int nc, int &i0, int &i1, double &dd,
+                                         double &de) {
+  double d = ddiv(dsub((double)xf, xxmin), dx);
+  int ix = (int)d;  // Fortran int(): truncation
+  if (d < 0.0) ix = ix - 1;
+  d = dsub(d, (double)ix);
+  double e = dsub(1.0, d);
+  int ixp1 = ix + 1;
+  if (ixp1 < 0) ixp1 += nc;
+  if (ix < 0) ix += nc;
+  if (ixp1 >= nc) ixp1 -= nc;
+  if (ix >= nc) ix -= nc;
+  i0 = ix;
+  i1 = ixp1;
+  dd = d;
+  de = e;
+}
+
+__device__ __forceinline__ bool in_zone_periodic(double x, double lo, double hi) {
+  return (x >= lo && x <= hi) || (x >= dadd(lo, 1.0) && x <= dadd(hi, 1.0)) ||
+         (x >= dsub(lo, 1.0) && x <= dsub(hi, 1.0));
+}
+
+struct CicConst {
+  double xxmin, xxmax, dx, kc;
+  int nc;
+};
+
+// deposit: 8 int64 atomics per particle, weights quantised to 2^-40
+__global__ void k_cic_deposit(const float4 *cube, long long n, CicConst k, unsigned long long *grid) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 p = cube[i];
+  if (!(in_zone_periodic(p.x, k.xxmin, k.xxmax) && in_zone_periodic(p.y, k.xxmin, k.xxmax) &&
+        in_zone_periodic(p.z, k.xxmin, k.xxmax)))
+    return;
+  int ix, ixp, iy, iyp, iz, izp;
+  double ddx, dex, ddy, dey, ddz, dez;
+  cic_axis(p.x, k.xxmin, k.dx, k.nc, ix, ixp, ddx, dex);
+  cic_axis(p.y, k.xxmin, k.dx, k.nc, iy, iyp, ddy, dey);
+  cic_axis(p.z, k.xxmin, k.dx, k.nc, iz, izp, ddz, dez);
+  const long long nc = k.nc;
+  const int cx[2] = {ix, ixp}, cy[2] = {iy, iyp}, cz[2] = {iz, izp};
+  const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    const int a = c & 1, b = (c >> 1) & 1, e = c >> 2;
+    double w = dmul(dmul(wx[a], wy[b]), wz[e]);
+    unsigned long long q = (unsigned long long)__double2ll_rn(dmul(w, FIX_ONE));
+    long long node = (long long)cx[a] + nc * ((long long)cy[b] + nc * (long long)cz[e]);
+    atomicAdd(&grid[node], q);
+  }
+}
+
+// interpolation: rho in the reference's term order (main:1368-1383)
+__global__ void k_cic_interp(const float4 *cube, long long n, CicConst k, const unsigned long long *grid,
+                             double *rho) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 p = cube[i];
+  unsigned idx = __float_as_uint(p.w) & PSOD_IDX_MASK;
+  if (!(in_zone_periodic(p.x, k.xxmin, k.xxmax) && in_zone_periodic(p.y, k.xxmin, k.xxmax) &&
+        in_zone_periodic(p.z, k.xxmin, k.xxmax))) {
+    rho[idx] = 0.0;
+    return;
+  }
+  int ix, ixp, iy, iyp, iz, izp;
+  double ddx, dex, ddy, dey, ddz, dez;
+  cic_axis(p.x, k.xxmin, k.dx, k.nc, ix, ixp, ddx, dex);
+  cic_axis(p.y, k.xxmin, k.dx, k.nc, iy, iyp, ddy, dey);
+  cic_axis(p.z, k.xxmin, k.dx, k.nc, iz, izp, ddz, dez);
+  const long long nc = k.nc;
+  const int cx[2] = {ix, ixp}, cy[2] = {iy, iyp}, cz[2] = {iz, izp};
+  const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
+  double r = 0.0;
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    const int a = c & 1, b = (c >> 1) & 1, e = c >> 2;
+    long long node = (long long)cx[a] + nc * ((long long)cy[b] + nc * (long long)cz[e]);
+    double g = dmul((double)(long long)grid[node], k.kc);
+    r = dadd(r, dmul(dmul(dmul(g, wx[a]), wy[b]), wz[e]));
+  }
+  rho[idx] = r;
+}
+
+__global__ void k_grid_to_double(const unsigned long long *grid, long long nnode, double kc, double *out) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nnode) out[i] = dmul((double)(long long)grid[i], kc);
+}
+
+// ---------------------------------------------------------------------------
+// seeds
+// ---------------------------------------------------------------------------
+__global__ void k_seed_flags(const double *rho, long long n, unsigned *flag, unsigned long long *minbits) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned f = 0;
+  unsigned long long mb = ~0ull;
+  if (i < n) {
+    double pd = ddiv(1.0, rho[i]);  // main:1022
+    if (pd < 0.01) {
+      f = 1;  // main:1029: 1/rho < 1/100
+    } else {
+      mb = dbits(pd);
+    }
+    flag[i] = f;
+  }
+  // block min of the non-seed keys
+  for (int o = 16; o > 0; o >>= 1) {
+    unsigned long long t = __shfl_down_sync(0xffffffffu, mb, o);
+    mb = t < mb ? t : mb;
+  }
+  if ((threadIdx.x & 31) == 0 && mb != ~0ull) atomicMin(minbits, mb);
+}
+
+__global__ void k_seed_extra_idx(const double *rho, long long n, unsigned long long minbits, unsigned *minidx) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double pd = ddiv(1.0, rho[i]);
+  if (!(pd < 0.01) && dbits(pd) == minbits) atomicMin(minidx, (unsigned)i);
+}
+
+__global__ void k_seed_compact(const double *rho, long long n, const unsigned *flag, const unsigned *pos,
+                               unsigned long long *keys, unsigned *vals) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !flag[i]) return;
+  unsigned o = pos[i];
+  keys[o] = dbits(ddiv(1.0, rho[i]));
+  vals[o] = (unsigned)i;
+}
+
+inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+int stage_cellsort(psod_ctx *c) {
+  const long long n = c->n;
+  const int nx = c->nx;
+  c->ncell = (unsigned long long)nx * nx * nx;
+  int st;
+  unsigned *cell = nullptr, *count = nullptr;
+  int *bad = nullptr;
+  if ((st = dalloc(c, &cell, (size_t)n))) return st;
+  if ((st = dalloc(c, &count, (size_t)c->ncell + 1))) return st;
+  if ((st = dalloc(c, &bad, 1))) return st;
+  if ((st = dalloc(c, &c->d_cell_start, (size_t)c->ncell + 1))) return st;
+  if ((st = dalloc(c, &c->d_cube, (size_t)n))) return st;
+  if ((st = dalloc(c, &c->d_cube_orig, (size_t)n))) return st;
+  if ((st = dalloc(c, &c->d_inv, (size_t)n))) return st;
+  PSOD_CUDA(c, cudaMemsetAsync(count, 0, sizeof(unsigned) * (c->ncell + 1), c->stream));
+  PSOD_CUDA(c, cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
+  const double xs = c->xxmin * c->scale;  // main:1565
+  k_cell_count<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_pos, n, (float)nx, xs, nx, cell, count, bad);
+  if ((st = scan_u32(c, count, c->d_cell_start, (long long)c->ncell, true))) return st;
+  PSOD_CUDA(c, cudaMemsetAsync(count, 0, sizeof(unsigned) * c->ncell, c->stream));
+  k_cell_scatter<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_pos, n, cell, c->d_cell_start, count, c->d_cube,
+                                                      c->d_inv);
+  int hbad = 0;
+  PSOD_CUDA(c, cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+  dfree(&cell);
+  dfree(&count);
+  dfree(&bad);
+  if (hbad) return set_err(c, PSOD_ERR_ARG, "particle positions must lie in [0,1] (box units)");
+
+  // The reference's run scan (main:1591-1604) files a final cell holding a
+  // single particle under the previous run.  Reproduce that by extending the
+  // previous cell's range over it.
+  c->has_quirk = 0;
+  c->quirk_pos = 0xffffffffu;
+  if (n >= 2) {
+    float4 last2[2];
+    PSOD_CUDA(c, cudaMemcpyAsync(last2, c->d_cube + (n - 2), sizeof(last2), cudaMemcpyDeviceToHost, c->stream));
+    PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+    auto host_cell = [&](const float4 &p) {
+      const float v[3] = {p.x, p.y, p.z};
+      unsigned idx[3];
+      for (int a = 0; a < 3; a++) {
+        float xg = v[a] * (float)nx;  // exact product rounded once, as on the device
+        int i = (int)std::floor((double)xg - xs);
+        if (i < 0) i += nx;
+        if (i >= nx) i -= nx;
+        idx[a] = (unsigned)i;
+      }
+      return idx[0] + (unsigned)nx * (idx[1] + (unsigned)nx * idx[2]);
+    };
+    unsigned ca = host_cell(last2[0]), cl = host_cell(last2[1]);
+    if (ca != cl) {
+      c->has_quirk = 1;
+      c->quirk_pos = (unsigned)(n - 1);
+      c->quirk_listed = ca;
+      c->quirk_phys = cl;
+      unsigned long long lo = (unsigned long long)ca + 1, hi = (unsigned long long)cl + 1;
+      k_set_range<<<nblk((long long)(hi - lo), 256), 256, 0, c->stream>>>(c->d_cell_start, lo, hi, (unsigned)n);
+    }
+  }
+  PSOD_CUDA(c, cudaMemcpyAsync(c->d_cube_orig, c->d_cube, sizeof(float4) * n, cudaMemcpyDeviceToDevice, c->stream));
+  PSOD_CUDA(c, cudaGetLastError());
+  PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+  return PSOD_OK;
+}
+
+static CicConst make_cic_const(const psod_ctx *c) {
+  CicConst k;
+  k.nc = 2 * c->nx;                                 // main:667
+  k.dx = 1.0 / (double)k.nc;                        // main:1126
+  k.xxmin = c->xxmin;                               // main:665
+  k.xxmax = -c->xxmin + 1.0;                        // zone + buffer upper edge
+  const double vol = (k.dx * k.dx) * k.dx;          // main:1263
+  k.kc = ((double)c->mpf / FIX_ONE) / vol;
+  return k;
+}
+
+int stage_cic(psod_ctx *c, double *grid_out) {
+  CicConst k = make_cic_const(c);
+  const long long nnode = (long long)k.nc * k.nc * k.nc;
+  int st;
+  if ((st = dalloc(c, &c->d_grid, (size_t)nnode))) return st;
+  PSOD_CUDA(c, cudaMemsetAsync(c->d_grid, 0, sizeof(unsigned long long) * nnode, c->stream));
+  k_cic_deposit<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->d_cube_orig, c->n, k, c->d_grid);
+  if ((st = dalloc(c, &c->d_rho, (size_t)c->n))) return st;
+  k_cic_interp<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->d_cube_orig, c->n, k, c->d_grid, c->d_rho);
+  PSOD_CUDA(c, cudaGetLastError());
+  if (grid_out) {
+    double *tmp = nullptr;
+    if (is_device_ptr(grid_out)) {
+      tmp = grid_out;
+    } else if ((st = dalloc(c, &tmp, (size_t)nnode))) {
+      return st;
+    }
+    k_grid_to_double<<<nblk(nnode, 256), 256, 0, c->stream>>>(c->d_grid, nnode, k.kc, tmp);
+    if (tmp != grid_out) {
+      st = copy_out(c, grid_out, tmp, sizeof(double) * nnode);
+      dfree(&tmp);
+      if (st) return st;
+    }
+  }
+  PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+  dfree(&c->d_grid);
+  c->cic_done = true;
+  c->rho_done = true;
+  return PSOD_OK;
+}
+
+int stage_cicm1(psod_ctx *c, double *rho_out) {
+  if (!c->rho_done) return set_err(c, PSOD_ERR_STATE, "psod_cicm1 needs psod_cic first");
+  if (rho_out) return copy_out(c, rho_out, c->d_rho, sizeof(double) * c->n);
+  return PSOD_OK;
+}
+
+int stage_tri_cic(psod_ctx *c, int64_t *isort_out) {
+  if (!c->rho_done) return set_err(c, PSOD_ERR_STATE, "psod_tri_cic needs psod_cic first");
+  const long long n = c->n;
+  int st;
+  unsigned *flag = nullptr, *posn = nullptr, *minidx = nullptr;
+  unsigned long long *minbits = nullptr, *keys = nullptr;
+  if ((st = dalloc(c, &flag, (size_t)n))) return st;
+  if ((st = dalloc(c, &posn, (size_t)n + 1))) return st;
+  if ((st = dalloc(c, &minbits, 1))) return st;
+  if ((st = dalloc(c, &minidx, 1))) return st;
+  PSOD_CUDA(c, cudaMemsetAsync(minbits, 0xff, sizeof(unsigned long long), c->stream));
+  PSOD_CUDA(c, cudaMemsetAsync(minidx, 0xff, sizeof(unsigned), c->stream));
+  k_seed_flags<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_rho, n, flag, minbits);
+  if ((st = scan_u32(c, flag, posn, n, true))) return st;
+  unsigned nd = 0;
+  unsigned long long hmin = 0;
+  PSOD_CUDA(c, cudaMemcpyAsync(&nd, posn + n, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+  PSOD_CUDA(c, cudaMemcpyAsync(&hmin, minbits, sizeof(hmin), cudaMemcpyDeviceToHost, c->stream));
+  PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+  const bool has_extra = hmin != ~0ull;
+  if (has_extra) k_seed_extra_idx<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_rho, n, hmin, minidx);
+  const long long nseed = (long long)nd + (has_extra ? 1 : 0);
+  if ((st = dalloc(c, &keys, (size_t)nd + 1))) return st;
+  if ((st = dalloc(c, &c->d_seed_idx, (size_t)nseed + 1))) return st;
+  k_seed_compact<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_rho, n, flag, posn, keys, c->d_seed_idx);
+  // seeds arrive in input order; a stable sort on 1/rho leaves ties in
+  // input order
+  if ((st = radix_sort_u64(c, keys, c->d_seed_idx, (long long)nd, 64))) return st;
+  if (has_extra)
+    PSOD_CUDA(c, cudaMemcpyAsync(c->d_seed_idx + nd, minidx, sizeof(unsigned), cudaMemcpyDeviceToDevice, c->stream));
+  PSOD_CUDA(c, cudaGetLastError());
+  PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+  dfree(&flag);
+  dfree(&posn);
+  dfree(&minbits);
+  dfree(&minidx);
+  dfree(&keys);
+  c->nseed_dense = nd;
+  c->npart_new = nseed;  // main:1032 (clamped to n when every particle is dense)
+  if (isort_out && nseed > 0) {
+    std::vector<unsigned> h((size_t)nseed);
+    PSOD_CUDA(c, cudaMemcpy(h.data(), c->d_seed_idx, sizeof(unsigned) * nseed, cudaMemcpyDeviceToHost));
+    if (is_device_ptr(isort_out)) {
+      std::vector<int64_t> hh(h.begin(), h.end());
+      PSOD_CUDA(c, cudaMemcpy(isort_out, hh.data(), sizeof(int64_t) * nseed, cudaMemcpyHostToDevice));
+    } else {
+      for (long long i = 0; i < nseed; i++) isort_out[i] = (int64_t)h[(size_t)i];
+    }
+  }
+  c->seeds_done = true;
+  return PSOD_OK;
+}
+
+}  // namespace psod

@@ -1,0 +1,176 @@
+"""Host-side mirror of the reference's SOD interface.
+
+``SphericalOverdensity`` exposes the four subroutines the Fortran driver of
+sod/sod_profile_rdfof_parallel_hdf5.f90 calls (cic main:673, cicm1 main:679,
+tri_cic main:713, spherover main:740) with the same argument meaning, on
+top of the C-ABI in include/psod.h. Errors raise ``PsodError`` carrying the
+C status (``ERR_NSEL`` / ``ERR_SELRADIUS`` keep the reference's "zone output
+lost" meaning).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import capi
+
+
+class PsodError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"psod status {status}: {message}")
+        self.status = status
+
+
+@dataclass
+class HaloTable:
+    halo_id: np.ndarray
+    halo_mass: np.ndarray
+    halo_rank: np.ndarray
+    halo_center: np.ndarray
+    halo_rdelta: np.ndarray
+    halo_mass2: np.ndarray
+    halo_mextra: np.ndarray
+    halo_profile: np.ndarray
+    member_offset: np.ndarray
+    member_index: np.ndarray
+    member_id: np.ndarray
+
+    @property
+    def nhalo(self) -> int:
+        return int(self.halo_id.shape[0])
+
+
+def _ptr(t):
+    if t is None:
+        return None
+    if isinstance(t, torch.Tensor):
+        return C.c_void_p(t.data_ptr())
+    return C.c_void_p(t.ctypes.data)
+
+
+class SphericalOverdensity:
+    """One zone of the SOD stage on one GPU (the reference's 1-rank run)."""
+
+    def __init__(self, nx: int, device: int = 0, **params):
+        self.lib = capi.load()
+        self.params = capi.default_params(nx, device=device, **params)
+        h = C.c_void_p()
+        st = self.lib.psod_ctx_create(C.byref(self.params), C.byref(h))
+        if st != capi.OK:
+            raise PsodError(st, "psod_ctx_create failed (invalid parameters or no CUDA device)")
+        self.ctx = h
+        self.n = 0
+
+    # -- lifecycle -----------------------------------------------------
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.psod_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int):
+        if st != capi.OK:
+            msg = self.lib.psod_last_error(self.ctx)
+            raise PsodError(st, msg.decode() if msg else "")
+
+    def set_stream(self, stream: torch.cuda.Stream):
+        self._check(self.lib.psod_set_stream(self.ctx, C.c_void_p(stream.cuda_stream)))
+
+    # -- the reference's entry points ---------------------------------
+    def load(self, pos, ids, vel=None, npart_total: int = 0):
+        """posf(3,N), idf(N), velf(3,N) of modvar (main:8-9); host or device."""
+        pos = _contig(pos, torch.float32)
+        ids = _contig(ids, torch.int64)
+        vel = _contig(vel, torch.float32) if vel is not None else None
+        n = int(pos.numel() // 3)
+        self.n = n
+        self._keep = (pos, ids, vel)
+        self._check(self.lib.psod_load_particles(self.ctx, n, _ptr(pos), _ptr(vel), _ptr(ids), int(npart_total)))
+
+    def cic(self, want_grid: bool = False):
+        """cic (main:1077-1265). Returns the (2nx)^3 grid [z,y,x] if asked."""
+        grid = None
+        if want_grid:
+            nc = 2 * self.params.nx
+            grid = np.zeros(nc**3, np.float64)
+        self._check(self.lib.psod_cic(self.ctx, _ptr(grid)))
+        return None if grid is None else grid.reshape(nc, nc, nc)
+
+    def cicm1(self, want_rho: bool = True):
+        """cicm1 (main:1268-1390): per-particle density, input order."""
+        rho = np.zeros(self.n, np.float64) if want_rho else None
+        self._check(self.lib.psod_cicm1(self.ctx, _ptr(rho)))
+        return rho
+
+    def tri_cic(self, want_isort: bool = True):
+        """tri_cic (main:998-1037): (isort[:npart_new] 0-based, npart_new)."""
+        nn = C.c_int64(0)
+        self._check(self.lib.psod_tri_cic(self.ctx, None, C.byref(nn)))
+        if not want_isort:
+            return None, int(nn.value)
+        isort = np.zeros(max(int(nn.value), 1), np.int64)
+        self._check(self.lib.psod_tri_cic(self.ctx, _ptr(isort), C.byref(nn)))
+        return isort[: int(nn.value)], int(nn.value)
+
+    def spherover(self) -> dict:
+        """spherover compute (main:1396-2201); returns run statistics."""
+        st = capi.RunStats()
+        self._check(self.lib.psod_spherover(self.ctx, C.byref(st)))
+        return st.as_dict()
+
+    def run(self) -> dict:
+        st = capi.RunStats()
+        self._check(self.lib.psod_run(self.ctx, C.byref(st)))
+        return st.as_dict()
+
+    def halos(self, members: bool = True) -> HaloTable:
+        nh, nm = C.c_int64(0), C.c_int64(0)
+        self._check(self.lib.psod_halo_count(self.ctx, C.byref(nh), C.byref(nm)))
+        h, m = int(nh.value), int(nm.value)
+        nb = self.params.nbins
+        ne = self.params.ndelta_extra
+        t = HaloTable(
+            halo_id=np.zeros(h, np.int64),
+            halo_mass=np.zeros(h, np.int64),
+            halo_rank=np.zeros(h, np.int64),
+            halo_center=np.zeros((h, 3), np.float32),
+            halo_rdelta=np.zeros(h, np.float64),
+            halo_mass2=np.zeros(h, np.int64),
+            halo_mextra=np.zeros((h, ne), np.int64),
+            halo_profile=np.zeros((h, nb), np.int64),
+            member_offset=np.zeros(h + 1, np.int64),
+            member_index=np.zeros(m if members else 0, np.int64),
+            member_id=np.zeros(m if members else 0, np.int64),
+        )
+        ct = capi.HaloTable()
+        for f, _ in capi.HaloTable._fields_:
+            a = getattr(t, f)
+            if f.startswith("member_") and f != "member_offset" and not members:
+                setattr(ct, f, None)
+            elif a.size == 0:
+                setattr(ct, f, None)
+            else:
+                setattr(ct, f, a.ctypes.data)
+        self._check(self.lib.psod_get_halos(self.ctx, C.byref(ct)))
+        return t
+
+
+def _contig(x, dtype):
+    if isinstance(x, torch.Tensor):
+        return x.to(dtype).contiguous()
+    return np.ascontiguousarray(x, dtype=torch.empty(0, dtype=dtype).numpy().dtype)

@@ -1,0 +1,177 @@
+"""GPU parity: the sm_100a path through the C-ABI against the CPU oracle.
+
+Bit-exact against the oracle's canonical arithmetic (int64 fixed-point CIC
+and refinement sums, index tie-breaks) for every output, and against the
+reference arithmetic for N_delta, halo IDs, R_delta and member sets on boxes
+without near-ties.  The CIC grid and rho are within 1e-6 relative of the
+reference's FP64 values.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from psod_b200.sod import PsodError, SphericalOverdensity  # noqa: E402
+from tests.boxes import hole_ball_box, holes_and_balls, lattice_box  # noqa: E402
+
+GRID_RTOL = 1e-6
+
+
+def gpu_run(nx, pos, ids, **params):
+    s = SphericalOverdensity(nx, **params)
+    s.load(pos, ids)
+    s.cic()
+    rho = s.cicm1()
+    isort, nn = s.tri_cic()
+    stats = s.spherover()
+    t = s.halos()
+    s.close()
+    return rho, isort, nn, stats, t
+
+
+def oparams(oracle, nx, **kw):
+    return oracle.Params(nx=nx, **kw)
+
+
+def assert_same_halos(t, r, exact_members_order=True):
+    assert t.nhalo == r.nhalo
+    assert np.array_equal(t.halo_mass, r.halo_mass)
+    assert np.array_equal(t.halo_id, r.halo_id)
+    assert np.array_equal(t.halo_rank, r.halo_rank)
+    assert np.array_equal(t.halo_center, r.halo_center)
+    assert np.array_equal(t.halo_rdelta, r.halo_rdelta)
+    assert np.array_equal(t.member_offset, r.member_offset)
+    if exact_members_order:
+        assert np.array_equal(t.member_index, r.member_index)
+    else:
+        for h in range(r.nhalo):
+            a = t.member_index[t.member_offset[h] : t.member_offset[h + 1]]
+            b = r.member_index[r.member_offset[h] : r.member_offset[h + 1]]
+            assert np.array_equal(np.sort(a), np.sort(b))
+
+
+def test_cic_grid_and_rho(oracle):
+    from psod_b200 import synth
+
+    b = synth.make_box(32, nmax_halo=2000, seed=21)
+    pos = b.pos.numpy()
+    s = SphericalOverdensity(32)
+    s.load(pos, b.ids.numpy())
+    grid = s.cic(want_grid=True)
+    rho = s.cicm1()
+    s.close()
+    p = oparams(oracle, 32)
+    g_ref = oracle.cic_grid(p, pos, oracle.REFERENCE)
+    g_can = oracle.cic_grid(p, pos, oracle.CANONICAL)
+    assert np.array_equal(grid, g_can)
+    np.testing.assert_allclose(grid, g_ref, rtol=GRID_RTOL, atol=GRID_RTOL)
+    r_can = oracle.rho(p, pos, oracle.CANONICAL, grid=g_can)
+    r_ref = oracle.rho(p, pos, oracle.REFERENCE, grid=g_ref)
+    assert np.array_equal(rho, r_can)
+    np.testing.assert_allclose(rho, r_ref, rtol=GRID_RTOL)
+
+
+def test_seed_order_matches_oracle(oracle):
+    from psod_b200 import synth
+
+    b = synth.make_box(32, nmax_halo=2000, seed=22)
+    rho, isort, nn, _, _ = gpu_run(32, b.pos.numpy(), b.ids.numpy())
+    ci, cnn = oracle.tri_cic(rho, oracle.CANONICAL)
+    assert nn == cnn
+    assert np.array_equal(isort, ci[:nn])
+
+
+def test_lattice_no_halo():
+    pos, ids = lattice_box(16)
+    rho, isort, nn, st, t = gpu_run(16, pos, ids)
+    assert np.all(rho == 8.0)
+    assert nn == 1
+    assert t.nhalo == 0
+
+
+def test_isolated_ball(oracle):
+    nx = 24
+    pos, ids, balls = hole_ball_box(nx, [(11.3, 12.6, 9.9)], r_hole=3.6, r_ball=0.3)
+    _, _, _, st, t = gpu_run(nx, pos, ids)
+    r = oracle.run(oparams(oracle, nx), pos, ids, oracle.CANONICAL)
+    assert t.nhalo == 1 and t.halo_mass[0] == balls[0].size
+    assert_same_halos(t, r)
+    assert np.array_equal(t.halo_profile, r.halo_profile)
+
+
+def test_periodic_ball(oracle):
+    nx = 24
+    pos, ids, balls = hole_ball_box(nx, [(0.2, 23.9, 12.0)], r_hole=3.6, r_ball=0.3, seed=9)
+    _, _, _, st, t = gpu_run(nx, pos, ids)
+    r = oracle.run(oparams(oracle, nx), pos, ids, oracle.CANONICAL)
+    assert_same_halos(t, r)
+
+
+def test_overlapping_balls(oracle):
+    nx = 32
+    ca, cb = (15.3, 16.2, 15.7), (16.2, 16.2, 15.7)
+    pos, ids, balls = holes_and_balls(nx, [(ca, 5.0)], [(ca, 0.35, 400), (cb, 0.6, None)], seed=11)
+    _, _, _, st, t = gpu_run(nx, pos, ids, nmin=10)
+    r = oracle.run(oparams(oracle, nx, nmin=10), pos, ids, oracle.CANONICAL)
+    assert r.nhalo == 2
+    assert_same_halos(t, r)
+
+
+def test_error_paths():
+    nx = 24
+    pos, ids, _ = hole_ball_box(nx, [(12.0, 12.0, 12.0)], r_hole=3.6, r_ball=0.3)
+    with pytest.raises(PsodError) as e:
+        gpu_run(nx, pos, ids, nsel=50)
+    assert e.value.status == 1
+    pos, ids, _ = hole_ball_box(32, [(16.0, 16.0, 16.0)], r_hole=12.0, r_ball=0.3, seed=4)
+    with pytest.raises(PsodError) as e:
+        gpu_run(32, pos, ids, ncut=2)
+    assert e.value.status == 2
+
+
+@pytest.mark.parametrize("nx,nmax,seed", [(32, 2000, 123), (48, 5000, 5), (64, 8000, 77)])
+def test_clustered_box_matches_oracle(oracle, nx, nmax, seed):
+    from psod_b200 import synth
+
+    b = synth.make_box(nx, nmax_halo=nmax, seed=seed)
+    pos, ids = b.pos.numpy(), b.ids.numpy()
+    _, _, nn, st, t = gpu_run(nx, pos, ids, delta_extra=(500.0, 178.0))
+    p = oparams(oracle, nx, delta_extra=(500.0, 178.0))
+    rc = oracle.run(p, pos, ids, oracle.CANONICAL)
+    assert rc.status == 0 and rc.nhalo > 0
+    assert nn == rc.npart_new
+    assert st["nprocessed"] == rc.nprocessed
+    assert_same_halos(t, rc)
+    assert np.array_equal(t.halo_profile, rc.halo_profile)
+    assert np.array_equal(t.halo_mass2, rc.halo_mass2)
+    assert np.array_equal(t.halo_mextra, rc.halo_mextra)
+    assert np.array_equal(t.member_id, ids[t.member_index])
+    # reference arithmetic: same N_delta, IDs, radii and member sets
+    rr = oracle.run(p, pos, ids, oracle.REFERENCE)
+    assert rr.status == 0
+    assert np.array_equal(t.halo_mass, rr.halo_mass)
+    assert np.array_equal(t.halo_id, rr.halo_id)
+    assert np.array_equal(t.halo_rdelta, rr.halo_rdelta)
+    assert_same_halos(t, rr, exact_members_order=False)
+
+
+def test_device_inputs_and_repeat(oracle):
+    from psod_b200 import synth
+
+    b = synth.make_box(32, nmax_halo=2000, seed=31)
+    s = SphericalOverdensity(32)
+    s.load(b.pos.cuda(), b.ids.cuda())
+    st1 = s.run()
+    t1 = s.halos()
+    st2 = s.run()
+    t2 = s.halos()
+    s.close()
+    assert st1["nhalo"] == st2["nhalo"]
+    assert np.array_equal(t1.member_index, t2.member_index)
+    rc = oracle.run(oparams(oracle, 32), b.pos, b.ids, oracle.CANONICAL)
+    assert_same_halos(t1, rc)

@@ -1,0 +1,189 @@
+"""CPU oracle: known-answer cases restated from the reference's semantics.
+
+The reference has no tests or golden vectors for the SOD path, so the
+oracle is pinned here against analytic boxes (lattice, isolated ball,
+overlapping balls, periodic boundary, error paths) and its two arithmetic
+modes are checked against each other.
+"""
+
+import numpy as np
+import pytest
+
+from tests.boxes import hole_ball_box, lattice_box, ref_d2
+
+
+def test_quick_sort_sorts_and_permutes(oracle):
+    rng = np.random.default_rng(1)
+    for n in (1, 2, 5, 6, 7, 13, 100, 1000):
+        v = rng.integers(0, 7, n).astype(np.float64)  # many ties
+        s, order = oracle.quick_sort(v)
+        assert np.all(np.diff(s) >= 0)
+        assert np.array_equal(np.sort(order), np.arange(n))
+        assert np.array_equal(v[order], s)
+
+
+def test_quick_sort_interchange_tie_order(oracle):
+    # n <= 6 uses the interchange sort (main:2552-2569): a swap happens only
+    # on a strict '>' so equal keys keep their relative order
+    s, order = oracle.quick_sort(np.array([2.0, 1.0, 2.0, 1.0]))
+    assert list(s) == [1.0, 1.0, 2.0, 2.0]
+    # trace: i=0: swap(0,1) -> [1,2,2,1]; j=3: swap(0,3)? 1>1 no.
+    # i=1: 2>2 no; 2>1 swap(1,3) -> [1,1,2,2] order [1,3,2,0]
+    assert list(order) == [1, 3, 2, 0]
+
+
+def test_cic_lattice_density(oracle):
+    nx = 16
+    pos, ids = lattice_box(nx)
+    p = oracle.Params(nx=nx)
+    for mode in (oracle.REFERENCE, oracle.CANONICAL):
+        rho = oracle.rho(p, pos, mode)
+        # a cell-centred particle sits on a node of the 2nx grid: rho = 8
+        assert np.all(rho == 8.0)
+
+
+def test_cic_mass_conservation(oracle):
+    rng = np.random.default_rng(5)
+    nx = 16
+    pos = rng.random((nx**3, 3)).astype(np.float32)
+    p = oracle.Params(nx=nx)
+    for mode in (oracle.REFERENCE, oracle.CANONICAL):
+        g = oracle.cic_grid(p, pos, mode)
+        # mean of the (2nx)^3 grid in units of the mean density is 1
+        assert abs(g.mean() - 1.0) < 1e-9
+
+
+def test_cic_modes_agree(oracle):
+    rng = np.random.default_rng(6)
+    nx = 16
+    pos = (rng.random((nx**3, 3)) ** 2).astype(np.float32)
+    p = oracle.Params(nx=nx)
+    g0 = oracle.cic_grid(p, pos, oracle.REFERENCE)
+    g1 = oracle.cic_grid(p, pos, oracle.CANONICAL)
+    assert np.allclose(g1, g0, rtol=1e-9, atol=1e-9)
+
+
+def test_lattice_has_no_halo(oracle):
+    nx = 16
+    pos, ids = lattice_box(nx)
+    for mode in (oracle.REFERENCE, oracle.CANONICAL):
+        r = oracle.run(oracle.Params(nx=nx), pos, ids, mode)
+        assert r.status == 0
+        assert r.npart_new == 1  # only the first particle at rho <= 100
+        assert r.nhalo == 0
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_isolated_ball_exact(oracle, mode):
+    nx = 24
+    c = (11.3, 12.6, 9.9)
+    pos, ids, balls = hole_ball_box(nx, [c], r_hole=3.6, r_ball=0.3)
+    ball = balls[0]
+    r = oracle.run(oracle.Params(nx=nx), pos, ids, mode)
+    assert r.status == 0
+    assert r.nhalo == 1
+    assert r.halo_mass[0] == ball.size
+    members = np.sort(r.member_index[r.member_offset[0] : r.member_offset[1]])
+    assert np.array_equal(members, ball)
+    # R_delta is the largest member distance from the centre particle
+    d2 = ref_d2(pos, nx, int(r.halo_cidx[0]))
+    assert r.halo_rdelta[0] == np.sqrt(d2[ball].max())
+    # members come out in ascending distance
+    md = d2[r.member_index]
+    assert np.all(np.diff(md) >= 0)
+    # halo ID is the centre particle's ID; centre is that particle's position
+    assert r.halo_id[0] == ids[r.halo_cidx[0]]
+    pg = (pos.astype(np.float64) * nx).astype(np.float32)
+    assert np.array_equal(r.halo_center[0], (pg[r.halo_cidx[0]].astype(np.float64) / nx).astype(np.float32))
+    # cumulative profile: last edge is R_delta itself (excluded), first >= 1
+    assert r.halo_profile[0, 0] >= 1
+    assert np.all(np.diff(r.halo_profile[0]) >= 0)
+    assert r.halo_profile[0, -1] <= ball.size
+
+
+def test_ball_across_periodic_boundary(oracle):
+    nx = 24
+    c = (0.2, 23.9, 12.0)
+    pos, ids, balls = hole_ball_box(nx, [c], r_hole=3.6, r_ball=0.3, seed=9)
+    for mode in (oracle.REFERENCE, oracle.CANONICAL):
+        r = oracle.run(oracle.Params(nx=nx), pos, ids, mode)
+        assert r.status == 0 and r.nhalo == 1
+        assert np.array_equal(np.sort(r.member_index), balls[0])
+
+
+def overlap_box():
+    # ball A (dense) and ball B whose near half lies inside A's R_200
+    from tests.boxes import holes_and_balls
+
+    nx = 32
+    ca, cb = (15.3, 16.2, 15.7), (16.2, 16.2, 15.7)
+    return nx, holes_and_balls(nx, [(ca, 5.0)], [(ca, 0.35, 400), (cb, 0.6, None)], seed=11)
+
+
+def test_overlapping_balls_claim_order(oracle):
+    # the denser ball is processed first and claims B's near half; B's halo
+    # is built from what is left (main:1628, 2148-2166)
+    nx, (pos, ids, balls) = overlap_box()
+    res = [oracle.run(oracle.Params(nx=nx, nmin=10), pos, ids, m) for m in (0, 1)]
+    for r in res:
+        assert r.status == 0
+        assert r.nhalo == 2
+        assert np.all(np.diff(r.halo_rank) > 0)
+        assert np.unique(r.member_index).size == r.member_index.size
+        a = set(r.member_index[r.member_offset[0] : r.member_offset[1]].tolist())
+        b = set(r.member_index[r.member_offset[1] : r.member_offset[2]].tolist())
+        assert set(balls[0].tolist()) <= a  # all of A
+        taken = len(a & set(balls[1].tolist()))
+        assert 0 < taken < balls[1].size  # part of B went to A
+        assert b <= set(balls[1].tolist()) | set(range(pos.shape[0]))
+    assert np.array_equal(res[0].halo_mass, res[1].halo_mass)
+    assert np.array_equal(np.sort(res[0].member_index), np.sort(res[1].member_index))
+
+
+def test_error_nsel(oracle):
+    nx = 24
+    pos, ids, balls = hole_ball_box(nx, [(12.0, 12.0, 12.0)], r_hole=3.6, r_ball=0.3)
+    r = oracle.run(oracle.Params(nx=nx, nsel=50), pos, ids, oracle.CANONICAL)
+    assert r.status == 1  # main:1681-1693: the zone's output is lost
+    assert r.nhalo == 0
+
+
+def test_error_selection_radius(oracle):
+    # a concentrated ball whose R_200 exceeds ncut = 2 cells
+    nx = 32
+    pos, ids, balls = hole_ball_box(nx, [(16.0, 16.0, 16.0)], r_hole=12.0, r_ball=0.3, seed=4)
+    assert balls[0].size > 6800
+    r = oracle.run(oracle.Params(nx=nx, ncut=2), pos, ids, oracle.CANONICAL)
+    assert r.status == 2  # main:2072-2089
+    assert r.nhalo == 0
+
+
+def test_modes_agree_on_clustered_box(oracle):
+    from psod_b200 import synth
+
+    b = synth.make_box(32, nmax_halo=2000, seed=123)
+    r0 = oracle.run(oracle.Params(nx=32), b.pos, b.ids, oracle.REFERENCE)
+    r1 = oracle.run(oracle.Params(nx=32), b.pos, b.ids, oracle.CANONICAL)
+    assert r0.status == r1.status == 0
+    assert r0.nhalo == r1.nhalo > 0
+    assert np.array_equal(r0.halo_mass, r1.halo_mass)
+    assert np.array_equal(r0.halo_id, r1.halo_id)
+    assert np.array_equal(r0.halo_rdelta, r1.halo_rdelta)
+    assert np.array_equal(r0.member_offset, r1.member_offset)
+    for h in range(r0.nhalo):
+        a = r0.member_index[r0.member_offset[h] : r0.member_offset[h + 1]]
+        b_ = r1.member_index[r1.member_offset[h] : r1.member_offset[h + 1]]
+        assert np.array_equal(np.sort(a), np.sort(b_))
+
+
+def test_extra_deltas_bracket_primary(oracle):
+    from psod_b200 import synth
+
+    b = synth.make_box(32, nmax_halo=2000, seed=7)
+    r = oracle.run(oracle.Params(nx=32, delta_extra=(500.0, 178.0)), b.pos, b.ids, oracle.CANONICAL)
+    assert r.status == 0 and r.nhalo > 0
+    m500, m178 = r.halo_mextra[:, 0], r.halo_mextra[:, 1]
+    ok = (m500 >= 0) & (m178 >= 0)
+    assert ok.mean() > 0.5
+    # a higher threshold stops no later on average
+    assert np.median(m500[ok]) <= np.median(r.halo_mass[ok]) <= np.median(m178[ok])
