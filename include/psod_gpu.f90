@@ -1,0 +1,103 @@
+! psod_gpu.f90 -- iso_c_binding interface of libpsod.so for the Fortran
+! driver of sod/sod_profile_rdfof_parallel_hdf5.f90.
+!
+! Mirrors include/psod.h.  The driver keeps its zone loop, reader and
+! writers; the four hot-path calls (cic main:673, cicm1 main:679,
+! tri_cic main:713, spherover main:740) become psod_* calls on a context.
+! Compile with any Fortran 2003 compiler and link -lpsod.
+module psod_gpu
+  use iso_c_binding
+  implicit none
+
+  integer(c_int), parameter :: PSOD_OK = 0, PSOD_ERR_NSEL = 1, &
+       PSOD_ERR_SELRADIUS = 2, PSOD_ERR_TIMEOUT = 3, PSOD_ERR_CUDA = 4, &
+       PSOD_ERR_ARG = 5, PSOD_ERR_STATE = 6, PSOD_ERR_NOMEM = 7
+  integer(c_int), parameter :: PSOD_MODE_PLAIN = 0, PSOD_MODE_BATCHED = 1, &
+       PSOD_MODE_LEARNED = 2
+
+  type, bind(C) :: psod_params
+     integer(c_int32_t) :: nx
+     integer(c_int32_t) :: nmin
+     real(c_double)     :: delta
+     real(c_double)     :: delta2
+     integer(c_int32_t) :: ncut
+     integer(c_int64_t) :: nsel
+     integer(c_int32_t) :: nxbuffer
+     integer(c_int64_t) :: npu
+     integer(c_int32_t) :: nbins
+     real(c_double)     :: rbin_lo
+     real(c_double)     :: rbin_hi
+     integer(c_int32_t) :: ndelta_extra
+     real(c_double)     :: delta_extra(4)
+     integer(c_int32_t) :: mode
+     integer(c_int32_t) :: device
+  end type psod_params
+
+  type, bind(C) :: psod_halo_table
+     type(c_ptr) :: halo_id, halo_mass, halo_rank, halo_center, halo_rdelta
+     type(c_ptr) :: halo_mass2, halo_mextra, halo_profile
+     type(c_ptr) :: member_offset, member_index, member_id
+  end type psod_halo_table
+
+  type, bind(C) :: psod_run_stats
+     integer(c_int64_t) :: npart_new, nprocessed, nhalo, nmember, rounds
+     integer(c_int64_t) :: fail_rank, touched
+     real(c_double)     :: ms_total, ms_sod_kernel
+     integer(c_int64_t) :: sod_launches, kernel_launches
+  end type psod_run_stats
+
+  interface
+     subroutine psod_params_default(p) bind(C, name="psod_params_default")
+       import :: psod_params
+       type(psod_params), intent(out) :: p
+     end subroutine
+     integer(c_int) function psod_ctx_create(p, ctx) bind(C, name="psod_ctx_create")
+       import :: c_int, c_ptr, psod_params
+       type(psod_params), intent(in) :: p
+       type(c_ptr), intent(out) :: ctx
+     end function
+     integer(c_int) function psod_ctx_destroy(ctx) bind(C, name="psod_ctx_destroy")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx
+     end function
+     integer(c_int) function psod_load_particles(ctx, n, pos, vel, id, npart_total) &
+          bind(C, name="psod_load_particles")
+       import :: c_int, c_ptr, c_int64_t
+       type(c_ptr), value :: ctx
+       integer(c_int64_t), value :: n, npart_total
+       type(c_ptr), value :: pos, vel, id
+     end function
+     integer(c_int) function psod_cic(ctx, grid) bind(C, name="psod_cic")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx, grid
+     end function
+     integer(c_int) function psod_cicm1(ctx, rho) bind(C, name="psod_cicm1")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: ctx, rho
+     end function
+     integer(c_int) function psod_tri_cic(ctx, isort, npart_new) bind(C, name="psod_tri_cic")
+       import :: c_int, c_ptr, c_int64_t
+       type(c_ptr), value :: ctx, isort
+       integer(c_int64_t), intent(out) :: npart_new
+     end function
+     integer(c_int) function psod_spherover(ctx, stats) bind(C, name="psod_spherover")
+       import :: c_int, c_ptr, psod_run_stats
+       type(c_ptr), value :: ctx
+       type(psod_run_stats), intent(out) :: stats
+     end function
+     integer(c_int) function psod_halo_count(ctx, nhalo, nmember) bind(C, name="psod_halo_count")
+       import :: c_int, c_ptr, c_int64_t
+       type(c_ptr), value :: ctx
+       integer(c_int64_t), intent(out) :: nhalo, nmember
+     end function
+     integer(c_int) function psod_get_halos(ctx, t) bind(C, name="psod_get_halos")
+       import :: c_int, c_ptr, psod_halo_table
+       type(c_ptr), value :: ctx
+       type(psod_halo_table), intent(in) :: t
+     end function
+     type(c_ptr) function psod_last_error(ctx) bind(C, name="psod_last_error")
+       import :: c_ptr
+       type(c_ptr), value :: ctx
+     end function
+  end interface
+end module psod_gpu

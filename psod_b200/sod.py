@@ -97,7 +97,7 @@ class SphericalOverdensity:
         pos = _contig(pos, torch.float32)
         ids = _contig(ids, torch.int64)
         vel = _contig(vel, torch.float32) if vel is not None else None
-        n = int(pos.numel() // 3)
+        n = int((pos.numel() if isinstance(pos, torch.Tensor) else pos.size) // 3)
         self.n = n
         self._keep = (pos, ids, vel)
         self._check(self.lib.psod_load_particles(self.ctx, n, _ptr(pos), _ptr(vel), _ptr(ids), int(npart_total)))
