@@ -108,9 +108,16 @@ typedef struct psod_run_stats {
   int64_t fail_rank;     /* failing seed rank, -1 if none */
   int64_t touched;       /* particle records read by the SOD kernels */
   double ms_total;       /* device time of psod_spherover */
-  double ms_sod_kernel;  /* device time inside the per-seed kernels */
+  double ms_sod_kernel;  /* device time of the per-seed phase kernels */
   int64_t sod_launches;  /* per-seed kernel launches */
   int64_t kernel_launches; /* all kernels launched by psod_spherover */
+  double ms_sched;       /* scheduler kernels */
+  double ms_prep;        /* preselect count + candidate lists */
+  double ms_refine;      /* approximate centre-refinement sums */
+  double ms_select;      /* exact contender sums + argmax */
+  double ms_cross;       /* crossing, profile, claims */
+  int64_t ncandidates;   /* refinement candidates */
+  int64_t refine_pairs;  /* candidate-neighbour records visited */
 } psod_run_stats;
 
 typedef struct psod_ctx psod_ctx;

@@ -44,6 +44,8 @@ module psod_gpu
      integer(c_int64_t) :: fail_rank, touched
      real(c_double)     :: ms_total, ms_sod_kernel
      integer(c_int64_t) :: sod_launches, kernel_launches
+     real(c_double)     :: ms_sched, ms_prep, ms_refine, ms_select, ms_cross
+     integer(c_int64_t) :: ncandidates, refine_pairs
   end type psod_run_stats
 
   interface

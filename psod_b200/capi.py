@@ -77,6 +77,13 @@ class RunStats(C.Structure):
         ("ms_sod_kernel", C.c_double),
         ("sod_launches", C.c_int64),
         ("kernel_launches", C.c_int64),
+        ("ms_sched", C.c_double),
+        ("ms_prep", C.c_double),
+        ("ms_refine", C.c_double),
+        ("ms_select", C.c_double),
+        ("ms_cross", C.c_double),
+        ("ncandidates", C.c_int64),
+        ("refine_pairs", C.c_int64),
     ]
 
     def as_dict(self):

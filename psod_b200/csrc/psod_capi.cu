@@ -17,6 +17,12 @@ int cuda_check(psod_ctx *c, cudaError_t e, const char *what) {
   return set_err(c, PSOD_ERR_CUDA, m);
 }
 
+void free_scratch(psod_ctx *c) {
+  for (auto &e : c->scratch)
+    if (e.first) cudaFree(e.first);
+  c->scratch.clear();
+}
+
 bool is_device_ptr(const void *p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -64,6 +70,7 @@ static void free_all(psod_ctx *c) {
   dfree(&c->d_h_rdelta);
   dfree(&c->d_m_offset);
   dfree(&c->d_m_index);
+  free_scratch(c);
 }
 
 extern "C" {

@@ -98,6 +98,8 @@ struct SodConst {
   double munit;     // per-particle mass after main:685
   double mmin;      // Mmin
   long long nsel;
+  long long n_total;    // records in the zone
+  unsigned mmin_count;  // smallest alive count reaching Mmin
   double zmin, zmax; // utile zone in grid units (main:691-696)
   double eps2;      // (scale/nx/2**6)**2 (main:1527)
   double rmin2;     // (scale/nx)**2 (main:1526)
@@ -164,6 +166,9 @@ struct psod_ctx {
   psod_run_stats last_stats{};
 
   std::vector<double> edge_fac;  // profile edge factors (host libm)
+
+  // device scratch kept across calls (grown on demand, freed at destroy)
+  std::vector<std::pair<void *, size_t>> scratch;
 };
 
 namespace psod {
@@ -200,6 +205,28 @@ void dfree(T **p) {
   if (*p) cudaFree(*p);
   *p = nullptr;
 }
+
+// scratch slot `id` of at least `count` elements, kept by the context
+template <typename T>
+int scratch(psod_ctx *c, int id, size_t count, T **out) {
+  if (c->scratch.size() <= (size_t)id) c->scratch.resize(id + 1, {nullptr, 0});
+  auto &e = c->scratch[id];
+  const size_t bytes = (count ? count : 1) * sizeof(T);
+  if (e.second < bytes) {
+    if (e.first) cudaFree(e.first);
+    e.first = nullptr;
+    e.second = 0;
+    if (cudaMalloc(&e.first, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      *out = nullptr;
+      return set_err(c, PSOD_ERR_NOMEM, "device scratch allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    e.second = bytes;
+  }
+  *out = (T *)e.first;
+  return PSOD_OK;
+}
+void free_scratch(psod_ctx *c);
 
 bool is_device_ptr(const void *p);
 int copy_out(psod_ctx *c, void *dst, const void *dsrc, size_t bytes);

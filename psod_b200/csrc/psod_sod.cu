@@ -49,7 +49,6 @@ struct SodBufs {
   unsigned char *processed;  // per rank
   const unsigned *ready;
   const unsigned *nready;
-  unsigned *work;            // work-stealing counter
   unsigned long long *err;   // (rank << 8) | code, atomicMin
   // halo records by slot
   unsigned long long *nhalo;
@@ -63,6 +62,22 @@ struct SodBufs {
   unsigned *pool_idx;            // input index
   unsigned long long *touched;
   unsigned long long *nprocessed;
+  // per ready slot (this round)
+  unsigned *st_active;  // 1: refine and cross
+  unsigned *st_na;      // alive particles in the preselect cube
+  unsigned *st_coff;    // candidate slice offset
+  unsigned *st_cn;      // candidate count
+  unsigned *st_centre;  // cube position of the refined centre
+  // candidates of this round
+  unsigned *cand_pos;
+  unsigned *cand_slot;  // owning ready slot
+  double *cand_s;       // approximate refinement sum
+  unsigned *cand_used;  // allocator
+  unsigned *work;       // [4] work-stealing counters: prep, refine, select, cross
+  unsigned *alive_cnt;  // alive records per cell (batched modes)
+  unsigned long long *pairs;       // candidate-neighbour records visited
+  unsigned long long *ncand_total; // candidates over all rounds
+  int mode;
 };
 
 struct Level {
@@ -133,6 +148,84 @@ __device__ __forceinline__ void for_cube(const SodConst &K, const SodBufs &B, in
       for (unsigned p = b + lane; p < e; p += 32) f(p, B.cube[p]);
     }
   }
+}
+
+// The part of a seed's preselect cube the crossing search visits: the whole
+// cube (rb2 < 0), or only the cube cells that intersect the ball of radius
+// rb around the centre.  Inside such a ball every alive particle of the cube
+// is visited, so ranks of particles with d2 <= rb2 are exact.
+struct Region {
+  int ic, jc, kc;     // seed cell: the cube centre
+  double xc, yc, zc;  // refined centre, grid units
+  double rb2;         // ball radius squared; < 0 means the whole cube
+  double rb;
+};
+
+// distance from ball-centre offset t0 (cells, relative to the seed cell
+// centre) to the cell at offset t, minus half a cell, periodic, >= 0
+__device__ __forceinline__ double cell_gap(double t0, int t, double nxd) {
+  double d = fabs((double)t - t0);
+  d = fmin(d, nxd - d);
+  return fmax(d - 0.5, 0.0);
+}
+
+template <typename F>
+__device__ __forceinline__ void for_region(const SodConst &K, const SodBufs &B, const Region &G, F f) {
+  if (G.rb2 < 0.0) {
+    for_cube(K, B, G.ic, G.jc, G.kc, K.ncut, f);
+    return;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int R = K.ncut, side = 2 * R + 1, nrow = side * side;
+  const unsigned nx = (unsigned)K.nx;
+  const double nxd = (double)K.nx;
+  // ball centre relative to the seed cell centre (cell i spans [i+xs, i+xs+1))
+  auto rel = [&](double x, int i) {
+    double d = x - ((double)i + K.xs + 0.5);
+    d = d - nxd * floor(d / nxd + 0.5);
+    return d;
+  };
+  const double tx = rel(G.xc, G.ic), ty = rel(G.yc, G.jc), tz = rel(G.zc, G.kc);
+  const double rm = G.rb + 1e-3;  // margin for rounding at cell edges
+  const double rm2 = rm * rm;
+  for (int row = w; row < nrow; row += NWARP) {
+    const int dj = row % side - R, dk = row / side - R;
+    const double gy = cell_gap(ty, dj, nxd), gz = cell_gap(tz, dk, nxd);
+    const double rem = rm2 - gy * gy - gz * gz;
+    if (rem < 0.0) continue;
+    const double wx = sqrt(rem);
+    int t0 = (int)ceil(tx - 0.5 - wx), t1 = (int)floor(tx + 0.5 + wx);
+    t0 = max(t0, -R);
+    t1 = min(t1, R);
+    if (t0 > t1) continue;
+    const unsigned jj = (unsigned)wrapi(G.jc + dj, K.nx), kk = (unsigned)wrapi(G.kc + dk, K.nx);
+    const unsigned long long base = (unsigned long long)nx * (jj + (unsigned long long)nx * kk);
+    const int x0 = G.ic + t0, x1 = G.ic + t1;
+    int pa[2], pb[2], np;
+    if (x0 < 0) {
+      pa[0] = x0 + K.nx; pb[0] = K.nx - 1; pa[1] = 0; pb[1] = x1; np = 2;
+      if (x1 < 0) { pa[0] = x0 + K.nx; pb[0] = x1 + K.nx; np = 1; }
+    } else if (x1 >= K.nx) {
+      pa[0] = x0; pb[0] = K.nx - 1; pa[1] = 0; pb[1] = x1 - K.nx; np = 2;
+      if (x0 >= K.nx) { pa[0] = x0 - K.nx; pb[0] = x1 - K.nx; np = 1; }
+    } else {
+      pa[0] = x0; pb[0] = x1; np = 1;
+    }
+    for (int q = 0; q < np; q++) {
+      const unsigned b = B.cs[base + (unsigned)pa[q]];
+      const unsigned e = B.cs[base + (unsigned)pb[q] + 1];
+      for (unsigned p = b + lane; p < e; p += 32) f(p, B.cube[p]);
+    }
+  }
+}
+
+// d2 of a record to the region's centre if it is alive and inside the
+// region's ball (always inside for the whole cube); else returns false
+__device__ __forceinline__ bool region_d2(const SodConst &K, const Region &G, float4 v, double &d2) {
+  if (__float_as_uint(v.w) & PSOD_DEAD_BIT) return false;
+  d2 = min_image_d2((double)to_grid(v.x, K.nxf), (double)to_grid(v.y, K.nxf), (double)to_grid(v.z, K.nxf), G.xc,
+                    G.yc, G.zc, K.tx);
+  return G.rb2 < 0.0 || d2 <= G.rb2;
 }
 
 __device__ __forceinline__ unsigned block_sum_u32(Smem &S, unsigned v) {
@@ -262,15 +355,13 @@ __device__ __forceinline__ bool keeps_going(const SodConst &K, long long i, doub
 
 // fill S.hist[l] with the bucket counts of alive records whose d2 bits lie
 // in [lo, hi]
-__device__ void build_hist(const SodConst &K, const SodBufs &B, Smem &S, int l, int ic, int jc, int kc, double xc,
-                           double yc, double zc) {
+__device__ void build_hist(const SodConst &K, const SodBufs &B, Smem &S, int l, const Region &G) {
   for (int k = threadIdx.x; k < NB; k += TPB) S.hist[l][k] = 0;
   __syncthreads();
   const Level L = S.lev[l];
-  for_cube(K, B, ic, jc, kc, K.ncut, [&](unsigned p, float4 v) {
-    if (__float_as_uint(v.w) & PSOD_DEAD_BIT) return;
-    double d2 = min_image_d2((double)to_grid(v.x, K.nxf), (double)to_grid(v.y, K.nxf), (double)to_grid(v.z, K.nxf),
-                             xc, yc, zc, K.tx);
+  for_region(K, B, G, [&](unsigned p, float4 v) {
+    double d2;
+    if (!region_d2(K, G, v, d2)) return;
     unsigned long long x = dbits(d2);
     if (l > 0 && (x < L.lo || x > L.hi)) return;
     atomicAdd(&S.hist[l][bucket_of(L, l, x)], 1u);
@@ -280,21 +371,19 @@ __device__ void build_hist(const SodConst &K, const SodBufs &B, Smem &S, int l, 
 
 // load alive records with d2 bits in [lo, hi] into S.skey/S.sidx, sort them
 // by (bits, input index); returns the count
-__device__ unsigned extract_sorted(const SodConst &K, const SodBufs &B, Smem &S, int ic, int jc, int kc, double xc,
-                                   double yc, double zc, unsigned long long lo, unsigned long long hi) {
+__device__ unsigned extract_sorted(const SodConst &K, const SodBufs &B, Smem &S, const Region &G,
+                                   unsigned long long lo, unsigned long long hi) {
   if (threadIdx.x == 0) S.nsorted = 0;
   __syncthreads();
-  for_cube(K, B, ic, jc, kc, K.ncut, [&](unsigned p, float4 v) {
-    unsigned wv = __float_as_uint(v.w);
-    if (wv & PSOD_DEAD_BIT) return;
-    double d2 = min_image_d2((double)to_grid(v.x, K.nxf), (double)to_grid(v.y, K.nxf), (double)to_grid(v.z, K.nxf),
-                             xc, yc, zc, K.tx);
+  for_region(K, B, G, [&](unsigned p, float4 v) {
+    double d2;
+    if (!region_d2(K, G, v, d2)) return;
     unsigned long long x = dbits(d2);
     if (x < lo || x > hi) return;
     unsigned s = atomicAdd(&S.nsorted, 1u);
     if (s < CAP) {
       S.skey[s] = x;
-      S.sidx[s] = wv & PSOD_IDX_MASK;
+      S.sidx[s] = __float_as_uint(v.w) & PSOD_IDX_MASK;
     }
   });
   __syncthreads();
@@ -333,9 +422,8 @@ __device__ unsigned extract_sorted(const SodConst &K, const SodBufs &B, Smem &S,
 //  mode 1 (backward): last position i in [2, imax] with overdensity > delta.
 // Returns 0 if not found, else the position; *d2_out its squared distance.
 // Returns -1 on an unresolvable bucket (more than CAP exact-equal keys).
-__device__ long long radial_search(const SodConst &K, const SodBufs &B, Smem &S, int ic, int jc, int kc, double xc,
-                                   double yc, double zc, long long na, double delta, int mode, long long imax,
-                                   double *d2_out) {
+__device__ long long radial_search(const SodConst &K, const SodBufs &B, Smem &S, const Region &G, long long na,
+                                   double delta, int mode, long long imax, double *d2_out) {
   // level 0 histogram is built by the caller
   int l = 0;
   if (threadIdx.x == 0) {
@@ -395,7 +483,7 @@ __device__ long long radial_search(const SodConst &K, const SodBufs &B, Smem &S,
     bucket_range(L, l, cand, lo, hi);
     const long long c0 = (long long)L.cum + S.pref[cand];
     if (nb <= CAP) {
-      unsigned n = extract_sorted(K, B, S, ic, jc, kc, xc, yc, zc, lo, hi);
+      unsigned n = extract_sorted(K, B, S, G, lo, hi);
       long long hit;
       if (mode == 0) {
         int best = 0x7fffffff;
@@ -439,23 +527,21 @@ __device__ long long radial_search(const SodConst &K, const SodBufs &B, Smem &S,
     }
     __syncthreads();
     l++;
-    build_hist(K, B, S, l, ic, jc, kc, xc, yc, zc);
+    build_hist(K, B, S, l, G);
   }
 }
 
 // the pos-th (1-based) element of the sorted sequence when it is the last
 // element below `below_lo`: the maximum (bits, index) under that bound
-__device__ void max_below(const SodConst &K, const SodBufs &B, Smem &S, int ic, int jc, int kc, double xc, double yc,
-                          double zc, unsigned long long below_lo, unsigned long long &kout, unsigned &iout) {
+__device__ void max_below(const SodConst &K, const SodBufs &B, Smem &S, const Region &G,
+                          unsigned long long below_lo, unsigned long long &kout, unsigned &iout) {
   unsigned long long a = 0, b = 0;
-  for_cube(K, B, ic, jc, kc, K.ncut, [&](unsigned p, float4 v) {
-    unsigned wv = __float_as_uint(v.w);
-    if (wv & PSOD_DEAD_BIT) return;
-    double d2 = min_image_d2((double)to_grid(v.x, K.nxf), (double)to_grid(v.y, K.nxf), (double)to_grid(v.z, K.nxf),
-                             xc, yc, zc, K.tx);
+  for_region(K, B, G, [&](unsigned p, float4 v) {
+    double d2;
+    if (!region_d2(K, G, v, d2)) return;
     unsigned long long x = dbits(d2);
     if (x >= below_lo) return;
-    unsigned long long ix = wv & PSOD_IDX_MASK;
+    unsigned long long ix = __float_as_uint(v.w) & PSOD_IDX_MASK;
     if (x > a || (x == a && ix > b)) { a = x; b = ix; }
   });
   block_max_pair(S, a, b);
@@ -467,147 +553,412 @@ __device__ void record_error(const SodBufs &B, unsigned rank, unsigned code) {
   atomicMin(B.err, ((unsigned long long)rank << 8) | code);
 }
 
-__device__ void process_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned rank) {
-  const unsigned sidx = B.seed_idx[rank];
-  const unsigned sp = B.inv[sidx];
-  const float4 sv = B.cube[sp];
-  if (__float_as_uint(sv.w) & PSOD_DEAD_BIT) return;  // claimed (main:1628)
-  // seed position and cell (main:1631-1654)
-  const double xs0 = (double)to_grid(sv.x, K.nxf), ys0 = (double)to_grid(sv.y, K.nxf),
-               zs0 = (double)to_grid(sv.z, K.nxf);
-  const int ic = sod_cell_axis(to_grid(sv.x, K.nxf), K.xs, K.nx);
-  const int jc = sod_cell_axis(to_grid(sv.y, K.nxf), K.xs, K.nx);
-  const int kc = sod_cell_axis(to_grid(sv.z, K.nxf), K.xs, K.nx);
+struct SeedGeo {
+  unsigned sp;  // cube position of the seed
+  int ic, jc, kc;
+};
 
-  // 1. preselect count (main:1657-1716)
-  unsigned cnt = 0, recs = 0;
-  for_cube(K, B, ic, jc, kc, K.ncut, [&](unsigned p, float4 v) {
-    recs++;
-    if (!(__float_as_uint(v.w) & PSOD_DEAD_BIT)) cnt++;
-  });
-  const unsigned na = block_sum_u32(S, cnt);
-  const unsigned nrec = block_sum_u32(S, recs);
-  if (threadIdx.x == 0) atomicAdd(B.touched, (unsigned long long)nrec);
-  if ((long long)na > K.nsel) {
-    if (threadIdx.x == 0) record_error(B, rank, PSOD_ERR_NSEL);
-    return;
+__device__ __forceinline__ SeedGeo seed_geo(const SodConst &K, const SodBufs &B, unsigned rank) {
+  SeedGeo g;
+  g.sp = B.inv[B.seed_idx[rank]];
+  const float4 v = B.cube[g.sp];
+  g.ic = sod_cell_axis(to_grid(v.x, K.nxf), K.xs, K.nx);
+  g.jc = sod_cell_axis(to_grid(v.y, K.nxf), K.xs, K.nx);
+  g.kc = sod_cell_axis(to_grid(v.z, K.nxf), K.xs, K.nx);
+  return g;
+}
+
+// CTA-level work stealing over the round's ready list
+__device__ __forceinline__ unsigned next_item(unsigned *ctr) {
+  __shared__ unsigned s_item;
+  __syncthreads();
+  if (threadIdx.x == 0) s_item = atomicAdd(ctr, 1u);
+  __syncthreads();
+  return s_item;
+}
+
+// records filed under the cube's cells (alive or not): one run per row
+__device__ unsigned cube_records(const SodConst &K, const SodBufs &B, Smem &S, int ic, int jc, int kc) {
+  const int R = K.ncut, side = 2 * R + 1;
+  unsigned sum = 0;
+  for (int row = threadIdx.x; row < side * side; row += TPB) {
+    const int dj = row % side - R, dk = row / side - R;
+    const unsigned jj = (unsigned)wrapi(jc + dj, K.nx), kk = (unsigned)wrapi(kc + dk, K.nx);
+    const unsigned long long base = (unsigned long long)K.nx * (jj + (unsigned long long)K.nx * kk);
+    const int x0 = ic - R, x1 = ic + R;
+    if (x0 < 0) {
+      sum += B.cs[base + K.nx] - B.cs[base + (unsigned)(x0 + K.nx)];
+      sum += B.cs[base + (unsigned)x1 + 1] - B.cs[base];
+    } else if (x1 >= K.nx) {
+      sum += B.cs[base + K.nx] - B.cs[base + (unsigned)x0];
+      sum += B.cs[base + (unsigned)(x1 - K.nx) + 1] - B.cs[base];
+    } else {
+      sum += B.cs[base + (unsigned)x1 + 1] - B.cs[base + (unsigned)x0];
+    }
   }
-  if (!(dmul((double)na, K.munit) >= K.mmin)) return;  // main:1759
-  if (threadIdx.x == 0) atomicAdd(B.nprocessed, 1ull);
+  return block_sum_u32(S, sum);
+}
 
-  // 2. centre refinement (main:1799-1909).  Warp per candidate; lanes stride
-  // over the candidate's 27 neighbour cells, keeping those filed within +-2
-  // cells of the seed (the x_sel2 set, main:1720-1755).
-  {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    unsigned long long my_sq = 0, my_key = ~0ull;
-    unsigned my_pos = 0xffffffffu;
-    bool have = false;
-    // enumerate candidate rows: 9 rows of 3 cells around the seed cell
-    for (int row = 0; row < 9; row++) {
-      const int dj = row % 3 - 1, dk = row / 3 - 1;
+__device__ __forceinline__ int zig(int a) { return (a & 1) ? -((a + 1) >> 1) : (a >> 1); }
+
+// alive particles of the cube from the per-cell counts, rows nearest the
+// seed first; stops once `need` is reached (returns the running sum)
+__device__ unsigned alive_rows(const SodConst &K, const SodBufs &B, Smem &S, int ic, int jc, int kc, unsigned need) {
+  const int R = K.ncut, side = 2 * R + 1, nrow = side * side;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned total = 0;
+  for (int r0 = 0; r0 < nrow; r0 += NWARP) {
+    const int row = r0 + w;
+    unsigned part = 0;
+    if (row < nrow) {
+      const int dj = zig(row % side), dk = zig(row / side);
       const unsigned jj = (unsigned)wrapi(jc + dj, K.nx), kk = (unsigned)wrapi(kc + dk, K.nx);
-      const unsigned long long rbase = (unsigned long long)K.nx * (jj + (unsigned long long)K.nx * kk);
-      for (int di = -1; di <= 1; di++) {
-        const unsigned ii = (unsigned)wrapi(ic + di, K.nx);
-        const unsigned cb = B.cs[rbase + ii], ce = B.cs[rbase + ii + 1];
-        // warps take candidates of this cell round-robin
-        for (unsigned cp = cb + w; cp < ce; cp += NWARP) {
-          const float4 cv = B.cube[cp];
-          const unsigned cw = __float_as_uint(cv.w);
-          if (cw & PSOD_DEAD_BIT) continue;
-          const float cxg = to_grid(cv.x, K.nxf), cyg = to_grid(cv.y, K.nxf), czg = to_grid(cv.z, K.nxf);
-          const double cx = cxg, cy = cyg, cz = czg;
-          const int pcx = sod_cell_axis(cxg, K.xs, K.nx), pcy = sod_cell_axis(cyg, K.xs, K.nx),
-                    pcz = sod_cell_axis(czg, K.xs, K.nx);
-          unsigned long long sq = 0;
-          for (int nrow = 0; nrow < 9; nrow++) {
-            const int ny = wrapi(pcy + nrow % 3 - 1, K.nx), nz = wrapi(pcz + nrow / 3 - 1, K.nx);
-            if (abs(pdiff(ny, jc, K.nx)) > 2 || abs(pdiff(nz, kc, K.nx)) > 2) continue;
-            const unsigned long long nbase = (unsigned long long)K.nx * ((unsigned)ny + (unsigned long long)K.nx * (unsigned)nz);
-            for (int ndi = -1; ndi <= 1; ndi++) {
-              const int nxc = wrapi(pcx + ndi, K.nx);
-              if (abs(pdiff(nxc, ic, K.nx)) > 2) continue;
-              const unsigned nb = B.cs[nbase + (unsigned)nxc], ne = B.cs[nbase + (unsigned)nxc + 1];
-              for (unsigned q = nb + lane; q < ne; q += 32) {
-                const float4 nv = B.cube[q];
-                if (__float_as_uint(nv.w) & PSOD_DEAD_BIT) continue;
-                double d2 = min_image_d2((double)to_grid(nv.x, K.nxf), (double)to_grid(nv.y, K.nxf),
-                                         (double)to_grid(nv.z, K.nxf), cx, cy, cz, K.tx);
-                if (d2 <= K.rmin2) {
-                  double t = ddiv(1.0, dsqrt(dadd(d2, K.eps2)));  // main:1854-1855
-                  sq += (unsigned long long)__double2ll_rn(dmul(t, 1099511627776.0));
-                }
-              }
-            }
-          }
-          // the particle the run scan files under another cell
-          if (K.has_quirk && lane == 0) {
-            const int ax = (int)(K.quirk_listed % K.nx), ay = (int)((K.quirk_listed / K.nx) % K.nx),
-                      az = (int)(K.quirk_listed / ((unsigned)K.nx * K.nx));
-            const bool listed_in_sel2 = abs(pdiff(ax, ic, K.nx)) <= 2 && abs(pdiff(ay, jc, K.nx)) <= 2 &&
-                                        abs(pdiff(az, kc, K.nx)) <= 2;
-            const bool seen = abs(pdiff(ax, pcx, K.nx)) <= 1 && abs(pdiff(ay, pcy, K.nx)) <= 1 &&
-                              abs(pdiff(az, pcz, K.nx)) <= 1;
-            if (listed_in_sel2 && !seen) {
-              const float4 qv = B.cube[K.quirk_pos];
-              if (!(__float_as_uint(qv.w) & PSOD_DEAD_BIT)) {
-                double d2 = min_image_d2((double)to_grid(qv.x, K.nxf), (double)to_grid(qv.y, K.nxf),
-                                         (double)to_grid(qv.z, K.nxf), cx, cy, cz, K.tx);
-                if (d2 <= K.rmin2) {
-                  double t = ddiv(1.0, dsqrt(dadd(d2, K.eps2)));
-                  sq += (unsigned long long)__double2ll_rn(dmul(t, 1099511627776.0));
-                }
-              }
-            }
-          }
-          for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(0xffffffffu, sq, o);
-          if (lane == 0) {
-            // scan-order key: listed cell offset (x outer, z inner), then index
-            int lx = di, ly = dj, lz = dk;
-            if (K.has_quirk && cp == K.quirk_pos) {
-              lx = pdiff((int)(K.quirk_listed % K.nx), ic, K.nx);
-              ly = pdiff((int)((K.quirk_listed / K.nx) % K.nx), jc, K.nx);
-              lz = pdiff((int)(K.quirk_listed / ((unsigned)K.nx * K.nx)), kc, K.nx);
-            }
-            const unsigned o = (unsigned)(((lx + 1) * 3 + (ly + 1)) * 3 + (lz + 1));
-            const unsigned long long key = ((unsigned long long)o << 32) | (cw & PSOD_IDX_MASK);
-            if (!have || sq > my_sq || (sq == my_sq && key < my_key)) {
-              have = true;
-              my_sq = sq;
-              my_key = key;
-              my_pos = cp;
-            }
-          }
+      const unsigned long long base = (unsigned long long)K.nx * (jj + (unsigned long long)K.nx * kk);
+      for (int t = lane; t < side; t += 32) part += B.alive_cnt[base + (unsigned)wrapi(ic - R + t, K.nx)];
+    }
+    total += block_sum_u32(S, part);
+    if (total >= need) break;
+  }
+  return total;
+}
+
+// ---------------------------------------------------------------------------
+// phase 1: preselect count (main:1657-1716) and the candidate list of the
+// +-1 cells (main:1807-1826)
+// ---------------------------------------------------------------------------
+__device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
+  if (threadIdx.x == 0) {
+    B.st_active[slot] = 0;
+    B.st_cn[slot] = 0;
+    B.processed[rank] = 1;
+  }
+  const SeedGeo g = seed_geo(K, B, rank);
+  if (__float_as_uint(B.cube[g.sp].w) & PSOD_DEAD_BIT) return;  // claimed (main:1628)
+  unsigned na = 0;
+  if (B.mode == PSOD_MODE_PLAIN) {
+    // the reference's preselect: every record of the cube
+    unsigned cnt = 0, recs = 0;
+    for_cube(K, B, g.ic, g.jc, g.kc, K.ncut, [&](unsigned p, float4 v) {
+      recs++;
+      if (!(__float_as_uint(v.w) & PSOD_DEAD_BIT)) cnt++;
+    });
+    na = block_sum_u32(S, cnt);
+    const unsigned nrec = block_sum_u32(S, recs);
+    if (threadIdx.x == 0) atomicAdd(B.touched, (unsigned long long)nrec);
+    if ((long long)na > K.nsel) {
+      if (threadIdx.x == 0) record_error(B, rank, PSOD_ERR_NSEL);
+      return;
+    }
+    if (!(dmul((double)na, K.munit) >= K.mmin)) return;  // main:1759
+  } else {
+    // same tests from the per-cell alive counts: nsel against the cube's
+    // record count (exact alive count only when that bound exceeds nsel),
+    // Mmin by summing rows nearest the seed first until it is reached
+    if (K.n_total > K.nsel) {
+      const unsigned recs = cube_records(K, B, S, g.ic, g.jc, g.kc);
+      if ((long long)recs > K.nsel) {
+        const unsigned exact = alive_rows(K, B, S, g.ic, g.jc, g.kc, ~0u);
+        if ((long long)exact > K.nsel) {
+          if (threadIdx.x == 0) record_error(B, rank, PSOD_ERR_NSEL);
+          return;
         }
       }
     }
-    // block argmax: larger sum wins; equal sums go to the smaller key.
-    // Encode as (sq, ~key) and take the lexicographic maximum.
-    unsigned long long a = have ? my_sq : 0ull, b = have ? ~my_key : 0ull;
-    unsigned long long pa = a, pb = b;
-    if (threadIdx.x == 0) S.best_pos = sp;  // no candidate: the seed stays the centre
-    block_max_pair(S, a, b);
-    if (have && a > 0 && pa == a && pb == b) S.best_pos = my_pos;
-    __syncthreads();
+    const unsigned need = K.mmin_count;
+    const unsigned got = alive_rows(K, B, S, g.ic, g.jc, g.kc, need);
+    if (got < need) return;  // main:1759
   }
-  const unsigned cpos = S.best_pos;
-  const float4 cvv = B.cube[cpos];
-  const double xc = (double)to_grid(cvv.x, K.nxf), yc = (double)to_grid(cvv.y, K.nxf),
-               zc = (double)to_grid(cvv.z, K.nxf);
-  const unsigned cidx = __float_as_uint(cvv.w) & PSOD_IDX_MASK;
-  (void)xs0; (void)ys0; (void)zs0;
-
-  // 3. crossing (main:2040-2100)
+  // candidates: alive records filed under the 27 cells around the seed cell
+  unsigned nc = 0;
+  for_cube(K, B, g.ic, g.jc, g.kc, 1, [&](unsigned p, float4 v) {
+    if (!(__float_as_uint(v.w) & PSOD_DEAD_BIT)) nc++;
+  });
+  const unsigned ncand = block_sum_u32(S, nc);
+  __shared__ unsigned s_off, s_fill;
   if (threadIdx.x == 0) {
-    S.lev[0].lo = 0;
-    S.lev[0].hi = 0x7fefffffffffffffull;
-    S.lev[0].shift = L1_SHIFT;
+    s_off = atomicAdd(B.cand_used, ncand);
+    s_fill = 0;
+    B.st_na[slot] = na;  // 0 when unknown (batched modes)
+    B.st_coff[slot] = s_off;
+    B.st_cn[slot] = ncand;
+    B.st_active[slot] = 1;
+    B.st_centre[slot] = g.sp;  // no candidate: the seed stays the centre
+    atomicAdd(B.nprocessed, 1ull);
   }
   __syncthreads();
-  build_hist(K, B, S, 0, ic, jc, kc, xc, yc, zc);
+  const unsigned off = s_off;
+  for_cube(K, B, g.ic, g.jc, g.kc, 1, [&](unsigned p, float4 v) {
+    if (__float_as_uint(v.w) & PSOD_DEAD_BIT) return;
+    const unsigned q = off + atomicAdd(&s_fill, 1u);
+    B.cand_pos[q] = p;
+    B.cand_slot[q] = slot;
+  });
+}
+
+__global__ void __launch_bounds__(TPB) k_prep(SodConst K, SodBufs B) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem &S = *reinterpret_cast<Smem *>(smem_raw);
+  while (true) {
+    const unsigned item = next_item(&B.work[0]);
+    if (item >= *B.nready) break;
+    prep_seed(K, B, S, item, B.ready[item]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// phase 2: approximate refinement sums, one warp per candidate over the whole
+// GPU.  Distances in FP32 with a relative error below 1e-6; pairs whose FP32
+// d2 lies within 1e-5 of the inclusion edge are decided in exact FP64; the
+// sum is accumulated in FP64.  |S_approx - S| <= REF_TOL * S.
+// ---------------------------------------------------------------------------
+constexpr double REF_TOL = 1e-5;
+
+// FP32 minimum-image |a - b| with one rounding on the small branch
+__device__ __forceinline__ float mi_dx(float a, float b, float nxf) {
+  const float hi = fmaxf(a, b), lo = fminf(a, b);
+  const float d1 = __fsub_rn(hi, lo);
+  const float d2 = __fadd_rn(__fsub_rn(nxf, hi), lo);
+  return fminf(d1, d2);
+}
+
+// does candidate cell (x,y,z) lie within +-2 cells of the seed (x_sel2)?
+__device__ __forceinline__ bool in_sel2(const SodConst &K, int x, int y, int z, int ic, int jc, int kc) {
+  return abs(pdiff(x, ic, K.nx)) <= 2 && abs(pdiff(y, jc, K.nx)) <= 2 && abs(pdiff(z, kc, K.nx)) <= 2;
+}
+
+// Refinement sum of one candidate, warp-cooperative.  exact: canonical
+// int64 fixed-point sum of FP64 terms (main:1840-1859); else the FP64 sum of
+// FP32 terms.  Result valid in lane 0.
+template <bool EXACT>
+__device__ void refine_sum(const SodConst &K, const SodBufs &B, unsigned cp, int ic, int jc, int kc,
+                           unsigned long long &sq_out, double &sf_out, unsigned *visits = nullptr) {
+  const int lane = threadIdx.x & 31;
+  const float4 cv = B.cube[cp];
+  const float cxg = to_grid(cv.x, K.nxf), cyg = to_grid(cv.y, K.nxf), czg = to_grid(cv.z, K.nxf);
+  const double cx = cxg, cy = cyg, cz = czg;
+  const int pcx = sod_cell_axis(cxg, K.xs, K.nx), pcy = sod_cell_axis(cyg, K.xs, K.nx),
+            pcz = sod_cell_axis(czg, K.xs, K.nx);
+  const float e2f = (float)K.eps2;
+  unsigned long long sq = 0;
+  double sf = 0.0;
+  for (int nrow = 0; nrow < 9; nrow++) {
+    const int ny = wrapi(pcy + nrow % 3 - 1, K.nx), nz = wrapi(pcz + nrow / 3 - 1, K.nx);
+    if (abs(pdiff(ny, jc, K.nx)) > 2 || abs(pdiff(nz, kc, K.nx)) > 2) continue;
+    const unsigned long long nbase = (unsigned long long)K.nx * ((unsigned)ny + (unsigned long long)K.nx * (unsigned)nz);
+    for (int ndi = -1; ndi <= 1; ndi++) {
+      const int nxc = wrapi(pcx + ndi, K.nx);
+      if (abs(pdiff(nxc, ic, K.nx)) > 2) continue;
+      const unsigned nb = B.cs[nbase + (unsigned)nxc], ne = B.cs[nbase + (unsigned)nxc + 1];
+      if (visits && lane == 0) *visits += ne - nb;
+      for (unsigned q = nb + lane; q < ne; q += 32) {
+        const float4 nv = B.cube[q];
+        if (__float_as_uint(nv.w) & PSOD_DEAD_BIT) continue;
+        const float nxg = to_grid(nv.x, K.nxf), nyg = to_grid(nv.y, K.nxf), nzg = to_grid(nv.z, K.nxf);
+        if (EXACT) {
+          const double d2 = min_image_d2((double)nxg, (double)nyg, (double)nzg, cx, cy, cz, K.tx);
+          if (d2 <= K.rmin2) {
+            const double t = ddiv(1.0, dsqrt(dadd(d2, K.eps2)));
+            sq += (unsigned long long)__double2ll_rn(dmul(t, 1099511627776.0));
+          }
+        } else {
+          const float dx = mi_dx(nxg, cxg, K.nxf), dy = mi_dx(nyg, cyg, K.nxf), dz = mi_dx(nzg, czg, K.nxf);
+          const float d2f = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+          bool in = d2f <= 0.99999f;
+          if (!in && d2f <= 1.00001f) {
+            const double d2 = min_image_d2((double)nxg, (double)nyg, (double)nzg, cx, cy, cz, K.tx);
+            in = d2 <= K.rmin2;
+          }
+          if (in) sf += (double)rsqrtf(__fadd_rn(d2f, e2f));
+        }
+      }
+    }
+  }
+  // the particle the run scan files under another cell
+  if (K.has_quirk && lane == 0) {
+    const int ax = (int)(K.quirk_listed % K.nx), ay = (int)((K.quirk_listed / K.nx) % K.nx),
+              az = (int)(K.quirk_listed / ((unsigned)K.nx * K.nx));
+    const bool listed_in_sel2 = in_sel2(K, ax, ay, az, ic, jc, kc);
+    const bool seen = abs(pdiff(ax, pcx, K.nx)) <= 1 && abs(pdiff(ay, pcy, K.nx)) <= 1 &&
+                      abs(pdiff(az, pcz, K.nx)) <= 1;
+    if (listed_in_sel2 && !seen) {
+      const float4 qv = B.cube[K.quirk_pos];
+      if (!(__float_as_uint(qv.w) & PSOD_DEAD_BIT)) {
+        const double d2 = min_image_d2((double)to_grid(qv.x, K.nxf), (double)to_grid(qv.y, K.nxf),
+                                       (double)to_grid(qv.z, K.nxf), cx, cy, cz, K.tx);
+        if (d2 <= K.rmin2) {
+          const double t = ddiv(1.0, dsqrt(dadd(d2, K.eps2)));
+          if (EXACT) sq += (unsigned long long)__double2ll_rn(dmul(t, 1099511627776.0));
+          else sf += t;
+        }
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    sq += __shfl_down_sync(0xffffffffu, sq, o);
+    sf += __shfl_down_sync(0xffffffffu, sf, o);
+  }
+  sq_out = sq;
+  sf_out = sf;
+}
+
+__global__ void __launch_bounds__(TPB) k_refine_approx(SodConst K, SodBufs B) {
+  const int lane = threadIdx.x & 31;
+  const unsigned total = *B.cand_used;
+  unsigned visits = 0;
+  while (true) {
+    unsigned q = 0;
+    if (lane == 0) q = atomicAdd(&B.work[1], 1u);
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (q >= total) break;
+    const unsigned slot = B.cand_slot[q];
+    const unsigned rank = B.ready[slot];
+    const SeedGeo g = seed_geo(K, B, rank);
+    unsigned long long sq;
+    double sf;
+    refine_sum<false>(K, B, B.cand_pos[q], g.ic, g.jc, g.kc, sq, sf, &visits);
+    if (lane == 0) B.cand_s[q] = sf;
+  }
+  if (lane == 0 && visits) atomicAdd(B.pairs, (unsigned long long)visits);
+  if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(B.ncand_total, (unsigned long long)total);
+}
+
+// ---------------------------------------------------------------------------
+// phase 3: exact sums for the contenders and the argmax (main:1864-1875):
+// largest sum wins, equal sums go to the first candidate in the reference's
+// scan order (listed cell offset x-outer/z-inner, then input index)
+// ---------------------------------------------------------------------------
+__device__ void select_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
+  if (!B.st_active[slot]) return;
+  const unsigned off = B.st_coff[slot], n = B.st_cn[slot];
+  if (n == 0) return;
+  const SeedGeo g = seed_geo(K, B, rank);
+  // max of the approximate sums (non-negative doubles order as their bits)
+  unsigned long long mb = 0, dummy = 0;
+  for (unsigned k = threadIdx.x; k < n; k += TPB) {
+    const unsigned long long b = dbits(B.cand_s[off + k]);
+    mb = b > mb ? b : mb;
+  }
+  block_max_pair(S, mb, dummy);
+  const double thr = dmul(bitsd(mb), 1.0 - 2.0 * REF_TOL);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  unsigned long long best_sq = 0, best_key = ~0ull;
+  unsigned best_pos = 0xffffffffu;
+  for (unsigned k = w; k < n; k += NWARP) {
+    if (!(B.cand_s[off + k] >= thr)) continue;  // cannot reach the maximum
+    const unsigned cp = B.cand_pos[off + k];
+    unsigned long long sq;
+    double sf;
+    refine_sum<true>(K, B, cp, g.ic, g.jc, g.kc, sq, sf);
+    if (lane == 0) {
+      const float4 cv = B.cube[cp];
+      const unsigned cw = __float_as_uint(cv.w);
+      int lx, ly, lz;
+      if (K.has_quirk && cp == K.quirk_pos) {
+        lx = pdiff((int)(K.quirk_listed % K.nx), g.ic, K.nx);
+        ly = pdiff((int)((K.quirk_listed / K.nx) % K.nx), g.jc, K.nx);
+        lz = pdiff((int)(K.quirk_listed / ((unsigned)K.nx * K.nx)), g.kc, K.nx);
+      } else {
+        lx = pdiff(sod_cell_axis(to_grid(cv.x, K.nxf), K.xs, K.nx), g.ic, K.nx);
+        ly = pdiff(sod_cell_axis(to_grid(cv.y, K.nxf), K.xs, K.nx), g.jc, K.nx);
+        lz = pdiff(sod_cell_axis(to_grid(cv.z, K.nxf), K.xs, K.nx), g.kc, K.nx);
+      }
+      const unsigned o = (unsigned)(((lx + 1) * 3 + (ly + 1)) * 3 + (lz + 1));
+      const unsigned long long key = ((unsigned long long)o << 32) | (cw & PSOD_IDX_MASK);
+      if (sq > best_sq || (sq == best_sq && key < best_key)) {
+        best_sq = sq;
+        best_key = key;
+        best_pos = cp;
+      }
+    }
+  }
+  unsigned long long a = best_sq, b = ~best_key;
+  const unsigned long long pa = a, pb = b;
+  block_max_pair(S, a, b);
+  if (lane == 0 && best_pos != 0xffffffffu && pa == a && pb == b) B.st_centre[slot] = best_pos;
+}
+
+__global__ void __launch_bounds__(TPB) k_select(SodConst K, SodBufs B) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem &S = *reinterpret_cast<Smem *>(smem_raw);
+  while (true) {
+    const unsigned item = next_item(&B.work[2]);
+    if (item >= *B.nready) break;
+    select_seed(K, B, S, item, B.ready[item]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// phase 4: crossing (main:2040-2100), profile (main:2103-2115), keep
+// (main:2118-2141) and claims (main:2148-2166)
+// ---------------------------------------------------------------------------
+// exact alive count of the whole cube (the reference's npart_sel)
+__device__ unsigned count_alive_cube(const SodConst &K, const SodBufs &B, Smem &S, int ic, int jc, int kc) {
+  unsigned cnt = 0;
+  for_cube(K, B, ic, jc, kc, K.ncut, [&](unsigned p, float4 v) {
+    if (!(__float_as_uint(v.w) & PSOD_DEAD_BIT)) cnt++;
+  });
+  return block_sum_u32(S, cnt);
+}
+
+// listed cell of a record for the alive-count bookkeeping
+__device__ __forceinline__ unsigned listed_cell(const SodConst &K, unsigned p, float4 v) {
+  if (K.has_quirk && p == K.quirk_pos) return K.quirk_listed;
+  const unsigned i = (unsigned)sod_cell_axis(to_grid(v.x, K.nxf), K.xs, K.nx);
+  const unsigned j = (unsigned)sod_cell_axis(to_grid(v.y, K.nxf), K.xs, K.nx);
+  const unsigned k = (unsigned)sod_cell_axis(to_grid(v.z, K.nxf), K.xs, K.nx);
+  return i + (unsigned)K.nx * (j + (unsigned)K.nx * k);
+}
+
+// Forward crossing search for threshold delta over a region that grows from
+// rb0 (cells) until the stop is proven inside it.  The plain mode starts from
+// the whole cube.  Returns the stop position; G is left at the region used.
+__device__ long long bracketed_stop(const SodConst &K, const SodBufs &B, Smem &S, Region &G, double rb0,
+                                    unsigned &na, bool &na_known, double delta, double *d2stop) {
+  double rb = rb0;
+  while (true) {
+    const bool full = !(rb > 0.0) || rb >= (double)K.ncut;
+    G.rb = full ? -1.0 : rb;
+    G.rb2 = full ? -1.0 : rb * rb;
+    if (full && !na_known) {
+      na = count_alive_cube(K, B, S, G.ic, G.jc, G.kc);
+      na_known = true;
+    }
+    if (threadIdx.x == 0) {
+      S.lev[0].lo = 0;
+      S.lev[0].hi = 0x7fefffffffffffffull;
+      S.lev[0].shift = L1_SHIFT;
+    }
+    __syncthreads();
+    build_hist(K, B, S, 0, G);
+    // inside a partial ball the cube's count is not reached: i < npart_sel holds
+    const long long na_eff = full ? (long long)na : 0x7fffffffffffffffll;
+    const long long i = radial_search(K, B, S, G, na_eff, delta, 0, 0, d2stop);
+    if (i != 0 || full) return i;
+    rb *= 2.0;
+  }
+}
+
+__device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
+  if (!B.st_active[slot]) return;
+  const SeedGeo g = seed_geo(K, B, rank);
+  unsigned na = B.st_na[slot];
+  bool na_known = (B.mode == PSOD_MODE_PLAIN);
+  const unsigned cpos = B.st_centre[slot];
+  const float4 cvv = B.cube[cpos];
+  Region G;
+  G.ic = g.ic;
+  G.jc = g.jc;
+  G.kc = g.kc;
+  G.xc = (double)to_grid(cvv.x, K.nxf);
+  G.yc = (double)to_grid(cvv.y, K.nxf);
+  G.zc = (double)to_grid(cvv.z, K.nxf);
+  const double xc = G.xc, yc = G.yc, zc = G.zc;
+  const unsigned cidx = __float_as_uint(cvv.w) & PSOD_IDX_MASK;
+  const double rb0 = (B.mode == PSOD_MODE_PLAIN) ? -1.0 : 1.5;
+
+  // 3. crossing (main:2040-2100)
   double d2stop = 0;
-  long long istop = radial_search(K, B, S, ic, jc, kc, xc, yc, zc, (long long)na, K.delta, 0, 0, &d2stop);
+  long long istop = bracketed_stop(K, B, S, G, rb0, na, na_known, K.delta, &d2stop);
   if (istop <= 0) {
     if (threadIdx.x == 0) record_error(B, rank, PSOD_ERR_STATE);
     return;
@@ -628,23 +979,27 @@ __device__ void process_seed(const SodConst &K, const SodBufs &B, Smem &S, unsig
       thr_key = S.skey[hk - 1];
       thr_idx = S.sidx[hk - 1];
     } else {
-      max_below(K, B, S, ic, jc, kc, xc, yc, zc, blo, thr_key, thr_idx);
+      max_below(K, B, S, G, blo, thr_key, thr_idx);
     }
   }
   const double rayon = dsqrt(bitsd(thr_key));
 
-  // seuil2 capture (main:2062-2069): last step i in [2, istop] above seuil2
+  // seuil2 capture (main:2062-2069): last step i in [2, istop] above seuil2;
+  // every such step lies inside the region that held the stop
   long long masse2 = 0;
   {
     double dd;
-    long long i2 = radial_search(K, B, S, ic, jc, kc, xc, yc, zc, (long long)na, K.delta2, 1, istop, &dd);
+    const long long na_eff = G.rb2 < 0.0 ? (long long)na : 0x7fffffffffffffffll;
+    long long i2 = radial_search(K, B, S, G, na_eff, K.delta2, 1, istop, &dd);
     if (i2 > 0) masse2 = i2;
   }
   // extra thresholds: the same stop rule, -1 when not crossed
   long long mext[PSOD_MAX_EXTRA_DELTA];
   for (int e = 0; e < K.ndx; e++) {
     double dd;
-    long long ie = radial_search(K, B, S, ic, jc, kc, xc, yc, zc, (long long)na, K.dx_extra[e], 0, 0, &dd);
+    Region Ge = G;
+    const double rbe = G.rb2 < 0.0 ? -1.0 : G.rb;
+    long long ie = bracketed_stop(K, B, S, Ge, rbe, na, na_known, K.dx_extra[e], &dd);
     mext[e] = (ie <= 0 || overdens(K, ie, dd) > K.dx_extra[e]) ? -1 : ie - 1;
   }
 
@@ -653,16 +1008,27 @@ __device__ void process_seed(const SodConst &K, const SodBufs &B, Smem &S, unsig
   const bool keep = amass >= K.mmin && xc <= K.zmax && xc > K.zmin && yc <= K.zmax && yc > K.zmin &&
                     zc <= K.zmax && zc > K.zmin;
 
-  // 4a. profile (main:2103-2115): cumulative counts below each edge
+  // 4a. profile (main:2103-2115): cumulative counts below each edge; the
+  // region must hold every particle closer than the last edge
   if (keep) {
     for (int j = threadIdx.x; j < K.nbins; j += TPB) S.edges[j] = dmul(rayon, B.edge_fac[j]);
     for (int j = threadIdx.x; j <= K.nbins; j += TPB) S.phist[j] = 0;
     __syncthreads();
     const double emax = S.edges[K.nbins - 1];
-    for_cube(K, B, ic, jc, kc, K.ncut, [&](unsigned p, float4 v) {
-      if (__float_as_uint(v.w) & PSOD_DEAD_BIT) return;
-      double d2 = min_image_d2((double)to_grid(v.x, K.nxf), (double)to_grid(v.y, K.nxf),
-                               (double)to_grid(v.z, K.nxf), xc, yc, zc, K.tx);
+    Region Gp = G;
+    if (Gp.rb2 >= 0.0 && !(emax * (1.0 + 1e-9) < Gp.rb)) {
+      const double r = emax * 1.01 + 0.01;
+      if (r >= (double)K.ncut) {
+        Gp.rb = -1.0;
+        Gp.rb2 = -1.0;
+      } else {
+        Gp.rb = r;
+        Gp.rb2 = r * r;
+      }
+    }
+    for_region(K, B, Gp, [&](unsigned p, float4 v) {
+      double d2;
+      if (!region_d2(K, Gp, v, d2)) return;
       double r = dsqrt(d2);
       if (!(r < emax)) return;
       int lo = 0, hi = K.nbins - 1;  // first edge with r < edge
@@ -686,19 +1052,19 @@ __device__ void process_seed(const SodConst &K, const SodBufs &B, Smem &S, unsig
 
   // 4b. claims (main:2148-2166): the masse nearest die, kept or not
   const unsigned long long pool_base = S.pool_base;
-  for_cube(K, B, ic, jc, kc, K.ncut, [&](unsigned p, float4 v) {
+  for_region(K, B, G, [&](unsigned p, float4 v) {
+    double d2;
+    if (!region_d2(K, G, v, d2)) return;
     const unsigned wv = __float_as_uint(v.w);
-    if (wv & PSOD_DEAD_BIT) return;
-    double d2 = min_image_d2((double)to_grid(v.x, K.nxf), (double)to_grid(v.y, K.nxf), (double)to_grid(v.z, K.nxf),
-                             xc, yc, zc, K.tx);
     const unsigned long long x = dbits(d2);
     const unsigned ix = wv & PSOD_IDX_MASK;
     if (x < thr_key || (x == thr_key && ix <= thr_idx)) {
       B.cube[p].w = __uint_as_float(wv | PSOD_DEAD_BIT);
-      const unsigned slot = atomicAdd(&S.claim_cnt, 1u);
-      if (keep && slot < (unsigned)masse) {
-        B.pool_key[pool_base + slot] = x;
-        B.pool_idx[pool_base + slot] = ix;
+      if (B.alive_cnt) atomicSub(&B.alive_cnt[listed_cell(K, p, v)], 1u);
+      const unsigned slot2 = atomicAdd(&S.claim_cnt, 1u);
+      if (keep && slot2 < (unsigned)masse) {
+        B.pool_key[pool_base + slot2] = x;
+        B.pool_idx[pool_base + slot2] = ix;
       }
     }
   });
@@ -710,52 +1076,40 @@ __device__ void process_seed(const SodConst &K, const SodBufs &B, Smem &S, unsig
   if (!keep) return;
 
   // 5. halo record
-  __shared__ unsigned long long s_slot;
   if (threadIdx.x == 0) {
-    const unsigned long long slot = atomicAdd(B.nhalo, 1ull);
-    s_slot = slot;
-    B.h_rank[slot] = rank;
-    B.h_id[slot] = B.ids[cidx];
-    B.h_mass[slot] = masse;
-    B.h_mass2[slot] = masse2;
-    B.h_rdelta[slot] = rayon;
-    B.h_center[3 * slot + 0] = __double2float_rn(ddiv(xc, K.scale));
-    B.h_center[3 * slot + 1] = __double2float_rn(ddiv(yc, K.scale));
-    B.h_center[3 * slot + 2] = __double2float_rn(ddiv(zc, K.scale));
-    B.h_pool[slot] = pool_base;
-    for (int e = 0; e < K.ndx; e++) B.h_mextra[slot * K.ndx + e] = mext[e];
-  }
-  __syncthreads();
-  {
-    const unsigned long long slot = s_slot;
+    const unsigned long long hs = atomicAdd(B.nhalo, 1ull);
+    B.h_rank[hs] = rank;
+    B.h_id[hs] = B.ids[cidx];
+    B.h_mass[hs] = masse;
+    B.h_mass2[hs] = masse2;
+    B.h_rdelta[hs] = rayon;
+    B.h_center[3 * hs + 0] = __double2float_rn(ddiv(xc, K.scale));
+    B.h_center[3 * hs + 1] = __double2float_rn(ddiv(yc, K.scale));
+    B.h_center[3 * hs + 2] = __double2float_rn(ddiv(zc, K.scale));
+    B.h_pool[hs] = pool_base;
+    for (int e = 0; e < K.ndx; e++) B.h_mextra[hs * K.ndx + e] = mext[e];
     unsigned run = 0;
-    // cumulative profile (serial over <= 128 bins)
-    if (threadIdx.x == 0) {
-      for (int j = 0; j < K.nbins; j++) {
-        run += S.phist[j];
-        B.h_profile[slot * K.nbins + j] = run;
-      }
+    for (int j = 0; j < K.nbins; j++) {
+      run += S.phist[j];
+      B.h_profile[hs * K.nbins + j] = run;
     }
   }
 }
 
-__global__ void __launch_bounds__(TPB) k_sod_seeds(SodConst K, SodBufs B) {
+__global__ void __launch_bounds__(TPB) k_cross(SodConst K, SodBufs B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem &S = *reinterpret_cast<Smem *>(smem_raw);
-  __shared__ unsigned s_item;
   while (true) {
-    if (threadIdx.x == 0) s_item = atomicAdd(B.work, 1u);
-    __syncthreads();
-    const unsigned item = s_item;
-    __syncthreads();
+    const unsigned item = next_item(&B.work[3]);
     if (item >= *B.nready) break;
-    const unsigned rank = B.ready[item];
-    process_seed(K, B, S, rank);
-    __syncthreads();
-    if (threadIdx.x == 0) B.processed[rank] = 1;
+    cross_seed(K, B, S, item, B.ready[item]);
   }
 }
 
+__global__ void k_init_alive(const unsigned *cs, unsigned long long ncell, unsigned *alive) {
+  unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < ncell) alive[c] = cs[c + 1] - cs[c];
+}
 
 // ---------------------------------------------------------------------------
 // scheduler
@@ -781,23 +1135,28 @@ __global__ void k_count_u32(const unsigned *keys, long long n, unsigned *count) 
 __global__ void k_heads(long long nblocks, const unsigned *bbegin, unsigned *cursor, const unsigned *blist,
                         const unsigned char *processed, const unsigned *seed_idx, const unsigned *inv,
                         const float4 *cube, unsigned *head, unsigned *gmin) {
-  long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nblocks) return;
-  unsigned cur = cursor[b];
-  const unsigned end = bbegin[b + 1];
+  const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned h = PSOD_INF_RANK;
-  while (cur < end) {
-    const unsigned r = blist[cur];
-    if (processed[r] || (__float_as_uint(cube[inv[seed_idx[r]]].w) & PSOD_DEAD_BIT)) {
-      cur++;
-      continue;
+  if (b < nblocks) {
+    unsigned cur = cursor[b];
+    const unsigned end = bbegin[b + 1];
+    while (cur < end) {
+      const unsigned r = blist[cur];
+      if (processed[r] || (__float_as_uint(cube[inv[seed_idx[r]]].w) & PSOD_DEAD_BIT)) {
+        cur++;
+        continue;
+      }
+      h = r;
+      break;
     }
-    h = r;
-    break;
+    cursor[b] = cur;
+    head[b] = h;
   }
-  cursor[b] = cur;
-  head[b] = h;
-  if (h != PSOD_INF_RANK) atomicMin(gmin, h);
+  if (gmin) {  // global minimum, needed only for the foreign-filed seed
+    unsigned m = h;
+    for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m != PSOD_INF_RANK) atomicMin(gmin, m);
+  }
 }
 
 // periodic sliding minimum of radius rb along one axis of the nb^3 grid
@@ -967,6 +1326,15 @@ SodConst make_sod_const(const psod_ctx *c) {
   K.munit = (double)c->munit;
   K.mmin = (double)c->p.nmin;                 // main:698
   K.nsel = c->nsel;
+  K.n_total = c->n;
+  // smallest alive count with count*munit >= Mmin (main:1759)
+  {
+    const double mu = (double)c->munit;
+    long long m = (long long)std::ceil((double)c->p.nmin / mu) - 2;
+    if (m < 0) m = 0;
+    while ((double)m * mu < (double)c->p.nmin) m++;
+    K.mmin_count = (unsigned)m;
+  }
   K.zmin = 0.0 * c->scale;                    // main:420, 691
   K.zmax = 1.0 * c->scale;                    // main:421, 692
   const double rmin = c->scale / c->nx;       // main:1526
@@ -983,36 +1351,44 @@ SodConst make_sod_const(const psod_ctx *c) {
   return K;
 }
 
-namespace {
-struct DevBuf {
-  std::vector<void *> ptrs;
-  ~DevBuf() {
-    for (void *p : ptrs) cudaFree(p);
+// scratch slots of the SOD stage (kept by the context between calls)
+enum {
+  SC_BLOCK_OF = 16, SC_BLIST, SC_BBEGIN, SC_CURSOR, SC_HEAD, SC_FILT_A, SC_FILT_B, SC_READY, SC_CTRS,
+  SC_PROCESSED, SC_U64, SC_EDGES, SC_HRANK, SC_HID, SC_HMASS, SC_HMASS2, SC_HMEXTRA, SC_HPROF, SC_HCENTER,
+  SC_HRDELTA, SC_HPOOL, SC_POOLKEY, SC_POOLIDX, SC_COUNTS, SC_ST_ACTIVE, SC_ST_NA, SC_ST_COFF, SC_ST_CN,
+  SC_ST_CENTRE, SC_CAND_POS, SC_CAND_SLOT, SC_CAND_S, SC_ORDER, SC_RKEYS, SC_MASS32, SC_MOFF, SC_TKEY, SC_TIDX,
+  SC_ALIVE
+};
+
+struct PhaseTimer {
+  cudaEvent_t a, b;
+  float total = 0.f;
+  PhaseTimer() {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
   }
-  template <typename T>
-  T *get(psod_ctx *c, size_t n, int *st) {
-    T *p = nullptr;
-    if (*st) return nullptr;
-    *st = dalloc(c, &p, n);
-    if (!*st) ptrs.push_back(p);
-    return p;
+  ~PhaseTimer() {
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  void start(cudaStream_t s) { cudaEventRecord(a, s); }
+  void stop(cudaStream_t s) { cudaEventRecord(b, s); }
+  void collect() {
+    float ms = 0.f;
+    cudaEventSynchronize(b);
+    cudaEventElapsedTime(&ms, a, b);
+    total += ms;
   }
 };
-}  // namespace
 
 int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   if (!c->seeds_done) return set_err(c, PSOD_ERR_STATE, "psod_spherover needs psod_tri_cic first");
   psod_run_stats st{};
   st.fail_rank = -1;
   st.npart_new = c->npart_new;
-  cudaEvent_t e0, e1, k0, k1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  cudaEventCreate(&k0);
-  cudaEventCreate(&k1);
-  cudaEventRecord(e0, c->stream);
+  PhaseTimer t_all, t_sched, t_prep, t_ref, t_sel, t_cross;
+  t_all.start(c->stream);
   int rc = PSOD_OK;
-  DevBuf tmp;
   const SodConst K = make_sod_const(c);
   const long long n = c->n;
   const long long nseed = c->npart_new;
@@ -1033,150 +1409,193 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   const long long nblocks = (long long)nb * nb * nb;
   const int rdep = c->ncut + std::max(c->ncut, 2);
   const int rb = (rdep + bs - 1) / bs;
-
-  unsigned *block_of = tmp.get<unsigned>(c, (size_t)nseed + 1, &rc);
-  unsigned *blist = tmp.get<unsigned>(c, (size_t)nseed + 1, &rc);
-  unsigned *bbegin = tmp.get<unsigned>(c, (size_t)nblocks + 1, &rc);
-  unsigned *cursor = tmp.get<unsigned>(c, (size_t)nblocks + 1, &rc);
-  unsigned *head = tmp.get<unsigned>(c, (size_t)nblocks, &rc);
-  unsigned *filt_a = tmp.get<unsigned>(c, (size_t)nblocks, &rc);
-  unsigned *filt_b = tmp.get<unsigned>(c, (size_t)nblocks, &rc);
-  unsigned *ready = tmp.get<unsigned>(c, (size_t)nblocks + 1, &rc);
-  unsigned *ctrs = tmp.get<unsigned>(c, 4, &rc);  // nready, work, gmin, quirk_rank
-  unsigned char *processed = tmp.get<unsigned char>(c, (size_t)nseed + 1, &rc);
-  unsigned long long *u64s = tmp.get<unsigned long long>(c, 6, &rc);  // err, nhalo, pool_used, touched, nprocessed
-  double *edge_fac = tmp.get<double>(c, (size_t)c->p.nbins, &rc);
-  // halo records by slot: at most one halo per Mmin particles
   const long long hcap = std::max<long long>(1, n / std::max(1, c->p.nmin) + 1);
-  unsigned *h_rank = tmp.get<unsigned>(c, (size_t)hcap, &rc);
-  long long *h_id = tmp.get<long long>(c, (size_t)hcap, &rc);
-  long long *h_mass = tmp.get<long long>(c, (size_t)hcap, &rc);
-  long long *h_mass2 = tmp.get<long long>(c, (size_t)hcap, &rc);
-  long long *h_mextra = tmp.get<long long>(c, (size_t)hcap * std::max(1, c->p.ndelta_extra), &rc);
-  long long *h_profile = tmp.get<long long>(c, (size_t)hcap * c->p.nbins, &rc);
-  float *h_center = tmp.get<float>(c, (size_t)hcap * 3, &rc);
-  double *h_rdelta = tmp.get<double>(c, (size_t)hcap, &rc);
-  unsigned long long *h_pool = tmp.get<unsigned long long>(c, (size_t)hcap, &rc);
-  unsigned long long *pool_key = tmp.get<unsigned long long>(c, (size_t)n, &rc);
-  unsigned *pool_idx = tmp.get<unsigned>(c, (size_t)n, &rc);
-  if (rc) return rc;
+  const int ne = std::max(1, c->p.ndelta_extra);
+
+  unsigned *block_of, *blist, *bbegin, *cursor, *head, *filt_a, *filt_b, *ready, *ctrs, *counts;
+  unsigned char *processed;
+  unsigned long long *u64s, *h_pool, *pool_key;
+  double *edge_fac, *h_rdelta, *cand_s;
+  unsigned *h_rank, *pool_idx, *st_active, *st_na, *st_coff, *st_cn, *st_centre, *cand_pos, *cand_slot;
+  long long *h_id, *h_mass, *h_mass2, *h_mextra, *h_profile;
+  float *h_center;
+  if ((rc = scratch(c, SC_BLOCK_OF, (size_t)nseed + 1, &block_of)) || (rc = scratch(c, SC_BLIST, (size_t)nseed + 1, &blist)) ||
+      (rc = scratch(c, SC_BBEGIN, (size_t)nblocks + 1, &bbegin)) || (rc = scratch(c, SC_CURSOR, (size_t)nblocks + 1, &cursor)) ||
+      (rc = scratch(c, SC_HEAD, (size_t)nblocks, &head)) || (rc = scratch(c, SC_FILT_A, (size_t)nblocks, &filt_a)) ||
+      (rc = scratch(c, SC_FILT_B, (size_t)nblocks, &filt_b)) || (rc = scratch(c, SC_READY, (size_t)nblocks + 1, &ready)) ||
+      (rc = scratch(c, SC_CTRS, 16, &ctrs)) || (rc = scratch(c, SC_COUNTS, (size_t)nblocks + 1, &counts)) ||
+      (rc = scratch(c, SC_PROCESSED, (size_t)nseed + 1, &processed)) || (rc = scratch(c, SC_U64, 8, &u64s)) ||
+      (rc = scratch(c, SC_EDGES, (size_t)c->p.nbins, &edge_fac)) || (rc = scratch(c, SC_HRANK, (size_t)hcap, &h_rank)) ||
+      (rc = scratch(c, SC_HID, (size_t)hcap, &h_id)) || (rc = scratch(c, SC_HMASS, (size_t)hcap, &h_mass)) ||
+      (rc = scratch(c, SC_HMASS2, (size_t)hcap, &h_mass2)) || (rc = scratch(c, SC_HMEXTRA, (size_t)hcap * ne, &h_mextra)) ||
+      (rc = scratch(c, SC_HPROF, (size_t)hcap * c->p.nbins, &h_profile)) || (rc = scratch(c, SC_HCENTER, (size_t)hcap * 3, &h_center)) ||
+      (rc = scratch(c, SC_HRDELTA, (size_t)hcap, &h_rdelta)) || (rc = scratch(c, SC_HPOOL, (size_t)hcap, &h_pool)) ||
+      (rc = scratch(c, SC_POOLKEY, (size_t)n, &pool_key)) || (rc = scratch(c, SC_POOLIDX, (size_t)n, &pool_idx)) ||
+      (rc = scratch(c, SC_ST_ACTIVE, (size_t)nblocks + 1, &st_active)) || (rc = scratch(c, SC_ST_NA, (size_t)nblocks + 1, &st_na)) ||
+      (rc = scratch(c, SC_ST_COFF, (size_t)nblocks + 1, &st_coff)) || (rc = scratch(c, SC_ST_CN, (size_t)nblocks + 1, &st_cn)) ||
+      (rc = scratch(c, SC_ST_CENTRE, (size_t)nblocks + 1, &st_centre)) || (rc = scratch(c, SC_CAND_POS, (size_t)n, &cand_pos)) ||
+      (rc = scratch(c, SC_CAND_SLOT, (size_t)n, &cand_slot)) || (rc = scratch(c, SC_CAND_S, (size_t)n, &cand_s)))
+    return rc;
+  // ctrs: 0 nready, 1..4 work counters, 5 gmin, 6 quirk rank, 7 cand_used
+  unsigned *nready_d = ctrs, *work = ctrs + 1, *gmin = ctrs + 5, *qrank_d = ctrs + 6, *cand_used = ctrs + 7;
 
   PSOD_CUDA(c, cudaMemcpyAsync(edge_fac, c->edge_fac.data(), sizeof(double) * c->p.nbins, cudaMemcpyHostToDevice,
                                c->stream));
   PSOD_CUDA(c, cudaMemsetAsync(processed, 0, (size_t)nseed + 1, c->stream));
-  PSOD_CUDA(c, cudaMemsetAsync(u64s, 0, sizeof(unsigned long long) * 6, c->stream));
+  PSOD_CUDA(c, cudaMemsetAsync(u64s, 0, sizeof(unsigned long long) * 8, c->stream));
   PSOD_CUDA(c, cudaMemsetAsync(u64s, 0xff, sizeof(unsigned long long), c->stream));  // err = none
-  PSOD_CUDA(c, cudaMemsetAsync(ctrs, 0xff, sizeof(unsigned) * 4, c->stream));
+  PSOD_CUDA(c, cudaMemsetAsync(ctrs, 0xff, sizeof(unsigned) * 16, c->stream));
 
   // seeds bucketed by scheduler block, in rank order within a block
   if (nseed > 0) {
     k_seed_blocks<<<nblk(nseed, 256), 256, 0, c->stream>>>(c->d_seed_idx, c->d_inv, c->d_cube, nseed, K, bs, nb,
                                                            block_of, blist);
-    kernels++;
-    unsigned *counts = tmp.get<unsigned>(c, (size_t)nblocks + 1, &rc);
-    if (rc) return rc;
     PSOD_CUDA(c, cudaMemsetAsync(counts, 0, sizeof(unsigned) * (nblocks + 1), c->stream));
     k_count_u32<<<nblk(nseed, 256), 256, 0, c->stream>>>(block_of, nseed, counts);
-    kernels++;
+    kernels += 2;
     if ((rc = scan_u32(c, counts, bbegin, nblocks, true))) return rc;
     if ((rc = radix_sort_u32(c, block_of, blist, nseed, 32))) return rc;
     PSOD_CUDA(c, cudaMemcpyAsync(cursor, bbegin, sizeof(unsigned) * nblocks, cudaMemcpyDeviceToDevice, c->stream));
     if (c->has_quirk) {
-      unsigned qidx = 0;
       float4 qv;
       PSOD_CUDA(c, cudaMemcpyAsync(&qv, c->d_cube_orig + c->quirk_pos, sizeof(qv), cudaMemcpyDeviceToHost, c->stream));
       PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+      unsigned qidx;
       memcpy(&qidx, &qv.w, 4);
       qidx &= PSOD_IDX_MASK;
-      k_find_rank<<<nblk(nseed, 256), 256, 0, c->stream>>>(c->d_seed_idx, nseed, qidx, ctrs + 3);
+      k_find_rank<<<nblk(nseed, 256), 256, 0, c->stream>>>(c->d_seed_idx, nseed, qidx, qrank_d);
       kernels++;
     }
   }
-
   unsigned quirk_rank = PSOD_INF_RANK;
-  PSOD_CUDA(c, cudaMemcpyAsync(&quirk_rank, ctrs + 3, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+  PSOD_CUDA(c, cudaMemcpyAsync(&quirk_rank, qrank_d, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
   PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
 
   const size_t smem = sizeof(Smem);
-  PSOD_CUDA(c, cudaFuncSetAttribute(k_sod_seeds, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  PSOD_CUDA(c, cudaFuncSetAttribute(k_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  PSOD_CUDA(c, cudaFuncSetAttribute(k_select, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  PSOD_CUDA(c, cudaFuncSetAttribute(k_cross, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int dev_sms = 148;
   cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->device);
   int per_sm = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sod_seeds, TPB, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_cross, TPB, smem);
   if (per_sm < 1) per_sm = 1;
   const unsigned seed_grid = (unsigned)(dev_sms * per_sm);
+  int per_sm_ref = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ref, k_refine_approx, TPB, 0);
+  const unsigned ref_grid = (unsigned)(dev_sms * std::max(1, per_sm_ref));
 
-  float sod_ms = 0.f;
-  long long rounds = 0, sod_launches = 0;
+  SodBufs B;
+  B.cube = c->d_cube;
+  B.cs = c->d_cell_start;
+  B.ids = c->d_ids;
+  B.seed_idx = c->d_seed_idx;
+  B.inv = c->d_inv;
+  B.edge_fac = edge_fac;
+  B.processed = processed;
+  B.ready = ready;
+  B.nready = nready_d;
+  B.err = u64s;
+  B.nhalo = u64s + 1;
+  B.pool_used = u64s + 2;
+  B.touched = u64s + 3;
+  B.nprocessed = u64s + 4;
+  B.h_rank = h_rank;
+  B.h_id = h_id;
+  B.h_mass = h_mass;
+  B.h_mass2 = h_mass2;
+  B.h_mextra = h_mextra;
+  B.h_profile = h_profile;
+  B.h_center = h_center;
+  B.h_rdelta = h_rdelta;
+  B.h_pool = h_pool;
+  B.pool_key = pool_key;
+  B.pool_idx = pool_idx;
+  B.st_active = st_active;
+  B.st_na = st_na;
+  B.st_coff = st_coff;
+  B.st_cn = st_cn;
+  B.st_centre = st_centre;
+  B.cand_pos = cand_pos;
+  B.cand_slot = cand_slot;
+  B.cand_s = cand_s;
+  B.cand_used = cand_used;
+  B.work = work;
+  B.alive_cnt = nullptr;
+  B.pairs = u64s + 5;
+  B.ncand_total = u64s + 6;
+  B.mode = c->p.mode;
+  if (c->p.mode != PSOD_MODE_PLAIN) {
+    unsigned *alive_cnt;
+    if ((rc = scratch(c, SC_ALIVE, (size_t)c->ncell, &alive_cnt))) return rc;
+    k_init_alive<<<nblk((long long)c->ncell, 256), 256, 0, c->stream>>>(c->d_cell_start, c->ncell, alive_cnt);
+    kernels++;
+    B.alive_cnt = alive_cnt;
+  }
+
+  long long rounds = 0, seed_launches = 0;
   while (nseed > 0) {
-    PSOD_CUDA(c, cudaMemsetAsync(ctrs, 0, sizeof(unsigned) * 2, c->stream));            // nready, work
-    PSOD_CUDA(c, cudaMemsetAsync(ctrs + 2, 0xff, sizeof(unsigned), c->stream));         // gmin
+    t_sched.start(c->stream);
+    PSOD_CUDA(c, cudaMemsetAsync(ctrs, 0, sizeof(unsigned) * 5, c->stream));  // nready, work[4]
+    PSOD_CUDA(c, cudaMemsetAsync(gmin, 0xff, sizeof(unsigned), c->stream));
+    PSOD_CUDA(c, cudaMemsetAsync(cand_used, 0, sizeof(unsigned), c->stream));
     k_heads<<<nblk(nblocks, 256), 256, 0, c->stream>>>(nblocks, bbegin, cursor, blist, processed, c->d_seed_idx,
-                                                       c->d_inv, c->d_cube, head, ctrs + 2);
+                                                       c->d_inv, c->d_cube, head,
+                                                       quirk_rank != PSOD_INF_RANK ? gmin : nullptr);
     k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(head, filt_a, nb, 0, rb);
     k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(filt_a, filt_b, nb, 1, rb);
     k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(filt_b, filt_a, nb, 2, rb);
-    k_ready<<<nblk(nblocks, 256), 256, 0, c->stream>>>(nblocks, head, filt_a, quirk_rank, ctrs + 2, ready, ctrs);
+    k_ready<<<nblk(nblocks, 256), 256, 0, c->stream>>>(nblocks, head, filt_a, quirk_rank, gmin, ready, nready_d);
+    t_sched.stop(c->stream);
     kernels += 5;
     unsigned nready = 0;
-    PSOD_CUDA(c, cudaMemcpyAsync(&nready, ctrs, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    PSOD_CUDA(c, cudaMemcpyAsync(&nready, nready_d, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
     PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+    t_sched.collect();
     if (nready == 0) break;
-    SodBufs B;
-    B.cube = c->d_cube;
-    B.cs = c->d_cell_start;
-    B.ids = c->d_ids;
-    B.seed_idx = c->d_seed_idx;
-    B.inv = c->d_inv;
-    B.edge_fac = edge_fac;
-    B.processed = processed;
-    B.ready = ready;
-    B.nready = ctrs;
-    B.work = ctrs + 1;
-    B.err = u64s;
-    B.nhalo = u64s + 1;
-    B.pool_used = u64s + 2;
-    B.touched = u64s + 3;
-    B.nprocessed = u64s + 4;
-    B.h_rank = h_rank;
-    B.h_id = h_id;
-    B.h_mass = h_mass;
-    B.h_mass2 = h_mass2;
-    B.h_mextra = h_mextra;
-    B.h_profile = h_profile;
-    B.h_center = h_center;
-    B.h_rdelta = h_rdelta;
-    B.h_pool = h_pool;
-    B.pool_key = pool_key;
-    B.pool_idx = pool_idx;
-    const unsigned grid = std::min<unsigned>(seed_grid, nready);
-    cudaEventRecord(k0, c->stream);
-    k_sod_seeds<<<grid, TPB, smem, c->stream>>>(K, B);
-    cudaEventRecord(k1, c->stream);
+    const unsigned g = std::min<unsigned>(seed_grid, nready);
+    t_prep.start(c->stream);
+    k_prep<<<g, TPB, smem, c->stream>>>(K, B);
+    t_prep.stop(c->stream);
+    t_ref.start(c->stream);
+    k_refine_approx<<<ref_grid, TPB, 0, c->stream>>>(K, B);
+    t_ref.stop(c->stream);
+    t_sel.start(c->stream);
+    k_select<<<g, TPB, smem, c->stream>>>(K, B);
+    t_sel.stop(c->stream);
+    t_cross.start(c->stream);
+    k_cross<<<g, TPB, smem, c->stream>>>(K, B);
+    t_cross.stop(c->stream);
     PSOD_CUDA(c, cudaGetLastError());
-    PSOD_CUDA(c, cudaEventSynchronize(k1));
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, k0, k1);
-    sod_ms += ms;
+    t_prep.collect();
+    t_ref.collect();
+    t_sel.collect();
+    t_cross.collect();
     rounds++;
-    sod_launches++;
-    kernels++;
+    seed_launches += 4;
+    kernels += 4;
   }
-  unsigned long long hv[6];
+  unsigned long long hv[8];
   PSOD_CUDA(c, cudaMemcpyAsync(hv, u64s, sizeof(hv), cudaMemcpyDeviceToHost, c->stream));
   PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
   st.rounds = rounds;
   st.touched = (int64_t)hv[3];
   st.nprocessed = (int64_t)hv[4];
-  st.ms_sod_kernel = sod_ms;
-  st.sod_launches = sod_launches;
+  st.ms_sched = t_sched.total;
+  st.ms_prep = t_prep.total;
+  st.ms_refine = t_ref.total;
+  st.ms_select = t_sel.total;
+  st.ms_cross = t_cross.total;
+  st.ms_sod_kernel = t_prep.total + t_ref.total + t_sel.total + t_cross.total;
+  st.sod_launches = seed_launches;
+  st.ncandidates = (int64_t)hv[6];
+  st.refine_pairs = (int64_t)hv[5];
   c->nhalo = 0;
   c->nmember = 0;
   c->sod_done = false;
   if (hv[0] != ~0ull) {
     const int code = (int)(hv[0] & 0xff);
     st.fail_rank = (int64_t)(hv[0] >> 8);
-    cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(k0); cudaEventDestroy(k1);
     st.kernel_launches = kernels;
     c->last_stats = st;
     if (out_stats) *out_stats = st;
@@ -1190,14 +1609,13 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     return set_err(c, PSOD_ERR_STATE, "internal consistency check failed at seed rank " + std::to_string(st.fail_rank));
   }
   const long long nh = (long long)hv[1];
-  // order halos by seed rank (the reference's output order)
-  unsigned *order = tmp.get<unsigned>(c, (size_t)nh + 1, &rc);
-  unsigned *rkeys = tmp.get<unsigned>(c, (size_t)nh + 1, &rc);
-  unsigned *mass32 = tmp.get<unsigned>(c, (size_t)nh + 1, &rc);
-  unsigned *moff = tmp.get<unsigned>(c, (size_t)nh + 1, &rc);
-  unsigned long long *tkey = tmp.get<unsigned long long>(c, (size_t)std::max<unsigned long long>(hv[2], 1), &rc);
-  unsigned *tidx = tmp.get<unsigned>(c, (size_t)std::max<unsigned long long>(hv[2], 1), &rc);
-  if (rc) return rc;
+  const unsigned long long npool = std::max<unsigned long long>(hv[2], 1);
+  unsigned *order, *rkeys, *mass32, *moff, *tidx;
+  unsigned long long *tkey;
+  if ((rc = scratch(c, SC_ORDER, (size_t)nh + 1, &order)) || (rc = scratch(c, SC_RKEYS, (size_t)nh + 1, &rkeys)) ||
+      (rc = scratch(c, SC_MASS32, (size_t)nh + 1, &mass32)) || (rc = scratch(c, SC_MOFF, (size_t)nh + 1, &moff)) ||
+      (rc = scratch(c, SC_TKEY, (size_t)npool, &tkey)) || (rc = scratch(c, SC_TIDX, (size_t)npool, &tidx)))
+    return rc;
   if (nh > 0) {
     std::vector<unsigned> iota((size_t)nh);
     for (long long i = 0; i < nh; i++) iota[(size_t)i] = (unsigned)i;
@@ -1206,7 +1624,6 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
     if ((rc = radix_sort_u32(c, rkeys, order, nh, 32))) return rc;
   }
-  const int ne = std::max(1, c->p.ndelta_extra);
   if ((rc = dalloc(c, &c->d_h_id, (size_t)nh))) return rc;
   if ((rc = dalloc(c, &c->d_h_mass, (size_t)nh))) return rc;
   if ((rc = dalloc(c, &c->d_h_rank, (size_t)nh))) return rc;
@@ -1216,7 +1633,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   if ((rc = dalloc(c, &c->d_h_center, (size_t)nh * 3))) return rc;
   if ((rc = dalloc(c, &c->d_h_rdelta, (size_t)nh))) return rc;
   if ((rc = dalloc(c, &c->d_m_offset, (size_t)nh + 1))) return rc;
-  if ((rc = dalloc(c, &c->d_m_index, (size_t)std::max<unsigned long long>(hv[2], 1)))) return rc;
+  if ((rc = dalloc(c, &c->d_m_index, (size_t)npool))) return rc;
   if (nh > 0) {
     const unsigned g1 = nblk(nh, 256);
     k_gather<long long><<<g1, 256, 0, c->stream>>>(h_id, order, nh, 1, c->d_h_id);
@@ -1239,11 +1656,9 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     PSOD_CUDA(c, cudaMemsetAsync(c->d_m_offset, 0, sizeof(long long), c->stream));
   }
   PSOD_CUDA(c, cudaGetLastError());
-  cudaEventRecord(e1, c->stream);
-  PSOD_CUDA(c, cudaEventSynchronize(e1));
-  float tot = 0.f;
-  cudaEventElapsedTime(&tot, e0, e1);
-  st.ms_total = tot;
+  t_all.stop(c->stream);
+  t_all.collect();
+  st.ms_total = t_all.total;
   st.nhalo = nh;
   st.nmember = (int64_t)hv[2];
   st.kernel_launches = kernels;
@@ -1252,7 +1667,6 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   c->sod_done = true;
   c->last_stats = st;
   if (out_stats) *out_stats = st;
-  cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(k0); cudaEventDestroy(k1);
   return PSOD_OK;
 }
 

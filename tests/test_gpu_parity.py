@@ -134,13 +134,14 @@ def test_error_paths():
     assert e.value.status == 2
 
 
+@pytest.mark.parametrize("mode", [0, 1])
 @pytest.mark.parametrize("nx,nmax,seed", [(32, 2000, 123), (48, 5000, 5), (64, 8000, 77)])
-def test_clustered_box_matches_oracle(oracle, nx, nmax, seed):
+def test_clustered_box_matches_oracle(oracle, nx, nmax, seed, mode):
     from psod_b200 import synth
 
     b = synth.make_box(nx, nmax_halo=nmax, seed=seed)
     pos, ids = b.pos.numpy(), b.ids.numpy()
-    _, _, nn, st, t = gpu_run(nx, pos, ids, delta_extra=(500.0, 178.0))
+    _, _, nn, st, t = gpu_run(nx, pos, ids, delta_extra=(500.0, 178.0), mode=mode)
     p = oparams(oracle, nx, delta_extra=(500.0, 178.0))
     rc = oracle.run(p, pos, ids, oracle.CANONICAL)
     assert rc.status == 0 and rc.nhalo > 0
@@ -158,6 +159,26 @@ def test_clustered_box_matches_oracle(oracle, nx, nmax, seed):
     assert np.array_equal(t.halo_id, rr.halo_id)
     assert np.array_equal(t.halo_rdelta, rr.halo_rdelta)
     assert_same_halos(t, rr, exact_members_order=False)
+
+
+@pytest.mark.parametrize("mode", [1])
+def test_modes_identical_128(mode):
+    """plain and batched schedules give bit-identical tables (1-rank 128^3 box)."""
+    from psod_b200 import synth
+
+    b = synth.make_box(128, nmax_halo=20000, seed=20261203, device="cuda")
+    tabs = []
+    for m in (0, mode):
+        s = SphericalOverdensity(128, mode=m, delta_extra=(500.0, 178.0))
+        s.load(b.pos, b.ids)
+        s.run()
+        tabs.append(s.halos())
+        s.close()
+    a, c = tabs
+    assert a.nhalo == c.nhalo > 500
+    for f in ("halo_id", "halo_mass", "halo_rank", "halo_center", "halo_rdelta", "halo_mass2", "halo_mextra",
+              "halo_profile", "member_offset", "member_index"):
+        assert np.array_equal(getattr(a, f), getattr(c, f)), f
 
 
 def test_device_inputs_and_repeat(oracle):
