@@ -146,7 +146,8 @@ struct psod_ctx {
 
   // cic
   double *d_rho = nullptr;  // input order
-  bool cic_done = false, rho_done = false;
+  long long rho_cap = 0;
+  bool cic_done = false, rho_done = false, cic_tiled = false;
   unsigned long long *d_grid = nullptr;  // fixed-point grid (tests only)
 
   // seeds

@@ -29,6 +29,7 @@ namespace psod {
 
 namespace {
 
+constexpr int RT_THREADS = 256;   // candidates per refinement work item
 constexpr int TPB = 256;          // threads per seed CTA
 constexpr int NWARP = TPB / 32;
 constexpr int NB = 4096;          // histogram buckets per level
@@ -77,6 +78,11 @@ struct SodBufs {
   unsigned *alive_cnt;  // alive records per cell (batched modes)
   unsigned long long *pairs;       // candidate-neighbour records visited
   unsigned long long *ncand_total; // candidates over all rounds
+  // refinement work: per (ready slot, candidate cell) counts, offsets into
+  // cand_pos, 256-candidate chunks and their exclusive prefix
+  unsigned *cell_cnt, *cell_off, *cell_chunks, *chunk_pref;
+  unsigned nitems_cells;           // 27 * nready
+  unsigned cap_ready;              // seeds processed per round at most
   int mode;
 };
 
@@ -668,31 +674,59 @@ __device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned
     const unsigned got = alive_rows(K, B, S, g.ic, g.jc, g.kc, need);
     if (got < need) return;  // main:1759
   }
-  // candidates: alive records filed under the 27 cells around the seed cell
-  unsigned nc = 0;
-  for_cube(K, B, g.ic, g.jc, g.kc, 1, [&](unsigned p, float4 v) {
-    if (!(__float_as_uint(v.w) & PSOD_DEAD_BIT)) nc++;
-  });
-  const unsigned ncand = block_sum_u32(S, nc);
-  __shared__ unsigned s_off, s_fill;
+  // candidates: alive records filed under the 27 cells around the seed cell,
+  // grouped by cell in the reference's scan order (x outer, z inner)
+  __shared__ unsigned s_cnt[27], s_coff[27], s_base;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int o = w; o < 27; o += NWARP) {
+    const int di = o / 9 - 1, dj = (o / 3) % 3 - 1, dk = o % 3 - 1;
+    const unsigned cell = (unsigned)wrapi(g.ic + di, K.nx) +
+                          (unsigned)K.nx * ((unsigned)wrapi(g.jc + dj, K.nx) + (unsigned)K.nx * (unsigned)wrapi(g.kc + dk, K.nx));
+    const unsigned b = B.cs[cell], e = B.cs[cell + 1];
+    unsigned c = 0;
+    for (unsigned p = b + lane; p < e; p += 32) c += !(__float_as_uint(B.cube[p].w) & PSOD_DEAD_BIT);
+    for (int sh = 16; sh > 0; sh >>= 1) c += __shfl_down_sync(0xffffffffu, c, sh);
+    if (lane == 0) s_cnt[o] = c;
+  }
+  __syncthreads();
   if (threadIdx.x == 0) {
-    s_off = atomicAdd(B.cand_used, ncand);
-    s_fill = 0;
+    unsigned tot = 0;
+    for (int o = 0; o < 27; o++) {
+      s_coff[o] = tot;
+      tot += s_cnt[o];
+    }
+    s_base = atomicAdd(B.cand_used, tot);
     B.st_na[slot] = na;  // 0 when unknown (batched modes)
-    B.st_coff[slot] = s_off;
-    B.st_cn[slot] = ncand;
+    B.st_coff[slot] = s_base;
+    B.st_cn[slot] = tot;
     B.st_active[slot] = 1;
     B.st_centre[slot] = g.sp;  // no candidate: the seed stays the centre
     atomicAdd(B.nprocessed, 1ull);
   }
   __syncthreads();
-  const unsigned off = s_off;
-  for_cube(K, B, g.ic, g.jc, g.kc, 1, [&](unsigned p, float4 v) {
-    if (__float_as_uint(v.w) & PSOD_DEAD_BIT) return;
-    const unsigned q = off + atomicAdd(&s_fill, 1u);
-    B.cand_pos[q] = p;
-    B.cand_slot[q] = slot;
-  });
+  if (threadIdx.x < 27) {
+    B.cell_cnt[slot * 27 + threadIdx.x] = s_cnt[threadIdx.x];
+    B.cell_off[slot * 27 + threadIdx.x] = s_base + s_coff[threadIdx.x];
+    B.cell_chunks[slot * 27 + threadIdx.x] = (s_cnt[threadIdx.x] + RT_THREADS - 1) / RT_THREADS;
+  }
+  for (int o = w; o < 27; o += NWARP) {
+    const int di = o / 9 - 1, dj = (o / 3) % 3 - 1, dk = o % 3 - 1;
+    const unsigned cell = (unsigned)wrapi(g.ic + di, K.nx) +
+                          (unsigned)K.nx * ((unsigned)wrapi(g.jc + dj, K.nx) + (unsigned)K.nx * (unsigned)wrapi(g.kc + dk, K.nx));
+    const unsigned b = B.cs[cell], e = B.cs[cell + 1];
+    unsigned q = s_base + s_coff[o];
+    for (unsigned p0 = b; p0 < e; p0 += 32) {
+      const unsigned p = p0 + lane;
+      const bool alive = p < e && !(__float_as_uint(B.cube[p].w) & PSOD_DEAD_BIT);
+      const unsigned m = __ballot_sync(0xffffffffu, alive);
+      if (alive) {
+        const unsigned at = q + __popc(m & ((1u << lane) - 1u));
+        B.cand_pos[at] = p;
+        B.cand_slot[at] = slot;
+      }
+      q += __popc(m);
+    }
+  }
 }
 
 __global__ void __launch_bounds__(TPB) k_prep(SodConst K, SodBufs B) {
@@ -700,7 +734,7 @@ __global__ void __launch_bounds__(TPB) k_prep(SodConst K, SodBufs B) {
   Smem &S = *reinterpret_cast<Smem *>(smem_raw);
   while (true) {
     const unsigned item = next_item(&B.work[0]);
-    if (item >= *B.nready) break;
+    if (item >= min(*B.nready, B.cap_ready)) break;
     prep_seed(K, B, S, item, B.ready[item]);
   }
 }
@@ -822,6 +856,163 @@ __global__ void __launch_bounds__(TPB) k_refine_approx(SodConst K, SodBufs B) {
   if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(B.ncand_total, (unsigned long long)total);
 }
 
+// Tiled form of the approximate sums: one work item is up to 256 candidates
+// of one candidate cell (a thread each); the records of the cell's 27
+// neighbour cells stream through shared memory and every thread reads each
+// record by broadcast.  Each term is FP32 with one rounding per difference
+// (relative error below 1e-6); 32 terms are summed in FP32 (below 2e-6) and
+// the partial sums in FP64, so |S_approx - S| <= 3e-6 S < REF_TOL S.  Dead
+// records are parked at 1e30 so they never pass the inclusion test.
+constexpr int RT_TILE = 1024;
+
+template <bool WRAPFREE>
+__device__ __forceinline__ double tile_terms(const float4 *tile, unsigned nt, float cx, float cy, float cz,
+                                             const SodConst &K) {
+  const float e2f = (float)K.eps2;
+  double sum = 0.0;
+  for (unsigned j0 = 0; j0 < nt; j0 += 32) {
+    const unsigned j1 = min(nt, j0 + 32);
+    float part = 0.f;
+    for (unsigned j = j0; j < j1; j++) {
+      const float4 nb = tile[j];
+      float dx, dy, dz;
+      if (WRAPFREE) {
+        dx = __fsub_rn(nb.x, cx);
+        dy = __fsub_rn(nb.y, cy);
+        dz = __fsub_rn(nb.z, cz);
+      } else {
+        dx = mi_dx(nb.x, cx, K.nxf);
+        dy = mi_dx(nb.y, cy, K.nxf);
+        dz = mi_dx(nb.z, cz, K.nxf);
+      }
+      const float d2 = fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz)));
+      bool in = d2 <= 0.99999f;
+      if (!in && d2 <= 1.00001f)
+        in = min_image_d2((double)nb.x, (double)nb.y, (double)nb.z, (double)cx, (double)cy, (double)cz, K.tx) <= K.rmin2;
+      if (in) part += rsqrtf(__fadd_rn(d2, e2f));
+    }
+    sum += (double)part;
+  }
+  return sum;
+}
+
+__global__ void __launch_bounds__(RT_THREADS) k_refine_tile(SodConst K, SodBufs B) {
+  __shared__ float4 tile[RT_TILE];
+  __shared__ unsigned s_item, s_ci, s_chunk, s_nitems;
+  __shared__ unsigned s_rb[18], s_rp[19];
+  __shared__ int s_nr, s_wrapfree;
+  const int t = threadIdx.x;
+  unsigned long long visits = 0;
+  if (t == 0) s_nitems = B.chunk_pref[B.nitems_cells];
+  while (true) {
+    __syncthreads();
+    if (t == 0) {
+      s_item = atomicAdd(&B.work[1], 1u);
+      if (s_item < s_nitems) {
+        unsigned lo = 0, hi = B.nitems_cells;  // last ci with chunk_pref[ci] <= item
+        while (hi - lo > 1) {
+          const unsigned mid = (lo + hi) >> 1;
+          if (B.chunk_pref[mid] <= s_item) lo = mid;
+          else hi = mid;
+        }
+        s_ci = lo;
+        s_chunk = s_item - B.chunk_pref[lo];
+      }
+    }
+    __syncthreads();
+    if (s_item >= s_nitems) break;
+    const unsigned ci = s_ci, slot = ci / 27, o = ci % 27;
+    const SeedGeo g = seed_geo(K, B, B.ready[slot]);
+    const int di = (int)(o / 9) - 1, dj = (int)((o / 3) % 3) - 1, dk = (int)(o % 3) - 1;
+    const int cxc = wrapi(g.ic + di, K.nx), cyc = wrapi(g.jc + dj, K.nx), czc = wrapi(g.kc + dk, K.nx);
+    const unsigned cnt = B.cell_cnt[ci];
+    const unsigned myk = s_chunk * RT_THREADS + (unsigned)t;
+    const bool have = myk < cnt;
+    const unsigned q = B.cell_off[ci] + myk;
+    const unsigned cp = have ? B.cand_pos[q] : 0u;
+    const bool quirk = have && K.has_quirk && cp == K.quirk_pos;
+    float cx = 0.f, cy = 0.f, cz = 0.f;
+    if (have) {
+      const float4 cv = B.cube[cp];
+      cx = to_grid(cv.x, K.nxf);
+      cy = to_grid(cv.y, K.nxf);
+      cz = to_grid(cv.z, K.nxf);
+    }
+    if (t == 0) {
+      // record runs of the 3x3x3 cells around the candidate cell: 9 rows,
+      // each one x-run of 3 cells (two when it wraps)
+      int nr = 0;
+      unsigned acc = 0;
+      for (int r = 0; r < 9; r++) {
+        const unsigned yy = (unsigned)wrapi(cyc + r % 3 - 1, K.nx), zz = (unsigned)wrapi(czc + r / 3 - 1, K.nx);
+        const unsigned long long base = (unsigned long long)K.nx * (yy + (unsigned long long)K.nx * zz);
+        const int x0 = cxc - 1, x1 = cxc + 1;
+        int pa[2], pb[2], np;
+        if (x0 < 0) { pa[0] = x0 + K.nx; pb[0] = K.nx - 1; pa[1] = 0; pb[1] = x1; np = 2; }
+        else if (x1 >= K.nx) { pa[0] = x0; pb[0] = K.nx - 1; pa[1] = 0; pb[1] = x1 - K.nx; np = 2; }
+        else { pa[0] = x0; pb[0] = x1; np = 1; }
+        for (int h = 0; h < np; h++) {
+          const unsigned b = B.cs[base + (unsigned)pa[h]], e = B.cs[base + (unsigned)pb[h] + 1];
+          s_rb[nr] = b;
+          s_rp[nr] = acc;
+          acc += e - b;
+          nr++;
+        }
+      }
+      s_rp[nr] = acc;
+      s_nr = nr;
+      // the 3-cell coordinate window of each axis stays clear of the box edge
+      auto clear = [&](int c) {
+        double s0 = (double)(c - 1) + K.xs;
+        s0 -= K.tx * floor(s0 / K.tx);
+        return s0 >= 1.0 && s0 + 3.0 <= K.tx - 1.0;
+      };
+      s_wrapfree = clear(cxc) && clear(cyc) && clear(czc);
+    }
+    __syncthreads();
+    const int nr = s_nr;
+    const unsigned total = s_rp[nr];
+    const bool wf = s_wrapfree;
+    double sum = 0.0;
+    for (unsigned base = 0; base < total; base += RT_TILE) {
+      const unsigned nt = min((unsigned)RT_TILE, total - base);
+      for (unsigned f = t; f < nt; f += RT_THREADS) {
+        const unsigned ff = base + f;
+        int r = 0;
+        while (s_rp[r + 1] <= ff) r++;
+        const float4 v = B.cube[s_rb[r] + (ff - s_rp[r])];
+        tile[f] = (__float_as_uint(v.w) & PSOD_DEAD_BIT)
+                      ? make_float4(1e30f, 1e30f, 1e30f, 0.f)
+                      : make_float4(to_grid(v.x, K.nxf), to_grid(v.y, K.nxf), to_grid(v.z, K.nxf), 0.f);
+      }
+      __syncthreads();
+      if (have && !quirk) sum += wf ? tile_terms<true>(tile, nt, cx, cy, cz, K) : tile_terms<false>(tile, nt, cx, cy, cz, K);
+      __syncthreads();
+    }
+    if (have && !quirk && K.has_quirk) {
+      // the particle the run scan files under another cell: counted if that
+      // cell is in x_sel2 but outside this candidate cell's 27 neighbours
+      const int ax = (int)(K.quirk_listed % K.nx), ay = (int)((K.quirk_listed / K.nx) % K.nx),
+                az = (int)(K.quirk_listed / ((unsigned)K.nx * K.nx));
+      const bool listed_in_sel2 = in_sel2(K, ax, ay, az, g.ic, g.jc, g.kc);
+      const bool seen = abs(pdiff(ax, cxc, K.nx)) <= 1 && abs(pdiff(ay, cyc, K.nx)) <= 1 && abs(pdiff(az, czc, K.nx)) <= 1;
+      if (listed_in_sel2 && !seen) {
+        const float4 qv = B.cube[K.quirk_pos];
+        if (!(__float_as_uint(qv.w) & PSOD_DEAD_BIT)) {
+          const double d2 = min_image_d2((double)to_grid(qv.x, K.nxf), (double)to_grid(qv.y, K.nxf),
+                                         (double)to_grid(qv.z, K.nxf), (double)cx, (double)cy, (double)cz, K.tx);
+          if (d2 <= K.rmin2) sum += ddiv(1.0, dsqrt(dadd(d2, K.eps2)));
+        }
+      }
+    }
+    // the foreign-filed particle as a candidate has other neighbours: leave
+    // it to the exact pass
+    if (have) B.cand_s[q] = quirk ? __longlong_as_double(0x7ff0000000000000ll) : sum;
+    if (t == 0) visits += (unsigned long long)min((unsigned)RT_THREADS, cnt - s_chunk * RT_THREADS) * total;
+  }
+  if (t == 0 && visits) atomicAdd(B.pairs, visits);
+}
+
 // ---------------------------------------------------------------------------
 // phase 3: exact sums for the contenders and the argmax (main:1864-1875):
 // largest sum wins, equal sums go to the first candidate in the reference's
@@ -832,11 +1023,12 @@ __device__ void select_seed(const SodConst &K, const SodBufs &B, Smem &S, unsign
   const unsigned off = B.st_coff[slot], n = B.st_cn[slot];
   if (n == 0) return;
   const SeedGeo g = seed_geo(K, B, rank);
-  // max of the approximate sums (non-negative doubles order as their bits)
+  // max of the finite approximate sums (non-negative doubles order as their
+  // bits); an infinite entry marks a candidate that always goes exact
   unsigned long long mb = 0, dummy = 0;
   for (unsigned k = threadIdx.x; k < n; k += TPB) {
     const unsigned long long b = dbits(B.cand_s[off + k]);
-    mb = b > mb ? b : mb;
+    if (b < 0x7ff0000000000000ull) mb = b > mb ? b : mb;
   }
   block_max_pair(S, mb, dummy);
   const double thr = dmul(bitsd(mb), 1.0 - 2.0 * REF_TOL);
@@ -882,7 +1074,7 @@ __global__ void __launch_bounds__(TPB) k_select(SodConst K, SodBufs B) {
   Smem &S = *reinterpret_cast<Smem *>(smem_raw);
   while (true) {
     const unsigned item = next_item(&B.work[2]);
-    if (item >= *B.nready) break;
+    if (item >= min(*B.nready, B.cap_ready)) break;
     select_seed(K, B, S, item, B.ready[item]);
   }
 }
@@ -1101,7 +1293,7 @@ __global__ void __launch_bounds__(TPB) k_cross(SodConst K, SodBufs B) {
   Smem &S = *reinterpret_cast<Smem *>(smem_raw);
   while (true) {
     const unsigned item = next_item(&B.work[3]);
-    if (item >= *B.nready) break;
+    if (item >= min(*B.nready, B.cap_ready)) break;
     cross_seed(K, B, S, item, B.ready[item]);
   }
 }
@@ -1131,40 +1323,72 @@ __global__ void k_count_u32(const unsigned *keys, long long n, unsigned *count) 
   if (i < n) atomicAdd(&count[keys[i]], 1u);
 }
 
-// advance each block's cursor past resolved seeds; head = lowest unresolved rank
-__global__ void k_heads(long long nblocks, const unsigned *bbegin, unsigned *cursor, const unsigned *blist,
-                        const unsigned char *processed, const unsigned *seed_idx, const unsigned *inv,
-                        const float4 *cube, unsigned *head, unsigned *gmin) {
-  const long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+// cube position of each seed in block order (saves an indirection per test)
+__global__ void k_seed_pos(const unsigned *blist, long long nseed, const unsigned *seed_idx, const unsigned *inv,
+                           unsigned *bpos) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < nseed) bpos[i] = inv[seed_idx[blist[i]]];
+}
+
+__global__ void k_init_active(long long nblocks, const unsigned *bbegin, unsigned *head, unsigned *active,
+                              unsigned *nactive) {
+  long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nblocks) return;
+  head[b] = PSOD_INF_RANK;
+  if (bbegin[b + 1] > bbegin[b]) active[atomicAdd(nactive, 1u)] = (unsigned)b;
+}
+
+// Warp per active block: advance the cursor past resolved (processed or
+// claimed) seeds, 256 entries per step with independent loads; head = the
+// lowest unresolved rank.  Blocks that still hold seeds go to next_active.
+__global__ void k_heads(const unsigned *active, unsigned nactive, const unsigned *bbegin, unsigned *cursor,
+                        const unsigned *blist, const unsigned *bpos, const unsigned char *processed,
+                        const float4 *cube, unsigned *head, unsigned *gmin, unsigned *next_active,
+                        unsigned *n_next) {
+  const unsigned wid = (unsigned)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (wid >= nactive) return;
+  const unsigned b = active[wid];
+  unsigned cur = cursor[b];
+  const unsigned end = bbegin[b + 1];
   unsigned h = PSOD_INF_RANK;
-  if (b < nblocks) {
-    unsigned cur = cursor[b];
-    const unsigned end = bbegin[b + 1];
-    while (cur < end) {
-      const unsigned r = blist[cur];
-      if (processed[r] || (__float_as_uint(cube[inv[seed_idx[r]]].w) & PSOD_DEAD_BIT)) {
-        cur++;
-        continue;
-      }
-      h = r;
+  while (cur < end) {
+    unsigned m[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      const unsigned idx = cur + (unsigned)(k * 32 + lane);
+      bool unres = false;
+      if (idx < end) unres = !processed[blist[idx]] && !(__float_as_uint(cube[bpos[idx]].w) & PSOD_DEAD_BIT);
+      m[k] = __ballot_sync(0xffffffffu, unres);
+    }
+    int found = -1;
+#pragma unroll
+    for (int k = 7; k >= 0; k--)
+      if (m[k]) found = k * 32 + __ffs(m[k]) - 1;
+    if (found >= 0) {
+      cur += (unsigned)found;
+      h = blist[cur];
       break;
     }
+    cur += 256u;
+  }
+  if (cur > end) cur = end;
+  if (lane == 0) {
     cursor[b] = cur;
     head[b] = h;
-  }
-  if (gmin) {  // global minimum, needed only for the foreign-filed seed
-    unsigned m = h;
-    for (int o = 16; o > 0; o >>= 1) m = min(m, __shfl_down_sync(0xffffffffu, m, o));
-    if ((threadIdx.x & 31) == 0 && m != PSOD_INF_RANK) atomicMin(gmin, m);
+    if (h != PSOD_INF_RANK) {
+      next_active[atomicAdd(n_next, 1u)] = b;
+      if (gmin) atomicMin(gmin, h);
+    }
   }
 }
 
 // periodic sliding minimum of radius rb along one axis of the nb^3 grid
 __global__ void k_minfilter(const unsigned *in, unsigned *out, int nb, int axis, int rb) {
-  long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long nbl = (long long)nb * nb * nb;
+  const unsigned nbl = (unsigned)nb * nb * nb;
+  const unsigned b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= nbl) return;
-  int c[3] = {(int)(b % nb), (int)((b / nb) % nb), (int)(b / ((long long)nb * nb))};
+  int c[3] = {(int)(b % (unsigned)nb), (int)((b / (unsigned)nb) % (unsigned)nb), (int)(b / ((unsigned)nb * nb))};
   const int full = (2 * rb + 1 >= nb);
   const int lo = full ? 0 : -rb, hi = full ? nb - 1 : rb;
   unsigned m = PSOD_INF_RANK;
@@ -1174,21 +1398,24 @@ __global__ void k_minfilter(const unsigned *in, unsigned *out, int nb, int axis,
     if (v < 0) v += nb;
     if (v >= nb) v -= nb;
     c[axis] = v;
-    unsigned x = in[(long long)c[0] + (long long)nb * ((long long)c[1] + (long long)nb * c[2])];
+    const unsigned x = in[(unsigned)c[0] + (unsigned)nb * ((unsigned)c[1] + (unsigned)nb * (unsigned)c[2])];
     m = x < m ? x : m;
   }
   out[b] = m;
 }
 
-__global__ void k_ready(long long nblocks, const unsigned *head, const unsigned *filt, unsigned quirk_rank,
-                        const unsigned *gmin, unsigned *ready, unsigned *nready) {
-  long long b = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= nblocks) return;
+__global__ void k_ready(const unsigned *active, const unsigned *nactive, const unsigned *head, const unsigned *filt,
+                        unsigned quirk_rank, const unsigned *gmin, unsigned *ready, unsigned *nready, unsigned cap) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *nactive) return;
+  const unsigned b = active[i];
   const unsigned h = head[b];
   if (h == PSOD_INF_RANK || h != filt[b]) return;
   // the particle filed under another cell waits until it is the global minimum
   if (h == quirk_rank && h != *gmin) return;
-  ready[atomicAdd(nready, 1u)] = h;
+  // seeds past the cap stay unprocessed and are ready again next round
+  const unsigned at = atomicAdd(nready, 1u);
+  if (at < cap) ready[at] = h;
 }
 
 __global__ void k_find_rank(const unsigned *seed_idx, long long nseed, unsigned idx, unsigned *out) {
@@ -1357,7 +1584,7 @@ enum {
   SC_PROCESSED, SC_U64, SC_EDGES, SC_HRANK, SC_HID, SC_HMASS, SC_HMASS2, SC_HMEXTRA, SC_HPROF, SC_HCENTER,
   SC_HRDELTA, SC_HPOOL, SC_POOLKEY, SC_POOLIDX, SC_COUNTS, SC_ST_ACTIVE, SC_ST_NA, SC_ST_COFF, SC_ST_CN,
   SC_ST_CENTRE, SC_CAND_POS, SC_CAND_SLOT, SC_CAND_S, SC_ORDER, SC_RKEYS, SC_MASS32, SC_MOFF, SC_TKEY, SC_TIDX,
-  SC_ALIVE
+  SC_ALIVE, SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS
 };
 
 struct PhaseTimer {
@@ -1398,16 +1625,18 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   PSOD_CUDA(c, cudaMemcpyAsync(c->d_cube, c->d_cube_orig, sizeof(float4) * n, cudaMemcpyDeviceToDevice, c->stream));
 
   // block grid of the scheduler
+  // block side: the largest power of two dividing nx and at most half the
+  // dependency radius, so the window spans 2-4 blocks each way
+  const int rdep = c->ncut + std::max(c->ncut, 2);
   int bs = 1;
-  for (int cand : {4, 2}) {
-    if (c->nx % cand == 0) {
+  for (int cand = 16; cand >= 2; cand >>= 1) {
+    if (c->nx % cand == 0 && cand <= std::max(1, rdep / 2)) {
       bs = cand;
       break;
     }
   }
   const int nb = c->nx / bs;
   const long long nblocks = (long long)nb * nb * nb;
-  const int rdep = c->ncut + std::max(c->ncut, 2);
   const int rb = (rdep + bs - 1) / bs;
   const long long hcap = std::max<long long>(1, n / std::max(1, c->p.nmin) + 1);
   const int ne = std::max(1, c->p.ndelta_extra);
@@ -1436,6 +1665,18 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       (rc = scratch(c, SC_ST_CENTRE, (size_t)nblocks + 1, &st_centre)) || (rc = scratch(c, SC_CAND_POS, (size_t)n, &cand_pos)) ||
       (rc = scratch(c, SC_CAND_SLOT, (size_t)n, &cand_slot)) || (rc = scratch(c, SC_CAND_S, (size_t)n, &cand_s)))
     return rc;
+  // seeds per round at most (bounds the per-round buffers)
+  const unsigned cap_ready = (unsigned)std::min<long long>(nblocks + 1, 1ll << 20);
+  unsigned *act_a, *act_b, *bpos;
+  if ((rc = scratch(c, SC_ACT_A, (size_t)nblocks + 1, &act_a)) || (rc = scratch(c, SC_ACT_B, (size_t)nblocks + 1, &act_b)) ||
+      (rc = scratch(c, SC_BPOS, (size_t)nseed + 1, &bpos)))
+    return rc;
+  unsigned *cell_cnt, *cell_off, *cell_chunks, *chunk_pref;
+  if ((rc = scratch(c, SC_CELLCNT, (size_t)cap_ready * 27, &cell_cnt)) ||
+      (rc = scratch(c, SC_CELLOFF, (size_t)cap_ready * 27, &cell_off)) ||
+      (rc = scratch(c, SC_CELLCHUNK, (size_t)cap_ready * 27, &cell_chunks)) ||
+      (rc = scratch(c, SC_CHUNKPREF, (size_t)cap_ready * 27 + 1, &chunk_pref)))
+    return rc;
   // ctrs: 0 nready, 1..4 work counters, 5 gmin, 6 quirk rank, 7 cand_used
   unsigned *nready_d = ctrs, *work = ctrs + 1, *gmin = ctrs + 5, *qrank_d = ctrs + 6, *cand_used = ctrs + 7;
 
@@ -1456,6 +1697,8 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     if ((rc = scan_u32(c, counts, bbegin, nblocks, true))) return rc;
     if ((rc = radix_sort_u32(c, block_of, blist, nseed, 32))) return rc;
     PSOD_CUDA(c, cudaMemcpyAsync(cursor, bbegin, sizeof(unsigned) * nblocks, cudaMemcpyDeviceToDevice, c->stream));
+    k_seed_pos<<<nblk(nseed, 256), 256, 0, c->stream>>>(blist, nseed, c->d_seed_idx, c->d_inv, bpos);
+    kernels++;
     if (c->has_quirk) {
       float4 qv;
       PSOD_CUDA(c, cudaMemcpyAsync(&qv, c->d_cube_orig + c->quirk_pos, sizeof(qv), cudaMemcpyDeviceToHost, c->stream));
@@ -1482,7 +1725,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   if (per_sm < 1) per_sm = 1;
   const unsigned seed_grid = (unsigned)(dev_sms * per_sm);
   int per_sm_ref = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ref, k_refine_approx, TPB, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ref, k_refine_tile, RT_THREADS, 0);
   const unsigned ref_grid = (unsigned)(dev_sms * std::max(1, per_sm_ref));
 
   SodBufs B;
@@ -1495,6 +1738,11 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.processed = processed;
   B.ready = ready;
   B.nready = nready_d;
+  B.cap_ready = cap_ready;
+  B.cell_cnt = cell_cnt;
+  B.cell_off = cell_off;
+  B.cell_chunks = cell_chunks;
+  B.chunk_pref = chunk_pref;
   B.err = u64s;
   B.nhalo = u64s + 1;
   B.pool_used = u64s + 2;
@@ -1534,31 +1782,48 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   }
 
   long long rounds = 0, seed_launches = 0;
-  while (nseed > 0) {
+  // ctrs[8]: active-block count of the current list, ctrs[9]: of the next
+  unsigned n_active = 0;
+  if (nseed > 0) {
+    PSOD_CUDA(c, cudaMemsetAsync(ctrs + 8, 0, sizeof(unsigned) * 2, c->stream));
+    k_init_active<<<nblk(nblocks, 256), 256, 0, c->stream>>>(nblocks, bbegin, head, act_a, ctrs + 8);
+    kernels++;
+    PSOD_CUDA(c, cudaMemcpyAsync(&n_active, ctrs + 8, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  while (nseed > 0 && n_active > 0) {
     t_sched.start(c->stream);
     PSOD_CUDA(c, cudaMemsetAsync(ctrs, 0, sizeof(unsigned) * 5, c->stream));  // nready, work[4]
     PSOD_CUDA(c, cudaMemsetAsync(gmin, 0xff, sizeof(unsigned), c->stream));
     PSOD_CUDA(c, cudaMemsetAsync(cand_used, 0, sizeof(unsigned), c->stream));
-    k_heads<<<nblk(nblocks, 256), 256, 0, c->stream>>>(nblocks, bbegin, cursor, blist, processed, c->d_seed_idx,
-                                                       c->d_inv, c->d_cube, head,
-                                                       quirk_rank != PSOD_INF_RANK ? gmin : nullptr);
+    PSOD_CUDA(c, cudaMemsetAsync(ctrs + 9, 0, sizeof(unsigned), c->stream));
+    k_heads<<<nblk((long long)n_active * 32, 256), 256, 0, c->stream>>>(
+        act_a, n_active, bbegin, cursor, blist, bpos, processed, c->d_cube, head,
+        quirk_rank != PSOD_INF_RANK ? gmin : nullptr, act_b, ctrs + 9);
     k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(head, filt_a, nb, 0, rb);
     k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(filt_a, filt_b, nb, 1, rb);
     k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(filt_b, filt_a, nb, 2, rb);
-    k_ready<<<nblk(nblocks, 256), 256, 0, c->stream>>>(nblocks, head, filt_a, quirk_rank, gmin, ready, nready_d);
+    k_ready<<<nblk(n_active, 256), 256, 0, c->stream>>>(act_b, ctrs + 9, head, filt_a, quirk_rank, gmin, ready,
+                                                         nready_d, cap_ready);
     t_sched.stop(c->stream);
     kernels += 5;
-    unsigned nready = 0;
-    PSOD_CUDA(c, cudaMemcpyAsync(&nready, nready_d, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    unsigned hc[10];
+    PSOD_CUDA(c, cudaMemcpyAsync(hc, ctrs, sizeof(hc), cudaMemcpyDeviceToHost, c->stream));
     PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
     t_sched.collect();
+    unsigned nready = hc[0];
+    n_active = hc[9];
+    std::swap(act_a, act_b);
     if (nready == 0) break;
+    nready = std::min(nready, cap_ready);
     const unsigned g = std::min<unsigned>(seed_grid, nready);
     t_prep.start(c->stream);
     k_prep<<<g, TPB, smem, c->stream>>>(K, B);
     t_prep.stop(c->stream);
     t_ref.start(c->stream);
-    k_refine_approx<<<ref_grid, TPB, 0, c->stream>>>(K, B);
+    B.nitems_cells = 27u * nready;
+    if ((rc = scan_u32(c, cell_chunks, chunk_pref, (long long)B.nitems_cells, true))) return rc;
+    k_refine_tile<<<ref_grid, RT_THREADS, 0, c->stream>>>(K, B);
     t_ref.stop(c->stream);
     t_sel.start(c->stream);
     k_select<<<g, TPB, smem, c->stream>>>(K, B);

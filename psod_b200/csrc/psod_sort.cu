@@ -95,7 +95,7 @@ __global__ void k_tile_scan(const unsigned *in, unsigned *out, long long n, cons
 
 }  // namespace
 
-int scan_u32(psod_ctx *c, const unsigned *in, unsigned *out, long long n, bool with_total) {
+static int scan_level(psod_ctx *c, const unsigned *in, unsigned *out, long long n, bool with_total, int level) {
   if (n <= 0) {
     if (with_total) PSOD_CUDA(c, cudaMemsetAsync(out, 0, sizeof(unsigned), c->stream));
     return PSOD_OK;
@@ -103,24 +103,22 @@ int scan_u32(psod_ctx *c, const unsigned *in, unsigned *out, long long n, bool w
   long long ntiles = (n + SCAN_TILE - 1) / SCAN_TILE;
   unsigned *partial = nullptr;
   if (ntiles > 1) {
-    int st = dalloc(c, &partial, (size_t)ntiles + 1);
+    // tile sums live in context scratch (slots 8.., one per recursion level)
+    int st = scratch(c, 8 + level, (size_t)ntiles + 1, &partial);
     if (st) return st;
     k_tile_reduce<<<(unsigned)ntiles, SCAN_THREADS, 0, c->stream>>>(in, n, partial);
-    st = scan_u32(c, partial, partial, ntiles, false);
-    if (st) {
-      dfree(&partial);
-      return st;
-    }
+    st = scan_level(c, partial, partial, ntiles, false, level + 1);
+    if (st) return st;
   }
   k_tile_scan<<<(unsigned)ntiles, SCAN_THREADS, 0, c->stream>>>(in, out, n, partial,
                                                                  with_total ? out + n : nullptr);
   cudaError_t e = cudaGetLastError();
-  if (partial) {
-    cudaStreamSynchronize(c->stream);
-    dfree(&partial);
-  }
   if (e != cudaSuccess) return cuda_check(c, e, "scan_u32");
   return PSOD_OK;
+}
+
+int scan_u32(psod_ctx *c, const unsigned *in, unsigned *out, long long n, bool with_total) {
+  return scan_level(c, in, out, n, with_total, 0);
 }
 
 // ---------------------------------------------------------------------------

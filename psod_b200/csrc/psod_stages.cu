@@ -146,6 +146,108 @@ __global__ void k_cic_interp(const float4 *cube, long long n, CicConst k, const 
   rho[idx] = r;
 }
 
+// Tile-fused CIC: one CTA owns CT^3 SOD cells.  It deposits the particles
+// of those cells and of a one-cell halo into a shared-memory window of
+// fixed-point nodes, then interpolates rho for its own particles.  Every
+// node the own particles read receives all its contributions inside the
+// window, so the integer node sums, and therefore rho, equal the global
+// grid's exactly.  Needs each particle's CIC cell to be one of the two fine
+// cells of its SOD cell (true when nx is a power of two); a particle that
+// breaks this sets *bad and the caller falls back to the global grid.
+constexpr int CT = 8;                 // SOD cells per tile side
+constexpr int CW = 2 * (CT + 2) + 1;  // window nodes per side
+constexpr int CW3 = CW * CW * CW;
+
+__global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsigned *cs, int nx, double xs, CicConst k,
+                                                  double *rho, int *bad) {
+  extern __shared__ __align__(16) unsigned long long win[];
+  const int ntile = nx / CT;
+  const int tx = blockIdx.x % ntile, ty = (blockIdx.x / ntile) % ntile, tz = blockIdx.x / (ntile * ntile);
+  const int x0 = tx * CT, y0 = ty * CT, z0 = tz * CT;
+  const int nc = k.nc;  // 2*nx fine cells
+  const float nxf = (float)nx;
+  for (int i = threadIdx.x; i < CW3; i += blockDim.x) win[i] = 0ull;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  auto widx = [&](int f, int o) {  // fine index -> window offset (periodic)
+    int d = f - o;
+    if (d < 0) d += nc;
+    if (d >= nc) d -= nc;
+    return d;
+  };
+  const int ox = 2 * (x0 - 1), oy = 2 * (y0 - 1), oz = 2 * (z0 - 1);
+  // rows of the tile plus halo
+  for (int row = w; row < (CT + 2) * (CT + 2); row += nw) {
+    const int yy = (y0 - 1 + row % (CT + 2) + nx) % nx, zz = (z0 - 1 + row / (CT + 2) + nx) % nx;
+    const unsigned long long base = (unsigned long long)nx * ((unsigned)yy + (unsigned long long)nx * (unsigned)zz);
+    const int xa = x0 - 1, xb = x0 + CT;  // inclusive, may wrap
+    int pa[2], pb[2], np;
+    if (xa < 0) { pa[0] = xa + nx; pb[0] = nx - 1; pa[1] = 0; pb[1] = xb; np = 2; }
+    else if (xb >= nx) { pa[0] = xa; pb[0] = nx - 1; pa[1] = 0; pb[1] = xb - nx; np = 2; }
+    else { pa[0] = xa; pb[0] = xb; np = 1; }
+    for (int q = 0; q < np; q++) {
+      const unsigned b = cs[base + (unsigned)pa[q]], e = cs[base + (unsigned)pb[q] + 1];
+      for (unsigned p = b + lane; p < e; p += 32) {
+        const float4 v = cube[p];
+        int ix, ixp, iy, iyp, iz, izp;
+        double ddx, dex, ddy, dey, ddz, dez;
+        cic_axis(v.x, k.xxmin, k.dx, nc, ix, ixp, ddx, dex);
+        cic_axis(v.y, k.xxmin, k.dx, nc, iy, iyp, ddy, dey);
+        cic_axis(v.z, k.xxmin, k.dx, nc, iz, izp, ddz, dez);
+        const int sx = sod_cell_axis(to_grid(v.x, nxf), xs, nx), sy = sod_cell_axis(to_grid(v.y, nxf), xs, nx),
+                  sz = sod_cell_axis(to_grid(v.z, nxf), xs, nx);
+        if ((ix >> 1) != sx || (iy >> 1) != sy || (iz >> 1) != sz) {
+          atomicOr(bad, 1);
+          continue;
+        }
+        const int cx[2] = {widx(ix, ox), widx(ixp, ox)}, cy[2] = {widx(iy, oy), widx(iyp, oy)},
+                  cz[2] = {widx(iz, oz), widx(izp, oz)};
+        const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+          const int a = c & 1, bb = (c >> 1) & 1, ee = c >> 2;
+          if (cx[a] >= CW || cy[bb] >= CW || cz[ee] >= CW) continue;
+          const double wgt = dmul(dmul(wx[a], wy[bb]), wz[ee]);
+          atomicAdd(&win[cx[a] + CW * (cy[bb] + CW * cz[ee])], (unsigned long long)__double2ll_rn(dmul(wgt, FIX_ONE)));
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // own particles: rho in the reference's term order (main:1368-1383)
+  for (int row = w; row < CT * CT; row += nw) {
+    const int yy = y0 + row % CT, zz = z0 + row / CT;
+    const unsigned long long base = (unsigned long long)nx * ((unsigned)yy + (unsigned long long)nx * (unsigned)zz);
+    const unsigned b = cs[base + (unsigned)x0], e = cs[base + (unsigned)(x0 + CT - 1) + 1];
+    for (unsigned p = b + lane; p < e; p += 32) {
+      const float4 v = cube[p];
+      const unsigned idx = __float_as_uint(v.w) & PSOD_IDX_MASK;
+      int ix, ixp, iy, iyp, iz, izp;
+      double ddx, dex, ddy, dey, ddz, dez;
+      cic_axis(v.x, k.xxmin, k.dx, nc, ix, ixp, ddx, dex);
+      cic_axis(v.y, k.xxmin, k.dx, nc, iy, iyp, ddy, dey);
+      cic_axis(v.z, k.xxmin, k.dx, nc, iz, izp, ddz, dez);
+      const int cx[2] = {widx(ix, ox), widx(ixp, ox)}, cy[2] = {widx(iy, oy), widx(iyp, oy)},
+                cz[2] = {widx(iz, oz), widx(izp, oz)};
+      const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
+      double r = 0.0;
+      bool ok = true;
+#pragma unroll
+      for (int c = 0; c < 8; c++) {
+        const int a = c & 1, bb = (c >> 1) & 1, ee = c >> 2;
+        if (cx[a] >= CW || cy[bb] >= CW || cz[ee] >= CW) {
+          ok = false;
+          continue;
+        }
+        const double gval = dmul((double)(long long)win[cx[a] + CW * (cy[bb] + CW * cz[ee])], k.kc);
+        r = dadd(r, dmul(dmul(dmul(gval, wx[a]), wy[bb]), wz[ee]));
+      }
+      if (!ok) atomicOr(bad, 1);
+      rho[idx] = r;
+    }
+  }
+}
+
 __global__ void k_grid_to_double(const unsigned long long *grid, long long nnode, double kc, double *out) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nnode) out[i] = dmul((double)(long long)grid[i], kc);
@@ -278,11 +380,33 @@ int stage_cic(psod_ctx *c, double *grid_out) {
   CicConst k = make_cic_const(c);
   const long long nnode = (long long)k.nc * k.nc * k.nc;
   int st;
-  if ((st = dalloc(c, &c->d_grid, (size_t)nnode))) return st;
-  PSOD_CUDA(c, cudaMemsetAsync(c->d_grid, 0, sizeof(unsigned long long) * nnode, c->stream));
-  k_cic_deposit<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->d_cube_orig, c->n, k, c->d_grid);
-  if ((st = dalloc(c, &c->d_rho, (size_t)c->n))) return st;
-  k_cic_interp<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->d_cube_orig, c->n, k, c->d_grid, c->d_rho);
+  if (!c->d_rho || c->rho_cap < c->n) {
+    if ((st = dalloc(c, &c->d_rho, (size_t)c->n))) return st;
+    c->rho_cap = c->n;
+  }
+  // fused tile path (no global grid) when the box tiles evenly
+  bool tiled = false;
+  if (c->nx % CT == 0 && c->nx >= 2 * (CT + 2) && c->xxmin <= 0.0 && -c->xxmin + 1.0 >= 1.0) {
+    int *bad = nullptr;
+    if ((st = scratch(c, 2, 1, &bad))) return st;
+    PSOD_CUDA(c, cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
+    const int smem = CW3 * (int)sizeof(unsigned long long);
+    PSOD_CUDA(c, cudaFuncSetAttribute(k_cic_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const long long ntiles = (long long)(c->nx / CT) * (c->nx / CT) * (c->nx / CT);
+    k_cic_tile<<<(unsigned)ntiles, 256, smem, c->stream>>>(c->d_cube_orig, c->d_cell_start, c->nx,
+                                                           c->xxmin * c->scale, k, c->d_rho, bad);
+    int hbad = 0;
+    PSOD_CUDA(c, cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+    tiled = (hbad == 0);
+  }
+  if (!tiled || grid_out) {
+    if ((st = dalloc(c, &c->d_grid, (size_t)nnode))) return st;
+    PSOD_CUDA(c, cudaMemsetAsync(c->d_grid, 0, sizeof(unsigned long long) * nnode, c->stream));
+    k_cic_deposit<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->d_cube_orig, c->n, k, c->d_grid);
+    if (!tiled) k_cic_interp<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->d_cube_orig, c->n, k, c->d_grid, c->d_rho);
+  }
+  c->cic_tiled = tiled;
   PSOD_CUDA(c, cudaGetLastError());
   if (grid_out) {
     double *tmp = nullptr;
