@@ -156,7 +156,10 @@ static int zone_setup(const psod_oracle_params *p, zone_t *z) {
   z->nxbuffer = p->nxbuffer;
   if (z->nxbuffer == 0) z->nxbuffer = z->nxzone / 2; /* main:380-381 */
   if (z->nxbuffer < p->ncut) return PSOD_ORACLE_ERR_ARG;     /* main:386 */
-  if (z->nxbuffer > z->nxzone) return PSOD_ORACLE_ERR_ARG;   /* main:392 */
+  /* main:392 allows nxbuffer == nxzone; the CIC indices of the last half
+   * cell then land in the reference's padding past the periodic grid, which
+   * is not restated here */
+  if (z->nxbuffer >= z->nxzone) return PSOD_ORACLE_ERR_ARG;
   /* main:401-402 with ixzone = 0, nxcpu = 1 */
   double q = (double)z->nxbuffer / (double)z->nxzone;
   z->xmin = (0.0 - q) / 1.0;

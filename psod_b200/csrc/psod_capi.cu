@@ -54,7 +54,6 @@ static void free_all(psod_ctx *c) {
   dfree(&c->d_vel);
   dfree(&c->d_ids);
   dfree(&c->d_cube);
-  dfree(&c->d_cube_orig);
   dfree(&c->d_cell_start);
   dfree(&c->d_inv);
   dfree(&c->d_rho);
@@ -133,7 +132,9 @@ int psod_ctx_create(const psod_params *pin, psod_ctx **out) {
   else if (!(p.delta > 0.0)) why = "delta must be positive";
   int nxbuffer = p.nxbuffer == 0 ? p.nx / 2 : p.nxbuffer;  // main:380-381, nxzone = nx
   if (why.empty() && nxbuffer < p.ncut) why = "nxbuffer must be >= ncut (main:386)";
-  if (why.empty() && nxbuffer > p.nx) why = "nxbuffer must be <= nx (main:392)";
+  // the reference allows nxbuffer == nx (main:392); its CIC array is then
+  // padded past the periodic grid, which this engine does not keep
+  if (why.empty() && nxbuffer >= p.nx) why = "nxbuffer must be < nx";
   if (!why.empty()) {
     delete c;
     return PSOD_ERR_ARG;
@@ -204,9 +205,18 @@ int psod_load_particles(psod_ctx *c, int64_t n, const float *pos, const float *v
   c->munit = (float)((double)c->mpf * (double)npart_total);   // main:685
   c->cic_done = c->rho_done = c->seeds_done = c->sod_done = false;
   int st;
-  if ((st = dalloc(c, &c->d_pos, (size_t)n * 3))) return st;
-  if ((st = dalloc(c, &c->d_ids, (size_t)n))) return st;
-  if ((st = copy_in(c, c->d_pos, pos, sizeof(float) * 3 * n))) return st;
+  // positions are only read by the cell sort: a device buffer is used in
+  // place, a host buffer goes through a temporary device copy
+  const float *dpos = pos;
+  if (!is_device_ptr(pos)) {
+    if ((st = dalloc(c, &c->d_pos, (size_t)n * 3))) return st;
+    if ((st = copy_in(c, c->d_pos, pos, sizeof(float) * 3 * n))) return st;
+    dpos = c->d_pos;
+  }
+  if (!c->d_ids || c->ids_cap < n) {
+    if ((st = dalloc(c, &c->d_ids, (size_t)n))) return st;
+    c->ids_cap = n;
+  }
   if ((st = copy_in(c, c->d_ids, id, sizeof(int64_t) * n))) return st;
   if (vel) {
     if ((st = dalloc(c, &c->d_vel, (size_t)n * 3))) return st;
@@ -214,7 +224,9 @@ int psod_load_particles(psod_ctx *c, int64_t n, const float *pos, const float *v
   } else {
     dfree(&c->d_vel);
   }
-  return stage_cellsort(c);
+  st = stage_cellsort(c, dpos);
+  dfree(&c->d_pos);
+  return st;
 }
 
 int psod_cic(psod_ctx *c, double *grid_out) {

@@ -23,6 +23,7 @@
 #define PSOD_IDX_MASK 0x7fffffffu
 #define PSOD_INF_RANK 0xffffffffu
 #define PSOD_MAX_BINS 128
+#define PSOD_STATIC_MAX_NX 64
 
 namespace psod {
 
@@ -136,8 +137,8 @@ struct psod_ctx {
   float *d_pos = nullptr;   // input order, 3n (box units)
   float *d_vel = nullptr;   // input order, 3n (optional)
   long long *d_ids = nullptr;
+  long long ids_cap = 0, cube_cap = 0, cs_cap = 0, inv_cap = 0;
   float4 *d_cube = nullptr;       // sorted
-  float4 *d_cube_orig = nullptr;  // pristine copy (alive flags reset)
   unsigned *d_cell_start = nullptr;
   unsigned *d_inv = nullptr;  // input index -> cube position
   unsigned long long ncell = 0;
@@ -201,6 +202,15 @@ int dalloc(psod_ctx *c, T **p, size_t count) {
   }
   return PSOD_OK;
 }
+// (re)allocate *p to hold count elements unless its capacity suffices
+template <typename T>
+int ensure(psod_ctx *c, T **p, long long *cap, size_t count) {
+  if (*p && *cap >= (long long)count) return PSOD_OK;
+  int st = dalloc(c, p, count);
+  *cap = st ? 0 : (long long)count;
+  return st;
+}
+
 template <typename T>
 void dfree(T **p) {
   if (*p) cudaFree(*p);
@@ -244,7 +254,7 @@ int radix_sort_u32(psod_ctx *c, unsigned *keys, unsigned *vals, long long n, int
 
 SodConst make_sod_const(const psod_ctx *c);
 
-int stage_cellsort(psod_ctx *c);
+int stage_cellsort(psod_ctx *c, const float *dpos);
 int stage_cic(psod_ctx *c, double *grid_out);
 int stage_cicm1(psod_ctx *c, double *rho_out);
 int stage_tri_cic(psod_ctx *c, int64_t *isort_out);

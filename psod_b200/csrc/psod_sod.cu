@@ -29,7 +29,6 @@ namespace psod {
 
 namespace {
 
-constexpr int RT_THREADS = 256;   // candidates per refinement work item
 constexpr int TPB = 256;          // threads per seed CTA
 constexpr int NWARP = TPB / 32;
 constexpr int NB = 4096;          // histogram buckets per level
@@ -707,7 +706,7 @@ __device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned
   if (threadIdx.x < 27) {
     B.cell_cnt[slot * 27 + threadIdx.x] = s_cnt[threadIdx.x];
     B.cell_off[slot * 27 + threadIdx.x] = s_base + s_coff[threadIdx.x];
-    B.cell_chunks[slot * 27 + threadIdx.x] = (s_cnt[threadIdx.x] + RT_THREADS - 1) / RT_THREADS;
+    B.cell_chunks[slot * 27 + threadIdx.x] = (s_cnt[threadIdx.x] + 31u) / 32u;
   }
   for (int o = w; o < 27; o += NWARP) {
     const int di = o / 9 - 1, dj = (o / 3) % 3 - 1, dk = o % 3 - 1;
@@ -835,36 +834,10 @@ __device__ void refine_sum(const SodConst &K, const SodBufs &B, unsigned cp, int
   sf_out = sf;
 }
 
-__global__ void __launch_bounds__(TPB) k_refine_approx(SodConst K, SodBufs B) {
-  const int lane = threadIdx.x & 31;
-  const unsigned total = *B.cand_used;
-  unsigned visits = 0;
-  while (true) {
-    unsigned q = 0;
-    if (lane == 0) q = atomicAdd(&B.work[1], 1u);
-    q = __shfl_sync(0xffffffffu, q, 0);
-    if (q >= total) break;
-    const unsigned slot = B.cand_slot[q];
-    const unsigned rank = B.ready[slot];
-    const SeedGeo g = seed_geo(K, B, rank);
-    unsigned long long sq;
-    double sf;
-    refine_sum<false>(K, B, B.cand_pos[q], g.ic, g.jc, g.kc, sq, sf, &visits);
-    if (lane == 0) B.cand_s[q] = sf;
-  }
-  if (lane == 0 && visits) atomicAdd(B.pairs, (unsigned long long)visits);
-  if (threadIdx.x == 0 && blockIdx.x == 0) atomicAdd(B.ncand_total, (unsigned long long)total);
-}
-
-// Tiled form of the approximate sums: one work item is up to 256 candidates
-// of one candidate cell (a thread each); the records of the cell's 27
-// neighbour cells stream through shared memory and every thread reads each
-// record by broadcast.  Each term is FP32 with one rounding per difference
+// Approximate refinement sums.  Each term is FP32 with one rounding per difference
 // (relative error below 1e-6); 32 terms are summed in FP32 (below 2e-6) and
 // the partial sums in FP64, so |S_approx - S| <= 3e-6 S < REF_TOL S.  Dead
 // records are parked at 1e30 so they never pass the inclusion test.
-constexpr int RT_TILE = 1024;
-
 template <bool WRAPFREE>
 __device__ __forceinline__ double tile_terms(const float4 *tile, unsigned nt, float cx, float cy, float cz,
                                              const SodConst &K) {
@@ -896,37 +869,42 @@ __device__ __forceinline__ double tile_terms(const float4 *tile, unsigned nt, fl
   return sum;
 }
 
-__global__ void __launch_bounds__(RT_THREADS) k_refine_tile(SodConst K, SodBufs B) {
-  __shared__ float4 tile[RT_TILE];
-  __shared__ unsigned s_item, s_ci, s_chunk, s_nitems;
-  __shared__ unsigned s_rb[18], s_rp[19];
-  __shared__ int s_nr, s_wrapfree;
-  const int t = threadIdx.x;
+// Warp-level work item: up to 32 candidates of one candidate cell, a lane
+// each.  The records of the cell's 3x3x3 neighbourhood pass through a
+// warp-private shared slice, 32 at a time, and every lane reads each one by
+// broadcast; warps never wait on one another.
+__global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
+  __shared__ float4 s_tile[8][32];
+  __shared__ unsigned s_rb[8][18], s_rp[8][19];
+  __shared__ int s_nr[8], s_wf[8];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned nitems = B.chunk_pref[B.nitems_cells];
   unsigned long long visits = 0;
-  if (t == 0) s_nitems = B.chunk_pref[B.nitems_cells];
   while (true) {
-    __syncthreads();
-    if (t == 0) {
-      s_item = atomicAdd(&B.work[1], 1u);
-      if (s_item < s_nitems) {
+    unsigned item = 0, ci = 0, chunk = 0;
+    if (lane == 0) {
+      item = atomicAdd(&B.work[1], 1u);
+      if (item < nitems) {
         unsigned lo = 0, hi = B.nitems_cells;  // last ci with chunk_pref[ci] <= item
         while (hi - lo > 1) {
           const unsigned mid = (lo + hi) >> 1;
-          if (B.chunk_pref[mid] <= s_item) lo = mid;
+          if (B.chunk_pref[mid] <= item) lo = mid;
           else hi = mid;
         }
-        s_ci = lo;
-        s_chunk = s_item - B.chunk_pref[lo];
+        ci = lo;
+        chunk = item - B.chunk_pref[lo];
       }
     }
-    __syncthreads();
-    if (s_item >= s_nitems) break;
-    const unsigned ci = s_ci, slot = ci / 27, o = ci % 27;
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= nitems) break;
+    ci = __shfl_sync(0xffffffffu, ci, 0);
+    chunk = __shfl_sync(0xffffffffu, chunk, 0);
+    const unsigned slot = ci / 27, o = ci % 27;
     const SeedGeo g = seed_geo(K, B, B.ready[slot]);
     const int di = (int)(o / 9) - 1, dj = (int)((o / 3) % 3) - 1, dk = (int)(o % 3) - 1;
     const int cxc = wrapi(g.ic + di, K.nx), cyc = wrapi(g.jc + dj, K.nx), czc = wrapi(g.kc + dk, K.nx);
     const unsigned cnt = B.cell_cnt[ci];
-    const unsigned myk = s_chunk * RT_THREADS + (unsigned)t;
+    const unsigned myk = chunk * 32u + (unsigned)lane;
     const bool have = myk < cnt;
     const unsigned q = B.cell_off[ci] + myk;
     const unsigned cp = have ? B.cand_pos[q] : 0u;
@@ -938,9 +916,9 @@ __global__ void __launch_bounds__(RT_THREADS) k_refine_tile(SodConst K, SodBufs 
       cy = to_grid(cv.y, K.nxf);
       cz = to_grid(cv.z, K.nxf);
     }
-    if (t == 0) {
-      // record runs of the 3x3x3 cells around the candidate cell: 9 rows,
-      // each one x-run of 3 cells (two when it wraps)
+    if (lane == 0) {
+      // record runs of the 3x3x3 cells around the candidate cell: 9 rows of a
+      // 3-cell x-run each (two runs when it wraps)
       int nr = 0;
       unsigned acc = 0;
       for (int r = 0; r < 9; r++) {
@@ -953,43 +931,44 @@ __global__ void __launch_bounds__(RT_THREADS) k_refine_tile(SodConst K, SodBufs 
         else { pa[0] = x0; pb[0] = x1; np = 1; }
         for (int h = 0; h < np; h++) {
           const unsigned b = B.cs[base + (unsigned)pa[h]], e = B.cs[base + (unsigned)pb[h] + 1];
-          s_rb[nr] = b;
-          s_rp[nr] = acc;
+          s_rb[w][nr] = b;
+          s_rp[w][nr] = acc;
           acc += e - b;
           nr++;
         }
       }
-      s_rp[nr] = acc;
-      s_nr = nr;
+      s_rp[w][nr] = acc;
+      s_nr[w] = nr;
       // the 3-cell coordinate window of each axis stays clear of the box edge
       auto clear = [&](int c) {
         double s0 = (double)(c - 1) + K.xs;
         s0 -= K.tx * floor(s0 / K.tx);
         return s0 >= 1.0 && s0 + 3.0 <= K.tx - 1.0;
       };
-      s_wrapfree = clear(cxc) && clear(cyc) && clear(czc);
+      s_wf[w] = clear(cxc) && clear(cyc) && clear(czc);
     }
-    __syncthreads();
-    const int nr = s_nr;
-    const unsigned total = s_rp[nr];
-    const bool wf = s_wrapfree;
+    __syncwarp();
+    const int nr = s_nr[w];
+    const unsigned total = s_rp[w][nr];
+    const bool wf = s_wf[w];
+    const bool active = have && !quirk;
     double sum = 0.0;
-    for (unsigned base = 0; base < total; base += RT_TILE) {
-      const unsigned nt = min((unsigned)RT_TILE, total - base);
-      for (unsigned f = t; f < nt; f += RT_THREADS) {
-        const unsigned ff = base + f;
+    for (unsigned base = 0; base < total; base += 32) {
+      const unsigned ff = base + (unsigned)lane;
+      if (ff < total) {
         int r = 0;
-        while (s_rp[r + 1] <= ff) r++;
-        const float4 v = B.cube[s_rb[r] + (ff - s_rp[r])];
-        tile[f] = (__float_as_uint(v.w) & PSOD_DEAD_BIT)
-                      ? make_float4(1e30f, 1e30f, 1e30f, 0.f)
-                      : make_float4(to_grid(v.x, K.nxf), to_grid(v.y, K.nxf), to_grid(v.z, K.nxf), 0.f);
+        while (s_rp[w][r + 1] <= ff) r++;
+        const float4 v = B.cube[s_rb[w][r] + (ff - s_rp[w][r])];
+        s_tile[w][lane] = (__float_as_uint(v.w) & PSOD_DEAD_BIT)
+                              ? make_float4(1e30f, 1e30f, 1e30f, 0.f)
+                              : make_float4(to_grid(v.x, K.nxf), to_grid(v.y, K.nxf), to_grid(v.z, K.nxf), 0.f);
       }
-      __syncthreads();
-      if (have && !quirk) sum += wf ? tile_terms<true>(tile, nt, cx, cy, cz, K) : tile_terms<false>(tile, nt, cx, cy, cz, K);
-      __syncthreads();
+      __syncwarp();
+      const unsigned nt = min(32u, total - base);
+      if (active) sum += wf ? tile_terms<true>(s_tile[w], nt, cx, cy, cz, K) : tile_terms<false>(s_tile[w], nt, cx, cy, cz, K);
+      __syncwarp();
     }
-    if (have && !quirk && K.has_quirk) {
+    if (active && K.has_quirk) {
       // the particle the run scan files under another cell: counted if that
       // cell is in x_sel2 but outside this candidate cell's 27 neighbours
       const int ax = (int)(K.quirk_listed % K.nx), ay = (int)((K.quirk_listed / K.nx) % K.nx),
@@ -1008,9 +987,9 @@ __global__ void __launch_bounds__(RT_THREADS) k_refine_tile(SodConst K, SodBufs 
     // the foreign-filed particle as a candidate has other neighbours: leave
     // it to the exact pass
     if (have) B.cand_s[q] = quirk ? __longlong_as_double(0x7ff0000000000000ll) : sum;
-    if (t == 0) visits += (unsigned long long)min((unsigned)RT_THREADS, cnt - s_chunk * RT_THREADS) * total;
+    if (lane == 0) visits += (unsigned long long)min(32u, cnt - chunk * 32u) * total;
   }
-  if (t == 0 && visits) atomicAdd(B.pairs, visits);
+  if (lane == 0 && visits) atomicAdd(B.pairs, visits);
 }
 
 // ---------------------------------------------------------------------------
@@ -1295,6 +1274,14 @@ __global__ void __launch_bounds__(TPB) k_cross(SodConst K, SodBufs B) {
     const unsigned item = next_item(&B.work[3]);
     if (item >= min(*B.nready, B.cap_ready)) break;
     cross_seed(K, B, S, item, B.ready[item]);
+  }
+}
+
+__global__ void k_clear_dead(float4 *cube, long long n) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    float *w = &cube[i].w;
+    *w = __uint_as_float(__float_as_uint(*w) & PSOD_IDX_MASK);
   }
 }
 
@@ -1622,7 +1609,8 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   long long kernels = 0;
 
   // reset alive flags: every call starts from the loaded cube
-  PSOD_CUDA(c, cudaMemcpyAsync(c->d_cube, c->d_cube_orig, sizeof(float4) * n, cudaMemcpyDeviceToDevice, c->stream));
+  k_clear_dead<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_cube, n);
+  kernels++;
 
   // block grid of the scheduler
   // block side: the largest power of two dividing nx and at most half the
@@ -1701,7 +1689,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     kernels++;
     if (c->has_quirk) {
       float4 qv;
-      PSOD_CUDA(c, cudaMemcpyAsync(&qv, c->d_cube_orig + c->quirk_pos, sizeof(qv), cudaMemcpyDeviceToHost, c->stream));
+      PSOD_CUDA(c, cudaMemcpyAsync(&qv, c->d_cube + c->quirk_pos, sizeof(qv), cudaMemcpyDeviceToHost, c->stream));
       PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
       unsigned qidx;
       memcpy(&qidx, &qv.w, 4);
@@ -1725,7 +1713,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   if (per_sm < 1) per_sm = 1;
   const unsigned seed_grid = (unsigned)(dev_sms * per_sm);
   int per_sm_ref = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ref, k_refine_tile, RT_THREADS, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ref, k_refine_warp, 256, 0);
   const unsigned ref_grid = (unsigned)(dev_sms * std::max(1, per_sm_ref));
 
   SodBufs B;
@@ -1823,7 +1811,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     t_ref.start(c->stream);
     B.nitems_cells = 27u * nready;
     if ((rc = scan_u32(c, cell_chunks, chunk_pref, (long long)B.nitems_cells, true))) return rc;
-    k_refine_tile<<<ref_grid, RT_THREADS, 0, c->stream>>>(K, B);
+    k_refine_warp<<<ref_grid, 256, 0, c->stream>>>(K, B);
     t_ref.stop(c->stream);
     t_sel.start(c->stream);
     k_select<<<g, TPB, smem, c->stream>>>(K, B);

@@ -298,34 +298,30 @@ inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 }  // namespace
 
 // ---------------------------------------------------------------------------
-int stage_cellsort(psod_ctx *c) {
+int stage_cellsort(psod_ctx *c, const float *dpos) {
   const long long n = c->n;
   const int nx = c->nx;
   c->ncell = (unsigned long long)nx * nx * nx;
   int st;
   unsigned *cell = nullptr, *count = nullptr;
   int *bad = nullptr;
-  if ((st = dalloc(c, &cell, (size_t)n))) return st;
-  if ((st = dalloc(c, &count, (size_t)c->ncell + 1))) return st;
-  if ((st = dalloc(c, &bad, 1))) return st;
-  if ((st = dalloc(c, &c->d_cell_start, (size_t)c->ncell + 1))) return st;
-  if ((st = dalloc(c, &c->d_cube, (size_t)n))) return st;
-  if ((st = dalloc(c, &c->d_cube_orig, (size_t)n))) return st;
-  if ((st = dalloc(c, &c->d_inv, (size_t)n))) return st;
+  if ((st = scratch(c, 3, (size_t)n, &cell))) return st;
+  if ((st = scratch(c, 4, (size_t)c->ncell + 1, &count))) return st;
+  if ((st = scratch(c, 5, 1, &bad))) return st;
+  if ((st = ensure(c, &c->d_cell_start, &c->cs_cap, (size_t)c->ncell + 1))) return st;
+  if ((st = ensure(c, &c->d_cube, &c->cube_cap, (size_t)n))) return st;
+  if ((st = ensure(c, &c->d_inv, &c->inv_cap, (size_t)n))) return st;
   PSOD_CUDA(c, cudaMemsetAsync(count, 0, sizeof(unsigned) * (c->ncell + 1), c->stream));
   PSOD_CUDA(c, cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
   const double xs = c->xxmin * c->scale;  // main:1565
-  k_cell_count<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_pos, n, (float)nx, xs, nx, cell, count, bad);
+  k_cell_count<<<nblk(n, 256), 256, 0, c->stream>>>(dpos, n, (float)nx, xs, nx, cell, count, bad);
   if ((st = scan_u32(c, count, c->d_cell_start, (long long)c->ncell, true))) return st;
   PSOD_CUDA(c, cudaMemsetAsync(count, 0, sizeof(unsigned) * c->ncell, c->stream));
-  k_cell_scatter<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_pos, n, cell, c->d_cell_start, count, c->d_cube,
+  k_cell_scatter<<<nblk(n, 256), 256, 0, c->stream>>>(dpos, n, cell, c->d_cell_start, count, c->d_cube,
                                                       c->d_inv);
   int hbad = 0;
   PSOD_CUDA(c, cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
-  dfree(&cell);
-  dfree(&count);
-  dfree(&bad);
   if (hbad) return set_err(c, PSOD_ERR_ARG, "particle positions must lie in [0,1] (box units)");
 
   // The reference's run scan (main:1591-1604) files a final cell holding a
@@ -359,7 +355,6 @@ int stage_cellsort(psod_ctx *c) {
       k_set_range<<<nblk((long long)(hi - lo), 256), 256, 0, c->stream>>>(c->d_cell_start, lo, hi, (unsigned)n);
     }
   }
-  PSOD_CUDA(c, cudaMemcpyAsync(c->d_cube_orig, c->d_cube, sizeof(float4) * n, cudaMemcpyDeviceToDevice, c->stream));
   PSOD_CUDA(c, cudaGetLastError());
   PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
   return PSOD_OK;
@@ -393,7 +388,7 @@ int stage_cic(psod_ctx *c, double *grid_out) {
     const int smem = CW3 * (int)sizeof(unsigned long long);
     PSOD_CUDA(c, cudaFuncSetAttribute(k_cic_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const long long ntiles = (long long)(c->nx / CT) * (c->nx / CT) * (c->nx / CT);
-    k_cic_tile<<<(unsigned)ntiles, 256, smem, c->stream>>>(c->d_cube_orig, c->d_cell_start, c->nx,
+    k_cic_tile<<<(unsigned)ntiles, 256, smem, c->stream>>>(c->d_cube, c->d_cell_start, c->nx,
                                                            c->xxmin * c->scale, k, c->d_rho, bad);
     int hbad = 0;
     PSOD_CUDA(c, cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -403,8 +398,8 @@ int stage_cic(psod_ctx *c, double *grid_out) {
   if (!tiled || grid_out) {
     if ((st = dalloc(c, &c->d_grid, (size_t)nnode))) return st;
     PSOD_CUDA(c, cudaMemsetAsync(c->d_grid, 0, sizeof(unsigned long long) * nnode, c->stream));
-    k_cic_deposit<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->d_cube_orig, c->n, k, c->d_grid);
-    if (!tiled) k_cic_interp<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->d_cube_orig, c->n, k, c->d_grid, c->d_rho);
+    k_cic_deposit<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->d_cube, c->n, k, c->d_grid);
+    if (!tiled) k_cic_interp<<<nblk(c->n, 256), 256, 0, c->stream>>>(c->d_cube, c->n, k, c->d_grid, c->d_rho);
   }
   c->cic_tiled = tiled;
   PSOD_CUDA(c, cudaGetLastError());

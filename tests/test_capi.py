@@ -54,6 +54,6 @@ def test_create_without_device_fails_cleanly():
 def test_invalid_params_rejected():
     lib = capi.load()
     h = C.c_void_p()
-    for kw in ({"ncut": 9}, {"nmin": 5}, {"nbins": 0}, {"nxbuffer": 2, "ncut": 4}):
+    for kw in ({"ncut": 9}, {"nmin": 5}, {"nbins": 0}, {"nxbuffer": 2, "ncut": 4}, {"nxbuffer": 16}):
         p = capi.default_params(16, **kw)
         assert lib.psod_ctx_create(C.byref(p), C.byref(h)) == capi.ERR_ARG
