@@ -145,7 +145,9 @@ def run_ours(args):
     wl = WORKLOADS.get(nx, dict(nmax_halo=20000, box=f"{nx}^3"))
     box = synth.make_box(nx, nmax_halo=wl["nmax_halo"], seed=args.seed + rank, device=f"cuda:{dev}")
     pos_d, ids_d = box.pos, box.ids
-    n = box.n
+    del box
+    torch.cuda.empty_cache()  # hand the generator's temporaries back before the engine allocates
+    n = int(pos_d.shape[0])
     params = dict(npu=npu_for(nx), mode=args.mode_id)
     if args.ndelta:
         params["delta_extra"] = (500.0, 178.0)

@@ -23,6 +23,13 @@ void free_scratch(psod_ctx *c) {
   c->scratch.clear();
 }
 
+void free_scratch_slot(psod_ctx *c, int id) {
+  if ((size_t)id < c->scratch.size() && c->scratch[id].first) {
+    cudaFree(c->scratch[id].first);
+    c->scratch[id] = {nullptr, 0};
+  }
+}
+
 bool is_device_ptr(const void *p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {

@@ -23,7 +23,6 @@
 #define PSOD_IDX_MASK 0x7fffffffu
 #define PSOD_INF_RANK 0xffffffffu
 #define PSOD_MAX_BINS 128
-#define PSOD_STATIC_MAX_NX 64
 
 namespace psod {
 
@@ -238,6 +237,7 @@ int scratch(psod_ctx *c, int id, size_t count, T **out) {
   return PSOD_OK;
 }
 void free_scratch(psod_ctx *c);
+void free_scratch_slot(psod_ctx *c, int id);
 
 bool is_device_ptr(const void *p);
 int copy_out(psod_ctx *c, void *dst, const void *dsrc, size_t bytes);

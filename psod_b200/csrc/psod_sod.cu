@@ -54,7 +54,8 @@ struct SodBufs {
   unsigned long long *nhalo;
   unsigned long long *pool_used;
   unsigned *h_rank;
-  long long *h_id, *h_mass, *h_mass2, *h_mextra, *h_profile;
+  long long *h_id, *h_mass, *h_mass2, *h_mextra;
+  unsigned *h_profile;         // cumulative counts (widened on output)
   float *h_center;
   double *h_rdelta;
   unsigned long long *h_pool;  // pool offset
@@ -81,6 +82,7 @@ struct SodBufs {
   // cand_pos, 256-candidate chunks and their exclusive prefix
   unsigned *cell_cnt, *cell_off, *cell_chunks, *chunk_pref;
   unsigned nitems_cells;           // 27 * nready
+  unsigned long long cand_cap;     // candidate buffer entries
   unsigned cap_ready;              // seeds processed per round at most
   int mode;
 };
@@ -637,6 +639,11 @@ __device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned
     B.st_cn[slot] = 0;
     B.processed[rank] = 1;
   }
+  // no refinement work unless this seed turns out active
+  if (threadIdx.x < 27) {
+    B.cell_cnt[slot * 27 + threadIdx.x] = 0;
+    B.cell_chunks[slot * 27 + threadIdx.x] = 0;
+  }
   const SeedGeo g = seed_geo(K, B, rank);
   if (__float_as_uint(B.cube[g.sp].w) & PSOD_DEAD_BIT) return;  // claimed (main:1628)
   unsigned na = 0;
@@ -695,14 +702,22 @@ __device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned
       tot += s_cnt[o];
     }
     s_base = atomicAdd(B.cand_used, tot);
-    B.st_na[slot] = na;  // 0 when unknown (batched modes)
-    B.st_coff[slot] = s_base;
-    B.st_cn[slot] = tot;
-    B.st_active[slot] = 1;
-    B.st_centre[slot] = g.sp;  // no candidate: the seed stays the centre
-    atomicAdd(B.nprocessed, 1ull);
+    if ((unsigned long long)s_base + tot > B.cand_cap) {
+      // candidate buffer full this round: the seed waits for the next one
+      s_base = 0xffffffffu;
+      B.processed[rank] = 0;
+      if (tot > B.cand_cap) record_error(B, rank, PSOD_ERR_STATE);
+    } else {
+      B.st_na[slot] = na;  // 0 when unknown (batched modes)
+      B.st_coff[slot] = s_base;
+      B.st_cn[slot] = tot;
+      B.st_active[slot] = 1;
+      B.st_centre[slot] = g.sp;  // no candidate: the seed stays the centre
+      atomicAdd(B.nprocessed, 1ull);
+    }
   }
   __syncthreads();
+  if (s_base == 0xffffffffu) return;
   if (threadIdx.x < 27) {
     B.cell_cnt[slot * 27 + threadIdx.x] = s_cnt[threadIdx.x];
     B.cell_off[slot * 27 + threadIdx.x] = s_base + s_coff[threadIdx.x];
@@ -1421,6 +1436,13 @@ __global__ void k_gather(const T *src, const unsigned *order, long long n, int w
   dst[i] = src[(long long)order[h] * width + k];
 }
 
+__global__ void k_gather_widen(const unsigned *src, const unsigned *order, long long n, int width, long long *dst) {
+  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * width) return;
+  long long h = i / width, k = i % width;
+  dst[i] = (long long)src[(long long)order[h] * width + k];
+}
+
 __global__ void k_mass_u32(const long long *mass, long long n, unsigned *out) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = (unsigned)mass[i];
@@ -1627,6 +1649,8 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   const long long nblocks = (long long)nb * nb * nb;
   const int rb = (rdep + bs - 1) / bs;
   const long long hcap = std::max<long long>(1, n / std::max(1, c->p.nmin) + 1);
+  // refinement candidates held per round (seeds that do not fit wait a round)
+  const long long cand_cap = std::min<long long>(n, 128ll << 20);
   const int ne = std::max(1, c->p.ndelta_extra);
 
   unsigned *block_of, *blist, *bbegin, *cursor, *head, *filt_a, *filt_b, *ready, *ctrs, *counts;
@@ -1634,7 +1658,8 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   unsigned long long *u64s, *h_pool, *pool_key;
   double *edge_fac, *h_rdelta, *cand_s;
   unsigned *h_rank, *pool_idx, *st_active, *st_na, *st_coff, *st_cn, *st_centre, *cand_pos, *cand_slot;
-  long long *h_id, *h_mass, *h_mass2, *h_mextra, *h_profile;
+  long long *h_id, *h_mass, *h_mass2, *h_mextra;
+  unsigned *h_profile;
   float *h_center;
   if ((rc = scratch(c, SC_BLOCK_OF, (size_t)nseed + 1, &block_of)) || (rc = scratch(c, SC_BLIST, (size_t)nseed + 1, &blist)) ||
       (rc = scratch(c, SC_BBEGIN, (size_t)nblocks + 1, &bbegin)) || (rc = scratch(c, SC_CURSOR, (size_t)nblocks + 1, &cursor)) ||
@@ -1650,8 +1675,8 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       (rc = scratch(c, SC_POOLKEY, (size_t)n, &pool_key)) || (rc = scratch(c, SC_POOLIDX, (size_t)n, &pool_idx)) ||
       (rc = scratch(c, SC_ST_ACTIVE, (size_t)nblocks + 1, &st_active)) || (rc = scratch(c, SC_ST_NA, (size_t)nblocks + 1, &st_na)) ||
       (rc = scratch(c, SC_ST_COFF, (size_t)nblocks + 1, &st_coff)) || (rc = scratch(c, SC_ST_CN, (size_t)nblocks + 1, &st_cn)) ||
-      (rc = scratch(c, SC_ST_CENTRE, (size_t)nblocks + 1, &st_centre)) || (rc = scratch(c, SC_CAND_POS, (size_t)n, &cand_pos)) ||
-      (rc = scratch(c, SC_CAND_SLOT, (size_t)n, &cand_slot)) || (rc = scratch(c, SC_CAND_S, (size_t)n, &cand_s)))
+      (rc = scratch(c, SC_ST_CENTRE, (size_t)nblocks + 1, &st_centre)) || (rc = scratch(c, SC_CAND_POS, (size_t)cand_cap, &cand_pos)) ||
+      (rc = scratch(c, SC_CAND_SLOT, (size_t)cand_cap, &cand_slot)) || (rc = scratch(c, SC_CAND_S, (size_t)cand_cap, &cand_s)))
     return rc;
   // seeds per round at most (bounds the per-round buffers)
   const unsigned cap_ready = (unsigned)std::min<long long>(nblocks + 1, 1ll << 20);
@@ -1727,6 +1752,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.ready = ready;
   B.nready = nready_d;
   B.cap_ready = cap_ready;
+  B.cand_cap = (unsigned long long)cand_cap;
   B.cell_cnt = cell_cnt;
   B.cell_off = cell_off;
   B.cell_chunks = cell_chunks;
@@ -1896,8 +1922,8 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     k_gather<float><<<nblk(nh * 3, 256), 256, 0, c->stream>>>(h_center, order, nh, 3, c->d_h_center);
     if (c->p.ndelta_extra > 0)
       k_gather<long long><<<nblk(nh * ne, 256), 256, 0, c->stream>>>(h_mextra, order, nh, ne, c->d_h_mextra);
-    k_gather<long long><<<nblk(nh * c->p.nbins, 256), 256, 0, c->stream>>>(h_profile, order, nh, c->p.nbins,
-                                                                           c->d_h_profile);
+    k_gather_widen<<<nblk(nh * c->p.nbins, 256), 256, 0, c->stream>>>(h_profile, order, nh, c->p.nbins,
+                                                                      c->d_h_profile);
     k_widen<<<g1, 256, 0, c->stream>>>(rkeys, nh, c->d_h_rank);
     k_mass_u32<<<g1, 256, 0, c->stream>>>(c->d_h_mass, nh, mass32);
     if ((rc = scan_u32(c, mass32, moff, nh, true))) return rc;

@@ -322,6 +322,9 @@ int stage_cellsort(psod_ctx *c, const float *dpos) {
   int hbad = 0;
   PSOD_CUDA(c, cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+  // the per-particle cell ids and per-cell counts are only needed here
+  free_scratch_slot(c, 3);
+  free_scratch_slot(c, 4);
   if (hbad) return set_err(c, PSOD_ERR_ARG, "particle positions must lie in [0,1] (box units)");
 
   // The reference's run scan (main:1591-1604) files a final cell holding a
