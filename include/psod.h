@@ -168,6 +168,27 @@ int psod_get_halos(psod_ctx *ctx, const psod_halo_table *t);
 /* Convenience: cic, cicm1, tri_cic and spherover in one call. */
 int psod_run(psod_ctx *ctx, psod_run_stats *stats);
 
+/* CIC density (cic + cicm1, the same fixed-point arithmetic) for a zone of
+ * at most 64 cells per side, without any device allocation.  This entry
+ * point has no counterpart in the reference.  It is for callers that cannot
+ * let the library allocate device memory: code recording a stream into a
+ * CUDA graph (cudaMalloc is not allowed during capture), and host codes that
+ * size all device memory themselves and forbid libraries from allocating.
+ * The node grid is a file-scope device array of (2*64)^3 int64 (16 MiB)
+ * that every device loading the library holds until exit.
+ *   pos      device, xyz-interleaved float32 box units [0,1], n particles
+ *   rho      device, n doubles, input order (as psod_cicm1)
+ *   bad_flag device int or NULL: set to 1 when a position lies outside
+ *            [0,1] (that particle is skipped and gets rho = 0), else 0
+ *   stream   cudaStream_t as void* (NULL: legacy default stream)
+ * Work is enqueued on the stream and not waited for.  Returns PSOD_ERR_ARG
+ * for nx > 64, nxbuffer >= nx or host pointers.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  All calls share the array, so
+ * calls that overlap on the GPU race: serialise them. */
+int psod_cic_rho_static(int64_t n, const float *pos, int32_t nx, int64_t npart_total, int32_t nxbuffer,
+                        double *rho, int *bad_flag, void *stream);
+
 const char *psod_last_error(const psod_ctx *ctx);
 const char *psod_status_string(int status);
 int psod_abi_version(void);

@@ -106,6 +106,7 @@ EXPORTS = [
     "psod_halo_count",
     "psod_get_halos",
     "psod_last_error",
+    "psod_cic_rho_static",
 ]
 
 _lib = None
@@ -145,6 +146,7 @@ def load(build_if_missing: bool = True):
     L.psod_halo_count.argtypes = [vp, P(C.c_int64), P(C.c_int64)]
     L.psod_get_halos.argtypes = [vp, P(HaloTable)]
     L.psod_last_error.argtypes = [vp]
+    L.psod_cic_rho_static.argtypes = [C.c_int64, vp, C.c_int32, C.c_int64, C.c_int32, vp, vp, vp]
     L.psod_last_error.restype = C.c_char_p
     for name in EXPORTS:
         L[name].restype = L[name].restype if name in ("psod_status_string", "psod_last_error", "psod_params_default") else C.c_int

@@ -23,6 +23,7 @@
 #define PSOD_IDX_MASK 0x7fffffffu
 #define PSOD_INF_RANK 0xffffffffu
 #define PSOD_MAX_BINS 128
+#define PSOD_STATIC_MAX_NX 64  // zone limit of psod_cic_rho_static
 
 namespace psod {
 
