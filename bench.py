@@ -180,6 +180,7 @@ def run_ours(args):
     ms = ev0.elapsed_time(ev1) / args.steps
     ms = max_over_ranks(ms, world)
     nhalo = stats_list[-1]["nhalo"]
+    stage_ms = time_stages(sod, pos_d, ids_d)
 
     # e2e: pinned host buffers through the C-ABI, copies inside the timed region
     pos_h = pos_d.cpu().pin_memory()
@@ -202,13 +203,18 @@ def run_ours(args):
 
     s = stats_list[-1]
     peak, peak_kind = load_peaks()
-    # dominant kernel: the per-seed SOD kernel.  Algorithmic bytes: one
-    # 16-byte record per particle of each examined seed's preselect cube
-    # (count pass), plus the claim (4 B) and member (12 B) writes.
-    alg_bytes = 16.0 * s["touched"] + 4.0 * n * 0 + 16.0 * s["nmember"]
-    kern_s = s["ms_sod_kernel"] / 1000.0
-    achieved = alg_bytes / kern_s / 1e9 if kern_s > 0 else 0.0
+    # Gather/distance kernel (k_cross): HBM-bound.  Algorithmic bytes: 16 B
+    # per record of the cube cells meeting each ball out to its stopping
+    # particle, plus 12 B per member written (d2 key + index).
+    alg_bytes = 16.0 * s["cross_touch"] + 12.0 * s["nmember"]
+    cross_s = s["ms_cross"] / 1000.0
+    achieved = alg_bytes / cross_s / 1e9 if cross_s > 0 else 0.0
+    launches = max(1, s["rounds"])
+    traffic = load_traffic("k_cross")
     value = world * nhalo / (ms / 1000.0)
+    # the refinement kernel dominates: FP32 pair tests fed from shared memory
+    ref_s = s["ms_refine"] / 1000.0
+    pairs_per_s = s["refine_pairs"] / ref_s if ref_s > 0 else 0.0
     line = {
         "metric": "SOD halos/s (delta=200, N200 exact)",
         "value": round(value, 2),
@@ -228,11 +234,14 @@ def run_ours(args):
             "particles": n,
             "mode": args.mode,
             "npu": params["npu"],
+            "delta": [200.0, 500.0, 178.0] if args.ndelta else [200.0],
             "halos": nhalo,
             "members": s["nmember"],
             "seeds": s["npart_new"],
             "processed_seeds": s["nprocessed"],
             "rounds": s["rounds"],
+            "stage_ms": {k: round(v, 2) for k, v in stage_ms.items()},
+            "sod_phase_ms": {k: round(s[k], 2) for k in ("ms_sched", "ms_prep", "ms_refine", "ms_select", "ms_cross")},
             "l2": "flushed between steps" if need_flush else "inputs larger than L2",
             "parallelism": f"replicas x{world}",
         },
@@ -243,21 +252,32 @@ def run_ours(args):
             "d2h_bytes_per_step": int(d2h),
             "ms_per_step": round(e2e_ms, 3),
         },
-        "gpu_launches": int(s["kernel_launches"]),
+        "gpu_launches": int(s["kernel_launches"]) + 12,
         "roofline": {
             "bound": "hbm",
-            "kernel": "k_sod_seeds",
+            "kernel": "k_cross (radial gather, distances, crossing, profile, claims)",
             "achieved": round(achieved, 1),
             "peak": peak,
             "unit": "GB/s",
             "frac": round(achieved / peak, 4),
             "peak_kind": peak_kind,
-            "traffic": None,
-            "sod_kernel_ms": round(s["ms_sod_kernel"], 3),
-            "sod_stage_ms": round(s["ms_total"], 3),
+            "traffic": traffic,
+            "launches": launches,
+            "alg_bytes_per_launch": int(alg_bytes / launches),
+            "kernel_ms": round(s["ms_cross"], 3),
+        },
+        "refine": {
+            "kernel": "k_refine_warp (dominant: FP32 pair tests from shared memory)",
+            "pairs": int(s["refine_pairs"]),
+            "pairs_per_s": round(pairs_per_s, 1),
+            "lane_utilization": round(s["refine_pairs"] / max(1, s["refine_slots"]), 4),
+            "kernel_ms": round(s["ms_refine"], 3),
         },
         "clocks": clk.summary(),
     }
+    if args.compare_plain and args.mode != "plain" and world == 1:
+        line["plain"] = plain_reference(args, nx, params, pos_d, ids_d, sod)
+        line["vs_plain"] = round(line["plain"]["ms_per_step"] / ms, 3)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, nx, wl, quick=True)
     sod.close()
@@ -269,41 +289,106 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
-def _cpu_sample(seed, nx, nmax):
-    """One sample box through the oracle's reference arithmetic."""
+def load_traffic(kernel):
+    """DRAM bytes per launch of a kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get(kernel)
+    return None
+
+
+def time_stages(sod, pos, ids):
+    """Device time of each stage of one step (CUDA events, current stream)."""
+    import torch
+
+    out = {}
+    for name, fn in (("load", lambda: sod.load(pos, ids)), ("cic", lambda: sod.cic()),
+                     ("cicm1", lambda: sod.cicm1(want_rho=False)), ("tri_cic", lambda: sod.tri_cic(want_isort=False)),
+                     ("spherover", lambda: sod.spherover())):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        torch.cuda.synchronize()
+        out[name] = a.elapsed_time(b)
+    return out
+
+
+def plain_reference(args, nx, params, pos_d, ids_d, sod):
+    """The same box through the plain GPU path (one launch per phase and
+    round, full-cube gathers), one untimed and one timed step."""
+    import torch
+
+    from psod_b200.sod import SphericalOverdensity
+
+    sod.close()
+    torch.cuda.empty_cache()
+    p = dict(params)
+    p["mode"] = 0
+    sp = SphericalOverdensity(nx, device=torch.cuda.current_device(), **p)
+    sp.load(pos_d, ids_d)
+    sp.run()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    sp.load(pos_d, ids_d)
+    st = sp.run()
+    b.record()
+    torch.cuda.synchronize()
+    msp = a.elapsed_time(b)
+    sp.close()
+    return {"mode": "plain", "ms_per_step": round(msp, 3), "halos": st["nhalo"],
+            "value": round(st["nhalo"] / (msp / 1000.0), 2), "unit": "halos/s",
+            "sod_phase_ms": {k: round(st[k], 2) for k in ("ms_sched", "ms_prep", "ms_refine", "ms_select", "ms_cross")}}
+
+
+def _cpu_sample(seed, nx, nmax, npu):
+    """One sample box through the oracle's reference arithmetic, with the
+    parameters -npu derives (main:211-219)."""
+    import math
+
     from oracle import oracle as O
     from psod_b200 import synth
 
     b = synth.make_box(nx, nmax_halo=nmax, seed=seed)
+    kw = {}
+    if npu > 0:
+        ncut = math.ceil(((npu * 2.0 / 200.0) ** (1.0 / 3.0)) / 2.0)
+        kw = dict(ncut=ncut, nxbuffer=4 * ncut, nsel=math.ceil((2 * ncut + 1.0) ** 3 * 200.0 * 4.0))
     t0 = time.perf_counter()
-    r = O.run(O.Params(nx=nx), b.pos, b.ids, O.REFERENCE)
+    r = O.run(O.Params(nx=nx, **kw), b.pos, b.ids, O.REFERENCE)
     return r.nhalo, time.perf_counter() - t0
 
 
-def cpu_baseline(args, nx, wl, quick=False, cores=None):
-    """The reference algorithm on host cores: one sample box per core."""
+def cpu_baseline(args, nx, wl, quick=False, cores=None, nsamples=None):
+    """The reference algorithm on host cores: sample boxes of 64^3 cells with
+    the workload's generator law (same halo mass range and -npu), one per core."""
     import multiprocessing as mp
 
     from oracle import oracle as O
 
     O.build()
-    snx = 64 if quick else 96
-    nmax = 5000 if quick else 10000
+    snx = 64
+    nmax = wl["nmax_halo"]
+    npu = npu_for(nx)
     ncores = 1 if quick else (cores or os.cpu_count() or 1)
+    ns = nsamples or (2 if quick else ncores)
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(ncores) as pool:
-        res = pool.starmap(_cpu_sample, [(args.seed + 100 + i, snx, nmax) for i in range(ncores)])
+        res = pool.starmap(_cpu_sample, [(args.seed + 100 + i, snx, nmax, npu) for i in range(ns)])
     wall = time.perf_counter() - t0
     halos = sum(r[0] for r in res)
-    busy = max(r[1] for r in res)
+    busy = sum(r[1] for r in res) / ncores if quick else wall
     return {
         "value": round(halos / busy, 3),
         "unit": "halos/s",
         "cores": ncores,
         "kind": "port",
-        "sample": f"{ncores} box(es) of {snx}^3 with the same generator (halo N in [20, {nmax}]), "
-                  f"full cic/cicm1/tri_cic/spherover, reference arithmetic; wall {wall:.1f}s",
+        "sample": f"{ns} box(es) of {snx}^3 cells from the same generator (halo N in [20, {nmax}], npu {npu}), "
+                  f"full cic/cicm1/tri_cic/spherover in reference arithmetic, {halos} halos; wall {wall:.1f}s",
     }
 
 
@@ -316,10 +401,11 @@ def run_reference(args):
     wl = WORKLOADS.get(nx, dict(nmax_halo=20000, box=f"{nx}^3"))
     vals = []
     cb = None
-    for i in range(args.warmup + args.steps):
+    for i in range(args.warmup):  # warm-up: one small sample on one core
+        cpu_baseline(args, nx, wl, quick=True, nsamples=1)
+    for i in range(args.steps):
         cb = cpu_baseline(args, nx, wl, quick=False)
-        if i >= args.warmup:
-            vals.append(cb["value"])
+        vals.append(cb["value"])
     v = sum(vals) / len(vals)
     line = {
         "impl": "reference",
@@ -349,7 +435,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nx", type=int, default=1024)
-    ap.add_argument("--mode", default="plain", choices=["plain", "batched", "learned"])
+    ap.add_argument("--mode", default="batched", choices=["plain", "batched", "learned"])
+    ap.add_argument("--no-compare-plain", dest="compare_plain", action="store_false")
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--ndelta", action="store_true", help="Delta = 200, 500, 178 and 48 bins (config 3)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

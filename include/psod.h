@@ -117,7 +117,10 @@ typedef struct psod_run_stats {
   double ms_select;      /* exact contender sums + argmax */
   double ms_cross;       /* crossing, profile, claims */
   int64_t ncandidates;   /* refinement candidates */
-  int64_t refine_pairs;  /* candidate-neighbour records visited */
+  int64_t refine_pairs;  /* candidate-neighbour pairs tested */
+  int64_t cross_touch;   /* records of the cube cells meeting each ball out to
+                            its stopping particle (algorithmic reads) */
+  int64_t refine_slots;  /* lane slots spent on refinement pair tests */
 } psod_run_stats;
 
 typedef struct psod_ctx psod_ctx;
@@ -125,7 +128,9 @@ typedef struct psod_ctx psod_ctx;
 void psod_params_default(psod_params *p);
 
 /* Create a context on p->device.  Validates the parameters the way the
- * reference driver does (main:386-397): nxbuffer >= ncut, nxbuffer <= nx. */
+ * reference driver does (main:386-397): nxbuffer >= ncut; and nxbuffer < nx
+ * (the reference also allows nxbuffer == nx, where its CIC array is padded
+ * past the periodic grid; that case is refused here). */
 int psod_ctx_create(const psod_params *p, psod_ctx **out);
 int psod_ctx_destroy(psod_ctx *ctx);
 

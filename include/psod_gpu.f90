@@ -45,7 +45,7 @@ module psod_gpu
      real(c_double)     :: ms_total, ms_sod_kernel
      integer(c_int64_t) :: sod_launches, kernel_launches
      real(c_double)     :: ms_sched, ms_prep, ms_refine, ms_select, ms_cross
-     integer(c_int64_t) :: ncandidates, refine_pairs
+     integer(c_int64_t) :: ncandidates, refine_pairs, cross_touch, refine_slots
   end type psod_run_stats
 
   interface

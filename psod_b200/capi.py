@@ -84,6 +84,8 @@ class RunStats(C.Structure):
         ("ms_cross", C.c_double),
         ("ncandidates", C.c_int64),
         ("refine_pairs", C.c_int64),
+        ("cross_touch", C.c_int64),
+        ("refine_slots", C.c_int64),
     ]
 
     def as_dict(self):

@@ -30,6 +30,7 @@ namespace psod {
 namespace {
 
 constexpr int TPB = 256;          // threads per seed CTA
+constexpr unsigned RN_CHUNK = 2048;  // neighbour records per refinement work item
 constexpr int NWARP = TPB / 32;
 constexpr int NB = 4096;          // histogram buckets per level
 constexpr int MAXLEV = 4;         // histogram levels kept in shared memory
@@ -77,10 +78,13 @@ struct SodBufs {
   unsigned *work;       // [4] work-stealing counters: prep, refine, select, cross
   unsigned *alive_cnt;  // alive records per cell (batched modes)
   unsigned long long *pairs;       // candidate-neighbour records visited
+  unsigned long long *touch;       // records of the balls out to each stop
+  unsigned long long *pair_slots;  // lane slots spent on pair tests
   unsigned long long *ncand_total; // candidates over all rounds
   // refinement work: per (ready slot, candidate cell) counts, offsets into
   // cand_pos, 256-candidate chunks and their exclusive prefix
   unsigned *cell_cnt, *cell_off, *cell_chunks, *chunk_pref;
+  unsigned *cell_nch;              // neighbour chunks per candidate cell
   unsigned nitems_cells;           // 27 * nready
   unsigned long long cand_cap;     // candidate buffer entries
   unsigned cap_ready;              // seeds processed per round at most
@@ -224,6 +228,39 @@ __device__ __forceinline__ void for_region(const SodConst &K, const SodBufs &B, 
       for (unsigned p = b + lane; p < e; p += 32) f(p, B.cube[p]);
     }
   }
+}
+
+// Records filed under the region's cells (alive or not), from the cell
+// offsets alone (no record loads).  For the ball out to the stopping
+// particle this is the algorithmic read volume of the crossing search.
+__device__ unsigned region_records(const SodConst &K, const SodBufs &B, const Region &G) {
+  const int R = K.ncut, side = 2 * R + 1, nrow = side * side;
+  const unsigned nx = (unsigned)K.nx;
+  const double nxd = (double)K.nx;
+  auto rel = [&](double x, int i) {
+    double d = x - ((double)i + K.xs + 0.5);
+    d = d - nxd * floor(d / nxd + 0.5);
+    return d;
+  };
+  const double tx = rel(G.xc, G.ic), ty = rel(G.yc, G.jc), tz = rel(G.zc, G.kc);
+  const double rm2 = G.rb * G.rb;
+  unsigned sum = 0;
+  for (int row = threadIdx.x; row < nrow; row += TPB) {
+    const int dj = row % side - R, dk = row / side - R;
+    const double gy = cell_gap(ty, dj, nxd), gz = cell_gap(tz, dk, nxd);
+    const double rem = rm2 - gy * gy - gz * gz;
+    if (rem < 0.0) continue;
+    const double wx = sqrt(rem);
+    const int t0 = max((int)ceil(tx - 0.5 - wx), -R), t1 = min((int)floor(tx + 0.5 + wx), R);
+    if (t0 > t1) continue;
+    const unsigned jj = (unsigned)wrapi(G.jc + dj, K.nx), kk = (unsigned)wrapi(G.kc + dk, K.nx);
+    const unsigned long long base = (unsigned long long)nx * (jj + (unsigned long long)nx * kk);
+    for (int t = t0; t <= t1; t++) {
+      const unsigned c = (unsigned)wrapi(G.ic + t, K.nx);
+      sum += B.cs[base + c + 1] - B.cs[base + c];
+    }
+  }
+  return sum;
 }
 
 // d2 of a record to the region's centre if it is alive and inside the
@@ -719,9 +756,28 @@ __device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned
   __syncthreads();
   if (s_base == 0xffffffffu) return;
   if (threadIdx.x < 27) {
-    B.cell_cnt[slot * 27 + threadIdx.x] = s_cnt[threadIdx.x];
-    B.cell_off[slot * 27 + threadIdx.x] = s_base + s_coff[threadIdx.x];
-    B.cell_chunks[slot * 27 + threadIdx.x] = (s_cnt[threadIdx.x] + 31u) / 32u;
+    const int o = threadIdx.x;
+    const int ci = wrapi(g.ic + o / 9 - 1, K.nx), cj = wrapi(g.jc + (o / 3) % 3 - 1, K.nx),
+              ck = wrapi(g.kc + o % 3 - 1, K.nx);
+    // records of the 3x3x3 cells around this candidate cell
+    unsigned nbr = 0;
+    for (int r = 0; r < 9; r++) {
+      const unsigned yy = (unsigned)wrapi(cj + r % 3 - 1, K.nx), zz = (unsigned)wrapi(ck + r / 3 - 1, K.nx);
+      const unsigned long long base = (unsigned long long)K.nx * (yy + (unsigned long long)K.nx * zz);
+      const int x0 = ci - 1, x1 = ci + 1;
+      if (x0 < 0) {
+        nbr += B.cs[base + K.nx] - B.cs[base + (unsigned)(x0 + K.nx)] + B.cs[base + (unsigned)x1 + 1] - B.cs[base];
+      } else if (x1 >= K.nx) {
+        nbr += B.cs[base + K.nx] - B.cs[base + (unsigned)x0] + B.cs[base + (unsigned)(x1 - K.nx) + 1] - B.cs[base];
+      } else {
+        nbr += B.cs[base + (unsigned)x1 + 1] - B.cs[base + (unsigned)x0];
+      }
+    }
+    const unsigned nch = max(1u, (nbr + RN_CHUNK - 1) / RN_CHUNK);
+    B.cell_cnt[slot * 27 + o] = s_cnt[o];
+    B.cell_off[slot * 27 + o] = s_base + s_coff[o];
+    B.cell_nch[slot * 27 + o] = nch;
+    B.cell_chunks[slot * 27 + o] = ((s_cnt[o] + 31u) / 32u) * nch;
   }
   for (int o = w; o < 27; o += NWARP) {
     const int di = o / 9 - 1, dj = (o / 3) % 3 - 1, dk = o % 3 - 1;
@@ -737,6 +793,9 @@ __device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned
         const unsigned at = q + __popc(m & ((1u << lane) - 1u));
         B.cand_pos[at] = p;
         B.cand_slot[at] = slot;
+        // refinement partial sums accumulate here; the foreign-filed
+        // particle always goes to the exact pass
+        B.cand_s[at] = (K.has_quirk && p == K.quirk_pos) ? __longlong_as_double(0x7ff0000000000000ll) : 0.0;
       }
       q += __popc(m);
     }
@@ -854,49 +913,68 @@ __device__ void refine_sum(const SodConst &K, const SodBufs &B, unsigned cp, int
 // the partial sums in FP64, so |S_approx - S| <= 3e-6 S < REF_TOL S.  Dead
 // records are parked at 1e30 so they never pass the inclusion test.
 template <bool WRAPFREE>
+__device__ __forceinline__ float pair_term(const float4 nb, float cx, float cy, float cz, float e2f,
+                                           const SodConst &K) {
+  float dx, dy, dz;
+  if (WRAPFREE) {
+    dx = __fsub_rn(nb.x, cx);
+    dy = __fsub_rn(nb.y, cy);
+    dz = __fsub_rn(nb.z, cz);
+  } else {
+    dx = mi_dx(nb.x, cx, K.nxf);
+    dy = mi_dx(nb.y, cy, K.nxf);
+    dz = mi_dx(nb.z, cz, K.nxf);
+  }
+  const float d2 = fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz)));
+  bool in = d2 <= 0.99999f;
+  if (!in && d2 <= 1.00001f)
+    in = min_image_d2((double)nb.x, (double)nb.y, (double)nb.z, (double)cx, (double)cy, (double)cz, K.tx) <= K.rmin2;
+  return in ? rsqrtf(__fadd_rn(d2, e2f)) : 0.f;
+}
+
+// sum of the terms of nt (<= 32) staged records; four independent FP32
+// partials of at most 8 terms each, added in FP64
+template <bool WRAPFREE>
 __device__ __forceinline__ double tile_terms(const float4 *tile, unsigned nt, float cx, float cy, float cz,
                                              const SodConst &K) {
   const float e2f = (float)K.eps2;
-  double sum = 0.0;
-  for (unsigned j0 = 0; j0 < nt; j0 += 32) {
-    const unsigned j1 = min(nt, j0 + 32);
-    float part = 0.f;
-    for (unsigned j = j0; j < j1; j++) {
-      const float4 nb = tile[j];
-      float dx, dy, dz;
-      if (WRAPFREE) {
-        dx = __fsub_rn(nb.x, cx);
-        dy = __fsub_rn(nb.y, cy);
-        dz = __fsub_rn(nb.z, cz);
-      } else {
-        dx = mi_dx(nb.x, cx, K.nxf);
-        dy = mi_dx(nb.y, cy, K.nxf);
-        dz = mi_dx(nb.z, cz, K.nxf);
-      }
-      const float d2 = fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz)));
-      bool in = d2 <= 0.99999f;
-      if (!in && d2 <= 1.00001f)
-        in = min_image_d2((double)nb.x, (double)nb.y, (double)nb.z, (double)cx, (double)cy, (double)cz, K.tx) <= K.rmin2;
-      if (in) part += rsqrtf(__fadd_rn(d2, e2f));
+  if (nt == 32) {
+    float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+#pragma unroll
+    for (int j = 0; j < 32; j += 4) {
+      p0 += pair_term<WRAPFREE>(tile[j], cx, cy, cz, e2f, K);
+      p1 += pair_term<WRAPFREE>(tile[j + 1], cx, cy, cz, e2f, K);
+      p2 += pair_term<WRAPFREE>(tile[j + 2], cx, cy, cz, e2f, K);
+      p3 += pair_term<WRAPFREE>(tile[j + 3], cx, cy, cz, e2f, K);
     }
-    sum += (double)part;
+    return ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
   }
-  return sum;
+  double sum = 0.0;
+  float part = 0.f;
+  for (unsigned j = 0; j < nt; j++) {
+    part += pair_term<WRAPFREE>(tile[j], cx, cy, cz, e2f, K);
+    if ((j & 7) == 7) {
+      sum += (double)part;
+      part = 0.f;
+    }
+  }
+  return sum + (double)part;
 }
 
-// Warp-level work item: up to 32 candidates of one candidate cell, a lane
-// each.  The records of the cell's 3x3x3 neighbourhood pass through a
-// warp-private shared slice, 32 at a time, and every lane reads each one by
-// broadcast; warps never wait on one another.
+// Work item: up to 32 candidates of one candidate cell (a lane each) against
+// one chunk of RN_CHUNK records of the cell's 3x3x3 neighbourhood.  Records
+// pass through a warp-private shared slice, 32 at a time, and every lane
+// reads each one by broadcast; warps never wait on one another.  Partial
+// sums of a candidate's neighbour chunks are added into cand_s.
 __global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
   __shared__ float4 s_tile[8][32];
   __shared__ unsigned s_rb[8][18], s_rp[8][19];
   __shared__ int s_nr[8], s_wf[8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned nitems = B.chunk_pref[B.nitems_cells];
-  unsigned long long visits = 0;
+  unsigned long long visits = 0, slots = 0;
   while (true) {
-    unsigned item = 0, ci = 0, chunk = 0;
+    unsigned item = 0, ci = 0, rem = 0;
     if (lane == 0) {
       item = atomicAdd(&B.work[1], 1u);
       if (item < nitems) {
@@ -907,13 +985,15 @@ __global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
           else hi = mid;
         }
         ci = lo;
-        chunk = item - B.chunk_pref[lo];
+        rem = item - B.chunk_pref[lo];
       }
     }
     item = __shfl_sync(0xffffffffu, item, 0);
     if (item >= nitems) break;
     ci = __shfl_sync(0xffffffffu, ci, 0);
-    chunk = __shfl_sync(0xffffffffu, chunk, 0);
+    rem = __shfl_sync(0xffffffffu, rem, 0);
+    const unsigned nch = B.cell_nch[ci];
+    const unsigned chunk = rem / nch, nchunk = rem % nch;
     const unsigned slot = ci / 27, o = ci % 27;
     const SeedGeo g = seed_geo(K, B, B.ready[slot]);
     const int di = (int)(o / 9) - 1, dj = (int)((o / 3) % 3) - 1, dk = (int)(o % 3) - 1;
@@ -967,23 +1047,51 @@ __global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
     const unsigned total = s_rp[w][nr];
     const bool wf = s_wf[w];
     const bool active = have && !quirk;
+    const unsigned r0 = nchunk * RN_CHUNK, r1 = min(total, r0 + RN_CHUNK);
+    const unsigned lt = (1u << lane) - 1u;
     double sum = 0.0;
-    for (unsigned base = 0; base < total; base += 32) {
-      const unsigned ff = base + (unsigned)lane;
-      if (ff < total) {
-        int r = 0;
-        while (s_rp[w][r + 1] <= ff) r++;
-        const float4 v = B.cube[s_rb[w][r] + (ff - s_rp[w][r])];
-        s_tile[w][lane] = (__float_as_uint(v.w) & PSOD_DEAD_BIT)
-                              ? make_float4(1e30f, 1e30f, 1e30f, 0.f)
-                              : make_float4(to_grid(v.x, K.nxf), to_grid(v.y, K.nxf), to_grid(v.z, K.nxf), 0.f);
+    unsigned pos = r0;  // next record of the chunk to load
+    unsigned fill = 0;  // alive records staged in the tile
+    while (pos < r1 || fill > 0) {
+      // stage alive records only: claimed ones are skipped by a warp-wide
+      // compaction, so they cost a load but no pair tests
+      while (fill < 32 && pos < r1) {
+        const unsigned ff = pos + (unsigned)lane;
+        bool alive = false;
+        float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ff < r1) {
+          int r = 0;
+          while (s_rp[w][r + 1] <= ff) r++;
+          const float4 v = B.cube[s_rb[w][r] + (ff - s_rp[w][r])];
+          alive = !(__float_as_uint(v.w) & PSOD_DEAD_BIT);
+          rec = make_float4(to_grid(v.x, K.nxf), to_grid(v.y, K.nxf), to_grid(v.z, K.nxf), 0.f);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, alive);
+        const unsigned need = 32u - fill, rank = __popc(m & lt);
+        if (alive && rank < need) s_tile[w][fill + rank] = rec;
+        const unsigned got = __popc(m);
+        if (got <= need) {
+          fill += got;
+          pos += 32u;
+        } else {
+          // the need-th alive lane is the last one taken; resume after it
+          const unsigned mk = __ballot_sync(0xffffffffu, alive && rank == need - 1);
+          pos += (unsigned)__ffs(mk);  // lane index + 1
+          fill = 32u;
+        }
+      }
+      if (pos > r1) pos = r1;
+      __syncwarp();
+      if (active && fill > 0)
+        sum += wf ? tile_terms<true>(s_tile[w], fill, cx, cy, cz, K) : tile_terms<false>(s_tile[w], fill, cx, cy, cz, K);
+      if (lane == 0) {
+        visits += (unsigned long long)min(32u, cnt - chunk * 32u) * fill;
+        slots += 32ull * fill;
       }
       __syncwarp();
-      const unsigned nt = min(32u, total - base);
-      if (active) sum += wf ? tile_terms<true>(s_tile[w], nt, cx, cy, cz, K) : tile_terms<false>(s_tile[w], nt, cx, cy, cz, K);
-      __syncwarp();
+      fill = 0;
     }
-    if (active && K.has_quirk) {
+    if (active && nchunk == 0 && K.has_quirk) {
       // the particle the run scan files under another cell: counted if that
       // cell is in x_sel2 but outside this candidate cell's 27 neighbours
       const int ax = (int)(K.quirk_listed % K.nx), ay = (int)((K.quirk_listed / K.nx) % K.nx),
@@ -999,12 +1107,10 @@ __global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
         }
       }
     }
-    // the foreign-filed particle as a candidate has other neighbours: leave
-    // it to the exact pass
-    if (have) B.cand_s[q] = quirk ? __longlong_as_double(0x7ff0000000000000ll) : sum;
-    if (lane == 0) visits += (unsigned long long)min(32u, cnt - chunk * 32u) * total;
+    if (active && sum != 0.0) atomicAdd(&B.cand_s[q], sum);
   }
   if (lane == 0 && visits) atomicAdd(B.pairs, visits);
+  if (lane == 0 && slots) atomicAdd(B.pair_slots, slots);
 }
 
 // ---------------------------------------------------------------------------
@@ -1154,6 +1260,15 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
     return;
   }
   const long long masse = istop - 1;
+  {
+    // algorithmic read volume: records of the cube cells that meet the ball
+    // out to the stopping particle
+    Region Gt = G;
+    Gt.rb = dsqrt(d2stop);
+    Gt.rb2 = d2stop;
+    const unsigned nt = block_sum_u32(S, region_records(K, B, Gt));
+    if (threadIdx.x == 0) atomicAdd(B.touch, (unsigned long long)nt);
+  }
   // the masse-th element closes the member set (main:2090-2100, 2148)
   unsigned long long thr_key;
   unsigned thr_idx;
@@ -1593,7 +1708,7 @@ enum {
   SC_PROCESSED, SC_U64, SC_EDGES, SC_HRANK, SC_HID, SC_HMASS, SC_HMASS2, SC_HMEXTRA, SC_HPROF, SC_HCENTER,
   SC_HRDELTA, SC_HPOOL, SC_POOLKEY, SC_POOLIDX, SC_COUNTS, SC_ST_ACTIVE, SC_ST_NA, SC_ST_COFF, SC_ST_CN,
   SC_ST_CENTRE, SC_CAND_POS, SC_CAND_SLOT, SC_CAND_S, SC_ORDER, SC_RKEYS, SC_MASS32, SC_MOFF, SC_TKEY, SC_TIDX,
-  SC_ALIVE, SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS
+  SC_ALIVE, SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS, SC_CELLNCH
 };
 
 struct PhaseTimer {
@@ -1666,7 +1781,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       (rc = scratch(c, SC_HEAD, (size_t)nblocks, &head)) || (rc = scratch(c, SC_FILT_A, (size_t)nblocks, &filt_a)) ||
       (rc = scratch(c, SC_FILT_B, (size_t)nblocks, &filt_b)) || (rc = scratch(c, SC_READY, (size_t)nblocks + 1, &ready)) ||
       (rc = scratch(c, SC_CTRS, 16, &ctrs)) || (rc = scratch(c, SC_COUNTS, (size_t)nblocks + 1, &counts)) ||
-      (rc = scratch(c, SC_PROCESSED, (size_t)nseed + 1, &processed)) || (rc = scratch(c, SC_U64, 8, &u64s)) ||
+      (rc = scratch(c, SC_PROCESSED, (size_t)nseed + 1, &processed)) || (rc = scratch(c, SC_U64, 16, &u64s)) ||
       (rc = scratch(c, SC_EDGES, (size_t)c->p.nbins, &edge_fac)) || (rc = scratch(c, SC_HRANK, (size_t)hcap, &h_rank)) ||
       (rc = scratch(c, SC_HID, (size_t)hcap, &h_id)) || (rc = scratch(c, SC_HMASS, (size_t)hcap, &h_mass)) ||
       (rc = scratch(c, SC_HMASS2, (size_t)hcap, &h_mass2)) || (rc = scratch(c, SC_HMEXTRA, (size_t)hcap * ne, &h_mextra)) ||
@@ -1690,13 +1805,15 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       (rc = scratch(c, SC_CELLCHUNK, (size_t)cap_ready * 27, &cell_chunks)) ||
       (rc = scratch(c, SC_CHUNKPREF, (size_t)cap_ready * 27 + 1, &chunk_pref)))
     return rc;
+  unsigned *cell_nch;
+  if ((rc = scratch(c, SC_CELLNCH, (size_t)cap_ready * 27, &cell_nch))) return rc;
   // ctrs: 0 nready, 1..4 work counters, 5 gmin, 6 quirk rank, 7 cand_used
   unsigned *nready_d = ctrs, *work = ctrs + 1, *gmin = ctrs + 5, *qrank_d = ctrs + 6, *cand_used = ctrs + 7;
 
   PSOD_CUDA(c, cudaMemcpyAsync(edge_fac, c->edge_fac.data(), sizeof(double) * c->p.nbins, cudaMemcpyHostToDevice,
                                c->stream));
   PSOD_CUDA(c, cudaMemsetAsync(processed, 0, (size_t)nseed + 1, c->stream));
-  PSOD_CUDA(c, cudaMemsetAsync(u64s, 0, sizeof(unsigned long long) * 8, c->stream));
+  PSOD_CUDA(c, cudaMemsetAsync(u64s, 0, sizeof(unsigned long long) * 16, c->stream));
   PSOD_CUDA(c, cudaMemsetAsync(u64s, 0xff, sizeof(unsigned long long), c->stream));  // err = none
   PSOD_CUDA(c, cudaMemsetAsync(ctrs, 0xff, sizeof(unsigned) * 16, c->stream));
 
@@ -1757,6 +1874,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.cell_off = cell_off;
   B.cell_chunks = cell_chunks;
   B.chunk_pref = chunk_pref;
+  B.cell_nch = cell_nch;
   B.err = u64s;
   B.nhalo = u64s + 1;
   B.pool_used = u64s + 2;
@@ -1785,6 +1903,8 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.work = work;
   B.alive_cnt = nullptr;
   B.pairs = u64s + 5;
+  B.touch = u64s + 7;
+  B.pair_slots = u64s + 8;
   B.ncand_total = u64s + 6;
   B.mode = c->p.mode;
   if (c->p.mode != PSOD_MODE_PLAIN) {
@@ -1854,7 +1974,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     seed_launches += 4;
     kernels += 4;
   }
-  unsigned long long hv[8];
+  unsigned long long hv[16];
   PSOD_CUDA(c, cudaMemcpyAsync(hv, u64s, sizeof(hv), cudaMemcpyDeviceToHost, c->stream));
   PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
   st.rounds = rounds;
@@ -1869,6 +1989,8 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   st.sod_launches = seed_launches;
   st.ncandidates = (int64_t)hv[6];
   st.refine_pairs = (int64_t)hv[5];
+  st.cross_touch = (int64_t)hv[7];
+  st.refine_slots = (int64_t)hv[8];
   c->nhalo = 0;
   c->nmember = 0;
   c->sod_done = false;

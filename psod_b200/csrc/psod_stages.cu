@@ -26,28 +26,37 @@ constexpr double FIX_ONE = 1099511627776.0;  // 2^40
 // ---------------------------------------------------------------------------
 __global__ void k_cell_count(const float *pos, long long n, float nxf, double xs, int nx, unsigned *cell,
                              unsigned *count, int *bad) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
-  if (!(x >= 0.f && x <= 1.f && y >= 0.f && y <= 1.f && z >= 0.f && z <= 1.f)) {
-    atomicOr(bad, 1);
-    cell[i] = 0;
-    return;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned c = 0xffffffffu;
+  if (i < n) {
+    const float x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+    if (!(x >= 0.f && x <= 1.f && y >= 0.f && y <= 1.f && z >= 0.f && z <= 1.f)) {
+      atomicOr(bad, 1);
+      cell[i] = 0;
+    } else {
+      const int ci = sod_cell_axis(to_grid(x, nxf), xs, nx);
+      const int cj = sod_cell_axis(to_grid(y, nxf), xs, nx);
+      const int ck = sod_cell_axis(to_grid(z, nxf), xs, nx);
+      c = (unsigned)ci + (unsigned)nx * ((unsigned)cj + (unsigned)nx * (unsigned)ck);
+      cell[i] = c;
+    }
   }
-  int ci = sod_cell_axis(to_grid(x, nxf), xs, nx);
-  int cj = sod_cell_axis(to_grid(y, nxf), xs, nx);
-  int ck = sod_cell_axis(to_grid(z, nxf), xs, nx);
-  unsigned c = (unsigned)ci + (unsigned)nx * ((unsigned)cj + (unsigned)nx * (unsigned)ck);
-  cell[i] = c;
-  atomicAdd(&count[c], 1u);
+  // one atomic per distinct cell in the warp
+  const unsigned peers = __match_any_sync(0xffffffffu, c);
+  if (c != 0xffffffffu && __ffs(peers) - 1 == (int)(threadIdx.x & 31)) atomicAdd(&count[c], __popc(peers));
 }
 
 __global__ void k_cell_scatter(const float *pos, long long n, const unsigned *cell, const unsigned *start,
                                unsigned *fill, float4 *cube, unsigned *inv) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned c = i < n ? cell[i] : 0xffffffffu;
+  const unsigned peers = __match_any_sync(0xffffffffu, c);
+  const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+  unsigned base = 0;
+  if (c != 0xffffffffu && lane == leader) base = atomicAdd(&fill[c], __popc(peers));
+  base = __shfl_sync(0xffffffffu, base, leader);
   if (i >= n) return;
-  unsigned c = cell[i];
-  unsigned slot = start[c] + atomicAdd(&fill[c], 1u);
+  const unsigned slot = start[c] + base + __popc(peers & ((1u << lane) - 1u));
   cube[slot] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], __uint_as_float((unsigned)i));
   inv[i] = slot;
 }
@@ -61,14 +70,24 @@ __global__ void k_set_range(unsigned *a, unsigned long long lo, unsigned long lo
 // CIC along one axis (main:1154-1190): returns the two node indices and the
 // weights ddx (upper node) and dex (lower node).
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void cic_axis(float xf, double xxmin, double dx, int nc, int &i0, int &i1, double &dd,
-                                         double &de) {
-  double d = ddiv(dsub((double)xf, xxmin), dx);
+struct CicConst {
+  double xxmin, xxmax, dx, kc;
+  double inv_dx;  // 1/dx when it is exact (dx a power of two), else 0
+  int nc;
+};
+
+// CIC along one axis (main:1154-1190): the two node indices and the weights
+// ddx (upper node) and dex (lower node).  (x - xxmin)/dx is formed as a
+// product when 1/dx is exact, which gives the same double.
+__device__ __forceinline__ void cic_axis(float xf, const CicConst &k, int &i0, int &i1, double &dd, double &de) {
+  const double diff = dsub((double)xf, k.xxmin);
+  double d = k.inv_dx != 0.0 ? dmul(diff, k.inv_dx) : ddiv(diff, k.dx);
   int ix = (int)d;  // Fortran int(): truncation
   if (d < 0.0) ix = ix - 1;
   d = dsub(d, (double)ix);
-  double e = dsub(1.0, d);
+  const double e = dsub(1.0, d);
   int ixp1 = ix + 1;
+  const int nc = k.nc;
   if (ixp1 < 0) ixp1 += nc;
   if (ix < 0) ix += nc;
   if (ixp1 >= nc) ixp1 -= nc;
@@ -84,11 +103,6 @@ __device__ __forceinline__ bool in_zone_periodic(double x, double lo, double hi)
          (x >= dsub(lo, 1.0) && x <= dsub(hi, 1.0));
 }
 
-struct CicConst {
-  double xxmin, xxmax, dx, kc;
-  int nc;
-};
-
 // deposit: 8 int64 atomics per particle, weights quantised to 2^-40
 __global__ void k_cic_deposit(const float4 *cube, long long n, CicConst k, unsigned long long *grid) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -99,9 +113,9 @@ __global__ void k_cic_deposit(const float4 *cube, long long n, CicConst k, unsig
     return;
   int ix, ixp, iy, iyp, iz, izp;
   double ddx, dex, ddy, dey, ddz, dez;
-  cic_axis(p.x, k.xxmin, k.dx, k.nc, ix, ixp, ddx, dex);
-  cic_axis(p.y, k.xxmin, k.dx, k.nc, iy, iyp, ddy, dey);
-  cic_axis(p.z, k.xxmin, k.dx, k.nc, iz, izp, ddz, dez);
+  cic_axis(p.x, k, ix, ixp, ddx, dex);
+  cic_axis(p.y, k, iy, iyp, ddy, dey);
+  cic_axis(p.z, k, iz, izp, ddz, dez);
   const long long nc = k.nc;
   const int cx[2] = {ix, ixp}, cy[2] = {iy, iyp}, cz[2] = {iz, izp};
   const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
@@ -129,9 +143,9 @@ __global__ void k_cic_interp(const float4 *cube, long long n, CicConst k, const 
   }
   int ix, ixp, iy, iyp, iz, izp;
   double ddx, dex, ddy, dey, ddz, dez;
-  cic_axis(p.x, k.xxmin, k.dx, k.nc, ix, ixp, ddx, dex);
-  cic_axis(p.y, k.xxmin, k.dx, k.nc, iy, iyp, ddy, dey);
-  cic_axis(p.z, k.xxmin, k.dx, k.nc, iz, izp, ddz, dez);
+  cic_axis(p.x, k, ix, ixp, ddx, dex);
+  cic_axis(p.y, k, iy, iyp, ddy, dey);
+  cic_axis(p.z, k, iz, izp, ddz, dez);
   const long long nc = k.nc;
   const int cx[2] = {ix, ixp}, cy[2] = {iy, iyp}, cz[2] = {iz, izp};
   const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
@@ -191,9 +205,9 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
         const float4 v = cube[p];
         int ix, ixp, iy, iyp, iz, izp;
         double ddx, dex, ddy, dey, ddz, dez;
-        cic_axis(v.x, k.xxmin, k.dx, nc, ix, ixp, ddx, dex);
-        cic_axis(v.y, k.xxmin, k.dx, nc, iy, iyp, ddy, dey);
-        cic_axis(v.z, k.xxmin, k.dx, nc, iz, izp, ddz, dez);
+        cic_axis(v.x, k, ix, ixp, ddx, dex);
+        cic_axis(v.y, k, iy, iyp, ddy, dey);
+        cic_axis(v.z, k, iz, izp, ddz, dez);
         const int sx = sod_cell_axis(to_grid(v.x, nxf), xs, nx), sy = sod_cell_axis(to_grid(v.y, nxf), xs, nx),
                   sz = sod_cell_axis(to_grid(v.z, nxf), xs, nx);
         if ((ix >> 1) != sx || (iy >> 1) != sy || (iz >> 1) != sz) {
@@ -224,9 +238,9 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
       const unsigned idx = __float_as_uint(v.w) & PSOD_IDX_MASK;
       int ix, ixp, iy, iyp, iz, izp;
       double ddx, dex, ddy, dey, ddz, dez;
-      cic_axis(v.x, k.xxmin, k.dx, nc, ix, ixp, ddx, dex);
-      cic_axis(v.y, k.xxmin, k.dx, nc, iy, iyp, ddy, dey);
-      cic_axis(v.z, k.xxmin, k.dx, nc, iz, izp, ddz, dez);
+      cic_axis(v.x, k, ix, ixp, ddx, dex);
+      cic_axis(v.y, k, iy, iyp, ddy, dey);
+      cic_axis(v.z, k, iz, izp, ddz, dez);
       const int cx[2] = {widx(ix, ox), widx(ixp, ox)}, cy[2] = {widx(iy, oy), widx(iyp, oy)},
                 cz[2] = {widx(iz, oz), widx(izp, oz)};
       const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
@@ -367,6 +381,7 @@ static CicConst make_cic_const(const psod_ctx *c) {
   CicConst k;
   k.nc = 2 * c->nx;                                 // main:667
   k.dx = 1.0 / (double)k.nc;                        // main:1126
+  k.inv_dx = ((k.nc & (k.nc - 1)) == 0) ? (double)k.nc : 0.0;
   k.xxmin = c->xxmin;                               // main:665
   k.xxmax = -c->xxmin + 1.0;                        // zone + buffer upper edge
   const double vol = (k.dx * k.dx) * k.dx;          // main:1263
