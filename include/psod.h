@@ -121,6 +121,8 @@ typedef struct psod_run_stats {
   int64_t cross_touch;   /* records of the cube cells meeting each ball out to
                             its stopping particle (algorithmic reads) */
   int64_t refine_slots;  /* lane slots spent on refinement pair tests */
+  double ms_setup;       /* seed bucketing before the first round */
+  double ms_output;      /* halo table ordering and member sort */
 } psod_run_stats;
 
 typedef struct psod_ctx psod_ctx;

@@ -46,6 +46,7 @@ module psod_gpu
      integer(c_int64_t) :: sod_launches, kernel_launches
      real(c_double)     :: ms_sched, ms_prep, ms_refine, ms_select, ms_cross
      integer(c_int64_t) :: ncandidates, refine_pairs, cross_touch, refine_slots
+     real(c_double) :: ms_setup, ms_output
   end type psod_run_stats
 
   interface

@@ -86,6 +86,8 @@ class RunStats(C.Structure):
         ("refine_pairs", C.c_int64),
         ("cross_touch", C.c_int64),
         ("refine_slots", C.c_int64),
+        ("ms_setup", C.c_double),
+        ("ms_output", C.c_double),
     ]
 
     def as_dict(self):

@@ -22,6 +22,8 @@
 //   4. profile counts (main:2103-2115) and claims (main:2148-2166).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 
 #include "psod_internal.cuh"
 
@@ -908,57 +910,86 @@ __device__ void refine_sum(const SodConst &K, const SodBufs &B, unsigned cp, int
   sf_out = sf;
 }
 
-// Approximate refinement sums.  Each term is FP32 with one rounding per difference
-// (relative error below 1e-6); 32 terms are summed in FP32 (below 2e-6) and
-// the partial sums in FP64, so |S_approx - S| <= 3e-6 S < REF_TOL S.  Dead
-// records are parked at 1e30 so they never pass the inclusion test.
+// Approximate refinement sums (fast path).  For a pair at FP32 offset
+// (dx,dy,dz) the term is rsqrt(d2e) with d2e = dx^2+dy^2+dz^2+eps^2 formed by
+// three FFMAs.  Each difference of two grid coordinates rounds at most once,
+// and d2e adds three roundings of positive quantities, so d2e is within
+// 3.6e-7 relative and the term, after rsqrtf, within 5e-7.  A pair is counted when d2e <= 1 + eps^2; the lane tracks how close
+// its pairs came to that edge and a tile with a pair within 1e-5 of it is
+// redone with the exact FP64 inclusion test.  Terms are summed in two FP32
+// partials of at most 16 positive terms (relative error below 1e-6) and the
+// partials in FP64, so |S_approx - S| <= 2e-6 S < REF_TOL S.
+// (REF_TOL bounds the gap that sends a candidate to the exact pass.)
+// reciprocal square root of a normal positive float (d2e >= eps^2 here), one
+// MUFU operation, relative error below 2^-22.9 (PTX rsqrt.approx)
+__device__ __forceinline__ float rsqrt_pos(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 template <bool WRAPFREE>
-__device__ __forceinline__ float pair_term(const float4 nb, float cx, float cy, float cz, float e2f,
-                                           const SodConst &K) {
+__device__ __forceinline__ void pair_fast(const float4 nb, float cx, float cy, float cz, float e2f, float limf,
+                                          float nxf, float &acc, float &edge) {
   float dx, dy, dz;
   if (WRAPFREE) {
     dx = __fsub_rn(nb.x, cx);
     dy = __fsub_rn(nb.y, cy);
     dz = __fsub_rn(nb.z, cz);
   } else {
-    dx = mi_dx(nb.x, cx, K.nxf);
-    dy = mi_dx(nb.y, cy, K.nxf);
-    dz = mi_dx(nb.z, cz, K.nxf);
+    dx = mi_dx(nb.x, cx, nxf);
+    dy = mi_dx(nb.y, cy, nxf);
+    dz = mi_dx(nb.z, cz, nxf);
   }
-  const float d2 = fmaf(dx, dx, fmaf(dy, dy, __fmul_rn(dz, dz)));
-  bool in = d2 <= 0.99999f;
-  if (!in && d2 <= 1.00001f)
-    in = min_image_d2((double)nb.x, (double)nb.y, (double)nb.z, (double)cx, (double)cy, (double)cz, K.tx) <= K.rmin2;
-  return in ? rsqrtf(__fadd_rn(d2, e2f)) : 0.f;
+  const float d2e = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmaf_rn(dz, dz, e2f)));
+  // e has the sign of d2e - limf (a rounded difference never changes sign)
+  const float e = __fsub_rn(d2e, limf);
+  edge = fminf(edge, fabsf(e));
+  const float t = rsqrt_pos(d2e);
+  asm("{\n\t.reg .pred p;\n\tsetp.le.f32 p, %1, 0f00000000;\n\t@p add.rn.f32 %0, %0, %2;\n\t}" : "+f"(acc) : "f"(e), "f"(t));
 }
 
-// sum of the terms of nt (<= 32) staged records; four independent FP32
-// partials of at most 8 terms each, added in FP64
+// a tile whose lane met a pair near the inclusion edge: the same FP32 terms,
+// with the inclusion decided by the FP64 minimum-image distance
+template <bool WRAPFREE>
+__device__ __noinline__ double tile_terms_edge(const float4 *tile, unsigned nt, float cx, float cy, float cz,
+                                               float e2f, float nxf, double tx, double rmin2) {
+  double sum = 0.0;
+  for (unsigned j = 0; j < nt; j++) {
+    const float4 nb = tile[j];
+    float dx, dy, dz;
+    if (WRAPFREE) {
+      dx = __fsub_rn(nb.x, cx);
+      dy = __fsub_rn(nb.y, cy);
+      dz = __fsub_rn(nb.z, cz);
+    } else {
+      dx = mi_dx(nb.x, cx, nxf);
+      dy = mi_dx(nb.y, cy, nxf);
+      dz = mi_dx(nb.z, cz, nxf);
+    }
+    const float d2e = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmaf_rn(dz, dz, e2f)));
+    if (min_image_d2((double)nb.x, (double)nb.y, (double)nb.z, (double)cx, (double)cy, (double)cz, tx) <= rmin2)
+      sum += (double)rsqrt_pos(d2e);
+  }
+  return sum;
+}
+
+// sum of the terms of nt staged records; the tile is padded with far
+// records up to a multiple of 8
 template <bool WRAPFREE>
 __device__ __forceinline__ double tile_terms(const float4 *tile, unsigned nt, float cx, float cy, float cz,
                                              const SodConst &K) {
-  const float e2f = (float)K.eps2;
-  if (nt == 32) {
-    float p0 = 0.f, p1 = 0.f, p2 = 0.f, p3 = 0.f;
+  const float e2f = (float)K.eps2, limf = (float)(1.0 + K.eps2);
+  float p0 = 0.f, p1 = 0.f, edge = 1.f;
+  for (unsigned j = 0; j < nt; j += 8) {
 #pragma unroll
-    for (int j = 0; j < 32; j += 4) {
-      p0 += pair_term<WRAPFREE>(tile[j], cx, cy, cz, e2f, K);
-      p1 += pair_term<WRAPFREE>(tile[j + 1], cx, cy, cz, e2f, K);
-      p2 += pair_term<WRAPFREE>(tile[j + 2], cx, cy, cz, e2f, K);
-      p3 += pair_term<WRAPFREE>(tile[j + 3], cx, cy, cz, e2f, K);
-    }
-    return ((double)p0 + (double)p1) + ((double)p2 + (double)p3);
-  }
-  double sum = 0.0;
-  float part = 0.f;
-  for (unsigned j = 0; j < nt; j++) {
-    part += pair_term<WRAPFREE>(tile[j], cx, cy, cz, e2f, K);
-    if ((j & 7) == 7) {
-      sum += (double)part;
-      part = 0.f;
+    for (int u = 0; u < 8; u += 2) {
+      pair_fast<WRAPFREE>(tile[j + u], cx, cy, cz, e2f, limf, K.nxf, p0, edge);
+      pair_fast<WRAPFREE>(tile[j + u + 1], cx, cy, cz, e2f, limf, K.nxf, p1, edge);
     }
   }
-  return sum + (double)part;
+  if (edge < 1e-5f) return tile_terms_edge<WRAPFREE>(tile, nt, cx, cy, cz, e2f, K.nxf, K.tx, K.rmin2);
+  return (double)p0 + (double)p1;
 }
 
 // Work item: up to 32 candidates of one candidate cell (a lane each) against
@@ -966,7 +997,7 @@ __device__ __forceinline__ double tile_terms(const float4 *tile, unsigned nt, fl
 // pass through a warp-private shared slice, 32 at a time, and every lane
 // reads each one by broadcast; warps never wait on one another.  Partial
 // sums of a candidate's neighbour chunks are added into cand_s.
-__global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
+__global__ void __launch_bounds__(256, 4) k_refine_warp(SodConst K, SodBufs B) {
   __shared__ float4 s_tile[8][32];
   __shared__ unsigned s_rb[8][18], s_rp[8][19];
   __shared__ int s_nr[8], s_wf[8];
@@ -1047,46 +1078,70 @@ __global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
     const unsigned total = s_rp[w][nr];
     const bool wf = s_wf[w];
     const bool active = have && !quirk;
-    const unsigned r0 = nchunk * RN_CHUNK, r1 = min(total, r0 + RN_CHUNK);
+    // bounding box of the item's candidates: records farther than 1 from it
+    // in every direction meet no candidate (wrap-free items only)
+    float lox = active ? cx : 3e38f, hix = active ? cx : -3e38f, loy = active ? cy : 3e38f,
+          hiy = active ? cy : -3e38f, loz = active ? cz : 3e38f, hiz = active ? cz : -3e38f;
+    for (int o = 16; o > 0; o >>= 1) {
+      lox = fminf(lox, __shfl_xor_sync(0xffffffffu, lox, o));
+      hix = fmaxf(hix, __shfl_xor_sync(0xffffffffu, hix, o));
+      loy = fminf(loy, __shfl_xor_sync(0xffffffffu, loy, o));
+      hiy = fmaxf(hiy, __shfl_xor_sync(0xffffffffu, hiy, o));
+      loz = fminf(loz, __shfl_xor_sync(0xffffffffu, loz, o));
+      hiz = fmaxf(hiz, __shfl_xor_sync(0xffffffffu, hiz, o));
+    }
+    const bool any_active = lox <= hix;
+    const unsigned r0 = nchunk * RN_CHUNK, r1 = any_active ? min(total, r0 + RN_CHUNK) : r0;
     const unsigned lt = (1u << lane) - 1u;
     double sum = 0.0;
     unsigned pos = r0;  // next record of the chunk to load
-    unsigned fill = 0;  // alive records staged in the tile
+    unsigned fill = 0;  // records staged in the tile
+    int rr = 0;         // run holding record pos
+    while (rr + 1 < nr && s_rp[w][rr + 1] <= pos) rr++;
     while (pos < r1 || fill > 0) {
-      // stage alive records only: claimed ones are skipped by a warp-wide
-      // compaction, so they cost a load but no pair tests
+      // stage alive records within reach of the box only: the others are
+      // skipped by a warp-wide compaction, so they cost a load but no pair
+      // tests
       while (fill < 32 && pos < r1) {
         const unsigned ff = pos + (unsigned)lane;
-        bool alive = false;
+        bool keep = false;
         float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
         if (ff < r1) {
-          int r = 0;
+          int r = rr;
           while (s_rp[w][r + 1] <= ff) r++;
           const float4 v = B.cube[s_rb[w][r] + (ff - s_rp[w][r])];
-          alive = !(__float_as_uint(v.w) & PSOD_DEAD_BIT);
           rec = make_float4(to_grid(v.x, K.nxf), to_grid(v.y, K.nxf), to_grid(v.z, K.nxf), 0.f);
+          keep = !(__float_as_uint(v.w) & PSOD_DEAD_BIT);
+          if (wf) {
+            const float ex = fmaxf(fmaxf(lox - rec.x, rec.x - hix), 0.f), ey = fmaxf(fmaxf(loy - rec.y, rec.y - hiy), 0.f),
+                        ez = fmaxf(fmaxf(loz - rec.z, rec.z - hiz), 0.f);
+            keep = keep && fmaf(ex, ex, fmaf(ey, ey, ez * ez)) <= 1.0001f;
+          }
         }
-        const unsigned m = __ballot_sync(0xffffffffu, alive);
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
         const unsigned need = 32u - fill, rank = __popc(m & lt);
-        if (alive && rank < need) s_tile[w][fill + rank] = rec;
+        if (keep && rank < need) s_tile[w][fill + rank] = rec;
         const unsigned got = __popc(m);
         if (got <= need) {
           fill += got;
           pos += 32u;
         } else {
-          // the need-th alive lane is the last one taken; resume after it
-          const unsigned mk = __ballot_sync(0xffffffffu, alive && rank == need - 1);
+          // the need-th kept lane is the last one taken; resume after it
+          const unsigned mk = __ballot_sync(0xffffffffu, keep && rank == need - 1);
           pos += (unsigned)__ffs(mk);  // lane index + 1
           fill = 32u;
         }
+        while (rr + 1 < nr && s_rp[w][rr + 1] <= pos) rr++;
       }
       if (pos > r1) pos = r1;
+      // pad to a multiple of 8 with records far from every candidate
+      if ((unsigned)lane < ((8u - (fill & 7u)) & 7u)) s_tile[w][fill + lane] = make_float4(1e18f, 1e18f, 1e18f, 0.f);
       __syncwarp();
       if (active && fill > 0)
         sum += wf ? tile_terms<true>(s_tile[w], fill, cx, cy, cz, K) : tile_terms<false>(s_tile[w], fill, cx, cy, cz, K);
       if (lane == 0) {
         visits += (unsigned long long)min(32u, cnt - chunk * 32u) * fill;
-        slots += 32ull * fill;
+        slots += 32ull * ((fill + 7u) & ~7u);
       }
       __syncwarp();
       fill = 0;
@@ -1713,7 +1768,7 @@ enum {
 
 struct PhaseTimer {
   cudaEvent_t a, b;
-  float total = 0.f;
+  float total = 0.f, last = 0.f;
   PhaseTimer() {
     cudaEventCreate(&a);
     cudaEventCreate(&b);
@@ -1728,6 +1783,7 @@ struct PhaseTimer {
     float ms = 0.f;
     cudaEventSynchronize(b);
     cudaEventElapsedTime(&ms, a, b);
+    last = ms;
     total += ms;
   }
 };
@@ -1737,7 +1793,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   psod_run_stats st{};
   st.fail_rank = -1;
   st.npart_new = c->npart_new;
-  PhaseTimer t_all, t_sched, t_prep, t_ref, t_sel, t_cross;
+  PhaseTimer t_all, t_sched, t_prep, t_ref, t_sel, t_cross, t_setup, t_out;
   t_all.start(c->stream);
   int rc = PSOD_OK;
   const SodConst K = make_sod_const(c);
@@ -1818,6 +1874,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   PSOD_CUDA(c, cudaMemsetAsync(ctrs, 0xff, sizeof(unsigned) * 16, c->stream));
 
   // seeds bucketed by scheduler block, in rank order within a block
+  t_setup.start(c->stream);
   if (nseed > 0) {
     k_seed_blocks<<<nblk(nseed, 256), 256, 0, c->stream>>>(c->d_seed_idx, c->d_inv, c->d_cube, nseed, K, bs, nb,
                                                            block_of, blist);
@@ -1842,7 +1899,9 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   }
   unsigned quirk_rank = PSOD_INF_RANK;
   PSOD_CUDA(c, cudaMemcpyAsync(&quirk_rank, qrank_d, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+  t_setup.stop(c->stream);
   PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+  t_setup.collect();
 
   const size_t smem = sizeof(Smem);
   PSOD_CUDA(c, cudaFuncSetAttribute(k_prep, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1916,6 +1975,10 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   }
 
   long long rounds = 0, seed_launches = 0;
+  // PSOD_TRACE=1: one line per round on stderr (ready seeds, active blocks,
+  // candidates, phase times)
+  const char *trace_env = getenv("PSOD_TRACE");
+  const bool trace = trace_env && trace_env[0] == '1';
   // ctrs[8]: active-block count of the current list, ctrs[9]: of the next
   unsigned n_active = 0;
   if (nseed > 0) {
@@ -1970,6 +2033,12 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     t_ref.collect();
     t_sel.collect();
     t_cross.collect();
+    if (trace) {
+      unsigned cu = 0;
+      cudaMemcpy(&cu, cand_used, sizeof(unsigned), cudaMemcpyDeviceToHost);
+      fprintf(stderr, "psod round %lld ready %u active %u cand %u sched %.3f prep %.3f refine %.3f select %.3f cross %.3f\n",
+              rounds, nready, n_active, cu, t_sched.last, t_prep.last, t_ref.last, t_sel.last, t_cross.last);
+    }
     rounds++;
     seed_launches += 4;
     kernels += 4;
@@ -2009,6 +2078,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
                                                 std::to_string(st.fail_rank) + " (zone output lost; increase -sel)");
     return set_err(c, PSOD_ERR_STATE, "internal consistency check failed at seed rank " + std::to_string(st.fail_rank));
   }
+  t_out.start(c->stream);
   const long long nh = (long long)hv[1];
   const unsigned long long npool = std::max<unsigned long long>(hv[2], 1);
   unsigned *order, *rkeys, *mass32, *moff, *tidx;
@@ -2057,9 +2127,13 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     PSOD_CUDA(c, cudaMemsetAsync(c->d_m_offset, 0, sizeof(long long), c->stream));
   }
   PSOD_CUDA(c, cudaGetLastError());
+  t_out.stop(c->stream);
   t_all.stop(c->stream);
+  t_out.collect();
   t_all.collect();
   st.ms_total = t_all.total;
+  st.ms_setup = t_setup.total;
+  st.ms_output = t_out.total;
   st.nhalo = nh;
   st.nmember = (int64_t)hv[2];
   st.kernel_launches = kernels;

@@ -46,17 +46,92 @@ __global__ void k_cell_count(const float *pos, long long n, float nxf, double xs
   if (c != 0xffffffffu && __ffs(peers) - 1 == (int)(threadIdx.x & 31)) atomicAdd(&count[c], __popc(peers));
 }
 
+// Cells holding at least SUB_MIN particles are ordered inside by a 4x4x4
+// sub-cell key (Morton order), so that consecutive records of a dense cell lie
+// close together.  Records inside a cell carry no order of their own (every
+// later result is ordered by input index), so this changes no output; it lets
+// the refinement hand a warp 32 nearby candidates.
+constexpr unsigned SUB_MIN = 64;
+constexpr unsigned SUB_N = 64;
+constexpr unsigned BIG_FLAG = 0x80000000u;
+
+__device__ __forceinline__ unsigned sub_axis(float xg, double xs) {
+  const double d = dsub((double)xg, xs);
+  const int s = (int)(dsub(d, floor(d)) * 4.0);
+  return (unsigned)min(max(s, 0), 3);
+}
+
+__device__ __forceinline__ unsigned sub_key(const float *p, float nxf, double xs) {
+  const unsigned a = sub_axis(to_grid(p[0], nxf), xs), b = sub_axis(to_grid(p[1], nxf), xs),
+                 c = sub_axis(to_grid(p[2], nxf), xs);
+  return (a & 1u) | ((b & 1u) << 1) | ((c & 1u) << 2) | ((a >> 1) << 3) | ((b >> 1) << 4) | ((c >> 1) << 5);
+}
+
+// count[c] becomes BIG_FLAG | table index for cells of SUB_MIN or more
+// particles, else 0 (the fill counter of the scatter).  With assign false it
+// only counts them.
+__global__ void k_mark_big(unsigned *count, unsigned long long ncell, unsigned *nbig, bool assign,
+                           unsigned *bigcell) {
+  const unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool big = c < ncell && count[c] >= SUB_MIN;
+  const unsigned m = __ballot_sync(0xffffffffu, big);
+  const int lane = threadIdx.x & 31;
+  unsigned base = 0;
+  if (lane == 0 && m) base = atomicAdd(nbig, (unsigned)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (!assign || c >= ncell) return;
+  if (big) {
+    const unsigned idx = base + __popc(m & ((1u << lane) - 1u));
+    bigcell[idx] = (unsigned)c;
+    count[c] = BIG_FLAG | idx;
+  } else {
+    count[c] = 0;
+  }
+}
+
+__global__ void k_sub_count(const float *pos, long long n, const unsigned *cell, const unsigned *count, float nxf,
+                            double xs, unsigned *tab) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned v = count[cell[i]];
+  if (v & BIG_FLAG) atomicAdd(&tab[(unsigned long long)(v & ~BIG_FLAG) * SUB_N + sub_key(pos + 3 * i, nxf, xs)], 1u);
+}
+
+// one warp per dense cell: sub-cell counts -> absolute start slots
+__global__ void k_sub_scan(unsigned *tab, const unsigned *bigcell, unsigned nbig, const unsigned *start) {
+  const unsigned b = (unsigned)(((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (b >= nbig) return;
+  unsigned *t = tab + (unsigned long long)b * SUB_N;
+  const unsigned a0 = t[2 * lane], a1 = t[2 * lane + 1];
+  unsigned x = a0 + a1;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  const unsigned excl = start[bigcell[b]] + x - (a0 + a1);
+  t[2 * lane] = excl;
+  t[2 * lane + 1] = excl + a0;
+}
+
 __global__ void k_cell_scatter(const float *pos, long long n, const unsigned *cell, const unsigned *start,
-                               unsigned *fill, float4 *cube, unsigned *inv) {
+                               unsigned *fill, unsigned *tab, float nxf, double xs, float4 *cube, unsigned *inv) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned c = i < n ? cell[i] : 0xffffffffu;
-  const unsigned peers = __match_any_sync(0xffffffffu, c);
+  const unsigned v = i < n ? fill[c] : 0u;  // the flag bit never changes under the atomics below
+  const bool big = (v & BIG_FLAG) != 0;
+  const unsigned long long key =
+      i >= n ? ~0ull
+      : big  ? (1ull << 63) | ((unsigned long long)(v & ~BIG_FLAG) * SUB_N + sub_key(pos + 3 * i, nxf, xs))
+             : (unsigned long long)c;
+  const unsigned peers = __match_any_sync(0xffffffffu, key);
   const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
   unsigned base = 0;
-  if (c != 0xffffffffu && lane == leader) base = atomicAdd(&fill[c], __popc(peers));
+  if (i < n && lane == leader)
+    base = big ? atomicAdd(&tab[key & ~(1ull << 63)], __popc(peers)) : start[c] + atomicAdd(&fill[c], __popc(peers));
   base = __shfl_sync(0xffffffffu, base, leader);
   if (i >= n) return;
-  const unsigned slot = start[c] + base + __popc(peers & ((1u << lane) - 1u));
+  const unsigned slot = base + __popc(peers & ((1u << lane) - 1u));
   cube[slot] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], __uint_as_float((unsigned)i));
   inv[i] = slot;
 }
@@ -172,17 +247,37 @@ constexpr int CT = 8;                 // SOD cells per tile side
 constexpr int CW = 2 * (CT + 2) + 1;  // window nodes per side
 constexpr int CW3 = CW * CW * CW;
 
+constexpr int CRNG = 2 * (CT + 2) * (CT + 2);  // record ranges of a tile plus halo (two where x wraps)
+
+// exclusive prefix of s_len[0..n) into s_pre[0..n], n <= 32 * 8, by warp 0
+__device__ __forceinline__ void range_prefix(const unsigned *s_len, unsigned *s_pre, int n) {
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x, per = (n + 31) / 32, lo = lane * per;
+  unsigned t = 0;
+  for (int i = lo; i < min(n, lo + per); i++) t += s_len[i];
+  unsigned x = t;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  unsigned run = x - t;
+  for (int i = lo; i < min(n, lo + per); i++) {
+    s_pre[i] = run;
+    run += s_len[i];
+  }
+  if (lane == 31) s_pre[n] = x;
+}
+
 __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsigned *cs, int nx, double xs, CicConst k,
                                                   double *rho, int *bad) {
   extern __shared__ __align__(16) unsigned long long win[];
+  __shared__ unsigned s_rb[CRNG], s_len[CRNG], s_pre[CRNG + 1];
   const int ntile = nx / CT;
   const int tx = blockIdx.x % ntile, ty = (blockIdx.x / ntile) % ntile, tz = blockIdx.x / (ntile * ntile);
   const int x0 = tx * CT, y0 = ty * CT, z0 = tz * CT;
   const int nc = k.nc;  // 2*nx fine cells
   const float nxf = (float)nx;
   for (int i = threadIdx.x; i < CW3; i += blockDim.x) win[i] = 0ull;
-  __syncthreads();
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   auto widx = [&](int f, int o) {  // fine index -> window offset (periodic)
     int d = f - o;
     if (d < 0) d += nc;
@@ -190,75 +285,98 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
     return d;
   };
   const int ox = 2 * (x0 - 1), oy = 2 * (y0 - 1), oz = 2 * (z0 - 1);
-  // rows of the tile plus halo
-  for (int row = w; row < (CT + 2) * (CT + 2); row += nw) {
+  // record ranges of the rows of the tile plus halo; the particles are then
+  // dealt to all threads of the CTA evenly, whatever their spread over rows
+  for (int row = threadIdx.x; row < (CT + 2) * (CT + 2); row += blockDim.x) {
     const int yy = (y0 - 1 + row % (CT + 2) + nx) % nx, zz = (z0 - 1 + row / (CT + 2) + nx) % nx;
     const unsigned long long base = (unsigned long long)nx * ((unsigned)yy + (unsigned long long)nx * (unsigned)zz);
     const int xa = x0 - 1, xb = x0 + CT;  // inclusive, may wrap
-    int pa[2], pb[2], np;
-    if (xa < 0) { pa[0] = xa + nx; pb[0] = nx - 1; pa[1] = 0; pb[1] = xb; np = 2; }
-    else if (xb >= nx) { pa[0] = xa; pb[0] = nx - 1; pa[1] = 0; pb[1] = xb - nx; np = 2; }
-    else { pa[0] = xa; pb[0] = xb; np = 1; }
-    for (int q = 0; q < np; q++) {
-      const unsigned b = cs[base + (unsigned)pa[q]], e = cs[base + (unsigned)pb[q] + 1];
-      for (unsigned p = b + lane; p < e; p += 32) {
-        const float4 v = cube[p];
-        int ix, ixp, iy, iyp, iz, izp;
-        double ddx, dex, ddy, dey, ddz, dez;
-        cic_axis(v.x, k, ix, ixp, ddx, dex);
-        cic_axis(v.y, k, iy, iyp, ddy, dey);
-        cic_axis(v.z, k, iz, izp, ddz, dez);
-        const int sx = sod_cell_axis(to_grid(v.x, nxf), xs, nx), sy = sod_cell_axis(to_grid(v.y, nxf), xs, nx),
-                  sz = sod_cell_axis(to_grid(v.z, nxf), xs, nx);
-        if ((ix >> 1) != sx || (iy >> 1) != sy || (iz >> 1) != sz) {
-          atomicOr(bad, 1);
-          continue;
-        }
-        const int cx[2] = {widx(ix, ox), widx(ixp, ox)}, cy[2] = {widx(iy, oy), widx(iyp, oy)},
-                  cz[2] = {widx(iz, oz), widx(izp, oz)};
-        const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
-#pragma unroll
-        for (int c = 0; c < 8; c++) {
-          const int a = c & 1, bb = (c >> 1) & 1, ee = c >> 2;
-          if (cx[a] >= CW || cy[bb] >= CW || cz[ee] >= CW) continue;
-          const double wgt = dmul(dmul(wx[a], wy[bb]), wz[ee]);
-          atomicAdd(&win[cx[a] + CW * (cy[bb] + CW * cz[ee])], (unsigned long long)__double2ll_rn(dmul(wgt, FIX_ONE)));
-        }
+    int pa[2] = {0, 0}, pb[2] = {-1, -1};
+    if (xa < 0) { pa[0] = xa + nx; pb[0] = nx - 1; pa[1] = 0; pb[1] = xb; }
+    else if (xb >= nx) { pa[0] = xa; pb[0] = nx - 1; pa[1] = 0; pb[1] = xb - nx; }
+    else { pa[0] = xa; pb[0] = xb; }
+    for (int q = 0; q < 2; q++) {
+      unsigned rb = 0, len = 0;
+      if (pb[q] >= pa[q]) {
+        rb = cs[base + (unsigned)pa[q]];
+        len = cs[base + (unsigned)pb[q] + 1] - rb;
       }
+      s_rb[2 * row + q] = rb;
+      s_len[2 * row + q] = len;
     }
   }
   __syncthreads();
-  // own particles: rho in the reference's term order (main:1368-1383)
-  for (int row = w; row < CT * CT; row += nw) {
-    const int yy = y0 + row % CT, zz = z0 + row / CT;
-    const unsigned long long base = (unsigned long long)nx * ((unsigned)yy + (unsigned long long)nx * (unsigned)zz);
-    const unsigned b = cs[base + (unsigned)x0], e = cs[base + (unsigned)(x0 + CT - 1) + 1];
-    for (unsigned p = b + lane; p < e; p += 32) {
-      const float4 v = cube[p];
-      const unsigned idx = __float_as_uint(v.w) & PSOD_IDX_MASK;
+  range_prefix(s_len, s_pre, CRNG);
+  __syncthreads();
+  {
+    const unsigned total = s_pre[CRNG];
+    int r = 0;
+    for (unsigned f = threadIdx.x; f < total; f += blockDim.x) {
+      while (s_pre[r + 1] <= f) r++;
+      const float4 v = cube[s_rb[r] + (f - s_pre[r])];
       int ix, ixp, iy, iyp, iz, izp;
       double ddx, dex, ddy, dey, ddz, dez;
       cic_axis(v.x, k, ix, ixp, ddx, dex);
       cic_axis(v.y, k, iy, iyp, ddy, dey);
       cic_axis(v.z, k, iz, izp, ddz, dez);
+      const int sx = sod_cell_axis(to_grid(v.x, nxf), xs, nx), sy = sod_cell_axis(to_grid(v.y, nxf), xs, nx),
+                sz = sod_cell_axis(to_grid(v.z, nxf), xs, nx);
+      if ((ix >> 1) != sx || (iy >> 1) != sy || (iz >> 1) != sz) {
+        atomicOr(bad, 1);
+        continue;
+      }
       const int cx[2] = {widx(ix, ox), widx(ixp, ox)}, cy[2] = {widx(iy, oy), widx(iyp, oy)},
                 cz[2] = {widx(iz, oz), widx(izp, oz)};
       const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
-      double r = 0.0;
-      bool ok = true;
 #pragma unroll
       for (int c = 0; c < 8; c++) {
         const int a = c & 1, bb = (c >> 1) & 1, ee = c >> 2;
-        if (cx[a] >= CW || cy[bb] >= CW || cz[ee] >= CW) {
-          ok = false;
-          continue;
-        }
-        const double gval = dmul((double)(long long)win[cx[a] + CW * (cy[bb] + CW * cz[ee])], k.kc);
-        r = dadd(r, dmul(dmul(dmul(gval, wx[a]), wy[bb]), wz[ee]));
+        if (cx[a] >= CW || cy[bb] >= CW || cz[ee] >= CW) continue;
+        const double wgt = dmul(dmul(wx[a], wy[bb]), wz[ee]);
+        atomicAdd(&win[cx[a] + CW * (cy[bb] + CW * cz[ee])], (unsigned long long)__double2ll_rn(dmul(wgt, FIX_ONE)));
       }
-      if (!ok) atomicOr(bad, 1);
-      rho[idx] = r;
     }
+  }
+  __syncthreads();
+  // own particles: rho in the reference's term order (main:1368-1383)
+  for (int row = threadIdx.x; row < CT * CT; row += blockDim.x) {
+    const int yy = y0 + row % CT, zz = z0 + row / CT;
+    const unsigned long long base = (unsigned long long)nx * ((unsigned)yy + (unsigned long long)nx * (unsigned)zz);
+    const unsigned rb = cs[base + (unsigned)x0];
+    s_rb[row] = rb;
+    s_len[row] = cs[base + (unsigned)(x0 + CT - 1) + 1] - rb;
+  }
+  __syncthreads();
+  range_prefix(s_len, s_pre, CT * CT);
+  __syncthreads();
+  const unsigned total = s_pre[CT * CT];
+  int r = 0;
+  for (unsigned f = threadIdx.x; f < total; f += blockDim.x) {
+    while (s_pre[r + 1] <= f) r++;
+    const float4 v = cube[s_rb[r] + (f - s_pre[r])];
+    const unsigned idx = __float_as_uint(v.w) & PSOD_IDX_MASK;
+    int ix, ixp, iy, iyp, iz, izp;
+    double ddx, dex, ddy, dey, ddz, dez;
+    cic_axis(v.x, k, ix, ixp, ddx, dex);
+    cic_axis(v.y, k, iy, iyp, ddy, dey);
+    cic_axis(v.z, k, iz, izp, ddz, dez);
+    const int cx[2] = {widx(ix, ox), widx(ixp, ox)}, cy[2] = {widx(iy, oy), widx(iyp, oy)},
+              cz[2] = {widx(iz, oz), widx(izp, oz)};
+    const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
+    double rr = 0.0;
+    bool ok = true;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int a = c & 1, bb = (c >> 1) & 1, ee = c >> 2;
+      if (cx[a] >= CW || cy[bb] >= CW || cz[ee] >= CW) {
+        ok = false;
+        continue;
+      }
+      const double gval = dmul((double)(long long)win[cx[a] + CW * (cy[bb] + CW * cz[ee])], k.kc);
+      rr = dadd(rr, dmul(dmul(dmul(gval, wx[a]), wy[bb]), wz[ee]));
+    }
+    if (!ok) atomicOr(bad, 1);
+    rho[idx] = rr;
   }
 }
 
@@ -321,24 +439,45 @@ int stage_cellsort(psod_ctx *c, const float *dpos) {
   int *bad = nullptr;
   if ((st = scratch(c, 3, (size_t)n, &cell))) return st;
   if ((st = scratch(c, 4, (size_t)c->ncell + 1, &count))) return st;
-  if ((st = scratch(c, 5, 1, &bad))) return st;
+  if ((st = scratch(c, 5, 2, &bad))) return st;
   if ((st = ensure(c, &c->d_cell_start, &c->cs_cap, (size_t)c->ncell + 1))) return st;
   if ((st = ensure(c, &c->d_cube, &c->cube_cap, (size_t)n))) return st;
   if ((st = ensure(c, &c->d_inv, &c->inv_cap, (size_t)n))) return st;
   PSOD_CUDA(c, cudaMemsetAsync(count, 0, sizeof(unsigned) * (c->ncell + 1), c->stream));
-  PSOD_CUDA(c, cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
+  PSOD_CUDA(c, cudaMemsetAsync(bad, 0, 2 * sizeof(int), c->stream));
   const double xs = c->xxmin * c->scale;  // main:1565
   k_cell_count<<<nblk(n, 256), 256, 0, c->stream>>>(dpos, n, (float)nx, xs, nx, cell, count, bad);
   if ((st = scan_u32(c, count, c->d_cell_start, (long long)c->ncell, true))) return st;
-  PSOD_CUDA(c, cudaMemsetAsync(count, 0, sizeof(unsigned) * c->ncell, c->stream));
-  k_cell_scatter<<<nblk(n, 256), 256, 0, c->stream>>>(dpos, n, cell, c->d_cell_start, count, c->d_cube,
-                                                      c->d_inv);
-  int hbad = 0;
-  PSOD_CUDA(c, cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  unsigned *nbig = reinterpret_cast<unsigned *>(bad + 1);
+  const long long ncell = (long long)c->ncell;
+  k_mark_big<<<nblk(ncell, 256), 256, 0, c->stream>>>(count, c->ncell, nbig, false, nullptr);
+  int hflags[2] = {0, 0};
+  PSOD_CUDA(c, cudaMemcpyAsync(hflags, bad, sizeof(hflags), cudaMemcpyDeviceToHost, c->stream));
   PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
-  // the per-particle cell ids and per-cell counts are only needed here
+  const int hbad = hflags[0];
+  const unsigned hnbig = (unsigned)hflags[1];
+  unsigned *tab = nullptr, *bigcell = nullptr;
+  if (!hbad) {
+    if ((st = scratch(c, 6, (size_t)hnbig * SUB_N + 1, &tab))) return st;
+    if ((st = scratch(c, 7, (size_t)hnbig + 1, &bigcell))) return st;
+    PSOD_CUDA(c, cudaMemsetAsync(nbig, 0, sizeof(unsigned), c->stream));
+    PSOD_CUDA(c, cudaMemsetAsync(tab, 0, sizeof(unsigned) * ((size_t)hnbig * SUB_N + 1), c->stream));
+    k_mark_big<<<nblk(ncell, 256), 256, 0, c->stream>>>(count, c->ncell, nbig, true, bigcell);
+    if (hnbig) {
+      k_sub_count<<<nblk(n, 256), 256, 0, c->stream>>>(dpos, n, cell, count, (float)nx, xs, tab);
+      k_sub_scan<<<nblk((long long)hnbig * 32, 256), 256, 0, c->stream>>>(tab, bigcell, hnbig, c->d_cell_start);
+    }
+    k_cell_scatter<<<nblk(n, 256), 256, 0, c->stream>>>(dpos, n, cell, c->d_cell_start, count, tab, (float)nx, xs,
+                                                        c->d_cube, c->d_inv);
+    PSOD_CUDA(c, cudaGetLastError());
+    PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+  }
+  // the per-particle cell ids, per-cell counts and sub-cell tables are only
+  // needed here
   free_scratch_slot(c, 3);
   free_scratch_slot(c, 4);
+  free_scratch_slot(c, 6);
+  free_scratch_slot(c, 7);
   if (hbad) return set_err(c, PSOD_ERR_ARG, "particle positions must lie in [0,1] (box units)");
 
   // The reference's run scan (main:1591-1604) files a final cell holding a
