@@ -57,25 +57,21 @@ int copy_in(psod_ctx *c, void *ddst, const void *src, size_t bytes) {
 using namespace psod;
 
 static void free_all(psod_ctx *c) {
-  dfree(&c->d_pos);
-  dfree(&c->d_vel);
   dfree(&c->d_ids);
   dfree(&c->d_cube);
   dfree(&c->d_cell_start);
   dfree(&c->d_inv);
   dfree(&c->d_rho);
   dfree(&c->d_grid);
-  dfree(&c->d_seed_idx);
-  dfree(&c->d_h_id);
-  dfree(&c->d_h_mass);
-  dfree(&c->d_h_rank);
-  dfree(&c->d_h_mass2);
-  dfree(&c->d_h_mextra);
-  dfree(&c->d_h_profile);
-  dfree(&c->d_h_center);
-  dfree(&c->d_h_rdelta);
-  dfree(&c->d_m_offset);
-  dfree(&c->d_m_index);
+  // the remaining arrays live in scratch slots
+  c->d_pos = nullptr;
+  c->d_vel = nullptr;
+  c->d_seed_idx = nullptr;
+  c->d_h_id = c->d_h_mass = c->d_h_rank = c->d_h_mass2 = c->d_h_mextra = c->d_h_profile = nullptr;
+  c->d_h_center = nullptr;
+  c->d_h_rdelta = nullptr;
+  c->d_m_offset = nullptr;
+  c->d_m_index = nullptr;
   free_scratch(c);
 }
 
@@ -216,7 +212,7 @@ int psod_load_particles(psod_ctx *c, int64_t n, const float *pos, const float *v
   // place, a host buffer goes through a temporary device copy
   const float *dpos = pos;
   if (!is_device_ptr(pos)) {
-    if ((st = dalloc(c, &c->d_pos, (size_t)n * 3))) return st;
+    if ((st = scratch(c, SLOT_HOST_POS, (size_t)n * 3, &c->d_pos))) return st;
     if ((st = copy_in(c, c->d_pos, pos, sizeof(float) * 3 * n))) return st;
     dpos = c->d_pos;
   }
@@ -226,14 +222,12 @@ int psod_load_particles(psod_ctx *c, int64_t n, const float *pos, const float *v
   }
   if ((st = copy_in(c, c->d_ids, id, sizeof(int64_t) * n))) return st;
   if (vel) {
-    if ((st = dalloc(c, &c->d_vel, (size_t)n * 3))) return st;
+    if ((st = scratch(c, SLOT_VEL, (size_t)n * 3, &c->d_vel))) return st;
     if ((st = copy_in(c, c->d_vel, vel, sizeof(float) * 3 * n))) return st;
   } else {
-    dfree(&c->d_vel);
+    c->d_vel = nullptr;
   }
-  st = stage_cellsort(c, dpos);
-  dfree(&c->d_pos);
-  return st;
+  return stage_cellsort(c, dpos);
 }
 
 int psod_cic(psod_ctx *c, double *grid_out) {
@@ -310,19 +304,24 @@ int psod_get_halos(psod_ctx *c, const psod_halo_table *t) {
   if (t->member_offset && (st = copy_out(c, t->member_offset, c->d_m_offset, sizeof(int64_t) * (nh + 1))))
     return st;
   if ((t->member_index || t->member_id) && nm > 0) {
+    // device destinations are written in place; host ones are staged
     long long *d_idx = nullptr, *d_id = nullptr;
-    if (t->member_index && (st = dalloc(c, &d_idx, (size_t)nm))) return st;
-    if (t->member_id && (st = dalloc(c, &d_id, (size_t)nm))) {
-      dfree(&d_idx);
-      return st;
+    if (t->member_index) {
+      if (is_device_ptr(t->member_index)) d_idx = reinterpret_cast<long long *>(t->member_index);
+      else if ((st = scratch(c, SLOT_OUT_IDX, (size_t)nm, &d_idx))) return st;
+    }
+    if (t->member_id) {
+      if (is_device_ptr(t->member_id)) d_id = reinterpret_cast<long long *>(t->member_id);
+      else if ((st = scratch(c, SLOT_OUT_ID, (size_t)nm, &d_id))) return st;
     }
     k_member_ids<<<(unsigned)((nm + 255) / 256), 256, 0, c->stream>>>(c->d_m_index, nm, c->d_ids, d_idx, d_id);
     st = PSOD_OK;
-    if (t->member_index) st = copy_out(c, t->member_index, d_idx, sizeof(int64_t) * nm);
-    if (!st && t->member_id) st = copy_out(c, t->member_id, d_id, sizeof(int64_t) * nm);
-    dfree(&d_idx);
-    dfree(&d_id);
+    if (t->member_index && (void *)d_idx != (void *)t->member_index)
+      st = copy_out(c, t->member_index, d_idx, sizeof(int64_t) * nm);
+    if (!st && t->member_id && (void *)d_id != (void *)t->member_id)
+      st = copy_out(c, t->member_id, d_id, sizeof(int64_t) * nm);
     if (st) return st;
+    PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
   }
   return PSOD_OK;
 }

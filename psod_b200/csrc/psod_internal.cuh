@@ -240,6 +240,42 @@ int scratch(psod_ctx *c, int id, size_t count, T **out) {
 void free_scratch(psod_ctx *c);
 void free_scratch_slot(psod_ctx *c, int id);
 
+// Scratch slots.  Device buffers beyond the particle arrays live in numbered
+// slots that only grow and are kept until the context is destroyed, so that
+// repeated steps allocate nothing.  Stages that never hold a slot at the same
+// time share it.  Slots 8-15 are the scan levels; 16-79 belong to the SOD
+// stage.
+enum : int {
+  SLOT_CIC_FLAG = 2,    // CIC: out-of-tile flag
+  SLOT_BIG_TAB = 3,     // cell sort: sub-cell slot tables of dense cells
+  SLOT_BIG_CELL = 4,    // cell sort: the dense cells
+  SLOT_LOAD_FLAGS = 5,  // cell sort: bad-position flag, dense-cell count
+  SLOT_PART_U32 = 6,    // n u32: cell ids (load), seed flags (tri_cic), member pool indices (SOD)
+  SLOT_PART_U64 = 7,    // n u64: seed prefix sums (tri_cic), member pool keys (SOD)
+  SLOT_CELL_U32 = 80,   // ncell+1 u32: cell counts (load), alive counts per cell (SOD)
+  SLOT_SORT_KEYS = 81,  // radix sort: key ping-pong buffer
+  SLOT_SORT_VALS = 82,  // radix sort: value ping-pong buffer
+  SLOT_SORT_HIST = 83,  // radix sort: per-tile digit counts
+  SLOT_SORT_RNG = 84,   // radix sort: key range
+  SLOT_TRI_KEYS = 85,   // tri_cic: seed sort keys
+  SLOT_TRI_MIN = 86,    // tri_cic: densest-non-seed key and index
+  SLOT_HOST_POS = 87,   // load: device copy of host positions
+  SLOT_VEL = 88,        // load: velocities
+  SLOT_SEED_IDX = 89,   // tri_cic: seed order (persistent)
+  SLOT_OUT_IDX = 90,    // psod_get_halos: member indices staged for a host copy
+  SLOT_OUT_ID = 91,     // psod_get_halos: member IDs staged for a host copy
+  SLOT_H_ID = 92,       // halo table (persistent until the next SOD call)
+  SLOT_H_MASS,
+  SLOT_H_RANK,
+  SLOT_H_MASS2,
+  SLOT_H_MEXTRA,
+  SLOT_H_PROFILE,
+  SLOT_H_CENTER,
+  SLOT_H_RDELTA,
+  SLOT_M_OFFSET,
+  SLOT_M_INDEX
+};
+
 bool is_device_ptr(const void *p);
 int copy_out(psod_ctx *c, void *dst, const void *dsrc, size_t bytes);
 int copy_in(psod_ctx *c, void *ddst, const void *src, size_t bytes);

@@ -37,6 +37,7 @@ constexpr int NWARP = TPB / 32;
 constexpr int NB = 4096;          // histogram buckets per level
 constexpr int MAXLEV = 4;         // histogram levels kept in shared memory
 constexpr int CAP = 2048;         // elements sorted in shared memory
+constexpr unsigned long long POOL_SORTED = 1ull << 63;
 constexpr unsigned long long L1_BASE = 128896ull;  // (1023-16) << 7
 constexpr int L1_SHIFT = 45;
 
@@ -61,7 +62,7 @@ struct SodBufs {
   unsigned *h_profile;         // cumulative counts (widened on output)
   float *h_center;
   double *h_rdelta;
-  unsigned long long *h_pool;  // pool offset
+  unsigned long long *h_pool;  // pool offset; top bit: members already in (d2, index) order
   unsigned long long *pool_key;  // d2 bits
   unsigned *pool_idx;            // input index
   unsigned long long *touched;
@@ -460,6 +461,75 @@ __device__ unsigned extract_sorted(const SodConst &K, const SodBufs &B, Smem &S,
     }
   }
   return n;
+}
+
+// Small balls.  When a seed's ball holds at most CAP alive records, one pass
+// loads them all (d2 bits, input index, cube position) and one bitonic sort
+// orders them by (d2 bits, index).  The crossing searches, the profile and
+// the claims then read the sorted list instead of visiting the cells again.
+// The positions live in the deepest histogram level, which this path never
+// uses.
+__device__ __forceinline__ unsigned *small_pos(Smem &S) { return S.hist[MAXLEV - 1]; }
+
+// every alive record of region G, sorted; returns the count, or CAP + 1 when
+// the region holds more than CAP (the list is then unusable)
+__device__ unsigned load_ball_sorted(const SodConst &K, const SodBufs &B, Smem &S, const Region &G) {
+  unsigned *spos = small_pos(S);
+  if (threadIdx.x == 0) S.nsorted = 0;
+  __syncthreads();
+  for_region(K, B, G, [&](unsigned p, float4 v) {
+    double d2;
+    if (!region_d2(K, G, v, d2)) return;
+    const unsigned s = atomicAdd(&S.nsorted, 1u);
+    if (s < CAP) {
+      S.skey[s] = dbits(d2);
+      S.sidx[s] = __float_as_uint(v.w) & PSOD_IDX_MASK;
+      spos[s] = p;
+    }
+  });
+  __syncthreads();
+  const unsigned n = S.nsorted;
+  __syncthreads();
+  if (n > CAP) return CAP + 1;
+  unsigned m = 1;
+  while (m < n) m <<= 1;
+  for (unsigned k = n + threadIdx.x; k < m; k += TPB) {
+    S.skey[k] = ~0ull;
+    S.sidx[k] = 0xffffffffu;
+  }
+  __syncthreads();
+  for (unsigned size = 2; size <= m; size <<= 1) {
+    for (unsigned stride = size >> 1; stride > 0; stride >>= 1) {
+      for (unsigned k = threadIdx.x; k < m / 2; k += TPB) {
+        const unsigned a = 2 * k - (k & (stride - 1)), bb = a + stride;
+        const bool up = ((a & size) == 0);
+        const unsigned long long ka = S.skey[a], kb = S.skey[bb];
+        const unsigned ia = S.sidx[a], ib = S.sidx[bb];
+        const bool gt = (ka > kb) || (ka == kb && ia > ib);
+        if (gt == up) {
+          S.skey[a] = kb;
+          S.skey[bb] = ka;
+          S.sidx[a] = ib;
+          S.sidx[bb] = ia;
+          const unsigned pa = spos[a];
+          spos[a] = spos[bb];
+          spos[bb] = pa;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  return n;
+}
+
+// forward crossing search over the sorted list [0, n): the first 1-based
+// position i >= 10 where the reference's loop stops (main:2046); 0 if none
+__device__ long long sorted_stop(const SodConst &K, Smem &S, unsigned n, long long na, double delta) {
+  int best = 0x7fffffff;
+  for (unsigned k = 9 + threadIdx.x; k < n; k += TPB)
+    if (!keeps_going(K, (long long)k + 1, bitsd(S.skey[k]), na, delta)) best = min(best, (int)k);
+  best = block_min_i(S, best);
+  return best == 0x7fffffff ? 0 : (long long)best + 1;
 }
 
 // Search over the sorted d2 sequence of the cube.
@@ -1003,7 +1073,7 @@ __global__ void __launch_bounds__(256, 4) k_refine_warp(SodConst K, SodBufs B) {
   __shared__ int s_nr[8], s_wf[8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned nitems = B.chunk_pref[B.nitems_cells];
-  unsigned long long visits = 0, slots = 0;
+  unsigned long long visits = 0, slots = 0, loaded = 0;
   while (true) {
     unsigned item = 0, ci = 0, rem = 0;
     if (lane == 0) {
@@ -1119,6 +1189,7 @@ __global__ void __launch_bounds__(256, 4) k_refine_warp(SodConst K, SodBufs B) {
           }
         }
         const unsigned m = __ballot_sync(0xffffffffu, keep);
+        loaded += min(32u, r1 - pos);
         const unsigned need = 32u - fill, rank = __popc(m & lt);
         if (keep && rank < need) s_tile[w][fill + rank] = rec;
         const unsigned got = __popc(m);
@@ -1166,6 +1237,7 @@ __global__ void __launch_bounds__(256, 4) k_refine_warp(SodConst K, SodBufs B) {
   }
   if (lane == 0 && visits) atomicAdd(B.pairs, visits);
   if (lane == 0 && slots) atomicAdd(B.pair_slots, slots);
+  if (lane == 0 && loaded) atomicAdd(B.pair_slots + 1, loaded);
 }
 
 // ---------------------------------------------------------------------------
@@ -1303,9 +1375,37 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
   const unsigned cidx = __float_as_uint(cvv.w) & PSOD_IDX_MASK;
   const double rb0 = (B.mode == PSOD_MODE_PLAIN) ? -1.0 : 1.5;
 
-  // 3. crossing (main:2040-2100)
+  // 3. crossing (main:2040-2100).  Balls of at most CAP alive records are
+  // sorted whole (small path); larger ones go through the histogram search
+  // from the first ball that overflowed.
   double d2stop = 0;
-  long long istop = bracketed_stop(K, B, S, G, rb0, na, na_known, K.delta, &d2stop);
+  long long istop = 0;
+  bool small = false;
+  unsigned nball = 0;
+  {
+    double rb = rb0;
+    while (true) {
+      const bool full = !(rb > 0.0) || rb >= (double)K.ncut;
+      G.rb = full ? -1.0 : rb;
+      G.rb2 = full ? -1.0 : rb * rb;
+      if (full && !na_known) {
+        na = count_alive_cube(K, B, S, G.ic, G.jc, G.kc);
+        na_known = true;
+      }
+      const unsigned n = load_ball_sorted(K, B, S, G);
+      if (n > CAP) break;
+      const long long i = sorted_stop(K, S, n, full ? (long long)na : 0x7fffffffffffffffll, K.delta);
+      if (i != 0 || full) {
+        istop = i;
+        if (i > 0) d2stop = bitsd(S.skey[i - 1]);
+        small = true;
+        nball = n;
+        break;
+      }
+      rb *= 2.0;
+    }
+    if (!small) istop = bracketed_stop(K, B, S, G, G.rb2 < 0.0 ? -1.0 : G.rb, na, na_known, K.delta, &d2stop);
+  }
   if (istop <= 0) {
     if (threadIdx.x == 0) record_error(B, rank, PSOD_ERR_STATE);
     return;
@@ -1327,7 +1427,10 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
   // the masse-th element closes the member set (main:2090-2100, 2148)
   unsigned long long thr_key;
   unsigned thr_idx;
-  {
+  if (small) {
+    thr_key = S.skey[masse - 1];
+    thr_idx = S.sidx[masse - 1];
+  } else {
     const int hk = S.res_k;
     const unsigned long long blo = S.res_lo;
     __syncthreads();
@@ -1343,7 +1446,13 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
   // seuil2 capture (main:2062-2069): last step i in [2, istop] above seuil2;
   // every such step lies inside the region that held the stop
   long long masse2 = 0;
-  {
+  if (small) {
+    int best = -1;
+    for (unsigned k = 1 + threadIdx.x; k < (unsigned)istop; k += TPB)
+      if (overdens(K, (long long)k + 1, bitsd(S.skey[k])) > K.delta2) best = max(best, (int)k);
+    best = block_max_i(S, best);
+    if (best >= 0) masse2 = best + 1;
+  } else {
     double dd;
     const long long na_eff = G.rb2 < 0.0 ? (long long)na : 0x7fffffffffffffffll;
     long long i2 = radial_search(K, B, S, G, na_eff, K.delta2, 1, istop, &dd);
@@ -1352,10 +1461,20 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
   // extra thresholds: the same stop rule, -1 when not crossed
   long long mext[PSOD_MAX_EXTRA_DELTA];
   for (int e = 0; e < K.ndx; e++) {
-    double dd;
-    Region Ge = G;
-    const double rbe = G.rb2 < 0.0 ? -1.0 : G.rb;
-    long long ie = bracketed_stop(K, B, S, Ge, rbe, na, na_known, K.dx_extra[e], &dd);
+    double dd = 0.0;
+    long long ie = 0;
+    if (small) {
+      ie = sorted_stop(K, S, nball, G.rb2 < 0.0 ? (long long)na : 0x7fffffffffffffffll, K.dx_extra[e]);
+      if (ie > 0) dd = bitsd(S.skey[ie - 1]);
+    }
+    if (!small || (ie == 0 && G.rb2 >= 0.0)) {
+      // the stop lies outside the sorted ball: the histogram search takes
+      // over, and the list is no longer valid
+      small = false;
+      Region Ge = G;
+      const double rbe = G.rb2 < 0.0 ? -1.0 : G.rb;
+      ie = bracketed_stop(K, B, S, Ge, rbe, na, na_known, K.dx_extra[e], &dd);
+    }
     mext[e] = (ie <= 0 || overdens(K, ie, dd) > K.dx_extra[e]) ? -1 : ie - 1;
   }
 
@@ -1371,6 +1490,22 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
     for (int j = threadIdx.x; j <= K.nbins; j += TPB) S.phist[j] = 0;
     __syncthreads();
     const double emax = S.edges[K.nbins - 1];
+    if (small && (G.rb2 < 0.0 || emax * (1.0 + 1e-9) < G.rb)) {
+      // every particle closer than the last edge is in the sorted list:
+      // cumulative counts by binary search, one bin per thread
+      for (int j = threadIdx.x; j < K.nbins; j += TPB) {
+        unsigned lo = 0, hi = nball;  // first k with r_k >= edge
+        while (lo < hi) {
+          const unsigned mid = (lo + hi) >> 1;
+          if (dsqrt(bitsd(S.skey[mid])) < S.edges[j]) lo = mid + 1;
+          else hi = mid;
+        }
+        S.pref[j] = lo;
+      }
+      __syncthreads();
+      for (int j = threadIdx.x; j < K.nbins; j += TPB) S.phist[j] = S.pref[j] - (j > 0 ? S.pref[j - 1] : 0u);
+      __syncthreads();
+    } else {
     Region Gp = G;
     if (Gp.rb2 >= 0.0 && !(emax * (1.0 + 1e-9) < Gp.rb)) {
       const double r = emax * 1.01 + 0.01;
@@ -1396,6 +1531,7 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
       atomicAdd(&S.phist[lo], 1u);
     });
     __syncthreads();
+    }
     if (threadIdx.x == 0) {
       S.pool_base = atomicAdd(B.pool_used, (unsigned long long)masse);
       S.claim_cnt = 0;
@@ -1408,6 +1544,21 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
 
   // 4b. claims (main:2148-2166): the masse nearest die, kept or not
   const unsigned long long pool_base = S.pool_base;
+  if (small) {
+    // the first masse entries of the sorted list
+    const unsigned *spos = small_pos(S);
+    for (unsigned k = threadIdx.x; k < (unsigned)masse; k += TPB) {
+      const unsigned p = spos[k];
+      const float4 v = B.cube[p];
+      B.cube[p].w = __uint_as_float(__float_as_uint(v.w) | PSOD_DEAD_BIT);
+      if (B.alive_cnt) atomicSub(&B.alive_cnt[listed_cell(K, p, v)], 1u);
+      if (keep) {
+        B.pool_key[pool_base + k] = S.skey[k];
+        B.pool_idx[pool_base + k] = S.sidx[k];
+      }
+    }
+    if (threadIdx.x == 0) S.claim_cnt = (unsigned)masse;
+  } else
   for_region(K, B, G, [&](unsigned p, float4 v) {
     double d2;
     if (!region_d2(K, G, v, d2)) return;
@@ -1442,7 +1593,7 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
     B.h_center[3 * hs + 0] = __double2float_rn(ddiv(xc, K.scale));
     B.h_center[3 * hs + 1] = __double2float_rn(ddiv(yc, K.scale));
     B.h_center[3 * hs + 2] = __double2float_rn(ddiv(zc, K.scale));
-    B.h_pool[hs] = pool_base;
+    B.h_pool[hs] = pool_base | (small ? POOL_SORTED : 0ull);
     for (int e = 0; e < K.ndx; e++) B.h_mextra[hs * K.ndx + e] = mext[e];
     unsigned run = 0;
     for (int j = 0; j < K.nbins; j++) {
@@ -1513,46 +1664,68 @@ __global__ void k_init_active(long long nblocks, const unsigned *bbegin, unsigne
 // Warp per active block: advance the cursor past resolved (processed or
 // claimed) seeds, 256 entries per step with independent loads; head = the
 // lowest unresolved rank.  Blocks that still hold seeds go to next_active.
+// One lane per active block: the head is the block's first unresolved seed
+// at or after its cursor.  Most heads are the cursor's own slot; blocks whose
+// cursor slot was resolved are walked by the whole warp, 32 slots a step.
 __global__ void k_heads(const unsigned *active, unsigned nactive, const unsigned *bbegin, unsigned *cursor,
                         const unsigned *blist, const unsigned *bpos, const unsigned char *processed,
                         const float4 *cube, unsigned *head, unsigned *gmin, unsigned *next_active,
                         unsigned *n_next) {
-  const unsigned wid = (unsigned)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
-  if (wid >= nactive) return;
-  const unsigned b = active[wid];
-  unsigned cur = cursor[b];
-  const unsigned end = bbegin[b + 1];
-  unsigned h = PSOD_INF_RANK;
-  while (cur < end) {
-    unsigned m[8];
-#pragma unroll
-    for (int k = 0; k < 8; k++) {
-      const unsigned idx = cur + (unsigned)(k * 32 + lane);
+  const bool have = i < nactive;
+  unsigned b = 0, cur = 0, end = 0, h = PSOD_INF_RANK;
+  bool walk = false;
+  if (have) {
+    b = active[i];
+    cur = cursor[b];
+    end = bbegin[b + 1];
+    if (cur < end) {
+      if (!processed[blist[cur]] && !(__float_as_uint(cube[bpos[cur]].w) & PSOD_DEAD_BIT)) {
+        h = blist[cur];
+      } else {
+        walk = true;
+        cur++;
+      }
+    }
+  }
+  unsigned wm = __ballot_sync(0xffffffffu, walk);
+  while (wm) {
+    const int src = __ffs(wm) - 1;
+    wm &= wm - 1;
+    unsigned c = __shfl_sync(0xffffffffu, cur, src);
+    const unsigned e = __shfl_sync(0xffffffffu, end, src);
+    unsigned hh = PSOD_INF_RANK;
+    while (c < e) {
+      const unsigned idx = c + (unsigned)lane;
       bool unres = false;
-      if (idx < end) unres = !processed[blist[idx]] && !(__float_as_uint(cube[bpos[idx]].w) & PSOD_DEAD_BIT);
-      m[k] = __ballot_sync(0xffffffffu, unres);
+      if (idx < e) unres = !processed[blist[idx]] && !(__float_as_uint(cube[bpos[idx]].w) & PSOD_DEAD_BIT);
+      const unsigned m = __ballot_sync(0xffffffffu, unres);
+      if (m) {
+        c += (unsigned)(__ffs(m) - 1);
+        hh = blist[c];
+        break;
+      }
+      c += 32u;
     }
-    int found = -1;
-#pragma unroll
-    for (int k = 7; k >= 0; k--)
-      if (m[k]) found = k * 32 + __ffs(m[k]) - 1;
-    if (found >= 0) {
-      cur += (unsigned)found;
-      h = blist[cur];
-      break;
-    }
-    cur += 256u;
-  }
-  if (cur > end) cur = end;
-  if (lane == 0) {
-    cursor[b] = cur;
-    head[b] = h;
-    if (h != PSOD_INF_RANK) {
-      next_active[atomicAdd(n_next, 1u)] = b;
-      if (gmin) atomicMin(gmin, h);
+    if (c > e) c = e;
+    if (lane == src) {
+      cur = c;
+      h = hh;
     }
   }
+  const bool live = have && h != PSOD_INF_RANK;
+  const unsigned lm = __ballot_sync(0xffffffffu, live);
+  unsigned base = 0;
+  if (lane == 0 && lm) base = atomicAdd(n_next, (unsigned)__popc(lm));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  unsigned hmin = live ? h : PSOD_INF_RANK;
+  for (int o = 16; o > 0; o >>= 1) hmin = min(hmin, __shfl_xor_sync(0xffffffffu, hmin, o));
+  if (gmin && lane == 0 && hmin != PSOD_INF_RANK) atomicMin(gmin, hmin);
+  if (!have) return;
+  cursor[b] = cur;
+  head[b] = h;
+  if (live) next_active[base + __popc(lm & ((1u << lane) - 1u))] = b;
 }
 
 // periodic sliding minimum of radius rb along one axis of the nb^3 grid
@@ -1639,8 +1812,14 @@ __global__ void __launch_bounds__(256) k_member_sort(const unsigned *order, long
   __shared__ unsigned si[MS_CHUNK];
   for (long long h = blockIdx.x; h < nh; h += gridDim.x) {
     const unsigned slot = order[h];
-    const unsigned long long base = h_pool[slot];
+    const unsigned long long base = h_pool[slot] & ~POOL_SORTED;
     const unsigned m = (unsigned)h_mass_sorted[h];
+    if (h_pool[slot] & POOL_SORTED) {
+      // claimed from a sorted list: already in (d2, index) order
+      const unsigned o = moff[h];
+      for (unsigned k = threadIdx.x; k < m; k += blockDim.x) m_index[o + k] = pidx[base + k];
+      continue;
+    }
     unsigned long long *ka = pkey + base, *kb = tkey + base;
     unsigned *ia = pidx + base, *ib = tidx + base;
     // 1. sort chunks in shared memory
@@ -1761,9 +1940,9 @@ SodConst make_sod_const(const psod_ctx *c) {
 enum {
   SC_BLOCK_OF = 16, SC_BLIST, SC_BBEGIN, SC_CURSOR, SC_HEAD, SC_FILT_A, SC_FILT_B, SC_READY, SC_CTRS,
   SC_PROCESSED, SC_U64, SC_EDGES, SC_HRANK, SC_HID, SC_HMASS, SC_HMASS2, SC_HMEXTRA, SC_HPROF, SC_HCENTER,
-  SC_HRDELTA, SC_HPOOL, SC_POOLKEY, SC_POOLIDX, SC_COUNTS, SC_ST_ACTIVE, SC_ST_NA, SC_ST_COFF, SC_ST_CN,
+  SC_HRDELTA, SC_HPOOL, SC_COUNTS, SC_ST_ACTIVE, SC_ST_NA, SC_ST_COFF, SC_ST_CN,
   SC_ST_CENTRE, SC_CAND_POS, SC_CAND_SLOT, SC_CAND_S, SC_ORDER, SC_RKEYS, SC_MASS32, SC_MOFF, SC_TKEY, SC_TIDX,
-  SC_ALIVE, SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS, SC_CELLNCH
+  SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS, SC_CELLNCH
 };
 
 struct PhaseTimer {
@@ -1843,7 +2022,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       (rc = scratch(c, SC_HMASS2, (size_t)hcap, &h_mass2)) || (rc = scratch(c, SC_HMEXTRA, (size_t)hcap * ne, &h_mextra)) ||
       (rc = scratch(c, SC_HPROF, (size_t)hcap * c->p.nbins, &h_profile)) || (rc = scratch(c, SC_HCENTER, (size_t)hcap * 3, &h_center)) ||
       (rc = scratch(c, SC_HRDELTA, (size_t)hcap, &h_rdelta)) || (rc = scratch(c, SC_HPOOL, (size_t)hcap, &h_pool)) ||
-      (rc = scratch(c, SC_POOLKEY, (size_t)n, &pool_key)) || (rc = scratch(c, SC_POOLIDX, (size_t)n, &pool_idx)) ||
+      (rc = scratch(c, SLOT_PART_U64, (size_t)n, &pool_key)) || (rc = scratch(c, SLOT_PART_U32, (size_t)n, &pool_idx)) ||
       (rc = scratch(c, SC_ST_ACTIVE, (size_t)nblocks + 1, &st_active)) || (rc = scratch(c, SC_ST_NA, (size_t)nblocks + 1, &st_na)) ||
       (rc = scratch(c, SC_ST_COFF, (size_t)nblocks + 1, &st_coff)) || (rc = scratch(c, SC_ST_CN, (size_t)nblocks + 1, &st_cn)) ||
       (rc = scratch(c, SC_ST_CENTRE, (size_t)nblocks + 1, &st_centre)) || (rc = scratch(c, SC_CAND_POS, (size_t)cand_cap, &cand_pos)) ||
@@ -1968,7 +2147,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.mode = c->p.mode;
   if (c->p.mode != PSOD_MODE_PLAIN) {
     unsigned *alive_cnt;
-    if ((rc = scratch(c, SC_ALIVE, (size_t)c->ncell, &alive_cnt))) return rc;
+    if ((rc = scratch(c, SLOT_CELL_U32, (size_t)c->ncell, &alive_cnt))) return rc;
     k_init_alive<<<nblk((long long)c->ncell, 256), 256, 0, c->stream>>>(c->d_cell_start, c->ncell, alive_cnt);
     kernels++;
     B.alive_cnt = alive_cnt;
@@ -1994,7 +2173,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     PSOD_CUDA(c, cudaMemsetAsync(gmin, 0xff, sizeof(unsigned), c->stream));
     PSOD_CUDA(c, cudaMemsetAsync(cand_used, 0, sizeof(unsigned), c->stream));
     PSOD_CUDA(c, cudaMemsetAsync(ctrs + 9, 0, sizeof(unsigned), c->stream));
-    k_heads<<<nblk((long long)n_active * 32, 256), 256, 0, c->stream>>>(
+    k_heads<<<nblk((long long)n_active, 256), 256, 0, c->stream>>>(
         act_a, n_active, bbegin, cursor, blist, bpos, processed, c->d_cube, head,
         quirk_rank != PSOD_INF_RANK ? gmin : nullptr, act_b, ctrs + 9);
     k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(head, filt_a, nb, 0, rb);
@@ -2035,9 +2214,14 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     t_cross.collect();
     if (trace) {
       unsigned cu = 0;
+      unsigned long long tv[16];
       cudaMemcpy(&cu, cand_used, sizeof(unsigned), cudaMemcpyDeviceToHost);
-      fprintf(stderr, "psod round %lld ready %u active %u cand %u sched %.3f prep %.3f refine %.3f select %.3f cross %.3f\n",
-              rounds, nready, n_active, cu, t_sched.last, t_prep.last, t_ref.last, t_sel.last, t_cross.last);
+      cudaMemcpy(tv, u64s, sizeof(tv), cudaMemcpyDeviceToHost);
+      fprintf(stderr,
+              "psod round %lld ready %u active %u cand %u sched %.3f prep %.3f refine %.3f select %.3f cross %.3f "
+              "pairs %llu slots %llu staged %llu\n",
+              rounds, nready, n_active, cu, t_sched.last, t_prep.last, t_ref.last, t_sel.last, t_cross.last, tv[5], tv[8],
+              tv[9]);
     }
     rounds++;
     seed_launches += 4;
@@ -2095,16 +2279,16 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
     if ((rc = radix_sort_u32(c, rkeys, order, nh, 32))) return rc;
   }
-  if ((rc = dalloc(c, &c->d_h_id, (size_t)nh))) return rc;
-  if ((rc = dalloc(c, &c->d_h_mass, (size_t)nh))) return rc;
-  if ((rc = dalloc(c, &c->d_h_rank, (size_t)nh))) return rc;
-  if ((rc = dalloc(c, &c->d_h_mass2, (size_t)nh))) return rc;
-  if ((rc = dalloc(c, &c->d_h_mextra, (size_t)nh * ne))) return rc;
-  if ((rc = dalloc(c, &c->d_h_profile, (size_t)nh * c->p.nbins))) return rc;
-  if ((rc = dalloc(c, &c->d_h_center, (size_t)nh * 3))) return rc;
-  if ((rc = dalloc(c, &c->d_h_rdelta, (size_t)nh))) return rc;
-  if ((rc = dalloc(c, &c->d_m_offset, (size_t)nh + 1))) return rc;
-  if ((rc = dalloc(c, &c->d_m_index, (size_t)npool))) return rc;
+  if ((rc = scratch(c, SLOT_H_ID, (size_t)nh, &c->d_h_id)) || (rc = scratch(c, SLOT_H_MASS, (size_t)nh, &c->d_h_mass)) ||
+      (rc = scratch(c, SLOT_H_RANK, (size_t)nh, &c->d_h_rank)) ||
+      (rc = scratch(c, SLOT_H_MASS2, (size_t)nh, &c->d_h_mass2)) ||
+      (rc = scratch(c, SLOT_H_MEXTRA, (size_t)nh * ne, &c->d_h_mextra)) ||
+      (rc = scratch(c, SLOT_H_PROFILE, (size_t)nh * c->p.nbins, &c->d_h_profile)) ||
+      (rc = scratch(c, SLOT_H_CENTER, (size_t)nh * 3, &c->d_h_center)) ||
+      (rc = scratch(c, SLOT_H_RDELTA, (size_t)nh, &c->d_h_rdelta)) ||
+      (rc = scratch(c, SLOT_M_OFFSET, (size_t)nh + 1, &c->d_m_offset)) ||
+      (rc = scratch(c, SLOT_M_INDEX, (size_t)npool, &c->d_m_index)))
+    return rc;
   if (nh > 0) {
     const unsigned g1 = nblk(nh, 256);
     k_gather<long long><<<g1, 256, 0, c->stream>>>(h_id, order, nh, 1, c->d_h_id);

@@ -208,7 +208,7 @@ int radix_sort_impl(psod_ctx *c, K *keys, unsigned *vals, long long n, int end_b
   if (n <= 1) return PSOD_OK;
   // digits every key shares need no pass: find the highest differing bit
   unsigned long long *d_rng = nullptr;
-  int st = dalloc(c, &d_rng, 2);
+  int st = scratch(c, SLOT_SORT_RNG, 2, &d_rng);
   if (st) return st;
   unsigned long long init[2] = {~0ull, 0ull};
   PSOD_CUDA(c, cudaMemcpyAsync(d_rng, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
@@ -216,7 +216,6 @@ int radix_sort_impl(psod_ctx *c, K *keys, unsigned *vals, long long n, int end_b
   unsigned long long rng[2] = {0, ~0ull};
   PSOD_CUDA(c, cudaMemcpyAsync(rng, d_rng, sizeof(rng), cudaMemcpyDeviceToHost, c->stream));
   PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
-  dfree(&d_rng);
   unsigned long long diff = rng[0] ^ rng[1];
   if (diff == 0) return PSOD_OK;  // all keys equal: a stable sort is the identity
   int hi_bit = 64 - __builtin_clzll(diff);
@@ -225,16 +224,9 @@ int radix_sort_impl(psod_ctx *c, K *keys, unsigned *vals, long long n, int end_b
   long long ntiles = (n + RS_TILE - 1) / RS_TILE;
   K *tk = nullptr;
   unsigned *tv = nullptr, *hist = nullptr;
-  if ((st = dalloc(c, &tk, (size_t)n))) return st;
-  if ((st = dalloc(c, &tv, (size_t)n))) {
-    dfree(&tk);
-    return st;
-  }
-  if ((st = dalloc(c, &hist, (size_t)ntiles * RS_RADIX + 1))) {
-    dfree(&tk);
-    dfree(&tv);
-    return st;
-  }
+  if ((st = scratch(c, SLOT_SORT_KEYS, (size_t)n, &tk))) return st;
+  if ((st = scratch(c, SLOT_SORT_VALS, (size_t)n, &tv))) return st;
+  if ((st = scratch(c, SLOT_SORT_HIST, (size_t)ntiles * RS_RADIX + 1, &hist))) return st;
   K *ka = keys, *kb = tk;
   unsigned *va = vals, *vb = tv;
   for (int dgt = 0; dgt < ndigits; dgt++) {
@@ -256,9 +248,6 @@ int radix_sort_impl(psod_ctx *c, K *keys, unsigned *vals, long long n, int end_b
   }
   cudaError_t e = cudaGetLastError();
   cudaStreamSynchronize(c->stream);
-  dfree(&tk);
-  dfree(&tv);
-  dfree(&hist);
   if (st) return st;
   if (e != cudaSuccess) return cuda_check(c, e, "radix_sort");
   return PSOD_OK;

@@ -437,9 +437,9 @@ int stage_cellsort(psod_ctx *c, const float *dpos) {
   int st;
   unsigned *cell = nullptr, *count = nullptr;
   int *bad = nullptr;
-  if ((st = scratch(c, 3, (size_t)n, &cell))) return st;
-  if ((st = scratch(c, 4, (size_t)c->ncell + 1, &count))) return st;
-  if ((st = scratch(c, 5, 2, &bad))) return st;
+  if ((st = scratch(c, SLOT_PART_U32, (size_t)n, &cell))) return st;
+  if ((st = scratch(c, SLOT_CELL_U32, (size_t)c->ncell + 1, &count))) return st;
+  if ((st = scratch(c, SLOT_LOAD_FLAGS, 2, &bad))) return st;
   if ((st = ensure(c, &c->d_cell_start, &c->cs_cap, (size_t)c->ncell + 1))) return st;
   if ((st = ensure(c, &c->d_cube, &c->cube_cap, (size_t)n))) return st;
   if ((st = ensure(c, &c->d_inv, &c->inv_cap, (size_t)n))) return st;
@@ -458,8 +458,8 @@ int stage_cellsort(psod_ctx *c, const float *dpos) {
   const unsigned hnbig = (unsigned)hflags[1];
   unsigned *tab = nullptr, *bigcell = nullptr;
   if (!hbad) {
-    if ((st = scratch(c, 6, (size_t)hnbig * SUB_N + 1, &tab))) return st;
-    if ((st = scratch(c, 7, (size_t)hnbig + 1, &bigcell))) return st;
+    if ((st = scratch(c, SLOT_BIG_TAB, (size_t)hnbig * SUB_N + 1, &tab))) return st;
+    if ((st = scratch(c, SLOT_BIG_CELL, (size_t)hnbig + 1, &bigcell))) return st;
     PSOD_CUDA(c, cudaMemsetAsync(nbig, 0, sizeof(unsigned), c->stream));
     PSOD_CUDA(c, cudaMemsetAsync(tab, 0, sizeof(unsigned) * ((size_t)hnbig * SUB_N + 1), c->stream));
     k_mark_big<<<nblk(ncell, 256), 256, 0, c->stream>>>(count, c->ncell, nbig, true, bigcell);
@@ -472,12 +472,6 @@ int stage_cellsort(psod_ctx *c, const float *dpos) {
     PSOD_CUDA(c, cudaGetLastError());
     PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
   }
-  // the per-particle cell ids, per-cell counts and sub-cell tables are only
-  // needed here
-  free_scratch_slot(c, 3);
-  free_scratch_slot(c, 4);
-  free_scratch_slot(c, 6);
-  free_scratch_slot(c, 7);
   if (hbad) return set_err(c, PSOD_ERR_ARG, "particle positions must lie in [0,1] (box units)");
 
   // The reference's run scan (main:1591-1604) files a final cell holding a
@@ -540,7 +534,7 @@ int stage_cic(psod_ctx *c, double *grid_out) {
   bool tiled = false;
   if (c->nx % CT == 0 && c->nx >= 2 * (CT + 2) && c->xxmin <= 0.0 && -c->xxmin + 1.0 >= 1.0) {
     int *bad = nullptr;
-    if ((st = scratch(c, 2, 1, &bad))) return st;
+    if ((st = scratch(c, SLOT_CIC_FLAG, 1, &bad))) return st;
     PSOD_CUDA(c, cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
     const int smem = CW3 * (int)sizeof(unsigned long long);
     PSOD_CUDA(c, cudaFuncSetAttribute(k_cic_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -593,10 +587,10 @@ int stage_tri_cic(psod_ctx *c, int64_t *isort_out) {
   int st;
   unsigned *flag = nullptr, *posn = nullptr, *minidx = nullptr;
   unsigned long long *minbits = nullptr, *keys = nullptr;
-  if ((st = dalloc(c, &flag, (size_t)n))) return st;
-  if ((st = dalloc(c, &posn, (size_t)n + 1))) return st;
-  if ((st = dalloc(c, &minbits, 1))) return st;
-  if ((st = dalloc(c, &minidx, 1))) return st;
+  if ((st = scratch(c, SLOT_PART_U32, (size_t)n, &flag))) return st;
+  if ((st = scratch(c, SLOT_PART_U64, (size_t)n + 1, &posn))) return st;
+  if ((st = scratch(c, SLOT_TRI_MIN, 2, &minbits))) return st;
+  minidx = reinterpret_cast<unsigned *>(minbits + 1);
   PSOD_CUDA(c, cudaMemsetAsync(minbits, 0xff, sizeof(unsigned long long), c->stream));
   PSOD_CUDA(c, cudaMemsetAsync(minidx, 0xff, sizeof(unsigned), c->stream));
   k_seed_flags<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_rho, n, flag, minbits);
@@ -609,8 +603,8 @@ int stage_tri_cic(psod_ctx *c, int64_t *isort_out) {
   const bool has_extra = hmin != ~0ull;
   if (has_extra) k_seed_extra_idx<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_rho, n, hmin, minidx);
   const long long nseed = (long long)nd + (has_extra ? 1 : 0);
-  if ((st = dalloc(c, &keys, (size_t)nd + 1))) return st;
-  if ((st = dalloc(c, &c->d_seed_idx, (size_t)nseed + 1))) return st;
+  if ((st = scratch(c, SLOT_TRI_KEYS, (size_t)nd + 1, &keys))) return st;
+  if ((st = scratch(c, SLOT_SEED_IDX, (size_t)nseed + 1, &c->d_seed_idx))) return st;
   k_seed_compact<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_rho, n, flag, posn, keys, c->d_seed_idx);
   // seeds arrive in input order; a stable sort on 1/rho leaves ties in
   // input order
@@ -619,11 +613,6 @@ int stage_tri_cic(psod_ctx *c, int64_t *isort_out) {
     PSOD_CUDA(c, cudaMemcpyAsync(c->d_seed_idx + nd, minidx, sizeof(unsigned), cudaMemcpyDeviceToDevice, c->stream));
   PSOD_CUDA(c, cudaGetLastError());
   PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
-  dfree(&flag);
-  dfree(&posn);
-  dfree(&minbits);
-  dfree(&minidx);
-  dfree(&keys);
   c->nseed_dense = nd;
   c->npart_new = nseed;  // main:1032 (clamped to n when every particle is dense)
   if (isort_out && nseed > 0) {
