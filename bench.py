@@ -39,6 +39,11 @@ WORKLOADS = {
 }
 
 
+# the 1024^3 workload computes three thresholds in one pass, with 48 bins
+EXTRA_DELTAS = (500.0, 178.0)
+EXTRA_BINS = 48
+
+
 def npu_for(nx):
     return {128: 0, 256: 0, 512: 200000, 1024: 1000000}.get(nx, 0)
 
@@ -136,7 +141,7 @@ def run_ours(args):
     import torch
 
     from psod_b200 import synth
-    from psod_b200.sod import SphericalOverdensity
+    from psod_b200.sod import HaloTable, SphericalOverdensity
 
     world, rank, local = dist_setup()
     dev = local if world > 1 else 0
@@ -150,8 +155,8 @@ def run_ours(args):
     n = int(pos_d.shape[0])
     params = dict(npu=npu_for(nx), mode=args.mode_id)
     if args.ndelta:
-        params["delta_extra"] = (500.0, 178.0)
-        params["nbins"] = 48
+        params["delta_extra"] = EXTRA_DELTAS
+        params["nbins"] = EXTRA_BINS
     sod = SphericalOverdensity(nx, device=dev, **params)
     # L2 flush buffer (used when the inputs are smaller than L2)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
@@ -186,14 +191,17 @@ def run_ours(args):
     pos_h = pos_d.cpu().pin_memory()
     ids_h = ids_d.cpu().pin_memory()
     t = sod.halos(members=True)
-    nm = t.member_index.shape[0]
+    # pinned host buffers for the halo table, reused every step
+    tdt = {np.dtype(np.int64): torch.int64, np.dtype(np.float32): torch.float32, np.dtype(np.float64): torch.float64}
+    out = HaloTable(**{f: torch.empty(max(1, getattr(t, f).size), dtype=tdt[getattr(t, f).dtype], pin_memory=True)
+                       for f in HaloTable.__dataclass_fields__})
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         sod.load(pos_h, ids_h)
         sod.run()
-        t = sod.halos(members=True)
+        sod.halos(members=True, out=out)
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
     e2e_ms = max_over_ranks(e2e_ms, world)
@@ -215,6 +223,13 @@ def run_ours(args):
     # the refinement kernel dominates: FP32 pair tests fed from shared memory
     ref_s = s["ms_refine"] / 1000.0
     pairs_per_s = s["refine_pairs"] / ref_s if ref_s > 0 else 0.0
+    # issue ceiling of the pair test: 12 warp instructions per 32 pairs (one
+    # shared load, 3 FADD + 3 FFMA for d2 + eps^2, edge FADD + FMNMX, FSETP,
+    # MUFU.RSQ, predicated FADD), one instruction per clock per sub-partition
+    clocks = clk.summary()
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    props = torch.cuda.get_device_properties(dev)
+    ceiling = props.multi_processor_count * 4 * sm_mhz * 1e6 * 32 / 12.0
     line = {
         "metric": "SOD halos/s (delta=200, N200 exact)",
         "value": round(value, 2),
@@ -241,7 +256,8 @@ def run_ours(args):
             "processed_seeds": s["nprocessed"],
             "rounds": s["rounds"],
             "stage_ms": {k: round(v, 2) for k, v in stage_ms.items()},
-            "sod_phase_ms": {k: round(s[k], 2) for k in ("ms_sched", "ms_prep", "ms_refine", "ms_select", "ms_cross")},
+            "sod_phase_ms": {k: round(s[k], 2) for k in ("ms_setup", "ms_sched", "ms_prep", "ms_refine", "ms_select",
+                                                         "ms_cross", "ms_output")},
             "l2": "flushed between steps" if need_flush else "inputs larger than L2",
             "parallelism": f"replicas x{world}",
         },
@@ -267,13 +283,16 @@ def run_ours(args):
             "kernel_ms": round(s["ms_cross"], 3),
         },
         "refine": {
-            "kernel": "k_refine_warp (dominant: FP32 pair tests from shared memory)",
+            "kernel": "k_refine_warp (dominant by time: FP32/MUFU pair tests fed from shared memory)",
+            "bound": "instruction issue (neither hbm nor tensor)",
             "pairs": int(s["refine_pairs"]),
             "pairs_per_s": round(pairs_per_s, 1),
+            "issue_ceiling_pairs_per_s": round(ceiling, 1),
+            "frac_of_issue_ceiling": round(pairs_per_s / ceiling, 4) if ceiling > 0 else None,
             "lane_utilization": round(s["refine_pairs"] / max(1, s["refine_slots"]), 4),
             "kernel_ms": round(s["ms_refine"], 3),
         },
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
     if args.compare_plain and args.mode != "plain" and world == 1:
         line["plain"] = plain_reference(args, nx, params, pos_d, ids_d, sod)
@@ -341,12 +360,13 @@ def plain_reference(args, nx, params, pos_d, ids_d, sod):
     sp.close()
     return {"mode": "plain", "ms_per_step": round(msp, 3), "halos": st["nhalo"],
             "value": round(st["nhalo"] / (msp / 1000.0), 2), "unit": "halos/s",
-            "sod_phase_ms": {k: round(st[k], 2) for k in ("ms_sched", "ms_prep", "ms_refine", "ms_select", "ms_cross")}}
+            "sod_phase_ms": {k: round(st[k], 2) for k in ("ms_setup", "ms_sched", "ms_prep", "ms_refine", "ms_select",
+                                                          "ms_cross", "ms_output")}}
 
 
-def _cpu_sample(seed, nx, nmax, npu):
+def _cpu_sample(seed, nx, nmax, npu, ndelta):
     """One sample box through the oracle's reference arithmetic, with the
-    parameters -npu derives (main:211-219)."""
+    parameters -npu derives (main:211-219) and the workload's thresholds."""
     import math
 
     from oracle import oracle as O
@@ -357,6 +377,8 @@ def _cpu_sample(seed, nx, nmax, npu):
     if npu > 0:
         ncut = math.ceil(((npu * 2.0 / 200.0) ** (1.0 / 3.0)) / 2.0)
         kw = dict(ncut=ncut, nxbuffer=4 * ncut, nsel=math.ceil((2 * ncut + 1.0) ** 3 * 200.0 * 4.0))
+    if ndelta:
+        kw.update(delta_extra=EXTRA_DELTAS, nbins=EXTRA_BINS)
     t0 = time.perf_counter()
     r = O.run(O.Params(nx=nx, **kw), b.pos, b.ids, O.REFERENCE)
     return r.nhalo, time.perf_counter() - t0
@@ -378,7 +400,7 @@ def cpu_baseline(args, nx, wl, quick=False, cores=None, nsamples=None):
     ctx = mp.get_context("spawn")
     t0 = time.perf_counter()
     with ctx.Pool(ncores) as pool:
-        res = pool.starmap(_cpu_sample, [(args.seed + 100 + i, snx, nmax, npu) for i in range(ns)])
+        res = pool.starmap(_cpu_sample, [(args.seed + 100 + i, snx, nmax, npu, args.ndelta) for i in range(ns)])
     wall = time.perf_counter() - t0
     halos = sum(r[0] for r in res)
     busy = sum(r[1] for r in res) / ncores if quick else wall
@@ -388,6 +410,7 @@ def cpu_baseline(args, nx, wl, quick=False, cores=None, nsamples=None):
         "cores": ncores,
         "kind": "port",
         "sample": f"{ns} box(es) of {snx}^3 cells from the same generator (halo N in [20, {nmax}], npu {npu}), "
+                  f"{'Delta 200/500/178, 48 bins, ' if args.ndelta else ''}"
                   f"full cic/cicm1/tri_cic/spherover in reference arithmetic, {halos} halos; wall {wall:.1f}s",
     }
 
@@ -438,7 +461,8 @@ def main():
     ap.add_argument("--mode", default="batched", choices=["plain", "batched", "learned"])
     ap.add_argument("--no-compare-plain", dest="compare_plain", action="store_false")
     ap.add_argument("--seed", type=int, default=20261203)
-    ap.add_argument("--ndelta", action="store_true", help="Delta = 200, 500, 178 and 48 bins (config 3)")
+    ap.add_argument("--delta200-only", dest="ndelta", action="store_false",
+                    help="Delta = 200 and 60 bins only (default: 200, 500 and 178 in one pass, 48 bins)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.mode_id = {"plain": 0, "batched": 1, "learned": 2}[args.mode]

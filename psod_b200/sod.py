@@ -138,12 +138,39 @@ class SphericalOverdensity:
         self._check(self.lib.psod_run(self.ctx, C.byref(st)))
         return st.as_dict()
 
-    def halos(self, members: bool = True) -> HaloTable:
+    def halo_count(self) -> tuple[int, int]:
         nh, nm = C.c_int64(0), C.c_int64(0)
         self._check(self.lib.psod_halo_count(self.ctx, C.byref(nh), C.byref(nm)))
-        h, m = int(nh.value), int(nm.value)
+        return int(nh.value), int(nm.value)
+
+    def halos(self, members: bool = True, out: HaloTable | None = None) -> HaloTable:
+        """The halo table of the last spherover call.  ``out`` (optional)
+        supplies the arrays to fill: numpy arrays or torch tensors (pinned
+        host or device), each at least as long as the table needs; the
+        returned table holds views of exactly the table's length."""
+        h, m = self.halo_count()
         nb = self.params.nbins
         ne = self.params.ndelta_extra
+        if out is not None:
+            need = dict(halo_id=h, halo_mass=h, halo_rank=h, halo_center=3 * h, halo_rdelta=h, halo_mass2=h,
+                        halo_mextra=h * ne, halo_profile=h * nb, member_offset=h + 1,
+                        member_index=m if members else 0, member_id=m if members else 0)
+            views = {}
+            for f, k in need.items():
+                a = getattr(out, f)
+                flat = a.reshape(-1)
+                if flat.shape[0] < k:
+                    raise ValueError(f"halos(out=...): {f} holds {flat.shape[0]} entries, needs {k}")
+                views[f] = flat[:k]
+            ct = capi.HaloTable()
+            for f, _ in capi.HaloTable._fields_:
+                v = views[f]
+                setattr(ct, f, None if v.shape[0] == 0 else _ptr(v).value)
+            self._check(self.lib.psod_get_halos(self.ctx, C.byref(ct)))
+            views["halo_center"] = views["halo_center"].reshape(h, 3)
+            views["halo_mextra"] = views["halo_mextra"].reshape(h, ne)
+            views["halo_profile"] = views["halo_profile"].reshape(h, nb)
+            return HaloTable(**views)
         t = HaloTable(
             halo_id=np.zeros(h, np.int64),
             halo_mass=np.zeros(h, np.int64),
