@@ -218,7 +218,14 @@ def run_ours(args):
     cross_s = s["ms_cross"] / 1000.0
     achieved = alg_bytes / cross_s / 1e9 if cross_s > 0 else 0.0
     launches = max(1, s["rounds"])
-    traffic = load_traffic("k_cross")
+    # DRAM bytes per launch: the ratio of DRAM traffic to algorithmic bytes
+    # measured by ncu on the 256^3 box, applied to this workload's launches
+    tr = load_traffic("k_cross")
+    traffic = None
+    if tr:
+        traffic = {"bytes_per_launch": int(tr["dram_bytes_per_algorithmic_byte"] * alg_bytes / launches),
+                   "dram_per_algorithmic_byte": tr["dram_bytes_per_algorithmic_byte"],
+                   "from": "ncu DRAM capture at 256^3, scaled by algorithmic bytes"}
     value = world * nhalo / (ms / 1000.0)
     # the refinement kernel dominates: FP32 pair tests fed from shared memory
     ref_s = s["ms_refine"] / 1000.0
