@@ -52,8 +52,13 @@ typedef enum psod_status {
 typedef enum psod_mode {
   PSOD_MODE_PLAIN = 0,   /* one launch per round, full-cube gather */
   PSOD_MODE_BATCHED = 1, /* size-classed seeds, graph-captured rounds */
-  PSOD_MODE_LEARNED = 2  /* batched + learned radius bracket */
+  PSOD_MODE_LEARNED = 2  /* batched + learned first ball of the crossing
+                            search (psod_learn_*); batched without a model */
 } psod_mode;
+
+#define PSOD_LEARN_FEATURES 10     /* network inputs per seed */
+#define PSOD_LEARN_PARAMS 5768     /* weights and biases (padded layout) */
+#define PSOD_LEARN_MODEL_FLOATS 5804 /* 36 scales + PSOD_LEARN_PARAMS */
 
 /* Parameters: the reference's CLI flags (read_params, main:767-906) and the
  * hard-coded constants of spherover.  psod_params_default() fills the
@@ -123,6 +128,11 @@ typedef struct psod_run_stats {
   int64_t refine_slots;  /* lane slots spent on refinement pair tests */
   double ms_setup;       /* seed bucketing before the first round */
   double ms_output;      /* halo table ordering and member sort */
+  double ms_learn;       /* bracket features and network inference */
+  int64_t bracket_hits;  /* seeds whose first crossing ball held every stop */
+  int64_t bracket_seeds; /* seeds that ran the crossing search (batched modes) */
+  int64_t cross_balls;   /* ball passes of the crossing search */
+  int64_t cross_records; /* alive records inside those balls, summed */
 } psod_run_stats;
 
 typedef struct psod_ctx psod_ctx;
@@ -195,6 +205,50 @@ int psod_run(psod_ctx *ctx, psod_run_stats *stats);
  * calls that overlap on the GPU race: serialise them. */
 int psod_cic_rho_static(int64_t n, const float *pos, int32_t nx, int64_t npart_total, int32_t nxbuffer,
                         double *rho, int *bad_flag, void *stream);
+
+/* ---- Learned radius bracket (no counterpart in the reference) ----------
+ * The crossing search of psod_spherover grows a ball around each centre
+ * until the Delta stop lies inside it (1.5 cells, doubling, in the batched
+ * mode).  In PSOD_MODE_LEARNED a small network predicts the first ball from
+ * ten seed-local features; a miss falls back to the growing search, so the
+ * halo table is identical with or without a model.  The network (10 -> 64 ->
+ * 64 -> 2, ReLU, bf16 tensor-core GEMMs with FP32 accumulation, Adam) is
+ * trained on the GPU on samples the engine itself produces:
+ *   psod_learn_collect(ctx, cap)   record (features, targets) of every seed
+ *                                  that crosses in later psod_spherover
+ *                                  calls (batched or learned mode); cap 0
+ *                                  stops recording.  Restarts the count.
+ *   psod_learn_samples             count and copies of the samples (x: 10
+ *                                  floats, t: log stop radius in cells and
+ *                                  log N_delta per sample; NULL skips)
+ *   psod_learn_train               scales from the samples, then Adam
+ *   psod_learn_get/set_model       the model as PSOD_LEARN_MODEL_FLOATS floats:
+ *                                  mu_x[16], sigma_x[16], mu_y[2], sigma_y[2],
+ *                                  W1[64][16], b1[64], W2[64][64], b2[64],
+ *                                  W3[8][64], b3[8] (rows/columns beyond the
+ *                                  real sizes are zero)
+ *   psod_learn_forward             outputs (original units) for raw features
+ *   psod_learn_gradient            gradient of 0.5*mean|y_std - t_std|^2 over
+ *                                  all PSOD_LEARN_PARAMS parameters
+ *   psod_learn_set_margin          first ball = exp(y0) * margin (default 1.1) */
+typedef struct psod_train_params {
+  int32_t epochs;  /* passes over the samples (20) */
+  int32_t batch;   /* samples per step, a multiple of 64 (4096) */
+  float lr;        /* Adam step (1e-3) */
+  float beta1;     /* 0: 0.9 */
+  float beta2;     /* 0: 0.999 */
+  float eps;       /* 0: 1e-8 */
+  uint64_t seed;   /* weight initialisation and batch order */
+} psod_train_params;
+
+int psod_learn_collect(psod_ctx *ctx, int64_t capacity);
+int psod_learn_samples(psod_ctx *ctx, int64_t *n, float *x_out, float *t_out);
+int psod_learn_train(psod_ctx *ctx, const psod_train_params *tp, float *loss_per_epoch);
+int psod_learn_get_model(psod_ctx *ctx, float *model, int64_t nfloats);
+int psod_learn_set_model(psod_ctx *ctx, const float *model, int64_t nfloats);
+int psod_learn_set_margin(psod_ctx *ctx, float margin);
+int psod_learn_forward(psod_ctx *ctx, int64_t n, const float *x, float *y);
+int psod_learn_gradient(psod_ctx *ctx, int64_t n, const float *x, const float *t, float *grad, float *loss);
 
 const char *psod_last_error(const psod_ctx *ctx);
 const char *psod_status_string(int status);

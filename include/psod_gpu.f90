@@ -46,8 +46,15 @@ module psod_gpu
      integer(c_int64_t) :: sod_launches, kernel_launches
      real(c_double)     :: ms_sched, ms_prep, ms_refine, ms_select, ms_cross
      integer(c_int64_t) :: ncandidates, refine_pairs, cross_touch, refine_slots
-     real(c_double) :: ms_setup, ms_output
+     real(c_double) :: ms_setup, ms_output, ms_learn
+     integer(c_int64_t) :: bracket_hits, bracket_seeds, cross_balls, cross_records
   end type psod_run_stats
+
+  type, bind(C) :: psod_train_params
+     integer(c_int32_t) :: epochs, batch
+     real(c_float)      :: lr, beta1, beta2, eps
+     integer(c_int64_t) :: seed
+  end type psod_train_params
 
   interface
      subroutine psod_params_default(p) bind(C, name="psod_params_default")
@@ -97,6 +104,27 @@ module psod_gpu
        import :: c_int, c_ptr, psod_halo_table
        type(c_ptr), value :: ctx
        type(psod_halo_table), intent(in) :: t
+     end function
+     integer(c_int) function psod_learn_collect(ctx, capacity) bind(C, name="psod_learn_collect")
+       import :: c_int, c_ptr, c_int64_t
+       type(c_ptr), value :: ctx
+       integer(c_int64_t), value :: capacity
+     end function
+     integer(c_int) function psod_learn_train(ctx, tp, loss) bind(C, name="psod_learn_train")
+       import :: c_int, c_ptr, psod_train_params
+       type(c_ptr), value :: ctx
+       type(psod_train_params), intent(in) :: tp
+       type(c_ptr), value :: loss
+     end function
+     integer(c_int) function psod_learn_get_model(ctx, model, nfloats) bind(C, name="psod_learn_get_model")
+       import :: c_int, c_ptr, c_int64_t
+       type(c_ptr), value :: ctx, model
+       integer(c_int64_t), value :: nfloats
+     end function
+     integer(c_int) function psod_learn_set_model(ctx, model, nfloats) bind(C, name="psod_learn_set_model")
+       import :: c_int, c_ptr, c_int64_t
+       type(c_ptr), value :: ctx, model
+       integer(c_int64_t), value :: nfloats
      end function
      type(c_ptr) function psod_last_error(ctx) bind(C, name="psod_last_error")
        import :: c_ptr

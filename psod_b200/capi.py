@@ -88,6 +88,11 @@ class RunStats(C.Structure):
         ("refine_slots", C.c_int64),
         ("ms_setup", C.c_double),
         ("ms_output", C.c_double),
+        ("ms_learn", C.c_double),
+        ("bracket_hits", C.c_int64),
+        ("bracket_seeds", C.c_int64),
+        ("cross_balls", C.c_int64),
+        ("cross_records", C.c_int64),
     ]
 
     def as_dict(self):
@@ -111,7 +116,31 @@ EXPORTS = [
     "psod_get_halos",
     "psod_last_error",
     "psod_cic_rho_static",
+    "psod_learn_collect",
+    "psod_learn_samples",
+    "psod_learn_train",
+    "psod_learn_get_model",
+    "psod_learn_set_model",
+    "psod_learn_set_margin",
+    "psod_learn_forward",
+    "psod_learn_gradient",
 ]
+
+LEARN_FEATURES = 10
+LEARN_PARAMS = 5768
+LEARN_MODEL_FLOATS = 5804
+
+
+class TrainParams(C.Structure):
+    _fields_ = [
+        ("epochs", C.c_int32),
+        ("batch", C.c_int32),
+        ("lr", C.c_float),
+        ("beta1", C.c_float),
+        ("beta2", C.c_float),
+        ("eps", C.c_float),
+        ("seed", C.c_uint64),
+    ]
 
 _lib = None
 
@@ -151,6 +180,14 @@ def load(build_if_missing: bool = True):
     L.psod_get_halos.argtypes = [vp, P(HaloTable)]
     L.psod_last_error.argtypes = [vp]
     L.psod_cic_rho_static.argtypes = [C.c_int64, vp, C.c_int32, C.c_int64, C.c_int32, vp, vp, vp]
+    L.psod_learn_collect.argtypes = [vp, C.c_int64]
+    L.psod_learn_samples.argtypes = [vp, P(C.c_int64), vp, vp]
+    L.psod_learn_train.argtypes = [vp, P(TrainParams), vp]
+    L.psod_learn_get_model.argtypes = [vp, vp, C.c_int64]
+    L.psod_learn_set_model.argtypes = [vp, vp, C.c_int64]
+    L.psod_learn_set_margin.argtypes = [vp, C.c_float]
+    L.psod_learn_forward.argtypes = [vp, C.c_int64, vp, vp]
+    L.psod_learn_gradient.argtypes = [vp, C.c_int64, vp, vp, vp, vp]
     L.psod_last_error.restype = C.c_char_p
     for name in EXPORTS:
         L[name].restype = L[name].restype if name in ("psod_status_string", "psod_last_error", "psod_params_default") else C.c_int

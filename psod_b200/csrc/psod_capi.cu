@@ -73,6 +73,7 @@ static void free_all(psod_ctx *c) {
   c->d_m_offset = nullptr;
   c->d_m_index = nullptr;
   free_scratch(c);
+  learn_free(c);
 }
 
 extern "C" {

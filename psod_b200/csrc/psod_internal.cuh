@@ -117,6 +117,10 @@ struct SodConst {
 
 }  // namespace psod
 
+namespace psod {
+struct LearnState;
+}
+
 // ---------------------------------------------------------------------------
 // context
 // ---------------------------------------------------------------------------
@@ -171,6 +175,9 @@ struct psod_ctx {
 
   // device scratch kept across calls (grown on demand, freed at destroy)
   std::vector<std::pair<void *, size_t>> scratch;
+
+  // learned radius bracket (model, optimiser state, collected samples)
+  psod::LearnState *learn = nullptr;
 };
 
 namespace psod {
@@ -273,8 +280,21 @@ enum : int {
   SLOT_H_CENTER,
   SLOT_H_RDELTA,
   SLOT_M_OFFSET,
-  SLOT_M_INDEX
+  SLOT_M_INDEX,
+  SLOT_LEARN_X,         // learned bracket: raw feature rows of an API call
+  SLOT_LEARN_Y,         // learned bracket: outputs / raw targets of an API call
+  SLOT_LEARN_XB,        // learned bracket: standardised bf16 inputs
+  SLOT_LEARN_TS,        // learned bracket: standardised targets
+  SLOT_LEARN_PERM       // learned bracket: batch order
 };
+
+// learned radius bracket (psod_learn.cu)
+void learn_free(psod_ctx *c);
+bool learn_ready(const psod_ctx *c);
+bool learn_collecting(const psod_ctx *c);
+void learn_sample_buffers(const psod_ctx *c, float **x, float **t, unsigned long long **count,
+                          unsigned long long *cap);
+int learn_predict(psod_ctx *c, const float *feat, unsigned n, float *rb0);
 
 bool is_device_ptr(const void *p);
 int copy_out(psod_ctx *c, void *dst, const void *dsrc, size_t bytes);

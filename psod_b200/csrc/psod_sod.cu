@@ -92,6 +92,15 @@ struct SodBufs {
   unsigned long long cand_cap;     // candidate buffer entries
   unsigned cap_ready;              // seeds processed per round at most
   int mode;
+  // learned radius bracket
+  const double *rho;               // input order
+  unsigned long long *st_sbest;    // fixed-point refinement sum of the centre
+  float *st_feat;                  // [slot][16] raw features
+  float *st_rb0;                   // first ball radius (cells) when learn_use
+  int learn_use, learn_collect;
+  float *learn_x, *learn_t;        // collected samples
+  unsigned long long *learn_n, learn_cap;
+  unsigned long long *bracket_hits, *bracket_seeds, *cross_balls, *cross_records;
 };
 
 struct Level {
@@ -406,14 +415,20 @@ __device__ void build_hist(const SodConst &K, const SodBufs &B, Smem &S, int l, 
   for (int k = threadIdx.x; k < NB; k += TPB) S.hist[l][k] = 0;
   __syncthreads();
   const Level L = S.lev[l];
+  unsigned inball = 0;
   for_region(K, B, G, [&](unsigned p, float4 v) {
     double d2;
     if (!region_d2(K, G, v, d2)) return;
+    inball++;
     unsigned long long x = dbits(d2);
     if (l > 0 && (x < L.lo || x > L.hi)) return;
     atomicAdd(&S.hist[l][bucket_of(L, l, x)], 1u);
   });
   __syncthreads();
+  if (l == 0) {
+    const unsigned tot = block_sum_u32(S, inball);
+    if (threadIdx.x == 0) atomicAdd(B.cross_records, (unsigned long long)tot);
+  }
 }
 
 // load alive records with d2 bits in [lo, hi] into S.skey/S.sidx, sort them
@@ -489,6 +504,7 @@ __device__ unsigned load_ball_sorted(const SodConst &K, const SodBufs &B, Smem &
   });
   __syncthreads();
   const unsigned n = S.nsorted;
+  if (threadIdx.x == 0) atomicAdd(B.cross_records, (unsigned long long)n);
   __syncthreads();
   if (n > CAP) return CAP + 1;
   unsigned m = 1;
@@ -1294,6 +1310,7 @@ __device__ void select_seed(const SodConst &K, const SodBufs &B, Smem &S, unsign
   const unsigned long long pa = a, pb = b;
   block_max_pair(S, a, b);
   if (lane == 0 && best_pos != 0xffffffffu && pa == a && pb == b) B.st_centre[slot] = best_pos;
+  if (threadIdx.x == 0) B.st_sbest[slot] = a;
 }
 
 __global__ void __launch_bounds__(TPB) k_select(SodConst K, SodBufs B) {
@@ -1349,6 +1366,7 @@ __device__ long long bracketed_stop(const SodConst &K, const SodBufs &B, Smem &S
     }
     __syncthreads();
     build_hist(K, B, S, 0, G);
+    if (threadIdx.x == 0) atomicAdd(B.cross_balls, 1ull);
     // inside a partial ball the cube's count is not reached: i < npart_sel holds
     const long long na_eff = full ? (long long)na : 0x7fffffffffffffffll;
     const long long i = radial_search(K, B, S, G, na_eff, delta, 0, 0, d2stop);
@@ -1373,7 +1391,12 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
   G.zc = (double)to_grid(cvv.z, K.nxf);
   const double xc = G.xc, yc = G.yc, zc = G.zc;
   const unsigned cidx = __float_as_uint(cvv.w) & PSOD_IDX_MASK;
-  const double rb0 = (B.mode == PSOD_MODE_PLAIN) ? -1.0 : 1.5;
+  double rb0 = (B.mode == PSOD_MODE_PLAIN) ? -1.0 : 1.5;
+  if (B.learn_use) {
+    // learned first ball, clamped to [0.25, ncut] cells (ncut: whole cube)
+    const float r = B.st_rb0[slot];
+    if (r > 0.f) rb0 = fmin(fmax((double)r, 0.25), (double)K.ncut);
+  }
 
   // 3. crossing (main:2040-2100).  Balls of at most CAP alive records are
   // sorted whole (small path); larger ones go through the histogram search
@@ -1393,6 +1416,7 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
         na_known = true;
       }
       const unsigned n = load_ball_sorted(K, B, S, G);
+      if (threadIdx.x == 0) atomicAdd(B.cross_balls, 1ull);
       if (n > CAP) break;
       const long long i = sorted_stop(K, S, n, full ? (long long)na : 0x7fffffffffffffffll, K.delta);
       if (i != 0 || full) {
@@ -1460,6 +1484,7 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
   }
   // extra thresholds: the same stop rule, -1 when not crossed
   long long mext[PSOD_MAX_EXTRA_DELTA];
+  double d2far = d2stop;  // farthest stop over the thresholds
   for (int e = 0; e < K.ndx; e++) {
     double dd = 0.0;
     long long ie = 0;
@@ -1476,6 +1501,21 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
       ie = bracketed_stop(K, B, S, Ge, rbe, na, na_known, K.dx_extra[e], &dd);
     }
     mext[e] = (ie <= 0 || overdens(K, ie, dd) > K.dx_extra[e]) ? -1 : ie - 1;
+    if (ie > 0) d2far = fmax(d2far, dd);
+  }
+  // bracket bookkeeping: did the first ball hold every stop; samples for
+  // training the bracket (this seed's features, log stop radius, log N)
+  if (threadIdx.x == 0 && rb0 > 0.0) {
+    atomicAdd(B.bracket_seeds, 1ull);
+    if (d2far <= rb0 * rb0) atomicAdd(B.bracket_hits, 1ull);
+  }
+  if (threadIdx.x == 0 && B.learn_collect) {
+    const unsigned long long q = atomicAdd(B.learn_n, 1ull);
+    if (q < B.learn_cap) {
+      for (int k = 0; k < PSOD_LEARN_FEATURES; k++) B.learn_x[q * PSOD_LEARN_FEATURES + k] = B.st_feat[slot * 16 + k];
+      B.learn_t[2 * q] = (float)(0.5 * log(fmax(d2far, 1e-12)));
+      B.learn_t[2 * q + 1] = (float)log((double)masse);
+    }
   }
 
   // keep test (main:2118-2120)
@@ -1601,6 +1641,64 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
       B.h_profile[hs * K.nbins + j] = run;
     }
   }
+}
+
+// Learned-bracket features of each ready seed, once its centre is known
+// (warp per seed):
+//   0 log rho(seed)             1 log rho(centre)
+//   2..6 log(1 + alive records) in the cubes of half-width 0..4 cells
+//   7 log S(centre), the refinement sum   8 centre offset from the seed (cells)
+//   9 log(1 + refinement candidates)
+__global__ void k_features(SodConst K, SodBufs B) {
+  const unsigned slot = (unsigned)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (slot >= min(*B.nready, B.cap_ready)) return;
+  float *f = B.st_feat + (size_t)slot * 16;
+  if (!B.st_active[slot]) {
+    if (lane < 16) f[lane] = 0.f;
+    return;
+  }
+  const SeedGeo g = seed_geo(K, B, B.ready[slot]);
+  unsigned s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+  if (B.alive_cnt) {
+    for (int q = lane; q < 729; q += 32) {
+      const int dx = q % 9 - 4, dy = (q / 9) % 9 - 4, dz = q / 81 - 4;
+      const int d = max(abs(dx), max(abs(dy), abs(dz)));
+      const unsigned cell = (unsigned)wrapi(g.ic + dx, K.nx) +
+                            (unsigned)K.nx * ((unsigned)wrapi(g.jc + dy, K.nx) +
+                                              (unsigned)K.nx * (unsigned)wrapi(g.kc + dz, K.nx));
+      const unsigned v = B.alive_cnt[cell];
+      s4 += v;
+      if (d <= 3) s3 += v;
+      if (d <= 2) s2 += v;
+      if (d <= 1) s1 += v;
+      if (d == 0) s0 += v;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
+    s3 += __shfl_xor_sync(0xffffffffu, s3, o);
+    s4 += __shfl_xor_sync(0xffffffffu, s4, o);
+  }
+  if (lane != 0) return;
+  const float4 sv = B.cube[g.sp], cv = B.cube[B.st_centre[slot]];
+  const unsigned ci = __float_as_uint(cv.w) & PSOD_IDX_MASK;
+  const double d2 = min_image_d2((double)to_grid(sv.x, K.nxf), (double)to_grid(sv.y, K.nxf),
+                                 (double)to_grid(sv.z, K.nxf), (double)to_grid(cv.x, K.nxf),
+                                 (double)to_grid(cv.y, K.nxf), (double)to_grid(cv.z, K.nxf), K.tx);
+  f[0] = (float)log(fmax(B.rho[B.seed_idx[B.ready[slot]]], 1e-30));
+  f[1] = (float)log(fmax(B.rho[ci], 1e-30));
+  f[2] = (float)log1p((double)s0);
+  f[3] = (float)log1p((double)s1);
+  f[4] = (float)log1p((double)s2);
+  f[5] = (float)log1p((double)s3);
+  f[6] = (float)log1p((double)s4);
+  f[7] = (float)log(fmax((double)B.st_sbest[slot] * (1.0 / 1099511627776.0), 1e-30));
+  f[8] = (float)sqrt(d2);
+  f[9] = (float)log1p((double)B.st_cn[slot]);
+  for (int k = PSOD_LEARN_FEATURES; k < 16; k++) f[k] = 0.f;
 }
 
 __global__ void __launch_bounds__(TPB) k_cross(SodConst K, SodBufs B) {
@@ -1942,7 +2040,8 @@ enum {
   SC_PROCESSED, SC_U64, SC_EDGES, SC_HRANK, SC_HID, SC_HMASS, SC_HMASS2, SC_HMEXTRA, SC_HPROF, SC_HCENTER,
   SC_HRDELTA, SC_HPOOL, SC_COUNTS, SC_ST_ACTIVE, SC_ST_NA, SC_ST_COFF, SC_ST_CN,
   SC_ST_CENTRE, SC_CAND_POS, SC_CAND_SLOT, SC_CAND_S, SC_ORDER, SC_RKEYS, SC_MASS32, SC_MOFF, SC_TKEY, SC_TIDX,
-  SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS, SC_CELLNCH
+  SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS, SC_CELLNCH, SC_FEAT, SC_RB0,
+  SC_SBEST
 };
 
 struct PhaseTimer {
@@ -1972,7 +2071,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   psod_run_stats st{};
   st.fail_rank = -1;
   st.npart_new = c->npart_new;
-  PhaseTimer t_all, t_sched, t_prep, t_ref, t_sel, t_cross, t_setup, t_out;
+  PhaseTimer t_all, t_sched, t_prep, t_ref, t_sel, t_cross, t_setup, t_out, t_learn;
   t_all.start(c->stream);
   int rc = PSOD_OK;
   const SodConst K = make_sod_const(c);
@@ -2042,6 +2141,11 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     return rc;
   unsigned *cell_nch;
   if ((rc = scratch(c, SC_CELLNCH, (size_t)cap_ready * 27, &cell_nch))) return rc;
+  float *st_feat, *st_rb0;
+  unsigned long long *st_sbest;
+  if ((rc = scratch(c, SC_FEAT, (size_t)cap_ready * 16, &st_feat)) || (rc = scratch(c, SC_RB0, (size_t)cap_ready, &st_rb0)) ||
+      (rc = scratch(c, SC_SBEST, (size_t)cap_ready, &st_sbest)))
+    return rc;
   // ctrs: 0 nready, 1..4 work counters, 5 gmin, 6 quirk rank, 7 cand_used
   unsigned *nready_d = ctrs, *work = ctrs + 1, *gmin = ctrs + 5, *qrank_d = ctrs + 6, *cand_used = ctrs + 7;
 
@@ -2145,6 +2249,21 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.pair_slots = u64s + 8;
   B.ncand_total = u64s + 6;
   B.mode = c->p.mode;
+  B.rho = c->d_rho;
+  B.st_sbest = st_sbest;
+  B.st_feat = st_feat;
+  B.st_rb0 = st_rb0;
+  B.bracket_hits = u64s + 10;
+  B.bracket_seeds = u64s + 11;
+  B.cross_balls = u64s + 12;
+  B.cross_records = u64s + 13;
+  // the learned bracket needs the per-cell alive counts of the batched modes
+  B.learn_use = (c->p.mode == PSOD_MODE_LEARNED && learn_ready(c)) ? 1 : 0;
+  B.learn_collect = (c->p.mode != PSOD_MODE_PLAIN && learn_collecting(c)) ? 1 : 0;
+  B.learn_x = B.learn_t = nullptr;
+  B.learn_n = nullptr;
+  B.learn_cap = 0;
+  if (B.learn_collect) learn_sample_buffers(c, &B.learn_x, &B.learn_t, &B.learn_n, &B.learn_cap);
   if (c->p.mode != PSOD_MODE_PLAIN) {
     unsigned *alive_cnt;
     if ((rc = scratch(c, SLOT_CELL_U32, (size_t)c->ncell, &alive_cnt))) return rc;
@@ -2204,6 +2323,16 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     t_sel.start(c->stream);
     k_select<<<g, TPB, smem, c->stream>>>(K, B);
     t_sel.stop(c->stream);
+    if (B.learn_use || B.learn_collect) {
+      t_learn.start(c->stream);
+      k_features<<<nblk((long long)nready * 32, 256), 256, 0, c->stream>>>(K, B);
+      kernels++;
+      if (B.learn_use) {
+        if ((rc = learn_predict(c, st_feat, nready, st_rb0))) return rc;
+        kernels++;
+      }
+      t_learn.stop(c->stream);
+    }
     t_cross.start(c->stream);
     k_cross<<<g, TPB, smem, c->stream>>>(K, B);
     t_cross.stop(c->stream);
@@ -2212,6 +2341,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     t_ref.collect();
     t_sel.collect();
     t_cross.collect();
+    if (B.learn_use || B.learn_collect) t_learn.collect();
     if (trace) {
       unsigned cu = 0;
       unsigned long long tv[16];
@@ -2244,6 +2374,11 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   st.refine_pairs = (int64_t)hv[5];
   st.cross_touch = (int64_t)hv[7];
   st.refine_slots = (int64_t)hv[8];
+  st.ms_learn = t_learn.total;
+  st.bracket_hits = (int64_t)hv[10];
+  st.bracket_seeds = (int64_t)hv[11];
+  st.cross_balls = (int64_t)hv[12];
+  st.cross_records = (int64_t)hv[13];
   c->nhalo = 0;
   c->nmember = 0;
   c->sod_done = false;

@@ -138,6 +138,57 @@ class SphericalOverdensity:
         self._check(self.lib.psod_run(self.ctx, C.byref(st)))
         return st.as_dict()
 
+    # -- learned radius bracket ------------------------------------------
+    def learn_collect(self, capacity: int):
+        """Record (features, targets) of every crossing seed of later
+        spherover calls (batched or learned mode); 0 stops recording."""
+        self._check(self.lib.psod_learn_collect(self.ctx, int(capacity)))
+
+    def learn_samples(self):
+        """(x [n, 10], t [n, 2]) of the recorded samples, float32."""
+        n = C.c_int64(0)
+        self._check(self.lib.psod_learn_samples(self.ctx, C.byref(n), None, None))
+        x = np.zeros((max(n.value, 1), capi.LEARN_FEATURES), np.float32)
+        t = np.zeros((max(n.value, 1), 2), np.float32)
+        self._check(self.lib.psod_learn_samples(self.ctx, C.byref(n), _ptr(x), _ptr(t)))
+        return x[: n.value], t[: n.value]
+
+    def learn_train(self, epochs: int = 20, batch: int = 4096, lr: float = 1e-3, seed: int = 1) -> np.ndarray:
+        """Train the bracket network on the recorded samples with the
+        project's GPU kernels; returns the loss of each epoch."""
+        tp = capi.TrainParams(epochs=epochs, batch=batch, lr=lr, beta1=0.9, beta2=0.999, eps=1e-8, seed=seed)
+        loss = np.zeros(epochs, np.float32)
+        self._check(self.lib.psod_learn_train(self.ctx, C.byref(tp), _ptr(loss)))
+        return loss
+
+    def learn_get_model(self) -> np.ndarray:
+        m = np.zeros(capi.LEARN_MODEL_FLOATS, np.float32)
+        self._check(self.lib.psod_learn_get_model(self.ctx, _ptr(m), m.size))
+        return m
+
+    def learn_set_model(self, model):
+        m = np.ascontiguousarray(model, np.float32)
+        self._check(self.lib.psod_learn_set_model(self.ctx, _ptr(m), m.size))
+
+    def learn_set_margin(self, margin: float):
+        self._check(self.lib.psod_learn_set_margin(self.ctx, float(margin)))
+
+    def learn_forward(self, x) -> np.ndarray:
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.zeros((x.shape[0], 2), np.float32)
+        self._check(self.lib.psod_learn_forward(self.ctx, x.shape[0], _ptr(x), _ptr(y)))
+        return y
+
+    def learn_gradient(self, x, t):
+        """(gradient over the padded parameter layout, loss) of
+        0.5 * mean |y_std - t_std|^2 at the current model."""
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.zeros(capi.LEARN_PARAMS, np.float32)
+        loss = C.c_float(0)
+        self._check(self.lib.psod_learn_gradient(self.ctx, x.shape[0], _ptr(x), _ptr(t), _ptr(g), C.byref(loss)))
+        return g, float(loss.value)
+
     def halo_count(self) -> tuple[int, int]:
         nh, nm = C.c_int64(0), C.c_int64(0)
         self._check(self.lib.psod_halo_count(self.ctx, C.byref(nh), C.byref(nm)))
