@@ -7,6 +7,12 @@ particles already in HBM; ``e2e`` is the same through the C-ABI from pinned
 host buffers, with the host-to-device copy of the particles and the
 device-to-host copy of the halo table inside the timed region.
 
+The default mode is the learned bracket: before anything is timed, the
+bracket network is trained on samples from 128^3 boxes with the engine's GPU
+training kernels; the timed steps include its per-round inference.  The same
+box then runs once in the batched mode (no network) and once in the plain
+mode for comparison.
+
 One process per GPU (torchrun for N > 1).  The SOD of one box does not
 shard, so every rank runs an independent replica on its own box (weak
 scaling); the ranks only meet at a barrier and a max-reduction of the
@@ -148,16 +154,19 @@ def run_ours(args):
     torch.cuda.set_device(dev)
     nx = args.nx
     wl = WORKLOADS.get(nx, dict(nmax_halo=20000, box=f"{nx}^3"))
+    thresholds = dict(delta_extra=EXTRA_DELTAS, nbins=EXTRA_BINS) if args.ndelta else {}
+    model, bracket = None, None
+    if args.mode == "learned":
+        model, bracket = train_bracket(args, dev, thresholds)
     box = synth.make_box(nx, nmax_halo=wl["nmax_halo"], seed=args.seed + rank, device=f"cuda:{dev}")
     pos_d, ids_d = box.pos, box.ids
     del box
     torch.cuda.empty_cache()  # hand the generator's temporaries back before the engine allocates
     n = int(pos_d.shape[0])
-    params = dict(npu=npu_for(nx), mode=args.mode_id)
-    if args.ndelta:
-        params["delta_extra"] = EXTRA_DELTAS
-        params["nbins"] = EXTRA_BINS
+    params = dict(npu=npu_for(nx), mode=args.mode_id, **thresholds)
     sod = SphericalOverdensity(nx, device=dev, **params)
+    if model is not None:
+        sod.learn_set_model(model)
     # L2 flush buffer (used when the inputs are smaller than L2)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
     inputs_bytes = n * (12 + 8)
@@ -301,12 +310,23 @@ def run_ours(args):
         },
         "clocks": clocks,
     }
+    if bracket is not None:
+        bracket.update(hit_rate=round(s["bracket_hits"] / max(1, s["bracket_seeds"]), 4),
+                       seeds=int(s["bracket_seeds"]), cross_balls=int(s["cross_balls"]),
+                       cross_records=int(s["cross_records"]), ms_learn=round(s["ms_learn"], 2))
+        line["bracket"] = bracket
     if args.compare_plain and args.mode != "plain" and world == 1:
-        line["plain"] = plain_reference(args, nx, params, pos_d, ids_d, sod)
+        if args.mode == "learned":
+            line["batched"] = mode_reference(nx, params, pos_d, ids_d, sod, 1)
+            line["vs_batched"] = round(line["batched"]["ms_per_step"] / ms, 3)
+            sod = None
+        line["plain"] = mode_reference(nx, params, pos_d, ids_d, sod, 0)
         line["vs_plain"] = round(line["plain"]["ms_per_step"] / ms, 3)
+        sod = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, nx, wl, quick=True)
-    sod.close()
+    if sod is not None:
+        sod.close()
     if world > 1:
         import torch.distributed as dist
 
@@ -342,17 +362,19 @@ def time_stages(sod, pos, ids):
     return out
 
 
-def plain_reference(args, nx, params, pos_d, ids_d, sod):
-    """The same box through the plain GPU path (one launch per phase and
-    round, full-cube gathers), one untimed and one timed step."""
+def mode_reference(nx, params, pos_d, ids_d, sod, mode):
+    """The same box through another GPU mode (0 plain: full-cube gathers; 1
+    batched: growing balls from 1.5 cells, no network), one untimed and one
+    timed step.  Closes ``sod`` first to free its memory."""
     import torch
 
     from psod_b200.sod import SphericalOverdensity
 
-    sod.close()
+    if sod is not None:
+        sod.close()
     torch.cuda.empty_cache()
     p = dict(params)
-    p["mode"] = 0
+    p["mode"] = mode
     sp = SphericalOverdensity(nx, device=torch.cuda.current_device(), **p)
     sp.load(pos_d, ids_d)
     sp.run()
@@ -365,10 +387,43 @@ def plain_reference(args, nx, params, pos_d, ids_d, sod):
     torch.cuda.synchronize()
     msp = a.elapsed_time(b)
     sp.close()
-    return {"mode": "plain", "ms_per_step": round(msp, 3), "halos": st["nhalo"],
-            "value": round(st["nhalo"] / (msp / 1000.0), 2), "unit": "halos/s",
-            "sod_phase_ms": {k: round(st[k], 2) for k in ("ms_setup", "ms_sched", "ms_prep", "ms_refine", "ms_select",
-                                                          "ms_cross", "ms_output")}}
+    out = {"mode": {0: "plain", 1: "batched"}[mode], "ms_per_step": round(msp, 3), "halos": st["nhalo"],
+           "value": round(st["nhalo"] / (msp / 1000.0), 2), "unit": "halos/s",
+           "sod_phase_ms": {k: round(st[k], 2) for k in ("ms_setup", "ms_sched", "ms_prep", "ms_refine", "ms_select",
+                                                         "ms_cross", "ms_output")}}
+    if mode == 1:
+        out.update(hit_rate=round(st["bracket_hits"] / max(1, st["bracket_seeds"]), 4),
+                   cross_balls=int(st["cross_balls"]), cross_records=int(st["cross_records"]))
+    return out
+
+
+def train_bracket(args, dev, thresholds):
+    """The learned bracket network, trained untimed on the engine's own
+    samples from configuration-1 boxes (128^3, halo N in [20, 2e4]) with the
+    GPU training kernels: Adam, lr 1e-3, 20 epochs, batch 4096."""
+    import torch
+
+    from psod_b200 import synth
+    from psod_b200.sod import SphericalOverdensity
+
+    nbox = 32
+    t0 = time.perf_counter()
+    with SphericalOverdensity(128, device=dev, mode=1, **thresholds) as s:
+        s.learn_collect(1 << 21)
+        for i in range(nbox):
+            b = synth.make_box(128, nmax_halo=20000, seed=args.seed + 1000 + i, device=f"cuda:{dev}")
+            s.load(b.pos, b.ids)
+            s.run()
+            del b
+        x, _ = s.learn_samples()
+        loss = s.learn_train(epochs=20, batch=4096, lr=1e-3, seed=args.seed)
+        model = s.learn_get_model()
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    return model, {"trained_on": f"{nbox} boxes of 128^3 (halo N in [20, 2e4]), batched-mode samples",
+                   "samples": int(x.shape[0]), "epochs": 20, "batch": 4096, "lr": 1e-3,
+                   "loss_first_last": [round(float(loss[0]), 4), round(float(loss[-1]), 4)],
+                   "train_s": round(time.perf_counter() - t0, 2)}
 
 
 def _cpu_sample(seed, nx, nmax, npu, ndelta):
@@ -465,7 +520,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--nx", type=int, default=1024)
-    ap.add_argument("--mode", default="batched", choices=["plain", "batched", "learned"])
+    ap.add_argument("--mode", default="learned", choices=["plain", "batched", "learned"])
     ap.add_argument("--no-compare-plain", dest="compare_plain", action="store_false")
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--delta200-only", dest="ndelta", action="store_false",

@@ -154,7 +154,10 @@ int psod_set_stream(psod_ctx *ctx, void *stream);
  * (posf(3,n), modvar main:9), id int64 (idf, main:8), vel optional
  * (velf; copied for the member table only).  npart_total is the
  * simulation's particle count (nparttotal, main:302-310); mpf = 1/that.
- * Builds the cell-sorted cube (the linked list of main:1564-1604). */
+ * Builds the cell-sorted cube (the linked list of main:1564-1604).
+ * Device arrays are read on the context's stream: data written on another
+ * stream must be complete first (synchronise, or run the context on the
+ * producer's stream with psod_set_stream). */
 int psod_load_particles(psod_ctx *ctx, int64_t n, const float *pos,
                         const float *vel, const int64_t *id,
                         int64_t npart_total);

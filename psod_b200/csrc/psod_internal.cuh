@@ -187,10 +187,12 @@ namespace psod {
 // ---------------------------------------------------------------------------
 int set_err(psod_ctx *c, int code, const std::string &msg);
 int cuda_check(psod_ctx *c, cudaError_t e, const char *what);
-#define PSOD_CUDA(ctx, call)                               \
-  do {                                                     \
-    cudaError_t _e = (call);                               \
-    if (_e != cudaSuccess) return psod::cuda_check(ctx, _e, #call); \
+#define PSOD_STR2(x) #x
+#define PSOD_STR(x) PSOD_STR2(x)
+#define PSOD_CUDA(ctx, call)                                                                          \
+  do {                                                                                                \
+    cudaError_t _e = (call);                                                                          \
+    if (_e != cudaSuccess) return psod::cuda_check(ctx, _e, #call " (" __FILE__ ":" PSOD_STR(__LINE__) ")"); \
   } while (0)
 
 template <typename T>

@@ -359,7 +359,8 @@ __global__ void k_standardize(const float *x, const float *t, long long n, Norm 
 }
 
 // Forward pass of raw feature rows (row stride `stride`).  out: y in
-// original units (2 per row) when rb0 is null; else rb0[i] = exp(y0)*margin.
+// original units (2 per row) when rb0 is null; else rb0[i] = exp(y0)*margin,
+// or 0 (no prediction) for rows whose column 15 is set (stride 16 only).
 __global__ void __launch_bounds__(LTPB) k_mlp_forward(const float *x, int stride, long long n, Norm nm,
                                                       const Bf16W *gw, const float *params, float *out,
                                                       float *rb0, float margin) {
@@ -384,7 +385,7 @@ __global__ void __launch_bounds__(LTPB) k_mlp_forward(const float *x, int stride
     if (r >= n || col >= NOUT) continue;
     const float v = __fmaf_rn(y[0][e], nm.sgy[col], nm.muy[col]);
     if (rb0) {
-      if (col == 0) rb0[r] = expf(v) * margin;
+      if (col == 0) rb0[r] = x[r * stride + IN - 1] != 0.f ? 0.f : expf(v) * margin;
     } else {
       out[r * NOUT + col] = v;
     }
@@ -406,6 +407,7 @@ struct LearnState {
   float *d_x = nullptr, *d_t = nullptr;
   unsigned long long *d_count = nullptr;
   float margin = 1.1f;
+  bool attr_set = false;  // shared-memory attribute of the inference kernel
 };
 
 static int learn_alloc(psod_ctx *c) {
@@ -448,7 +450,10 @@ void learn_sample_buffers(const psod_ctx *c, float **x, float **t, unsigned long
 int learn_predict(psod_ctx *c, const float *feat, unsigned n, float *rb0) {
   if (n == 0) return PSOD_OK;
   LearnState &L = *c->learn;
-  PSOD_CUDA(c, cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem()));
+  if (!L.attr_set) {
+    PSOD_CUDA(c, cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)lsmem()));
+    L.attr_set = true;
+  }
   k_mlp_forward<<<(n + TILE - 1) / TILE, LTPB, lsmem(), c->stream>>>(feat, IN, n, L.norm, L.d_w, L.d_params, nullptr,
                                                                       rb0, L.margin);
   PSOD_CUDA(c, cudaGetLastError());

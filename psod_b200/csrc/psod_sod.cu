@@ -38,6 +38,7 @@ constexpr int NB = 4096;          // histogram buckets per level
 constexpr int MAXLEV = 4;         // histogram levels kept in shared memory
 constexpr int CAP = 2048;         // elements sorted in shared memory
 constexpr unsigned long long POOL_SORTED = 1ull << 63;
+constexpr double BALL0 = 1.5;      // first crossing ball of the batched mode (cells)
 constexpr unsigned long long L1_BASE = 128896ull;  // (1023-16) << 7
 constexpr int L1_SHIFT = 45;
 
@@ -1264,7 +1265,10 @@ __global__ void __launch_bounds__(256, 4) k_refine_warp(SodConst K, SodBufs B) {
 __device__ void select_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
   if (!B.st_active[slot]) return;
   const unsigned off = B.st_coff[slot], n = B.st_cn[slot];
-  if (n == 0) return;
+  if (n == 0) {
+    if (threadIdx.x == 0) B.st_sbest[slot] = 0;
+    return;
+  }
   const SeedGeo g = seed_geo(K, B, rank);
   // max of the finite approximate sums (non-negative doubles order as their
   // bits); an infinite entry marks a candidate that always goes exact
@@ -1313,6 +1317,66 @@ __device__ void select_seed(const SodConst &K, const SodBufs &B, Smem &S, unsign
   if (threadIdx.x == 0) B.st_sbest[slot] = a;
 }
 
+// Learned-bracket features of a ready seed, once its centre is known:
+//   0 log rho(seed)             1 log rho(centre)
+//   2..6 log(1 + alive records) in the cubes of half-width 0..4 cells
+//   7 log S(centre), the refinement sum   8 centre offset from the seed (cells)
+//   9 log(1 + refinement candidates)
+// In the learned mode only seeds with at least LEARN_MIN_CAND refinement
+// candidates get features and a prediction: a halo whose stops lie beyond the
+// first ball (1.5 cells, N above ~3000 at mean density one per cell) fills
+// its 27 central cells with far more candidates.  The others are marked in
+// column 15 and start at the batched mode's ball.  Collection for training
+// covers every seed.
+constexpr unsigned LEARN_MIN_CAND = 256;
+
+__device__ void seed_features(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
+  float *f = B.st_feat + (size_t)slot * 16;
+  if (!B.st_active[slot] || (!B.learn_collect && B.st_cn[slot] < LEARN_MIN_CAND)) {
+    if (threadIdx.x < 16) f[threadIdx.x] = threadIdx.x == 15 ? 1.f : 0.f;
+    return;
+  }
+  const SeedGeo g = seed_geo(K, B, rank);
+  unsigned s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
+  if (B.alive_cnt) {
+    for (int q = threadIdx.x; q < 729; q += TPB) {
+      const int dx = q % 9 - 4, dy = (q / 9) % 9 - 4, dz = q / 81 - 4;
+      const int d = max(abs(dx), max(abs(dy), abs(dz)));
+      const unsigned cell = (unsigned)wrapi(g.ic + dx, K.nx) +
+                            (unsigned)K.nx * ((unsigned)wrapi(g.jc + dy, K.nx) +
+                                              (unsigned)K.nx * (unsigned)wrapi(g.kc + dz, K.nx));
+      const unsigned v = B.alive_cnt[cell];
+      s4 += v;
+      if (d <= 3) s3 += v;
+      if (d <= 2) s2 += v;
+      if (d <= 1) s1 += v;
+      if (d == 0) s0 += v;
+    }
+  }
+  s0 = block_sum_u32(S, s0);
+  s1 = block_sum_u32(S, s1);
+  s2 = block_sum_u32(S, s2);
+  s3 = block_sum_u32(S, s3);
+  s4 = block_sum_u32(S, s4);
+  if (threadIdx.x != 0) return;
+  const float4 sv = B.cube[g.sp], cv = B.cube[B.st_centre[slot]];
+  const unsigned ci = __float_as_uint(cv.w) & PSOD_IDX_MASK;
+  const double d2 = min_image_d2((double)to_grid(sv.x, K.nxf), (double)to_grid(sv.y, K.nxf),
+                                 (double)to_grid(sv.z, K.nxf), (double)to_grid(cv.x, K.nxf),
+                                 (double)to_grid(cv.y, K.nxf), (double)to_grid(cv.z, K.nxf), K.tx);
+  f[0] = (float)log(fmax(B.rho[B.seed_idx[rank]], 1e-30));
+  f[1] = (float)log(fmax(B.rho[ci], 1e-30));
+  f[2] = (float)log1p((double)s0);
+  f[3] = (float)log1p((double)s1);
+  f[4] = (float)log1p((double)s2);
+  f[5] = (float)log1p((double)s3);
+  f[6] = (float)log1p((double)s4);
+  f[7] = (float)log(fmax((double)B.st_sbest[slot] * (1.0 / 1099511627776.0), 1e-30));
+  f[8] = (float)sqrt(d2);
+  f[9] = (float)log1p((double)B.st_cn[slot]);
+  for (int k = PSOD_LEARN_FEATURES; k < 16; k++) f[k] = 0.f;
+}
+
 __global__ void __launch_bounds__(TPB) k_select(SodConst K, SodBufs B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem &S = *reinterpret_cast<Smem *>(smem_raw);
@@ -1320,6 +1384,7 @@ __global__ void __launch_bounds__(TPB) k_select(SodConst K, SodBufs B) {
     const unsigned item = next_item(&B.work[2]);
     if (item >= min(*B.nready, B.cap_ready)) break;
     select_seed(K, B, S, item, B.ready[item]);
+    if (B.learn_use || B.learn_collect) seed_features(K, B, S, item, B.ready[item]);
   }
 }
 
@@ -1391,11 +1456,14 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
   G.zc = (double)to_grid(cvv.z, K.nxf);
   const double xc = G.xc, yc = G.yc, zc = G.zc;
   const unsigned cidx = __float_as_uint(cvv.w) & PSOD_IDX_MASK;
-  double rb0 = (B.mode == PSOD_MODE_PLAIN) ? -1.0 : 1.5;
+  double rb0 = (B.mode == PSOD_MODE_PLAIN) ? -1.0 : BALL0;
   if (B.learn_use) {
-    // learned first ball, clamped to [0.25, ncut] cells (ncut: whole cube)
+    // The learned radius only enlarges the first ball (up to the whole cube
+    // at ncut).  A smaller ball saves records but not time: a pass costs
+    // mostly its fixed walk and sort, and a miss adds a pass.  Starting at
+    // or above BALL0, the doubling never needs more passes than from BALL0.
     const float r = B.st_rb0[slot];
-    if (r > 0.f) rb0 = fmin(fmax((double)r, 0.25), (double)K.ncut);
+    if (r > 0.f) rb0 = fmin(fmax((double)r, BALL0), (double)K.ncut);
   }
 
   // 3. crossing (main:2040-2100).  Balls of at most CAP alive records are
@@ -1641,64 +1709,6 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
       B.h_profile[hs * K.nbins + j] = run;
     }
   }
-}
-
-// Learned-bracket features of each ready seed, once its centre is known
-// (warp per seed):
-//   0 log rho(seed)             1 log rho(centre)
-//   2..6 log(1 + alive records) in the cubes of half-width 0..4 cells
-//   7 log S(centre), the refinement sum   8 centre offset from the seed (cells)
-//   9 log(1 + refinement candidates)
-__global__ void k_features(SodConst K, SodBufs B) {
-  const unsigned slot = (unsigned)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  const int lane = threadIdx.x & 31;
-  if (slot >= min(*B.nready, B.cap_ready)) return;
-  float *f = B.st_feat + (size_t)slot * 16;
-  if (!B.st_active[slot]) {
-    if (lane < 16) f[lane] = 0.f;
-    return;
-  }
-  const SeedGeo g = seed_geo(K, B, B.ready[slot]);
-  unsigned s0 = 0, s1 = 0, s2 = 0, s3 = 0, s4 = 0;
-  if (B.alive_cnt) {
-    for (int q = lane; q < 729; q += 32) {
-      const int dx = q % 9 - 4, dy = (q / 9) % 9 - 4, dz = q / 81 - 4;
-      const int d = max(abs(dx), max(abs(dy), abs(dz)));
-      const unsigned cell = (unsigned)wrapi(g.ic + dx, K.nx) +
-                            (unsigned)K.nx * ((unsigned)wrapi(g.jc + dy, K.nx) +
-                                              (unsigned)K.nx * (unsigned)wrapi(g.kc + dz, K.nx));
-      const unsigned v = B.alive_cnt[cell];
-      s4 += v;
-      if (d <= 3) s3 += v;
-      if (d <= 2) s2 += v;
-      if (d <= 1) s1 += v;
-      if (d == 0) s0 += v;
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) {
-    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-    s2 += __shfl_xor_sync(0xffffffffu, s2, o);
-    s3 += __shfl_xor_sync(0xffffffffu, s3, o);
-    s4 += __shfl_xor_sync(0xffffffffu, s4, o);
-  }
-  if (lane != 0) return;
-  const float4 sv = B.cube[g.sp], cv = B.cube[B.st_centre[slot]];
-  const unsigned ci = __float_as_uint(cv.w) & PSOD_IDX_MASK;
-  const double d2 = min_image_d2((double)to_grid(sv.x, K.nxf), (double)to_grid(sv.y, K.nxf),
-                                 (double)to_grid(sv.z, K.nxf), (double)to_grid(cv.x, K.nxf),
-                                 (double)to_grid(cv.y, K.nxf), (double)to_grid(cv.z, K.nxf), K.tx);
-  f[0] = (float)log(fmax(B.rho[B.seed_idx[B.ready[slot]]], 1e-30));
-  f[1] = (float)log(fmax(B.rho[ci], 1e-30));
-  f[2] = (float)log1p((double)s0);
-  f[3] = (float)log1p((double)s1);
-  f[4] = (float)log1p((double)s2);
-  f[5] = (float)log1p((double)s3);
-  f[6] = (float)log1p((double)s4);
-  f[7] = (float)log(fmax((double)B.st_sbest[slot] * (1.0 / 1099511627776.0), 1e-30));
-  f[8] = (float)sqrt(d2);
-  f[9] = (float)log1p((double)B.st_cn[slot]);
-  for (int k = PSOD_LEARN_FEATURES; k < 16; k++) f[k] = 0.f;
 }
 
 __global__ void __launch_bounds__(TPB) k_cross(SodConst K, SodBufs B) {
@@ -2323,14 +2333,11 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     t_sel.start(c->stream);
     k_select<<<g, TPB, smem, c->stream>>>(K, B);
     t_sel.stop(c->stream);
-    if (B.learn_use || B.learn_collect) {
+    if (B.learn_use) {
+      // features were written by k_select; one inference launch per round
       t_learn.start(c->stream);
-      k_features<<<nblk((long long)nready * 32, 256), 256, 0, c->stream>>>(K, B);
+      if ((rc = learn_predict(c, st_feat, nready, st_rb0))) return rc;
       kernels++;
-      if (B.learn_use) {
-        if ((rc = learn_predict(c, st_feat, nready, st_rb0))) return rc;
-        kernels++;
-      }
       t_learn.stop(c->stream);
     }
     t_cross.start(c->stream);
@@ -2341,7 +2348,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     t_ref.collect();
     t_sel.collect();
     t_cross.collect();
-    if (B.learn_use || B.learn_collect) t_learn.collect();
+    if (B.learn_use) t_learn.collect();
     if (trace) {
       unsigned cu = 0;
       unsigned long long tv[16];

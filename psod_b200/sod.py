@@ -64,6 +64,10 @@ class SphericalOverdensity:
             raise PsodError(st, "psod_ctx_create failed (invalid parameters or no CUDA device)")
         self.ctx = h
         self.n = 0
+        # run on torch's current stream of the device: tensors torch wrote
+        # are complete before the library reads them, and torch events
+        # time the library's work on the same stream
+        self.set_stream(torch.cuda.current_stream(device))
 
     # -- lifecycle -----------------------------------------------------
     def close(self):

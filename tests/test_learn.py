@@ -5,7 +5,9 @@ The reference has no learned component; the checks are (a) the numpy
 restatement's gradient against finite differences (CPU), (b) the GPU forward
 and gradient kernels against the restatement with the same bfloat16 rounding
 points, (c) training lowers the loss, (d) the learned mode gives the batched
-mode's halo table bit for bit while its crossing search loads fewer records.
+mode's halo table bit for bit while its crossing search needs fewer ball
+passes (the network's first ball is never below the batched mode's, so
+every seed needs at most as many passes).
 """
 
 import numpy as np
@@ -121,5 +123,5 @@ def test_learned_bracket_trains_and_keeps_results():
     print(f"bracket hits: batched {hit_b:.3f}, learned {hit_l:.3f}; records in crossing balls: "
           f"batched {st_b['cross_records']}, learned {st_l['cross_records']}; ball passes: "
           f"batched {st_b['cross_balls']}, learned {st_l['cross_balls']}")
-    assert st_l["cross_records"] < st_b["cross_records"]
-    assert hit_l > 0.5
+    assert st_l["cross_balls"] < st_b["cross_balls"]
+    assert hit_l >= hit_b
