@@ -1084,13 +1084,16 @@ __device__ __forceinline__ double tile_terms(const float4 *tile, unsigned nt, fl
 // pass through a warp-private shared slice, 32 at a time, and every lane
 // reads each one by broadcast; warps never wait on one another.  Partial
 // sums of a candidate's neighbour chunks are added into cand_s.
-__global__ void __launch_bounds__(256, 4) k_refine_warp(SodConst K, SodBufs B) {
-  __shared__ float4 s_tile[8][32];
+__global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
+  __shared__ float4 s_tile[8][64];
   __shared__ unsigned s_rb[8][18], s_rp[8][19];
   __shared__ int s_nr[8], s_wf[8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const unsigned nitems = B.chunk_pref[B.nitems_cells];
-  unsigned long long visits = 0, slots = 0, loaded = 0;
+  // pair, slot and staged-record counts: per item in 32 bits, per warp in
+  // shared memory (keeps 64-bit totals out of the registers)
+  __shared__ unsigned long long s_count[8][3];
+  if (lane < 3) s_count[w][lane] = 0;
   while (true) {
     unsigned item = 0, ci = 0, rem = 0;
     if (lane == 0) {
@@ -1181,22 +1184,37 @@ __global__ void __launch_bounds__(256, 4) k_refine_warp(SodConst K, SodBufs B) {
     const unsigned r0 = nchunk * RN_CHUNK, r1 = any_active ? min(total, r0 + RN_CHUNK) : r0;
     const unsigned lt = (1u << lane) - 1u;
     double sum = 0.0;
-    unsigned pos = r0;  // next record of the chunk to load
-    unsigned fill = 0;  // records staged in the tile
-    int rr = 0;         // run holding record pos
-    while (rr + 1 < nr && s_rp[w][rr + 1] <= pos) rr++;
-    while (pos < r1 || fill > 0) {
-      // stage alive records within reach of the box only: the others are
-      // skipped by a warp-wide compaction, so they cost a load but no pair
-      // tests
-      while (fill < 32 && pos < r1) {
-        const unsigned ff = pos + (unsigned)lane;
+    unsigned visits = 0, slots = 0, loaded = 0;
+    // tile of 32 kept records: the pair tests of every candidate lane
+    auto consume = [&](unsigned nt) {
+      // pad to a multiple of 8 with records far from every candidate
+      if ((unsigned)lane < ((8u - (nt & 7u)) & 7u)) s_tile[w][nt + lane] = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+      __syncwarp();
+      if (active)
+        sum += wf ? tile_terms<true>(s_tile[w], nt, cx, cy, cz, K) : tile_terms<false>(s_tile[w], nt, cx, cy, cz, K);
+      if (lane == 0) {
+        visits += min(32u, cnt - chunk * 32u) * nt;
+        slots += 32u * ((nt + 7u) & ~7u);
+      }
+      __syncwarp();
+    };
+    // Stage the chunk's records run by run, lanes on consecutive records of
+    // one run.  Only alive records within reach of the candidates' box are
+    // kept (warp-wide compaction into a 64-entry buffer); each full tile of
+    // 32 is consumed at once and the overflow moves to the front, so no
+    // record is loaded twice.
+    unsigned fill = 0;
+    int r = 0;
+    while (r + 1 < nr && s_rp[w][r + 1] <= r0) r++;
+    for (unsigned pos = r0; pos < r1; r++) {
+      const unsigned run_end = min(s_rp[w][r + 1], r1);
+      const unsigned base = s_rb[w][r] - s_rp[w][r];  // cube slot = base + record number
+      for (unsigned x0 = pos; x0 < run_end; x0 += 32u) {
+        const unsigned x = x0 + (unsigned)lane;
         bool keep = false;
         float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (ff < r1) {
-          int r = rr;
-          while (s_rp[w][r + 1] <= ff) r++;
-          const float4 v = B.cube[s_rb[w][r] + (ff - s_rp[w][r])];
+        if (x < run_end) {
+          const float4 v = B.cube[base + x];
           rec = make_float4(to_grid(v.x, K.nxf), to_grid(v.y, K.nxf), to_grid(v.z, K.nxf), 0.f);
           keep = !(__float_as_uint(v.w) & PSOD_DEAD_BIT);
           if (wf) {
@@ -1206,33 +1224,23 @@ __global__ void __launch_bounds__(256, 4) k_refine_warp(SodConst K, SodBufs B) {
           }
         }
         const unsigned m = __ballot_sync(0xffffffffu, keep);
-        loaded += min(32u, r1 - pos);
-        const unsigned need = 32u - fill, rank = __popc(m & lt);
-        if (keep && rank < need) s_tile[w][fill + rank] = rec;
-        const unsigned got = __popc(m);
-        if (got <= need) {
-          fill += got;
-          pos += 32u;
-        } else {
-          // the need-th kept lane is the last one taken; resume after it
-          const unsigned mk = __ballot_sync(0xffffffffu, keep && rank == need - 1);
-          pos += (unsigned)__ffs(mk);  // lane index + 1
-          fill = 32u;
+        if (keep) s_tile[w][fill + __popc(m & lt)] = rec;  // fill < 32: index < 64
+        fill += (unsigned)__popc(m);
+        loaded += min(32u, run_end - x0);
+        if (fill >= 32u) {
+          consume(32u);
+          if ((unsigned)lane < fill - 32u) s_tile[w][lane] = s_tile[w][32 + lane];
+          __syncwarp();
+          fill -= 32u;
         }
-        while (rr + 1 < nr && s_rp[w][rr + 1] <= pos) rr++;
       }
-      if (pos > r1) pos = r1;
-      // pad to a multiple of 8 with records far from every candidate
-      if ((unsigned)lane < ((8u - (fill & 7u)) & 7u)) s_tile[w][fill + lane] = make_float4(1e18f, 1e18f, 1e18f, 0.f);
-      __syncwarp();
-      if (active && fill > 0)
-        sum += wf ? tile_terms<true>(s_tile[w], fill, cx, cy, cz, K) : tile_terms<false>(s_tile[w], fill, cx, cy, cz, K);
-      if (lane == 0) {
-        visits += (unsigned long long)min(32u, cnt - chunk * 32u) * fill;
-        slots += 32ull * ((fill + 7u) & ~7u);
-      }
-      __syncwarp();
-      fill = 0;
+      pos = run_end;
+    }
+    if (fill > 0) consume(fill);
+    if (lane == 0) {
+      s_count[w][0] += visits;
+      s_count[w][1] += slots;
+      s_count[w][2] += loaded;
     }
     if (active && nchunk == 0 && K.has_quirk) {
       // the particle the run scan files under another cell: counted if that
@@ -1252,9 +1260,11 @@ __global__ void __launch_bounds__(256, 4) k_refine_warp(SodConst K, SodBufs B) {
     }
     if (active && sum != 0.0) atomicAdd(&B.cand_s[q], sum);
   }
-  if (lane == 0 && visits) atomicAdd(B.pairs, visits);
-  if (lane == 0 && slots) atomicAdd(B.pair_slots, slots);
-  if (lane == 0 && loaded) atomicAdd(B.pair_slots + 1, loaded);
+  if (lane == 0) {
+    if (s_count[w][0]) atomicAdd(B.pairs, s_count[w][0]);
+    if (s_count[w][1]) atomicAdd(B.pair_slots, s_count[w][1]);
+    if (s_count[w][2]) atomicAdd(B.pair_slots + 1, s_count[w][2]);
+  }
 }
 
 // ---------------------------------------------------------------------------
