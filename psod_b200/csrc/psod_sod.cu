@@ -866,7 +866,7 @@ __device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned
     B.cell_cnt[slot * 27 + o] = s_cnt[o];
     B.cell_off[slot * 27 + o] = s_base + s_coff[o];
     B.cell_nch[slot * 27 + o] = nch;
-    B.cell_chunks[slot * 27 + o] = ((s_cnt[o] + 31u) / 32u) * nch;
+    B.cell_chunks[slot * 27 + o] = ((s_cnt[o] + 63u) / 64u) * nch;
   }
   for (int o = w; o < 27; o += NWARP) {
     const int di = o / 9 - 1, dj = (o / 3) % 3 - 1, dk = o % 3 - 1;
@@ -1079,12 +1079,32 @@ __device__ __forceinline__ double tile_terms(const float4 *tile, unsigned nt, fl
   return (double)p0 + (double)p1;
 }
 
-// Work item: up to 32 candidates of one candidate cell (a lane each) against
+// the same for two candidates per lane: each staged record serves both
+template <bool WRAPFREE>
+__device__ __forceinline__ void tile_terms2(const float4 *tile, unsigned nt, float ax, float ay, float az, float bx,
+                                            float by, float bz, const SodConst &K, double &sa, double &sb) {
+  const float e2f = (float)K.eps2, limf = (float)(1.0 + K.eps2);
+  float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f, ea = 1.f, eb = 1.f;
+  for (unsigned j = 0; j < nt; j += 8) {
+#pragma unroll
+    for (int u = 0; u < 8; u += 2) {
+      const float4 r0 = tile[j + u], r1 = tile[j + u + 1];
+      pair_fast<WRAPFREE>(r0, ax, ay, az, e2f, limf, K.nxf, a0, ea);
+      pair_fast<WRAPFREE>(r0, bx, by, bz, e2f, limf, K.nxf, b0, eb);
+      pair_fast<WRAPFREE>(r1, ax, ay, az, e2f, limf, K.nxf, a1, ea);
+      pair_fast<WRAPFREE>(r1, bx, by, bz, e2f, limf, K.nxf, b1, eb);
+    }
+  }
+  sa += ea < 1e-5f ? tile_terms_edge<WRAPFREE>(tile, nt, ax, ay, az, e2f, K.nxf, K.tx, K.rmin2) : (double)a0 + (double)a1;
+  sb += eb < 1e-5f ? tile_terms_edge<WRAPFREE>(tile, nt, bx, by, bz, e2f, K.nxf, K.tx, K.rmin2) : (double)b0 + (double)b1;
+}
+
+// Work item: up to 64 candidates of one candidate cell (a lane each) against
 // one chunk of RN_CHUNK records of the cell's 3x3x3 neighbourhood.  Records
 // pass through a warp-private shared slice, 32 at a time, and every lane
 // reads each one by broadcast; warps never wait on one another.  Partial
 // sums of a candidate's neighbour chunks are added into cand_s.
-__global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
+__global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
   __shared__ float4 s_tile[8][64];
   __shared__ unsigned s_rb[8][18], s_rp[8][19];
   __shared__ int s_nr[8], s_wf[8];
@@ -1120,17 +1140,27 @@ __global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
     const int di = (int)(o / 9) - 1, dj = (int)((o / 3) % 3) - 1, dk = (int)(o % 3) - 1;
     const int cxc = wrapi(g.ic + di, K.nx), cyc = wrapi(g.jc + dj, K.nx), czc = wrapi(g.kc + dk, K.nx);
     const unsigned cnt = B.cell_cnt[ci];
-    const unsigned myk = chunk * 32u + (unsigned)lane;
-    const bool have = myk < cnt;
-    const unsigned q = B.cell_off[ci] + myk;
-    const unsigned cp = have ? B.cand_pos[q] : 0u;
+    // candidates k0 = 64*chunk + lane and k1 = k0 + 32 of the cell; items of
+    // at most 32 candidates run one per lane
+    const unsigned k0 = chunk * 64u + (unsigned)lane, k1 = k0 + 32u;
+    const bool two = cnt > chunk * 64u + 32u;
+    const bool have = k0 < cnt, have1 = k1 < cnt;
+    const unsigned q = B.cell_off[ci] + k0, q1 = q + 32u;
+    const unsigned cp = have ? B.cand_pos[q] : 0u, cp1 = have1 ? B.cand_pos[q1] : 0u;
     const bool quirk = have && K.has_quirk && cp == K.quirk_pos;
-    float cx = 0.f, cy = 0.f, cz = 0.f;
+    const bool quirk1 = have1 && K.has_quirk && cp1 == K.quirk_pos;
+    float cx = 0.f, cy = 0.f, cz = 0.f, bx = 1e18f, by = 1e18f, bz = 1e18f;
     if (have) {
       const float4 cv = B.cube[cp];
       cx = to_grid(cv.x, K.nxf);
       cy = to_grid(cv.y, K.nxf);
       cz = to_grid(cv.z, K.nxf);
+    }
+    if (have1) {
+      const float4 cv = B.cube[cp1];
+      bx = to_grid(cv.x, K.nxf);
+      by = to_grid(cv.y, K.nxf);
+      bz = to_grid(cv.z, K.nxf);
     }
     if (lane == 0) {
       // record runs of the 3x3x3 cells around the candidate cell: 9 rows of a
@@ -1167,11 +1197,19 @@ __global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
     const int nr = s_nr[w];
     const unsigned total = s_rp[w][nr];
     const bool wf = s_wf[w];
-    const bool active = have && !quirk;
+    const bool active = have && !quirk, active1 = have1 && !quirk1;
     // bounding box of the item's candidates: records farther than 1 from it
     // in every direction meet no candidate (wrap-free items only)
     float lox = active ? cx : 3e38f, hix = active ? cx : -3e38f, loy = active ? cy : 3e38f,
           hiy = active ? cy : -3e38f, loz = active ? cz : 3e38f, hiz = active ? cz : -3e38f;
+    if (active1) {
+      lox = fminf(lox, bx);
+      hix = fmaxf(hix, bx);
+      loy = fminf(loy, by);
+      hiy = fmaxf(hiy, by);
+      loz = fminf(loz, bz);
+      hiz = fmaxf(hiz, bz);
+    }
     for (int o = 16; o > 0; o >>= 1) {
       lox = fminf(lox, __shfl_xor_sync(0xffffffffu, lox, o));
       hix = fmaxf(hix, __shfl_xor_sync(0xffffffffu, hix, o));
@@ -1183,18 +1221,24 @@ __global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
     const bool any_active = lox <= hix;
     const unsigned r0 = nchunk * RN_CHUNK, r1 = any_active ? min(total, r0 + RN_CHUNK) : r0;
     const unsigned lt = (1u << lane) - 1u;
-    double sum = 0.0;
+    double sum = 0.0, sum1 = 0.0;
     unsigned visits = 0, slots = 0, loaded = 0;
     // tile of 32 kept records: the pair tests of every candidate lane
     auto consume = [&](unsigned nt) {
       // pad to a multiple of 8 with records far from every candidate
       if ((unsigned)lane < ((8u - (nt & 7u)) & 7u)) s_tile[w][nt + lane] = make_float4(1e18f, 1e18f, 1e18f, 0.f);
       __syncwarp();
-      if (active)
+      if (two) {
+        if (active || active1) {
+          if (wf) tile_terms2<true>(s_tile[w], nt, cx, cy, cz, bx, by, bz, K, sum, sum1);
+          else tile_terms2<false>(s_tile[w], nt, cx, cy, cz, bx, by, bz, K, sum, sum1);
+        }
+      } else if (active) {
         sum += wf ? tile_terms<true>(s_tile[w], nt, cx, cy, cz, K) : tile_terms<false>(s_tile[w], nt, cx, cy, cz, K);
+      }
       if (lane == 0) {
-        visits += min(32u, cnt - chunk * 32u) * nt;
-        slots += 32u * ((nt + 7u) & ~7u);
+        visits += min(64u, cnt - chunk * 64u) * nt;
+        slots += (two ? 64u : 32u) * ((nt + 7u) & ~7u);
       }
       __syncwarp();
     };
@@ -1242,7 +1286,7 @@ __global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
       s_count[w][1] += slots;
       s_count[w][2] += loaded;
     }
-    if (active && nchunk == 0 && K.has_quirk) {
+    if (nchunk == 0 && K.has_quirk && (active || active1)) {
       // the particle the run scan files under another cell: counted if that
       // cell is in x_sel2 but outside this candidate cell's 27 neighbours
       const int ax = (int)(K.quirk_listed % K.nx), ay = (int)((K.quirk_listed / K.nx) % K.nx),
@@ -1252,13 +1296,20 @@ __global__ void __launch_bounds__(256) k_refine_warp(SodConst K, SodBufs B) {
       if (listed_in_sel2 && !seen) {
         const float4 qv = B.cube[K.quirk_pos];
         if (!(__float_as_uint(qv.w) & PSOD_DEAD_BIT)) {
-          const double d2 = min_image_d2((double)to_grid(qv.x, K.nxf), (double)to_grid(qv.y, K.nxf),
-                                         (double)to_grid(qv.z, K.nxf), (double)cx, (double)cy, (double)cz, K.tx);
-          if (d2 <= K.rmin2) sum += ddiv(1.0, dsqrt(dadd(d2, K.eps2)));
+          const double qx = to_grid(qv.x, K.nxf), qy = to_grid(qv.y, K.nxf), qz = to_grid(qv.z, K.nxf);
+          if (active) {
+            const double d2 = min_image_d2(qx, qy, qz, (double)cx, (double)cy, (double)cz, K.tx);
+            if (d2 <= K.rmin2) sum += ddiv(1.0, dsqrt(dadd(d2, K.eps2)));
+          }
+          if (active1) {
+            const double d2 = min_image_d2(qx, qy, qz, (double)bx, (double)by, (double)bz, K.tx);
+            if (d2 <= K.rmin2) sum1 += ddiv(1.0, dsqrt(dadd(d2, K.eps2)));
+          }
         }
       }
     }
     if (active && sum != 0.0) atomicAdd(&B.cand_s[q], sum);
+    if (active1 && sum1 != 0.0) atomicAdd(&B.cand_s[q1], sum1);
   }
   if (lane == 0) {
     if (s_count[w][0]) atomicAdd(B.pairs, s_count[w][0]);
