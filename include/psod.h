@@ -133,6 +133,7 @@ typedef struct psod_run_stats {
   int64_t bracket_seeds; /* seeds that ran the crossing search (batched modes) */
   int64_t cross_balls;   /* ball passes of the crossing search */
   int64_t cross_records; /* alive records inside those balls, summed */
+  double ms_refine_bound; /* refinement bound pass (part of ms_refine) */
 } psod_run_stats;
 
 typedef struct psod_ctx psod_ctx;

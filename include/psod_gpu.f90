@@ -48,6 +48,7 @@ module psod_gpu
      integer(c_int64_t) :: ncandidates, refine_pairs, cross_touch, refine_slots
      real(c_double) :: ms_setup, ms_output, ms_learn
      integer(c_int64_t) :: bracket_hits, bracket_seeds, cross_balls, cross_records
+     real(c_double) :: ms_refine_bound
   end type psod_run_stats
 
   type, bind(C) :: psod_train_params

@@ -93,6 +93,7 @@ class RunStats(C.Structure):
         ("bracket_seeds", C.c_int64),
         ("cross_balls", C.c_int64),
         ("cross_records", C.c_int64),
+        ("ms_refine_bound", C.c_double),
     ]
 
     def as_dict(self):

@@ -102,6 +102,14 @@ struct SodBufs {
   float *learn_x, *learn_t;        // collected samples
   unsigned long long *learn_n, learn_cap;
   unsigned long long *bracket_hits, *bracket_seeds, *cross_balls, *cross_records;
+  // refinement bounds: 64-candidate groups per (slot, candidate cell) and
+  // their prefix; per group upper bound U, lower bound L and finished
+  // record chunks; per slot the best lower bound (float bits)
+  unsigned *cell_groups, *group_pref;
+  float *g_u, *g_l;
+  unsigned *g_done, *s_lmax;
+  unsigned *work_bound;
+  int bound_on;
 };
 
 struct Level {
@@ -769,6 +777,7 @@ __device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned
   if (threadIdx.x < 27) {
     B.cell_cnt[slot * 27 + threadIdx.x] = 0;
     B.cell_chunks[slot * 27 + threadIdx.x] = 0;
+    B.cell_groups[slot * 27 + threadIdx.x] = 0;
   }
   const SeedGeo g = seed_geo(K, B, rank);
   if (__float_as_uint(B.cube[g.sp].w) & PSOD_DEAD_BIT) return;  // claimed (main:1628)
@@ -867,6 +876,7 @@ __device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned
     B.cell_off[slot * 27 + o] = s_base + s_coff[o];
     B.cell_nch[slot * 27 + o] = nch;
     B.cell_chunks[slot * 27 + o] = ((s_cnt[o] + 63u) / 64u) * nch;
+    B.cell_groups[slot * 27 + o] = (s_cnt[o] + 63u) / 64u;
   }
   for (int o = w; o < 27; o += NWARP) {
     const int di = o / 9 - 1, dj = (o / 3) % 3 - 1, dk = o % 3 - 1;
@@ -1099,11 +1109,26 @@ __device__ __forceinline__ void tile_terms2(const float4 *tile, unsigned nt, flo
   sb += eb < 1e-5f ? tile_terms_edge<WRAPFREE>(tile, nt, bx, by, bz, e2f, K.nxf, K.tx, K.rmin2) : (double)b0 + (double)b1;
 }
 
-// Work item: up to 64 candidates of one candidate cell (a lane each) against
+// Work item: up to 64 candidates of one candidate cell (two per lane) against
 // one chunk of RN_CHUNK records of the cell's 3x3x3 neighbourhood.  Records
 // pass through a warp-private shared slice, 32 at a time, and every lane
 // reads each one by broadcast; warps never wait on one another.  Partial
 // sums of a candidate's neighbour chunks are added into cand_s.
+//
+// BOUND: the same items, but each record adds only to two bounds of its
+// 64-candidate group, from the candidates' box: U = sum of k(d to the box)
+// over records within reach (no candidate of the group can have a larger
+// S) and L = sum of k(d to the farthest corner) over records surely within
+// reach of every candidate (each candidate's S is at least that).  With k
+// decreasing, max_G L(G) <= S of the argmax, so a group with U(G) below it
+// cannot hold the argmax and the pair pass skips it; its sums stay 0, below
+// the select threshold.  U is inflated and L deflated by 1e-3, far above
+// the FP32 error of the sums.
+// Seeds with fewer candidates than this are neither bounded nor pruned: their
+// pair work is small and the bound pass would cost as much as it saves.
+constexpr unsigned BOUND_MIN_CAND = 4096;
+
+template <bool BOUND>
 __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
   __shared__ float4 s_tile[8][64];
   __shared__ unsigned s_rb[8][18], s_rp[8][19];
@@ -1117,7 +1142,7 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
   while (true) {
     unsigned item = 0, ci = 0, rem = 0;
     if (lane == 0) {
-      item = atomicAdd(&B.work[1], 1u);
+      item = atomicAdd(BOUND ? B.work_bound : &B.work[1], 1u);
       if (item < nitems) {
         unsigned lo = 0, hi = B.nitems_cells;  // last ci with chunk_pref[ci] <= item
         while (hi - lo > 1) {
@@ -1136,6 +1161,10 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
     const unsigned nch = B.cell_nch[ci];
     const unsigned chunk = rem / nch, nchunk = rem % nch;
     const unsigned slot = ci / 27, o = ci % 27;
+    const unsigned grp = B.group_pref[ci] + chunk;
+    const bool bounded = B.bound_on && B.st_cn[slot] >= BOUND_MIN_CAND;
+    if (BOUND && !bounded) continue;
+    if (!BOUND && bounded && B.g_u[grp] < __uint_as_float(B.s_lmax[slot])) continue;  // cannot hold the argmax
     const SeedGeo g = seed_geo(K, B, B.ready[slot]);
     const int di = (int)(o / 9) - 1, dj = (int)((o / 3) % 3) - 1, dk = (int)(o % 3) - 1;
     const int cxc = wrapi(g.ic + di, K.nx), cyc = wrapi(g.jc + dj, K.nx), czc = wrapi(g.kc + dk, K.nx);
@@ -1248,9 +1277,11 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
     // 32 is consumed at once and the overflow moves to the front, so no
     // record is loaded twice.
     unsigned fill = 0;
+    float ub = (BOUND && !wf) ? __int_as_float(0x7f800000) : 0.f, lb = 0.f;  // bounds (BOUND)
+    const float e2b = (float)K.eps2;
     int r = 0;
     while (r + 1 < nr && s_rp[w][r + 1] <= r0) r++;
-    for (unsigned pos = r0; pos < r1; r++) {
+    for (unsigned pos = (BOUND && !wf) ? r1 : r0; pos < r1; r++) {
       const unsigned run_end = min(s_rp[w][r + 1], r1);
       const unsigned base = s_rb[w][r] - s_rp[w][r];  // cube slot = base + record number
       for (unsigned x0 = pos; x0 < run_end; x0 += 32u) {
@@ -1264,9 +1295,18 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
           if (wf) {
             const float ex = fmaxf(fmaxf(lox - rec.x, rec.x - hix), 0.f), ey = fmaxf(fmaxf(loy - rec.y, rec.y - hiy), 0.f),
                         ez = fmaxf(fmaxf(loz - rec.z, rec.z - hiz), 0.f);
-            keep = keep && fmaf(ex, ex, fmaf(ey, ey, ez * ez)) <= 1.0001f;
+            const float db2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+            keep = keep && db2 <= 1.0001f;
+            if (BOUND && keep) {
+              ub += rsqrt_pos(db2 + e2b);
+              const float fx = fmaxf(rec.x - lox, hix - rec.x), fy = fmaxf(rec.y - loy, hiy - rec.y),
+                          fz = fmaxf(rec.z - loz, hiz - rec.z);
+              const float dm2 = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
+              if (dm2 <= 0.9999f) lb += rsqrt_pos(dm2 + e2b);
+            }
           }
         }
+        if (BOUND) continue;
         const unsigned m = __ballot_sync(0xffffffffu, keep);
         if (keep) s_tile[w][fill + __popc(m & lt)] = rec;  // fill < 32: index < 64
         fill += (unsigned)__popc(m);
@@ -1279,6 +1319,26 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
         }
       }
       pos = run_end;
+    }
+    if (BOUND) {
+      for (int sh = 16; sh > 0; sh >>= 1) {
+        ub += __shfl_xor_sync(0xffffffffu, ub, sh);
+        lb += __shfl_xor_sync(0xffffffffu, lb, sh);
+      }
+      if (lane == 0 && any_active) {
+        // the particle the run scan files under another cell may add up to
+        // 1/eps = 64 to any candidate's sum outside these runs
+        atomicAdd(&B.g_u[grp], ub * 1.001f + ((K.has_quirk && nchunk == 0) ? 64.f : 0.f));
+        atomicAdd(&B.g_l[grp], lb * 0.999f);
+        __threadfence();
+        // the group's last record chunk publishes its lower bound
+        if (atomicAdd(&B.g_done[grp], 1u) == nch - 1) {
+          __threadfence();
+          const float L = atomicAdd(&B.g_l[grp], 0.f);
+          atomicMax(&B.s_lmax[slot], __float_as_uint(L));
+        }
+      }
+      continue;
     }
     if (fill > 0) consume(fill);
     if (lane == 0) {
@@ -1782,6 +1842,29 @@ __global__ void __launch_bounds__(TPB) k_cross(SodConst K, SodBufs B) {
   }
 }
 
+// Lower bound of each ready seed's best refinement sum: the seed is one of
+// its own candidates, so its sum (FP32 terms, relative error below 2e-6),
+// deflated by 1e-3, is at most the maximum.  Warp per seed.
+__global__ void k_seed_lower(SodConst K, SodBufs B) {
+  const unsigned slot = (unsigned)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (slot >= min(*B.nready, B.cap_ready) || !B.st_active[slot] || B.st_cn[slot] < BOUND_MIN_CAND) return;
+  const SeedGeo g = seed_geo(K, B, B.ready[slot]);
+  unsigned long long sq = 0;
+  double sf = 0.0;
+  refine_sum<false>(K, B, g.sp, g.ic, g.jc, g.kc, sq, sf);
+  if ((threadIdx.x & 31) == 0) atomicMax(&B.s_lmax[slot], __float_as_uint((float)(sf * 0.999)));
+}
+
+// zero the per-group bound arrays of this round (group count on the device)
+__global__ void k_zero_groups(const unsigned *total, float *u, float *l, unsigned *done) {
+  const unsigned n = *total;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    u[i] = 0.f;
+    l[i] = 0.f;
+    done[i] = 0u;
+  }
+}
+
 __global__ void k_clear_dead(float4 *cube, long long n) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {
@@ -2112,7 +2195,7 @@ enum {
   SC_HRDELTA, SC_HPOOL, SC_COUNTS, SC_ST_ACTIVE, SC_ST_NA, SC_ST_COFF, SC_ST_CN,
   SC_ST_CENTRE, SC_CAND_POS, SC_CAND_SLOT, SC_CAND_S, SC_ORDER, SC_RKEYS, SC_MASS32, SC_MOFF, SC_TKEY, SC_TIDX,
   SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS, SC_CELLNCH, SC_FEAT, SC_RB0,
-  SC_SBEST
+  SC_SBEST, SC_CELLGROUPS, SC_GROUPPREF, SC_GU, SC_GL, SC_GDONE, SC_LMAX
 };
 
 struct PhaseTimer {
@@ -2142,7 +2225,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   psod_run_stats st{};
   st.fail_rank = -1;
   st.npart_new = c->npart_new;
-  PhaseTimer t_all, t_sched, t_prep, t_ref, t_sel, t_cross, t_setup, t_out, t_learn;
+  PhaseTimer t_all, t_sched, t_prep, t_ref, t_sel, t_cross, t_setup, t_out, t_learn, t_bound;
   t_all.start(c->stream);
   int rc = PSOD_OK;
   const SodConst K = make_sod_const(c);
@@ -2212,6 +2295,15 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     return rc;
   unsigned *cell_nch;
   if ((rc = scratch(c, SC_CELLNCH, (size_t)cap_ready * 27, &cell_nch))) return rc;
+  // refinement bound groups: at most cand_cap/64 + 27 per ready seed
+  const size_t gcap = (size_t)cand_cap / 64 + (size_t)cap_ready * 27 + 1;
+  unsigned *cell_groups, *group_pref, *g_done, *s_lmax;
+  float *g_u, *g_l;
+  if ((rc = scratch(c, SC_CELLGROUPS, (size_t)cap_ready * 27, &cell_groups)) ||
+      (rc = scratch(c, SC_GROUPPREF, (size_t)cap_ready * 27 + 1, &group_pref)) ||
+      (rc = scratch(c, SC_GU, gcap, &g_u)) || (rc = scratch(c, SC_GL, gcap, &g_l)) ||
+      (rc = scratch(c, SC_GDONE, gcap, &g_done)) || (rc = scratch(c, SC_LMAX, (size_t)cap_ready, &s_lmax)))
+    return rc;
   float *st_feat, *st_rb0;
   unsigned long long *st_sbest;
   if ((rc = scratch(c, SC_FEAT, (size_t)cap_ready * 16, &st_feat)) || (rc = scratch(c, SC_RB0, (size_t)cap_ready, &st_rb0)) ||
@@ -2268,7 +2360,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   if (per_sm < 1) per_sm = 1;
   const unsigned seed_grid = (unsigned)(dev_sms * per_sm);
   int per_sm_ref = 1;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ref, k_refine_warp, 256, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_ref, k_refine_warp<false>, 256, 0);
   const unsigned ref_grid = (unsigned)(dev_sms * std::max(1, per_sm_ref));
 
   SodBufs B;
@@ -2328,6 +2420,14 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.bracket_seeds = u64s + 11;
   B.cross_balls = u64s + 12;
   B.cross_records = u64s + 13;
+  B.cell_groups = cell_groups;
+  B.group_pref = group_pref;
+  B.g_u = g_u;
+  B.g_l = g_l;
+  B.g_done = g_done;
+  B.s_lmax = s_lmax;
+  B.work_bound = ctrs + 10;
+  B.bound_on = 1;
   // the learned bracket needs the per-cell alive counts of the batched modes
   B.learn_use = (c->p.mode == PSOD_MODE_LEARNED && learn_ready(c)) ? 1 : 0;
   B.learn_collect = (c->p.mode != PSOD_MODE_PLAIN && learn_collecting(c)) ? 1 : 0;
@@ -2360,6 +2460,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   while (nseed > 0 && n_active > 0) {
     t_sched.start(c->stream);
     PSOD_CUDA(c, cudaMemsetAsync(ctrs, 0, sizeof(unsigned) * 5, c->stream));  // nready, work[4]
+    PSOD_CUDA(c, cudaMemsetAsync(ctrs + 10, 0, sizeof(unsigned), c->stream));  // bound pass work
     PSOD_CUDA(c, cudaMemsetAsync(gmin, 0xff, sizeof(unsigned), c->stream));
     PSOD_CUDA(c, cudaMemsetAsync(cand_used, 0, sizeof(unsigned), c->stream));
     PSOD_CUDA(c, cudaMemsetAsync(ctrs + 9, 0, sizeof(unsigned), c->stream));
@@ -2389,7 +2490,17 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     t_ref.start(c->stream);
     B.nitems_cells = 27u * nready;
     if ((rc = scan_u32(c, cell_chunks, chunk_pref, (long long)B.nitems_cells, true))) return rc;
-    k_refine_warp<<<ref_grid, 256, 0, c->stream>>>(K, B);
+    if ((rc = scan_u32(c, cell_groups, group_pref, (long long)B.nitems_cells, true))) return rc;
+    if (B.bound_on) {
+      t_bound.start(c->stream);
+      k_zero_groups<<<ref_grid, 256, 0, c->stream>>>(group_pref + B.nitems_cells, g_u, g_l, g_done);
+      PSOD_CUDA(c, cudaMemsetAsync(s_lmax, 0, sizeof(unsigned) * nready, c->stream));
+      k_seed_lower<<<nblk((long long)nready * 32, 256), 256, 0, c->stream>>>(K, B);
+      k_refine_warp<true><<<ref_grid, 256, 0, c->stream>>>(K, B);
+      t_bound.stop(c->stream);
+      kernels += 3;
+    }
+    k_refine_warp<false><<<ref_grid, 256, 0, c->stream>>>(K, B);
     t_ref.stop(c->stream);
     t_sel.start(c->stream);
     k_select<<<g, TPB, smem, c->stream>>>(K, B);
@@ -2410,6 +2521,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     t_sel.collect();
     t_cross.collect();
     if (B.learn_use) t_learn.collect();
+    if (B.bound_on) t_bound.collect();
     if (trace) {
       unsigned cu = 0;
       unsigned long long tv[16];
@@ -2447,6 +2559,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   st.bracket_seeds = (int64_t)hv[11];
   st.cross_balls = (int64_t)hv[12];
   st.cross_records = (int64_t)hv[13];
+  st.ms_refine_bound = t_bound.total;
   c->nhalo = 0;
   c->nmember = 0;
   c->sod_done = false;
