@@ -110,6 +110,7 @@ struct SodBufs {
   unsigned *g_done, *s_lmax;
   unsigned *work_bound;
   int bound_on;
+  unsigned *st_big;  // 1: the crossing needs the CTA path (null: CTA for all)
 };
 
 struct Level {
@@ -1832,12 +1833,366 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
   }
 }
 
+// ---------------------------------------------------------------------------
+// Crossing search of small balls, one warp per seed.  Most seeds are small
+// halos whose first ball holds a few hundred records; for them the CTA path's
+// block barriers cost more than the work.  A warp loads the ball (alive
+// records of the cells that meet it, d2 <= rb^2) into its own slice of
+// shared memory, sorts it by (d2 bits, index) with warp-synchronous bitonic
+// stages and runs the same searches as the CTA small path.  Everything is
+// decided before the first write: a ball of more than WCAP records, a ball
+// that reaches the whole cube, a threshold whose stop lies outside the ball
+// or a profile that needs a wider region marks the seed for the CTA kernel
+// (st_big), which then processes it from scratch in the same round.
+// ---------------------------------------------------------------------------
+constexpr int WCAP = 512;  // records per warp slice
+constexpr unsigned WARP_CROSS_MIN_READY = 2048;  // rounds with fewer seeds use the CTA kernel only
+struct WSlice {
+  unsigned long long key[WCAP];
+  unsigned idx[WCAP];
+  unsigned pos[WCAP];
+};
+
+__device__ __forceinline__ int warp_min_i(int v) {
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ int warp_max_i(int v) {
+  for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ unsigned warp_sum_u(unsigned v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// the bounded window of cube rows (dj, dk) that can meet a ball of radius rm
+// around (ty, tz) (cell offsets relative to the seed cell centre)
+__device__ __forceinline__ void ball_rows(const SodConst &K, double ty, double tz, double rm, int &jlo, int &jhi,
+                                          int &klo, int &khi) {
+  const int R = K.ncut;
+  jlo = max(-R, (int)floor(ty - rm - 0.5));
+  jhi = min(R, (int)ceil(ty + rm + 0.5));
+  klo = max(-R, (int)floor(tz - rm - 0.5));
+  khi = min(R, (int)ceil(tz + rm + 0.5));
+}
+
+// x-ranges of cube row (dj, dk) meeting the ball (the row rule of
+// for_region); returns the number of cell-start ranges (0..2)
+__device__ __forceinline__ int ball_row_ranges(const SodConst &K, const SodBufs &B, const Region &G, double tx,
+                                               double ty, double tz, double rm2, int dj, int dk, unsigned rb_[2],
+                                               unsigned re_[2]) {
+  const int R = K.ncut;
+  const double nxd = (double)K.nx;
+  const double gy = cell_gap(ty, dj, nxd), gz = cell_gap(tz, dk, nxd);
+  const double rem = rm2 - gy * gy - gz * gz;
+  if (rem < 0.0) return 0;
+  const double wx = sqrt(rem);
+  int t0 = (int)ceil(tx - 0.5 - wx), t1 = (int)floor(tx + 0.5 + wx);
+  t0 = max(t0, -R);
+  t1 = min(t1, R);
+  if (t0 > t1) return 0;
+  const unsigned nx = (unsigned)K.nx;
+  const unsigned jj = (unsigned)wrapi(G.jc + dj, K.nx), kk = (unsigned)wrapi(G.kc + dk, K.nx);
+  const unsigned long long base = (unsigned long long)nx * (jj + (unsigned long long)nx * kk);
+  const int x0 = G.ic + t0, x1 = G.ic + t1;
+  int pa[2], pb[2], np;
+  if (x0 < 0) {
+    pa[0] = x0 + K.nx; pb[0] = K.nx - 1; pa[1] = 0; pb[1] = x1; np = 2;
+    if (x1 < 0) { pa[0] = x0 + K.nx; pb[0] = x1 + K.nx; np = 1; }
+  } else if (x1 >= K.nx) {
+    pa[0] = x0; pb[0] = K.nx - 1; pa[1] = 0; pb[1] = x1 - K.nx; np = 2;
+    if (x0 >= K.nx) { pa[0] = x0 - K.nx; pb[0] = x1 - K.nx; np = 1; }
+  } else {
+    pa[0] = x0; pb[0] = x1; np = 1;
+  }
+  for (int q = 0; q < np; q++) {
+    rb_[q] = B.cs[base + (unsigned)pa[q]];
+    re_[q] = B.cs[base + (unsigned)pb[q] + 1];
+  }
+  return np;
+}
+
+// load the ball's alive records into the slice, sorted; returns the count
+// (above WCAP: overflow, slice unusable)
+__device__ unsigned warp_load_ball(const SodConst &K, const SodBufs &B, WSlice &W, const Region &G) {
+  const int lane = threadIdx.x & 31;
+  const double nxd = (double)K.nx;
+  auto rel = [&](double x, int i) {
+    double d = x - ((double)i + K.xs + 0.5);
+    d = d - nxd * floor(d / nxd + 0.5);
+    return d;
+  };
+  const double tx = rel(G.xc, G.ic), ty = rel(G.yc, G.jc), tz = rel(G.zc, G.kc);
+  const double rm = G.rb + 1e-3, rm2 = rm * rm;
+  int jlo, jhi, klo, khi;
+  ball_rows(K, ty, tz, rm, jlo, jhi, klo, khi);
+  unsigned n = 0;
+  for (int dk = klo; dk <= khi; dk++)
+    for (int dj = jlo; dj <= jhi; dj++) {
+      unsigned rb_[2], re_[2];
+      const int np = ball_row_ranges(K, B, G, tx, ty, tz, rm2, dj, dk, rb_, re_);
+      for (int q = 0; q < np; q++)
+        for (unsigned p0 = rb_[q]; p0 < re_[q]; p0 += 32u) {
+          const unsigned p = p0 + (unsigned)lane;
+          double d2 = 0.0;
+          float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+          bool in = false;
+          if (p < re_[q]) {
+            v = B.cube[p];
+            in = region_d2(K, G, v, d2);
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, in);
+          const unsigned at = n + __popc(m & ((1u << lane) - 1u));
+          if (in && at < WCAP) {
+            W.key[at] = dbits(d2);
+            W.idx[at] = __float_as_uint(v.w) & PSOD_IDX_MASK;
+            W.pos[at] = p;
+          }
+          n += __popc(m);
+        }
+    }
+  if (n > WCAP) return n;
+  unsigned m2 = 32;
+  while (m2 < n) m2 <<= 1;
+  for (unsigned k = n + lane; k < m2; k += 32) {
+    W.key[k] = ~0ull;
+    W.idx[k] = 0xffffffffu;
+  }
+  __syncwarp();
+  for (unsigned size = 2; size <= m2; size <<= 1)
+    for (unsigned stride = size >> 1; stride > 0; stride >>= 1) {
+      for (unsigned k = lane; k < m2 / 2; k += 32) {
+        const unsigned a = 2 * k - (k & (stride - 1)), bb = a + stride;
+        const bool up = ((a & size) == 0);
+        const unsigned long long ka = W.key[a], kb = W.key[bb];
+        const unsigned ia = W.idx[a], ib = W.idx[bb];
+        const bool gt = (ka > kb) || (ka == kb && ia > ib);
+        if (gt == up) {
+          W.key[a] = kb;
+          W.key[bb] = ka;
+          W.idx[a] = ib;
+          W.idx[bb] = ia;
+          const unsigned pa = W.pos[a];
+          W.pos[a] = W.pos[bb];
+          W.pos[bb] = pa;
+        }
+      }
+      __syncwarp();
+    }
+  return n;
+}
+
+// first 1-based i >= 10 of the sorted slice where the loop stops (partial
+// ball: i < npart_sel always holds); 0 if none
+__device__ long long warp_stop(const SodConst &K, const WSlice &W, unsigned n, double delta) {
+  const int lane = threadIdx.x & 31;
+  int best = 0x7fffffff;
+  for (unsigned k = 9 + lane; k < n; k += 32)
+    if (!keeps_going(K, (long long)k + 1, bitsd(W.key[k]), 0x7fffffffffffffffll, delta)) {
+      best = (int)k;
+      break;
+    }
+  best = warp_min_i(best);
+  return best == 0x7fffffff ? 0 : (long long)best + 1;
+}
+
+// records of the cube cells meeting the ball of radius rb (the touch count)
+__device__ unsigned warp_ball_records(const SodConst &K, const SodBufs &B, const Region &G) {
+  const int lane = threadIdx.x & 31;
+  const double nxd = (double)K.nx;
+  auto rel = [&](double x, int i) {
+    double d = x - ((double)i + K.xs + 0.5);
+    d = d - nxd * floor(d / nxd + 0.5);
+    return d;
+  };
+  const double tx = rel(G.xc, G.ic), ty = rel(G.yc, G.jc), tz = rel(G.zc, G.kc);
+  const double rm2 = G.rb * G.rb;
+  int jlo, jhi, klo, khi;
+  ball_rows(K, ty, tz, G.rb, jlo, jhi, klo, khi);
+  const int ny = jhi - jlo + 1, nrow = ny * (khi - klo + 1);
+  unsigned sum = 0;
+  for (int row = lane; row < nrow; row += 32) {
+    const int dj = jlo + row % ny, dk = klo + row / ny;
+    unsigned rb_[2], re_[2];
+    const int np = ball_row_ranges(K, B, G, tx, ty, tz, rm2, dj, dk, rb_, re_);
+    for (int q = 0; q < np; q++) sum += re_[q] - rb_[q];
+  }
+  return warp_sum_u(sum);
+}
+
+__global__ void __launch_bounds__(256) k_cross_warp(SodConst K, SodBufs B) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  WSlice &W = reinterpret_cast<WSlice *>(smem_raw)[w];
+  const unsigned slot = (unsigned)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  if (slot >= min(*B.nready, B.cap_ready) || !B.st_active[slot]) return;
+  if (lane == 0) B.st_big[slot] = 0;
+  const unsigned rank = B.ready[slot];
+  const SeedGeo g = seed_geo(K, B, rank);
+  const unsigned cpos = B.st_centre[slot];
+  const float4 cvv = B.cube[cpos];
+  Region G;
+  G.ic = g.ic;
+  G.jc = g.jc;
+  G.kc = g.kc;
+  G.xc = (double)to_grid(cvv.x, K.nxf);
+  G.yc = (double)to_grid(cvv.y, K.nxf);
+  G.zc = (double)to_grid(cvv.z, K.nxf);
+  const double xc = G.xc, yc = G.yc, zc = G.zc;
+  const unsigned cidx = __float_as_uint(cvv.w) & PSOD_IDX_MASK;
+  double rb0 = BALL0;
+  if (B.learn_use) {
+    const float r = B.st_rb0[slot];
+    if (r > 0.f) rb0 = fmin(fmax((double)r, BALL0), (double)K.ncut);
+  }
+  auto to_cta = [&]() {
+    if (lane == 0) B.st_big[slot] = 1;
+  };
+  // 3. crossing (main:2040-2100) in growing partial balls
+  unsigned passes = 0;
+  unsigned long long records = 0;
+  unsigned n = 0;
+  long long istop = 0;
+  double rb = rb0;
+  while (true) {
+    if (rb >= (double)K.ncut) {
+      to_cta();
+      return;
+    }
+    G.rb = rb;
+    G.rb2 = rb * rb;
+    n = warp_load_ball(K, B, W, G);
+    passes++;
+    records += n;
+    if (n > WCAP) {
+      to_cta();
+      return;
+    }
+    istop = warp_stop(K, W, n, K.delta);
+    if (istop != 0) break;
+    rb *= 2.0;
+  }
+  const double d2stop = bitsd(W.key[istop - 1]);
+  if (overdens(K, istop, d2stop) > K.delta) {  // main:2072
+    if (lane == 0) record_error(B, rank, PSOD_ERR_SELRADIUS);
+    return;
+  }
+  const long long masse = istop - 1;
+  const unsigned long long thr_key = W.key[masse - 1];
+  (void)thr_key;
+  const double rayon = dsqrt(bitsd(W.key[masse - 1]));
+  // seuil2 capture (main:2062-2069)
+  long long masse2 = 0;
+  {
+    int best = -1;
+    for (unsigned k = 1 + lane; k < (unsigned)istop; k += 32)
+      if (overdens(K, (long long)k + 1, bitsd(W.key[k])) > K.delta2) best = max(best, (int)k);
+    best = warp_max_i(best);
+    if (best >= 0) masse2 = best + 1;
+  }
+  // extra thresholds: their stops must lie in this ball too
+  long long mext[PSOD_MAX_EXTRA_DELTA];
+  double d2far = d2stop;
+  for (int e = 0; e < K.ndx; e++) {
+    const long long ie = warp_stop(K, W, n, K.dx_extra[e]);
+    if (ie == 0) {
+      to_cta();
+      return;
+    }
+    const double dd = bitsd(W.key[ie - 1]);
+    mext[e] = overdens(K, ie, dd) > K.dx_extra[e] ? -1 : ie - 1;
+    d2far = fmax(d2far, dd);
+  }
+  // keep test (main:2118-2120)
+  const double amass = dmul((double)masse, K.munit);
+  const bool keep = amass >= K.mmin && xc <= K.zmax && xc > K.zmin && yc <= K.zmax && yc > K.zmin &&
+                    zc <= K.zmax && zc > K.zmin;
+  if (keep) {
+    const double emax = dmul(rayon, B.edge_fac[K.nbins - 1]);
+    if (!(emax * (1.0 + 1e-9) < G.rb)) {
+      to_cta();
+      return;
+    }
+  }
+  // ---- committed: counters, bookkeeping, profile, claims, halo record ----
+  {
+    Region Gt = G;
+    Gt.rb = dsqrt(d2stop);
+    Gt.rb2 = d2stop;
+    const unsigned nt = warp_ball_records(K, B, Gt);
+    if (lane == 0) {
+      atomicAdd(B.touch, (unsigned long long)nt);
+      atomicAdd(B.cross_balls, (unsigned long long)passes);
+      atomicAdd(B.cross_records, records);
+      atomicAdd(B.bracket_seeds, 1ull);
+      if (d2far <= rb0 * rb0) atomicAdd(B.bracket_hits, 1ull);
+    }
+  }
+  if (lane == 0 && B.learn_collect) {
+    const unsigned long long q = atomicAdd(B.learn_n, 1ull);
+    if (q < B.learn_cap) {
+      for (int k = 0; k < PSOD_LEARN_FEATURES; k++) B.learn_x[q * PSOD_LEARN_FEATURES + k] = B.st_feat[slot * 16 + k];
+      B.learn_t[2 * q] = (float)(0.5 * log(fmax(d2far, 1e-12)));
+      B.learn_t[2 * q + 1] = (float)log((double)masse);
+    }
+  }
+  unsigned long long pool_base = 0;
+  unsigned long long hs = 0;
+  if (lane == 0) {
+    if (keep) {
+      pool_base = atomicAdd(B.pool_used, (unsigned long long)masse);
+      hs = atomicAdd(B.nhalo, 1ull);
+    }
+  }
+  pool_base = __shfl_sync(0xffffffffu, pool_base, 0);
+  hs = __shfl_sync(0xffffffffu, hs, 0);
+  // 4a. profile (main:2103-2115): cumulative counts below each edge
+  if (keep) {
+    for (int j = lane; j < K.nbins; j += 32) {
+      const double edge = dmul(rayon, B.edge_fac[j]);
+      unsigned lo = 0, hi = n;
+      while (lo < hi) {
+        const unsigned mid = (lo + hi) >> 1;
+        if (dsqrt(bitsd(W.key[mid])) < edge) lo = mid + 1;
+        else hi = mid;
+      }
+      B.h_profile[hs * K.nbins + j] = lo;
+    }
+  }
+  // 4b. claims (main:2148-2166): the masse nearest die, kept or not
+  for (unsigned k = lane; k < (unsigned)masse; k += 32) {
+    const unsigned p = W.pos[k];
+    const float4 v = B.cube[p];
+    B.cube[p].w = __uint_as_float(__float_as_uint(v.w) | PSOD_DEAD_BIT);
+    if (B.alive_cnt) atomicSub(&B.alive_cnt[listed_cell(K, p, v)], 1u);
+    if (keep) {
+      B.pool_key[pool_base + k] = W.key[k];
+      B.pool_idx[pool_base + k] = W.idx[k];
+    }
+  }
+  // 5. halo record
+  if (keep && lane == 0) {
+    B.h_rank[hs] = rank;
+    B.h_id[hs] = B.ids[cidx];
+    B.h_mass[hs] = masse;
+    B.h_mass2[hs] = masse2;
+    B.h_rdelta[hs] = rayon;
+    B.h_center[3 * hs + 0] = __double2float_rn(ddiv(xc, K.scale));
+    B.h_center[3 * hs + 1] = __double2float_rn(ddiv(yc, K.scale));
+    B.h_center[3 * hs + 2] = __double2float_rn(ddiv(zc, K.scale));
+    B.h_pool[hs] = pool_base | POOL_SORTED;
+    for (int e = 0; e < K.ndx; e++) B.h_mextra[hs * K.ndx + e] = mext[e];
+  }
+}
+
 __global__ void __launch_bounds__(TPB) k_cross(SodConst K, SodBufs B) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem &S = *reinterpret_cast<Smem *>(smem_raw);
   while (true) {
     const unsigned item = next_item(&B.work[3]);
     if (item >= min(*B.nready, B.cap_ready)) break;
+    if (B.st_big && !B.st_big[item]) continue;  // done by the warp pass
     cross_seed(K, B, S, item, B.ready[item]);
   }
 }
@@ -2195,7 +2550,7 @@ enum {
   SC_HRDELTA, SC_HPOOL, SC_COUNTS, SC_ST_ACTIVE, SC_ST_NA, SC_ST_COFF, SC_ST_CN,
   SC_ST_CENTRE, SC_CAND_POS, SC_CAND_SLOT, SC_CAND_S, SC_ORDER, SC_RKEYS, SC_MASS32, SC_MOFF, SC_TKEY, SC_TIDX,
   SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS, SC_CELLNCH, SC_FEAT, SC_RB0,
-  SC_SBEST, SC_CELLGROUPS, SC_GROUPPREF, SC_GU, SC_GL, SC_GDONE, SC_LMAX
+  SC_SBEST, SC_CELLGROUPS, SC_GROUPPREF, SC_GU, SC_GL, SC_GDONE, SC_LMAX, SC_BIG
 };
 
 struct PhaseTimer {
@@ -2304,6 +2659,8 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       (rc = scratch(c, SC_GU, gcap, &g_u)) || (rc = scratch(c, SC_GL, gcap, &g_l)) ||
       (rc = scratch(c, SC_GDONE, gcap, &g_done)) || (rc = scratch(c, SC_LMAX, (size_t)cap_ready, &s_lmax)))
     return rc;
+  unsigned *st_big;
+  if ((rc = scratch(c, SC_BIG, (size_t)cap_ready, &st_big))) return rc;
   float *st_feat, *st_rb0;
   unsigned long long *st_sbest;
   if ((rc = scratch(c, SC_FEAT, (size_t)cap_ready * 16, &st_feat)) || (rc = scratch(c, SC_RB0, (size_t)cap_ready, &st_rb0)) ||
@@ -2428,6 +2785,10 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.s_lmax = s_lmax;
   B.work_bound = ctrs + 10;
   B.bound_on = 1;
+  // small balls take the warp-per-seed crossing; the CTA kernel the rest
+  B.st_big = (c->p.mode != PSOD_MODE_PLAIN) ? st_big : nullptr;
+  const size_t wsmem = 8 * sizeof(WSlice);
+  PSOD_CUDA(c, cudaFuncSetAttribute(k_cross_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem));
   // the learned bracket needs the per-cell alive counts of the batched modes
   B.learn_use = (c->p.mode == PSOD_MODE_LEARNED && learn_ready(c)) ? 1 : 0;
   B.learn_collect = (c->p.mode != PSOD_MODE_PLAIN && learn_collecting(c)) ? 1 : 0;
@@ -2513,7 +2874,16 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       t_learn.stop(c->stream);
     }
     t_cross.start(c->stream);
-    k_cross<<<g, TPB, smem, c->stream>>>(K, B);
+    // The warp pass pays off when a round has many seeds; in the sparse tail
+    // a round lasts as long as its slowest seed, and a CTA handles one seed
+    // with eight warps.
+    SodBufs Bc = B;
+    if (!(B.st_big && nready >= WARP_CROSS_MIN_READY)) Bc.st_big = nullptr;
+    if (Bc.st_big) {
+      k_cross_warp<<<nblk((long long)nready * 32, 256), 256, wsmem, c->stream>>>(K, Bc);
+      kernels++;
+    }
+    k_cross<<<g, TPB, smem, c->stream>>>(K, Bc);
     t_cross.stop(c->stream);
     PSOD_CUDA(c, cudaGetLastError());
     t_prep.collect();
