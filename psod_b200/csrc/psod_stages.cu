@@ -246,6 +246,7 @@ __global__ void k_cic_interp(const float4 *cube, long long n, CicConst k, const 
 constexpr int CT = 8;                 // SOD cells per tile side
 constexpr int CW = 2 * (CT + 2) + 1;  // window nodes per side
 constexpr int CW3 = CW * CW * CW;
+constexpr unsigned DEP_RUN = 8;      // consecutive particles deposited per thread
 
 constexpr int CRNG = 2 * (CT + 2) * (CT + 2);  // record ranges of a tile plus halo (two where x wraps)
 
@@ -309,32 +310,65 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
   range_prefix(s_len, s_pre, CRNG);
   __syncthreads();
   {
+    // Each thread deposits runs of DEP_RUN consecutive particles.  Dense
+    // cells are sub-cell ordered, so consecutive particles mostly share a
+    // fine cell and its 8 nodes: their fixed-point weights are summed in
+    // registers and written with one atomic per node when the fine cell
+    // changes (integer sums, so the grid is the same).
     const unsigned total = s_pre[CRNG];
     int r = 0;
-    for (unsigned f = threadIdx.x; f < total; f += blockDim.x) {
-      while (s_pre[r + 1] <= f) r++;
-      const float4 v = cube[s_rb[r] + (f - s_pre[r])];
-      int ix, ixp, iy, iyp, iz, izp;
-      double ddx, dex, ddy, dey, ddz, dez;
-      cic_axis(v.x, k, ix, ixp, ddx, dex);
-      cic_axis(v.y, k, iy, iyp, ddy, dey);
-      cic_axis(v.z, k, iz, izp, ddz, dez);
-      const int sx = sod_cell_axis(to_grid(v.x, nxf), xs, nx), sy = sod_cell_axis(to_grid(v.y, nxf), xs, nx),
-                sz = sod_cell_axis(to_grid(v.z, nxf), xs, nx);
-      if ((ix >> 1) != sx || (iy >> 1) != sy || (iz >> 1) != sz) {
-        atomicOr(bad, 1);
-        continue;
-      }
-      const int cx[2] = {widx(ix, ox), widx(ixp, ox)}, cy[2] = {widx(iy, oy), widx(iyp, oy)},
-                cz[2] = {widx(iz, oz), widx(izp, oz)};
-      const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
+    unsigned long long acc[8];
+    int kx = -1, ky = -1, kz = -1;  // fine cell of the accumulated run
+    int ncx[2], ncy[2], ncz[2];     // its nodes' window offsets
+    auto flush = [&]() {
+      if (kx < 0) return;
 #pragma unroll
       for (int c = 0; c < 8; c++) {
         const int a = c & 1, bb = (c >> 1) & 1, ee = c >> 2;
-        if (cx[a] >= CW || cy[bb] >= CW || cz[ee] >= CW) continue;
-        const double wgt = dmul(dmul(wx[a], wy[bb]), wz[ee]);
-        atomicAdd(&win[cx[a] + CW * (cy[bb] + CW * cz[ee])], (unsigned long long)__double2ll_rn(dmul(wgt, FIX_ONE)));
+        if (ncx[a] < CW && ncy[bb] < CW && ncz[ee] < CW && acc[c])
+          atomicAdd(&win[ncx[a] + CW * (ncy[bb] + CW * ncz[ee])], acc[c]);
       }
+      kx = -1;
+    };
+    for (unsigned f0 = threadIdx.x * DEP_RUN; f0 < total; f0 += blockDim.x * DEP_RUN) {
+      const unsigned f1 = min(total, f0 + DEP_RUN);
+      for (unsigned f = f0; f < f1; f++) {
+        while (s_pre[r + 1] <= f) r++;
+        const float4 v = cube[s_rb[r] + (f - s_pre[r])];
+        int ix, ixp, iy, iyp, iz, izp;
+        double ddx, dex, ddy, dey, ddz, dez;
+        cic_axis(v.x, k, ix, ixp, ddx, dex);
+        cic_axis(v.y, k, iy, iyp, ddy, dey);
+        cic_axis(v.z, k, iz, izp, ddz, dez);
+        const int sx = sod_cell_axis(to_grid(v.x, nxf), xs, nx), sy = sod_cell_axis(to_grid(v.y, nxf), xs, nx),
+                  sz = sod_cell_axis(to_grid(v.z, nxf), xs, nx);
+        if ((ix >> 1) != sx || (iy >> 1) != sy || (iz >> 1) != sz) {
+          atomicOr(bad, 1);
+          continue;
+        }
+        if (ix != kx || iy != ky || iz != kz) {
+          flush();
+          kx = ix;
+          ky = iy;
+          kz = iz;
+          ncx[0] = widx(ix, ox);
+          ncx[1] = widx(ixp, ox);
+          ncy[0] = widx(iy, oy);
+          ncy[1] = widx(iyp, oy);
+          ncz[0] = widx(iz, oz);
+          ncz[1] = widx(izp, oz);
+#pragma unroll
+          for (int c = 0; c < 8; c++) acc[c] = 0ull;
+        }
+        const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+          const int a = c & 1, bb = (c >> 1) & 1, ee = c >> 2;
+          const double wgt = dmul(dmul(wx[a], wy[bb]), wz[ee]);
+          acc[c] += (unsigned long long)__double2ll_rn(dmul(wgt, FIX_ONE));
+        }
+      }
+      flush();
     }
   }
   __syncthreads();
