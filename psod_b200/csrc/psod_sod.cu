@@ -111,7 +111,15 @@ struct SodBufs {
   unsigned *work_bound;
   int bound_on;
   unsigned *st_big;  // 1: the crossing needs the CTA path (null: CTA for all)
+  // scheduler: one bit per seed in block-list order, set once the seed is
+  // processed or claimed; list position of each rank and of each cube slot
+  // (~0 for particles that are not seeds)
+  unsigned *resolved, *bidx_of_rank, *bidx_of_cube;
 };
+
+__device__ __forceinline__ void mark_resolved(const SodBufs &B, unsigned bi) {
+  if (bi != 0xffffffffu) atomicOr(&B.resolved[bi >> 5], 1u << (bi & 31));
+}
 
 struct Level {
   unsigned long long lo, hi;  // bit range of the level
@@ -773,6 +781,7 @@ __device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned
     B.st_active[slot] = 0;
     B.st_cn[slot] = 0;
     B.processed[rank] = 1;
+    mark_resolved(B, B.bidx_of_rank[rank]);
   }
   // no refinement work unless this seed turns out active
   if (threadIdx.x < 27) {
@@ -842,6 +851,10 @@ __device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned
       // candidate buffer full this round: the seed waits for the next one
       s_base = 0xffffffffu;
       B.processed[rank] = 0;
+      {
+        const unsigned bi = B.bidx_of_rank[rank];
+        atomicAnd(&B.resolved[bi >> 5], ~(1u << (bi & 31)));
+      }
       if (tot > B.cand_cap) record_error(B, rank, PSOD_ERR_STATE);
     } else {
       B.st_na[slot] = na;  // 0 when unknown (batched modes)
@@ -1781,6 +1794,7 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
       const unsigned p = spos[k];
       const float4 v = B.cube[p];
       B.cube[p].w = __uint_as_float(__float_as_uint(v.w) | PSOD_DEAD_BIT);
+      mark_resolved(B, B.bidx_of_cube[p]);
       if (B.alive_cnt) atomicSub(&B.alive_cnt[listed_cell(K, p, v)], 1u);
       if (keep) {
         B.pool_key[pool_base + k] = S.skey[k];
@@ -1797,6 +1811,7 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
     const unsigned ix = wv & PSOD_IDX_MASK;
     if (x < thr_key || (x == thr_key && ix <= thr_idx)) {
       B.cube[p].w = __uint_as_float(wv | PSOD_DEAD_BIT);
+      mark_resolved(B, B.bidx_of_cube[p]);
       if (B.alive_cnt) atomicSub(&B.alive_cnt[listed_cell(K, p, v)], 1u);
       const unsigned slot2 = atomicAdd(&S.claim_cnt, 1u);
       if (keep && slot2 < (unsigned)masse) {
@@ -2165,6 +2180,7 @@ __global__ void __launch_bounds__(256) k_cross_warp(SodConst K, SodBufs B) {
     const unsigned p = W.pos[k];
     const float4 v = B.cube[p];
     B.cube[p].w = __uint_as_float(__float_as_uint(v.w) | PSOD_DEAD_BIT);
+    mark_resolved(B, B.bidx_of_cube[p]);
     if (B.alive_cnt) atomicSub(&B.alive_cnt[listed_cell(K, p, v)], 1u);
     if (keep) {
       B.pool_key[pool_base + k] = W.key[k];
@@ -2271,55 +2287,31 @@ __global__ void k_init_active(long long nblocks, const unsigned *bbegin, unsigne
 // Warp per active block: advance the cursor past resolved (processed or
 // claimed) seeds, 256 entries per step with independent loads; head = the
 // lowest unresolved rank.  Blocks that still hold seeds go to next_active.
+// first index in [cur, end) whose resolved bit is clear, or end
+__device__ __forceinline__ unsigned first_unresolved(const unsigned *res, unsigned cur, unsigned end) {
+  while (cur < end) {
+    const unsigned sh = cur & 31u;
+    const unsigned zero = ~(res[cur >> 5] >> sh) & (0xffffffffu >> sh);
+    if (zero) return min(end, cur + (unsigned)(__ffs(zero) - 1));
+    cur = (cur | 31u) + 1u;
+  }
+  return end;
+}
+
 // One lane per active block: the head is the block's first unresolved seed
-// at or after its cursor.  Most heads are the cursor's own slot; blocks whose
-// cursor slot was resolved are walked by the whole warp, 32 slots a step.
+// at or after its cursor, found in the resolved bitmap (32 seeds a word).
 __global__ void k_heads(const unsigned *active, unsigned nactive, const unsigned *bbegin, unsigned *cursor,
-                        const unsigned *blist, const unsigned *bpos, const unsigned char *processed,
-                        const float4 *cube, unsigned *head, unsigned *gmin, unsigned *next_active,
-                        unsigned *n_next) {
+                        const unsigned *blist, const unsigned *resolved, unsigned *head, unsigned *gmin,
+                        unsigned *next_active, unsigned *n_next) {
   const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   const bool have = i < nactive;
-  unsigned b = 0, cur = 0, end = 0, h = PSOD_INF_RANK;
-  bool walk = false;
+  unsigned b = 0, cur = 0, h = PSOD_INF_RANK;
   if (have) {
     b = active[i];
-    cur = cursor[b];
-    end = bbegin[b + 1];
-    if (cur < end) {
-      if (!processed[blist[cur]] && !(__float_as_uint(cube[bpos[cur]].w) & PSOD_DEAD_BIT)) {
-        h = blist[cur];
-      } else {
-        walk = true;
-        cur++;
-      }
-    }
-  }
-  unsigned wm = __ballot_sync(0xffffffffu, walk);
-  while (wm) {
-    const int src = __ffs(wm) - 1;
-    wm &= wm - 1;
-    unsigned c = __shfl_sync(0xffffffffu, cur, src);
-    const unsigned e = __shfl_sync(0xffffffffu, end, src);
-    unsigned hh = PSOD_INF_RANK;
-    while (c < e) {
-      const unsigned idx = c + (unsigned)lane;
-      bool unres = false;
-      if (idx < e) unres = !processed[blist[idx]] && !(__float_as_uint(cube[bpos[idx]].w) & PSOD_DEAD_BIT);
-      const unsigned m = __ballot_sync(0xffffffffu, unres);
-      if (m) {
-        c += (unsigned)(__ffs(m) - 1);
-        hh = blist[c];
-        break;
-      }
-      c += 32u;
-    }
-    if (c > e) c = e;
-    if (lane == src) {
-      cur = c;
-      h = hh;
-    }
+    const unsigned end = bbegin[b + 1];
+    cur = first_unresolved(resolved, cursor[b], end);
+    if (cur < end) h = blist[cur];
   }
   const bool live = have && h != PSOD_INF_RANK;
   const unsigned lm = __ballot_sync(0xffffffffu, live);
@@ -2333,6 +2325,15 @@ __global__ void k_heads(const unsigned *active, unsigned nactive, const unsigned
   cursor[b] = cur;
   head[b] = h;
   if (live) next_active[base + __popc(lm & ((1u << lane) - 1u))] = b;
+}
+
+// list positions of the seeds: by rank and by cube slot
+__global__ void k_seed_index(const unsigned *blist, const unsigned *bpos, long long nseed, unsigned *bidx_of_rank,
+                             unsigned *bidx_of_cube) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nseed) return;
+  bidx_of_rank[blist[i]] = (unsigned)i;
+  bidx_of_cube[bpos[i]] = (unsigned)i;
 }
 
 // periodic sliding minimum of radius rb along one axis of the nb^3 grid
@@ -2550,7 +2551,8 @@ enum {
   SC_HRDELTA, SC_HPOOL, SC_COUNTS, SC_ST_ACTIVE, SC_ST_NA, SC_ST_COFF, SC_ST_CN,
   SC_ST_CENTRE, SC_CAND_POS, SC_CAND_SLOT, SC_CAND_S, SC_ORDER, SC_RKEYS, SC_MASS32, SC_MOFF, SC_TKEY, SC_TIDX,
   SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS, SC_CELLNCH, SC_FEAT, SC_RB0,
-  SC_SBEST, SC_CELLGROUPS, SC_GROUPPREF, SC_GU, SC_GL, SC_GDONE, SC_LMAX, SC_BIG
+  SC_SBEST, SC_CELLGROUPS, SC_GROUPPREF, SC_GU, SC_GL, SC_GDONE, SC_LMAX, SC_BIG, SC_RESOLVED, SC_BIDXRANK,
+  SC_BIDXCUBE
 };
 
 struct PhaseTimer {
@@ -2661,6 +2663,11 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     return rc;
   unsigned *st_big;
   if ((rc = scratch(c, SC_BIG, (size_t)cap_ready, &st_big))) return rc;
+  unsigned *resolved, *bidx_of_rank, *bidx_of_cube;
+  if ((rc = scratch(c, SC_RESOLVED, (size_t)nseed / 32 + 2, &resolved)) ||
+      (rc = scratch(c, SC_BIDXRANK, (size_t)nseed + 1, &bidx_of_rank)) ||
+      (rc = scratch(c, SC_BIDXCUBE, (size_t)n, &bidx_of_cube)))
+    return rc;
   float *st_feat, *st_rb0;
   unsigned long long *st_sbest;
   if ((rc = scratch(c, SC_FEAT, (size_t)cap_ready * 16, &st_feat)) || (rc = scratch(c, SC_RB0, (size_t)cap_ready, &st_rb0)) ||
@@ -2688,7 +2695,10 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     if ((rc = radix_sort_u32(c, block_of, blist, nseed, 32))) return rc;
     PSOD_CUDA(c, cudaMemcpyAsync(cursor, bbegin, sizeof(unsigned) * nblocks, cudaMemcpyDeviceToDevice, c->stream));
     k_seed_pos<<<nblk(nseed, 256), 256, 0, c->stream>>>(blist, nseed, c->d_seed_idx, c->d_inv, bpos);
-    kernels++;
+    PSOD_CUDA(c, cudaMemsetAsync(resolved, 0, sizeof(unsigned) * ((size_t)nseed / 32 + 2), c->stream));
+    PSOD_CUDA(c, cudaMemsetAsync(bidx_of_cube, 0xff, sizeof(unsigned) * (size_t)n, c->stream));
+    k_seed_index<<<nblk(nseed, 256), 256, 0, c->stream>>>(blist, bpos, nseed, bidx_of_rank, bidx_of_cube);
+    kernels += 2;
     if (c->has_quirk) {
       float4 qv;
       PSOD_CUDA(c, cudaMemcpyAsync(&qv, c->d_cube + c->quirk_pos, sizeof(qv), cudaMemcpyDeviceToHost, c->stream));
@@ -2787,6 +2797,9 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.bound_on = 1;
   // small balls take the warp-per-seed crossing; the CTA kernel the rest
   B.st_big = (c->p.mode != PSOD_MODE_PLAIN) ? st_big : nullptr;
+  B.resolved = resolved;
+  B.bidx_of_rank = bidx_of_rank;
+  B.bidx_of_cube = bidx_of_cube;
   const size_t wsmem = 8 * sizeof(WSlice);
   PSOD_CUDA(c, cudaFuncSetAttribute(k_cross_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem));
   // the learned bracket needs the per-cell alive counts of the batched modes
@@ -2826,7 +2839,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     PSOD_CUDA(c, cudaMemsetAsync(cand_used, 0, sizeof(unsigned), c->stream));
     PSOD_CUDA(c, cudaMemsetAsync(ctrs + 9, 0, sizeof(unsigned), c->stream));
     k_heads<<<nblk((long long)n_active, 256), 256, 0, c->stream>>>(
-        act_a, n_active, bbegin, cursor, blist, bpos, processed, c->d_cube, head,
+        act_a, n_active, bbegin, cursor, blist, resolved, head,
         quirk_rank != PSOD_INF_RANK ? gmin : nullptr, act_b, ctrs + 9);
     k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(head, filt_a, nb, 0, rb);
     k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(filt_a, filt_b, nb, 1, rb);
