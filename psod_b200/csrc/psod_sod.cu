@@ -1138,6 +1138,8 @@ __device__ __forceinline__ void tile_terms2(const float4 *tile, unsigned nt, flo
 // cannot hold the argmax and the pair pass skips it; its sums stay 0, below
 // the select threshold.  U is inflated and L deflated by 1e-3, far above
 // the FP32 error of the sums.
+constexpr unsigned ITEM_GRAB = 1;  // refinement items claimed per counter update
+
 // Seeds with fewer candidates than this are neither bounded nor pruned: their
 // pair work is small and the bound pass would cost as much as it saves.
 constexpr unsigned BOUND_MIN_CAND = 4096;
@@ -1153,10 +1155,18 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
   // shared memory (keeps 64-bit totals out of the registers)
   __shared__ unsigned long long s_count[8][3];
   if (lane < 3) s_count[w][lane] = 0;
+  // items are claimed ITEM_GRAB at a time (one counter update per group of
+  // consecutive items)
+  unsigned grab = 0, grab_left = 0;
   while (true) {
     unsigned item = 0, ci = 0, rem = 0;
     if (lane == 0) {
-      item = atomicAdd(BOUND ? B.work_bound : &B.work[1], 1u);
+      if (grab_left == 0) {
+        grab = atomicAdd(BOUND ? B.work_bound : &B.work[1], ITEM_GRAB);
+        grab_left = ITEM_GRAB;
+      }
+      item = grab++;
+      grab_left--;
       if (item < nitems) {
         unsigned lo = 0, hi = B.nitems_cells;  // last ci with chunk_pref[ci] <= item
         while (hi - lo > 1) {
@@ -2404,7 +2414,8 @@ __global__ void k_widen(const unsigned *in, long long n, long long *out) {
   if (i < n) out[i] = (long long)in[i];
 }
 
-constexpr int MS_CHUNK = 4096;
+constexpr int MS_CHUNK = 2048;
+constexpr unsigned MS_TILE = 2048;  // merge outputs staged per step (<= MS_CHUNK)
 
 __device__ __forceinline__ bool pair_less(unsigned long long ka, unsigned ia, unsigned long long kb, unsigned ib) {
   return ka < kb || (ka == kb && ia < ib);
@@ -2418,6 +2429,7 @@ __global__ void __launch_bounds__(256) k_member_sort(const unsigned *order, long
                                                      unsigned long long *tkey, unsigned *tidx, unsigned *m_index) {
   __shared__ unsigned long long sk[MS_CHUNK];
   __shared__ unsigned si[MS_CHUNK];
+  __shared__ unsigned s_split[2];
   for (long long h = blockIdx.x; h < nh; h += gridDim.x) {
     const unsigned slot = order[h];
     const unsigned long long base = h_pool[slot] & ~POOL_SORTED;
@@ -2461,35 +2473,64 @@ __global__ void __launch_bounds__(256) k_member_sort(const unsigned *order, long
       }
       __syncthreads();
     }
-    // 2. merge runs pairwise through global memory
+    // 2. merge runs pairwise, MS_TILE outputs at a time: the tile's split
+    // of the two runs is found by binary search on its diagonals (merge
+    // path), both pieces are staged in shared memory and each thread
+    // merges MS_TILE / 256 outputs there.  Keys (d2 bits, index) are
+    // unique, so the merge is exact.
     for (unsigned w = MS_CHUNK; w < m; w <<= 1) {
-      for (unsigned k = threadIdx.x; k < m; k += blockDim.x) {
-        const unsigned run = k / (2 * w);
-        const unsigned s0 = run * 2 * w;
-        const unsigned amid = min(s0 + w, m), aend = min(s0 + 2 * w, m);
-        const unsigned long long key = ka[k];
-        const unsigned ix = ia[k];
-        unsigned pos;
-        if (k < amid) {
-          // count of the other run strictly below
-          unsigned lo = amid, hi = aend;
-          while (lo < hi) {
-            unsigned mid = (lo + hi) >> 1;
-            if (pair_less(ka[mid], ia[mid], key, ix)) lo = mid + 1;
-            else hi = mid;
+      for (unsigned s0 = 0; s0 < m; s0 += 2 * w) {
+        const unsigned na = min(w, m - s0), nb = min(w, m - min(m, s0 + w));
+        const unsigned long long *A = ka + s0, *Bk = ka + s0 + na;
+        const unsigned *Ai = ia + s0, *Bi = ia + s0 + na;
+        for (unsigned o0 = 0; o0 < na + nb; o0 += MS_TILE) {
+          const unsigned o1 = min(o0 + MS_TILE, na + nb);
+          if (threadIdx.x < 2) {
+            const unsigned d = threadIdx.x == 0 ? o0 : o1;  // diagonal
+            unsigned lo = d > nb ? d - nb : 0u, hi = min(d, na);
+            while (lo < hi) {
+              const unsigned mid = (lo + hi) >> 1;
+              if (pair_less(Bk[d - mid - 1], Bi[d - mid - 1], A[mid], Ai[mid])) hi = mid;
+              else lo = mid + 1;
+            }
+            s_split[threadIdx.x] = lo;
           }
-          pos = s0 + (k - s0) + (lo - amid);
-        } else {
-          unsigned lo = s0, hi = amid;
-          while (lo < hi) {
-            unsigned mid = (lo + hi) >> 1;
-            if (pair_less(ka[mid], ia[mid], key, ix)) lo = mid + 1;
-            else hi = mid;
+          __syncthreads();
+          const unsigned a0 = s_split[0], a1 = s_split[1];
+          const unsigned b0 = o0 - a0, b1 = o1 - a1;
+          const unsigned la = a1 - a0, lb = b1 - b0;
+          for (unsigned k = threadIdx.x; k < la; k += blockDim.x) {
+            sk[k] = A[a0 + k];
+            si[k] = Ai[a0 + k];
           }
-          pos = s0 + (k - amid) + (lo - s0);
+          for (unsigned k = threadIdx.x; k < lb; k += blockDim.x) {
+            sk[la + k] = Bk[b0 + k];
+            si[la + k] = Bi[b0 + k];
+          }
+          __syncthreads();
+          // thread t: outputs [t*PER, t*PER + PER) of the tile
+          const unsigned per = MS_TILE / 256u, t0 = threadIdx.x * per;
+          if (t0 < la + lb) {
+            unsigned lo = t0 > lb ? t0 - lb : 0u, hi = min(t0, la);
+            while (lo < hi) {
+              const unsigned mid = (lo + hi) >> 1;
+              if (pair_less(sk[la + t0 - mid - 1], si[la + t0 - mid - 1], sk[mid], si[mid])) hi = mid;
+              else lo = mid + 1;
+            }
+            unsigned x = lo, y = t0 - lo;
+            const unsigned tend = min(t0 + per, la + lb);
+            for (unsigned q = t0; q < tend; q++) {
+              bool take_a;
+              if (x >= la) take_a = false;
+              else if (y >= lb) take_a = true;
+              else take_a = !pair_less(sk[la + y], si[la + y], sk[x], si[x]);
+              const unsigned src = take_a ? x++ : la + y++;
+              kb[s0 + o0 + q] = sk[src];
+              ib[s0 + o0 + q] = si[src];
+            }
+          }
+          __syncthreads();
         }
-        kb[pos] = key;
-        ib[pos] = ix;
       }
       __syncthreads();
       unsigned long long *tk = ka; ka = kb; kb = tk;

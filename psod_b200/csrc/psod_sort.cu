@@ -131,63 +131,92 @@ constexpr int RS_ITEMS = 16;
 constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
 constexpr int RS_RADIX = 256;
 
+// digit counts of a tile; lanes with equal digits are counted together
+// (the top digits of clustered keys are shared by most of a tile)
 template <typename K>
 __global__ void k_radix_hist(const K *keys, long long n, int shift, unsigned *hist, long long ntiles) {
   __shared__ unsigned s_h[RS_RADIX];
   s_h[threadIdx.x] = 0;
   __syncthreads();
+  const int lane = threadIdx.x & 31;
   long long base = (long long)blockIdx.x * RS_TILE;
 #pragma unroll 4
   for (int k = 0; k < RS_ITEMS; k++) {
-    long long i = base + (long long)k * RS_THREADS + threadIdx.x;
-    if (i < n) atomicAdd(&s_h[(unsigned)(keys[i] >> shift) & 0xffu], 1u);
+    const long long i = base + (long long)k * RS_THREADS + threadIdx.x;
+    const bool valid = i < n;
+    const unsigned d = valid ? ((unsigned)(keys[i] >> shift) & 0xffu) : (RS_RADIX + lane);
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    if (valid && lane == __ffs(peers) - 1) atomicAdd(&s_h[d], (unsigned)__popc(peers));
   }
   __syncthreads();
   hist[(long long)threadIdx.x * ntiles + blockIdx.x] = s_h[threadIdx.x];
 }
 
-// stable scatter: elements of a tile are ranked in order j*256 + t
+// Stable scatter.  Warp w of a tile owns its keys [w*512, (w+1)*512) and
+// ranks them 32 at a time in input order (match_any on the digit, running
+// per-warp digit counters); one scan over the warps per digit then gives
+// each warp's start within the tile's digit run.  Two barriers per tile.
+constexpr int RS_WARPS = RS_THREADS / 32;
+constexpr int RS_PER_LANE = RS_TILE / RS_THREADS;
+
 template <typename K>
-__global__ void k_radix_scatter(const K *keys, const unsigned *vals, K *okeys, unsigned *ovals, long long n,
-                                int shift, const unsigned *offsets, long long ntiles) {
+__global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const K *keys, const unsigned *vals, K *okeys,
+                                                              unsigned *ovals, long long n, int shift,
+                                                              const unsigned *offsets, long long ntiles) {
+  __shared__ unsigned s_cnt[RS_WARPS][RS_RADIX];
   __shared__ unsigned s_base[RS_RADIX];
-  __shared__ unsigned s_run[RS_RADIX];
-  __shared__ unsigned s_warp[RS_THREADS / 32][RS_RADIX];
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+#pragma unroll
+  for (int q = 0; q < RS_WARPS; q++) s_cnt[q][t] = 0;
   s_base[t] = offsets[(long long)t * ntiles + blockIdx.x];
-  s_run[t] = 0;
-  const unsigned lt_mask = (1u << lane) - 1u;
-  long long base = (long long)blockIdx.x * RS_TILE;
-  for (int j = 0; j < RS_ITEMS; j++) {
+  __syncthreads();
+  const long long base = (long long)blockIdx.x * RS_TILE + (long long)w * (32 * RS_PER_LANE);
+  const unsigned lt = (1u << lane) - 1u;
+  K k[RS_PER_LANE];
+  unsigned v[RS_PER_LANE], rk[RS_PER_LANE];
+  // all loads first (independent, in flight together), then the ranking
 #pragma unroll
-    for (int q = 0; q < RS_THREADS / 32; q++) s_warp[q][t] = 0;
-    __syncthreads();
-    long long i = base + (long long)j * RS_THREADS + t;
-    bool valid = i < n;
-    K key = valid ? keys[i] : (K)0;
-    unsigned val = valid ? vals[i] : 0u;
-    unsigned d = valid ? ((unsigned)(key >> shift) & 0xffu) : (RS_RADIX + lane);
-    unsigned peers = __match_any_sync(0xffffffffu, d);
-    unsigned rank_w = __popc(peers & lt_mask);
-    if (valid && rank_w == 0) s_warp[w][d] = __popc(peers);
-    __syncthreads();
-    {
-      unsigned run = s_run[t], acc = 0;
+  for (int r = 0; r < RS_PER_LANE; r++) {
+    const long long i = base + r * 32 + lane;
+    const bool valid = i < n;
+    k[r] = valid ? keys[i] : (K)0;
+    v[r] = valid ? vals[i] : 0u;
+  }
 #pragma unroll
-      for (int q = 0; q < RS_THREADS / 32; q++) {
-        unsigned cnt = s_warp[q][t];
-        s_warp[q][t] = run + acc;
-        acc += cnt;
-      }
-      s_run[t] = run + acc;
+  for (int r = 0; r < RS_PER_LANE; r++) {
+    const long long i = base + r * 32 + lane;
+    const bool valid = i < n;
+    const unsigned d = valid ? ((unsigned)(k[r] >> shift) & 0xffu) : (RS_RADIX + lane);
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const int leader = __ffs(peers) - 1;
+    unsigned prev = 0;
+    if (valid && lane == leader) {
+      prev = s_cnt[w][d];
+      s_cnt[w][d] = prev + __popc(peers);
     }
-    __syncthreads();
-    if (valid) {
-      unsigned pos = s_base[d] + s_warp[w][d] + rank_w;
-      okeys[pos] = key;
-      ovals[pos] = val;
+    prev = __shfl_sync(0xffffffffu, prev, leader);
+    rk[r] = prev + __popc(peers & lt);
+  }
+  __syncthreads();
+  {
+    unsigned run = 0;
+#pragma unroll
+    for (int q = 0; q < RS_WARPS; q++) {
+      const unsigned cnt = s_cnt[q][t];
+      s_cnt[q][t] = run;
+      run += cnt;
     }
-    __syncthreads();
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < RS_PER_LANE; r++) {
+    const long long i = base + r * 32 + lane;
+    if (i < n) {
+      const unsigned d = (unsigned)(k[r] >> shift) & 0xffu;
+      const unsigned pos = s_base[d] + s_cnt[w][d] + rk[r];
+      okeys[pos] = k[r];
+      ovals[pos] = v[r];
+    }
   }
 }
 
@@ -199,8 +228,15 @@ __global__ void k_key_range(const K *keys, long long n, unsigned long long *mn_m
     mn = k < mn ? k : mn;
     mx = k > mx ? k : mx;
   }
-  atomicMin(&mn_mx[0], mn);
-  atomicMax(&mn_mx[1], mx);
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long a = __shfl_down_sync(0xffffffffu, mn, o), b = __shfl_down_sync(0xffffffffu, mx, o);
+    mn = a < mn ? a : mn;
+    mx = b > mx ? b : mx;
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&mn_mx[0], mn);
+    atomicMax(&mn_mx[1], mx);
+  }
 }
 
 template <typename K>

@@ -11,6 +11,7 @@
 //                  reference's term order, FP64 without contraction.
 //  stage_tri_cic   tri_cic (main:998-1037): 1/rho < 0.01 compaction and a
 //                  stable radix sort of the seeds, ties by input index.
+#include <algorithm>
 #include <cmath>
 
 #include "psod_internal.cuh"
@@ -422,25 +423,34 @@ __global__ void k_grid_to_double(const unsigned long long *grid, long long nnode
 // ---------------------------------------------------------------------------
 // seeds
 // ---------------------------------------------------------------------------
-__global__ void k_seed_flags(const double *rho, long long n, unsigned *flag, unsigned long long *minbits) {
-  long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned f = 0;
+// Seed flags (1/rho < 0.01) and the smallest key of the others.  Fixed
+// grid, each thread over a strided range; one atomic per CTA (a per-warp
+// atomic on the single minimum serialises tens of millions of updates).
+__global__ void __launch_bounds__(256) k_seed_flags(const double *rho, long long n, unsigned *flag,
+                                                    unsigned long long *minbits) {
+  __shared__ unsigned long long s_min[8];
   unsigned long long mb = ~0ull;
-  if (i < n) {
-    double pd = ddiv(1.0, rho[i]);  // main:1022
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double pd = ddiv(1.0, rho[i]);  // main:1022
+    unsigned f = 0;
     if (pd < 0.01) {
       f = 1;  // main:1029: 1/rho < 1/100
     } else {
-      mb = dbits(pd);
+      const unsigned long long b = dbits(pd);
+      mb = b < mb ? b : mb;
     }
     flag[i] = f;
   }
-  // block min of the non-seed keys
   for (int o = 16; o > 0; o >>= 1) {
-    unsigned long long t = __shfl_down_sync(0xffffffffu, mb, o);
+    const unsigned long long t = __shfl_down_sync(0xffffffffu, mb, o);
     mb = t < mb ? t : mb;
   }
-  if ((threadIdx.x & 31) == 0 && mb != ~0ull) atomicMin(minbits, mb);
+  if ((threadIdx.x & 31) == 0) s_min[threadIdx.x >> 5] = mb;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (int)(blockDim.x >> 5); q++) mb = s_min[q] < mb ? s_min[q] : mb;
+    if (mb != ~0ull) atomicMin(minbits, mb);
+  }
 }
 
 __global__ void k_seed_extra_idx(const double *rho, long long n, unsigned long long minbits, unsigned *minidx) {
@@ -627,7 +637,12 @@ int stage_tri_cic(psod_ctx *c, int64_t *isort_out) {
   minidx = reinterpret_cast<unsigned *>(minbits + 1);
   PSOD_CUDA(c, cudaMemsetAsync(minbits, 0xff, sizeof(unsigned long long), c->stream));
   PSOD_CUDA(c, cudaMemsetAsync(minidx, 0xff, sizeof(unsigned), c->stream));
-  k_seed_flags<<<nblk(n, 256), 256, 0, c->stream>>>(c->d_rho, n, flag, minbits);
+  {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+    const unsigned grid = (unsigned)std::max<long long>(1, std::min<long long>(nblk(n, 256), (long long)sms * 8));
+    k_seed_flags<<<grid, 256, 0, c->stream>>>(c->d_rho, n, flag, minbits);
+  }
   if ((st = scan_u32(c, flag, posn, n, true))) return st;
   unsigned nd = 0;
   unsigned long long hmin = 0;
