@@ -49,6 +49,7 @@ module psod_gpu
      real(c_double) :: ms_setup, ms_output, ms_learn
      integer(c_int64_t) :: bracket_hits, bracket_seeds, cross_balls, cross_records
      real(c_double) :: ms_refine_bound
+     integer(c_int64_t) :: refine_items, refine_pruned
   end type psod_run_stats
 
   type, bind(C) :: psod_train_params

@@ -94,6 +94,8 @@ class RunStats(C.Structure):
         ("cross_balls", C.c_int64),
         ("cross_records", C.c_int64),
         ("ms_refine_bound", C.c_double),
+        ("refine_items", C.c_int64),
+        ("refine_pruned", C.c_int64),
     ]
 
     def as_dict(self):

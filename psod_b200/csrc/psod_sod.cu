@@ -110,6 +110,14 @@ struct SodBufs {
   unsigned *g_done, *s_lmax;
   unsigned *work_bound;
   int bound_on;
+  // per bounded seed the group with the largest upper bound (~0u: none),
+  // whose sums run first; pair-pass phase: 0 all items, 1 only those
+  // groups, 2 all other items
+  unsigned *s_top, *work_top;
+  // phase-1 items: per seed the top group's candidate cell, first item
+  // offset within the cell, item count, and the prefix sum of the counts
+  unsigned *top_ci, *top_rem0, *top_n, *top_pref;
+  int ref_phase;
   unsigned *st_big;  // 1: the crossing needs the CTA path (null: CTA for all)
   // scheduler: one bit per seed in block-list order, set once the seed is
   // processed or claimed; list position of each rank and of each cube slot
@@ -1150,11 +1158,14 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
   __shared__ unsigned s_rb[8][18], s_rp[8][19];
   __shared__ int s_nr[8], s_wf[8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const unsigned nitems = B.chunk_pref[B.nitems_cells];
+  const bool phase1 = !BOUND && B.ref_phase == 1;
+  const unsigned nready = min(*B.nready, B.cap_ready);
+  const unsigned nitems = phase1 ? B.top_pref[nready] : B.chunk_pref[B.nitems_cells];
   // pair, slot and staged-record counts: per item in 32 bits, per warp in
   // shared memory (keeps 64-bit totals out of the registers)
-  __shared__ unsigned long long s_count[8][3];
-  if (lane < 3) s_count[w][lane] = 0;
+  // (pair pass: also items taken and items pruned by the bound)
+  __shared__ unsigned long long s_count[8][5];
+  if (lane < 5) s_count[w][lane] = 0;
   // items are claimed ITEM_GRAB at a time (one counter update per group of
   // consecutive items)
   unsigned grab = 0, grab_left = 0;
@@ -1162,12 +1173,21 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
     unsigned item = 0, ci = 0, rem = 0;
     if (lane == 0) {
       if (grab_left == 0) {
-        grab = atomicAdd(BOUND ? B.work_bound : &B.work[1], ITEM_GRAB);
+        grab = atomicAdd(BOUND ? B.work_bound : (B.ref_phase == 1 ? B.work_top : &B.work[1]), ITEM_GRAB);
         grab_left = ITEM_GRAB;
       }
       item = grab++;
       grab_left--;
-      if (item < nitems) {
+      if (item < nitems && phase1) {
+        unsigned lo = 0, hi = nready;  // last seed with top_pref <= item
+        while (hi - lo > 1) {
+          const unsigned mid = (lo + hi) >> 1;
+          if (B.top_pref[mid] <= item) lo = mid;
+          else hi = mid;
+        }
+        ci = B.top_ci[lo];
+        rem = B.top_rem0[lo] + (item - B.top_pref[lo]);
+      } else if (item < nitems) {
         unsigned lo = 0, hi = B.nitems_cells;  // last ci with chunk_pref[ci] <= item
         while (hi - lo > 1) {
           const unsigned mid = (lo + hi) >> 1;
@@ -1188,7 +1208,13 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
     const unsigned grp = B.group_pref[ci] + chunk;
     const bool bounded = B.bound_on && B.st_cn[slot] >= BOUND_MIN_CAND;
     if (BOUND && !bounded) continue;
-    if (!BOUND && bounded && B.g_u[grp] < __uint_as_float(B.s_lmax[slot])) continue;  // cannot hold the argmax
+    if (!BOUND && B.ref_phase == 2 && bounded && grp == B.s_top[slot]) continue;  // done in phase 1
+    if (!BOUND && lane == 0) s_count[w][3]++;
+    if (!BOUND && B.ref_phase != 1 && bounded &&
+        B.g_u[grp] < __uint_as_float(B.s_lmax[slot])) {  // cannot hold the argmax
+      if (lane == 0) s_count[w][4]++;
+      continue;
+    }
     const SeedGeo g = seed_geo(K, B, B.ready[slot]);
     const int di = (int)(o / 9) - 1, dj = (int)((o / 3) % 3) - 1, dk = (int)(o % 3) - 1;
     const int cxc = wrapi(g.ic + di, K.nx), cyc = wrapi(g.jc + dj, K.nx), czc = wrapi(g.kc + dk, K.nx);
@@ -1399,6 +1425,8 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
     if (s_count[w][0]) atomicAdd(B.pairs, s_count[w][0]);
     if (s_count[w][1]) atomicAdd(B.pair_slots, s_count[w][1]);
     if (s_count[w][2]) atomicAdd(B.pair_slots + 1, s_count[w][2]);
+    if (!BOUND && s_count[w][3]) atomicAdd(B.pair_slots + 6, s_count[w][3]);
+    if (!BOUND && s_count[w][4]) atomicAdd(B.pair_slots + 7, s_count[w][4]);
   }
 }
 
@@ -2236,6 +2264,68 @@ __global__ void k_seed_lower(SodConst K, SodBufs B) {
   if ((threadIdx.x & 31) == 0) atomicMax(&B.s_lmax[slot], __float_as_uint((float)(sf * 0.999)));
 }
 
+// The group with the largest finite upper bound of each bounded seed (warp
+// per seed).  Its candidates are the likeliest to hold the maximum, so their
+// sums, computed before all others, give a lower bound close to it.
+__global__ void k_top_group(SodConst K, SodBufs B) {
+  const unsigned slot = (unsigned)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (slot >= min(*B.nready, B.cap_ready)) return;
+  float bu = -1.f;
+  unsigned best = 0xffffffffu;
+  if (B.bound_on && B.st_cn[slot] >= BOUND_MIN_CAND) {
+    const unsigned g0 = B.group_pref[slot * 27u], g1 = B.group_pref[slot * 27u + 27u];
+    for (unsigned gi = g0 + (unsigned)lane; gi < g1; gi += 32u) {
+      const float u = B.g_u[gi];
+      if (u <= 3e38f && u > bu) {  // an infinite bound (item near the periodic edge) says nothing
+        bu = u;
+        best = gi;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const float ou = __shfl_xor_sync(0xffffffffu, bu, o);
+    const unsigned og = __shfl_xor_sync(0xffffffffu, best, o);
+    if (ou > bu || (ou == bu && og < best)) {
+      bu = ou;
+      best = og;
+    }
+  }
+  if (lane != 0) return;
+  B.s_top[slot] = best;
+  unsigned n = 0;
+  if (best != 0xffffffffu) {
+    unsigned ci = slot * 27u;  // the candidate cell holding the group: last ci with group_pref[ci] <= best
+    while (ci + 1 < slot * 27u + 27u && B.group_pref[ci + 1] <= best) ci++;
+    n = B.cell_nch[ci];
+    B.top_ci[slot] = ci;
+    B.top_rem0[slot] = (best - B.group_pref[ci]) * n;
+  }
+  B.top_n[slot] = n;
+}
+
+// Lower bound from the top group's sums (warp per seed): every candidate's
+// sum is at most the maximum, and the approximate sums are within 2e-6 of
+// the exact ones, so max * (1 - 1e-5) is a lower bound of the maximum.
+// Candidates that always go to the exact pass (infinite entries) are skipped.
+__global__ void k_top_lower(SodConst K, SodBufs B) {
+  const unsigned slot = (unsigned)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (slot >= min(*B.nready, B.cap_ready)) return;
+  const unsigned top = B.s_top[slot];
+  if (top == 0xffffffffu) return;
+  unsigned ci = slot * 27u;  // the candidate cell holding the group: last ci with group_pref[ci] <= top
+  while (ci + 1 < slot * 27u + 27u && B.group_pref[ci + 1] <= top) ci++;
+  const unsigned chunk = top - B.group_pref[ci], cnt = B.cell_cnt[ci];
+  double m = 0.0;
+  for (unsigned k = chunk * 64u + (unsigned)lane; k < min(cnt, chunk * 64u + 64u); k += 32u) {
+    const double v = B.cand_s[B.cell_off[ci] + k];
+    if (v < 1e300 && v > m) m = v;
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0 && m > 0.0) atomicMax(&B.s_lmax[slot], __float_as_uint((float)(m * (1.0 - 1e-5))));
+}
+
 // zero the per-group bound arrays of this round (group count on the device)
 __global__ void k_zero_groups(const unsigned *total, float *u, float *l, unsigned *done) {
   const unsigned n = *total;
@@ -2294,9 +2384,6 @@ __global__ void k_init_active(long long nblocks, const unsigned *bbegin, unsigne
   if (bbegin[b + 1] > bbegin[b]) active[atomicAdd(nactive, 1u)] = (unsigned)b;
 }
 
-// Warp per active block: advance the cursor past resolved (processed or
-// claimed) seeds, 256 entries per step with independent loads; head = the
-// lowest unresolved rank.  Blocks that still hold seeds go to next_active.
 // first index in [cur, end) whose resolved bit is clear, or end
 __device__ __forceinline__ unsigned first_unresolved(const unsigned *res, unsigned cur, unsigned end) {
   while (cur < end) {
@@ -2308,8 +2395,10 @@ __device__ __forceinline__ unsigned first_unresolved(const unsigned *res, unsign
   return end;
 }
 
-// One lane per active block: the head is the block's first unresolved seed
-// at or after its cursor, found in the resolved bitmap (32 seeds a word).
+// One lane per active block: the head is the block's first unresolved
+// (neither processed nor claimed) seed at or after its cursor, found in the
+// resolved bitmap (32 seeds a word).  Blocks that still hold seeds go to
+// next_active.
 __global__ void k_heads(const unsigned *active, unsigned nactive, const unsigned *bbegin, unsigned *cursor,
                         const unsigned *blist, const unsigned *resolved, unsigned *head, unsigned *gmin,
                         unsigned *next_active, unsigned *n_next) {
@@ -2593,7 +2682,7 @@ enum {
   SC_ST_CENTRE, SC_CAND_POS, SC_CAND_SLOT, SC_CAND_S, SC_ORDER, SC_RKEYS, SC_MASS32, SC_MOFF, SC_TKEY, SC_TIDX,
   SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS, SC_CELLNCH, SC_FEAT, SC_RB0,
   SC_SBEST, SC_CELLGROUPS, SC_GROUPPREF, SC_GU, SC_GL, SC_GDONE, SC_LMAX, SC_BIG, SC_RESOLVED, SC_BIDXRANK,
-  SC_BIDXCUBE
+  SC_BIDXCUBE, SC_TOPG
 };
 
 struct PhaseTimer {
@@ -2702,6 +2791,8 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       (rc = scratch(c, SC_GU, gcap, &g_u)) || (rc = scratch(c, SC_GL, gcap, &g_l)) ||
       (rc = scratch(c, SC_GDONE, gcap, &g_done)) || (rc = scratch(c, SC_LMAX, (size_t)cap_ready, &s_lmax)))
     return rc;
+  unsigned *s_top;
+  if ((rc = scratch(c, SC_TOPG, (size_t)cap_ready * 5 + 1, &s_top))) return rc;
   unsigned *st_big;
   if ((rc = scratch(c, SC_BIG, (size_t)cap_ready, &st_big))) return rc;
   unsigned *resolved, *bidx_of_rank, *bidx_of_cube;
@@ -2835,6 +2926,13 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.g_done = g_done;
   B.s_lmax = s_lmax;
   B.work_bound = ctrs + 10;
+  B.work_top = ctrs + 11;
+  B.s_top = s_top;
+  B.top_ci = s_top + cap_ready;
+  B.top_rem0 = s_top + 2 * (size_t)cap_ready;
+  B.top_n = s_top + 3 * (size_t)cap_ready;
+  B.top_pref = s_top + 4 * (size_t)cap_ready;
+  B.ref_phase = 0;
   B.bound_on = 1;
   // small balls take the warp-per-seed crossing; the CTA kernel the rest
   B.st_big = (c->p.mode != PSOD_MODE_PLAIN) ? st_big : nullptr;
@@ -2875,7 +2973,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   while (nseed > 0 && n_active > 0) {
     t_sched.start(c->stream);
     PSOD_CUDA(c, cudaMemsetAsync(ctrs, 0, sizeof(unsigned) * 5, c->stream));  // nready, work[4]
-    PSOD_CUDA(c, cudaMemsetAsync(ctrs + 10, 0, sizeof(unsigned), c->stream));  // bound pass work
+    PSOD_CUDA(c, cudaMemsetAsync(ctrs + 10, 0, sizeof(unsigned) * 2, c->stream));  // bound and top-group pass work
     PSOD_CUDA(c, cudaMemsetAsync(gmin, 0xff, sizeof(unsigned), c->stream));
     PSOD_CUDA(c, cudaMemsetAsync(cand_used, 0, sizeof(unsigned), c->stream));
     PSOD_CUDA(c, cudaMemsetAsync(ctrs + 9, 0, sizeof(unsigned), c->stream));
@@ -2912,10 +3010,20 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       PSOD_CUDA(c, cudaMemsetAsync(s_lmax, 0, sizeof(unsigned) * nready, c->stream));
       k_seed_lower<<<nblk((long long)nready * 32, 256), 256, 0, c->stream>>>(K, B);
       k_refine_warp<true><<<ref_grid, 256, 0, c->stream>>>(K, B);
+      k_top_group<<<nblk((long long)nready * 32, 256), 256, 0, c->stream>>>(K, B);
+      if ((rc = scan_u32(c, B.top_n, B.top_pref, (long long)nready, true))) return rc;
       t_bound.stop(c->stream);
-      kernels += 3;
+      // the top groups' sums first, then the lower bound they give, then
+      // every other item against it
+      SodBufs Bt = B;
+      Bt.ref_phase = 1;
+      k_refine_warp<false><<<ref_grid, 256, 0, c->stream>>>(K, Bt);
+      k_top_lower<<<nblk((long long)nready * 32, 256), 256, 0, c->stream>>>(K, B);
+      kernels += 6;
     }
-    k_refine_warp<false><<<ref_grid, 256, 0, c->stream>>>(K, B);
+    SodBufs Bp = B;
+    Bp.ref_phase = B.bound_on ? 2 : 0;
+    k_refine_warp<false><<<ref_grid, 256, 0, c->stream>>>(K, Bp);
     t_ref.stop(c->stream);
     t_sel.start(c->stream);
     k_select<<<g, TPB, smem, c->stream>>>(K, B);
@@ -2953,9 +3061,9 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       cudaMemcpy(tv, u64s, sizeof(tv), cudaMemcpyDeviceToHost);
       fprintf(stderr,
               "psod round %lld ready %u active %u cand %u sched %.3f prep %.3f refine %.3f select %.3f cross %.3f "
-              "pairs %llu slots %llu staged %llu\n",
+              "pairs %llu slots %llu staged %llu bound %.3f items %llu pruned %llu\n",
               rounds, nready, n_active, cu, t_sched.last, t_prep.last, t_ref.last, t_sel.last, t_cross.last, tv[5], tv[8],
-              tv[9]);
+              tv[9], B.bound_on ? t_bound.last : 0.0, tv[14], tv[15]);
     }
     rounds++;
     seed_launches += 4;
@@ -2984,6 +3092,8 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   st.cross_balls = (int64_t)hv[12];
   st.cross_records = (int64_t)hv[13];
   st.ms_refine_bound = t_bound.total;
+  st.refine_items = (int64_t)hv[14];
+  st.refine_pruned = (int64_t)hv[15];
   c->nhalo = 0;
   c->nmember = 0;
   c->sod_done = false;

@@ -155,22 +155,35 @@ __global__ void k_radix_hist(const K *keys, long long n, int shift, unsigned *hi
 // Stable scatter.  Warp w of a tile owns its keys [w*512, (w+1)*512) and
 // ranks them 32 at a time in input order (match_any on the digit, running
 // per-warp digit counters); one scan over the warps per digit then gives
-// each warp's start within the tile's digit run.  Two barriers per tile.
+// each warp's start within the tile's digit run, and a scan over the digits
+// each digit run's start within the tile.  The tile is first ordered by
+// digit in shared memory, then written out by consecutive threads, so each
+// digit run of the tile leaves as contiguous, coalesced stores (written
+// straight from the ranking, a warp's 32 stores would hit up to 32 runs).
 constexpr int RS_WARPS = RS_THREADS / 32;
 constexpr int RS_PER_LANE = RS_TILE / RS_THREADS;
+
+template <typename K>
+constexpr size_t rs_smem_bytes() {
+  return (size_t)RS_TILE * (sizeof(K) + sizeof(unsigned));
+}
 
 template <typename K>
 __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const K *keys, const unsigned *vals, K *okeys,
                                                               unsigned *ovals, long long n, int shift,
                                                               const unsigned *offsets, long long ntiles) {
+  extern __shared__ __align__(16) unsigned char rs_smem[];
+  K *sk = reinterpret_cast<K *>(rs_smem);                     // the tile's keys in digit order
+  unsigned *sv = reinterpret_cast<unsigned *>(sk + RS_TILE);  // and their values
   __shared__ unsigned s_cnt[RS_WARPS][RS_RADIX];
-  __shared__ unsigned s_base[RS_RADIX];
+  __shared__ unsigned s_base[RS_RADIX], s_loc[RS_RADIX];
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
 #pragma unroll
   for (int q = 0; q < RS_WARPS; q++) s_cnt[q][t] = 0;
   s_base[t] = offsets[(long long)t * ntiles + blockIdx.x];
   __syncthreads();
-  const long long base = (long long)blockIdx.x * RS_TILE + (long long)w * (32 * RS_PER_LANE);
+  const long long tile0 = (long long)blockIdx.x * RS_TILE;
+  const long long base = tile0 + (long long)w * (32 * RS_PER_LANE);
   const unsigned lt = (1u << lane) - 1u;
   K k[RS_PER_LANE];
   unsigned v[RS_PER_LANE], rk[RS_PER_LANE];
@@ -206,6 +219,8 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const K *keys, con
       s_cnt[q][t] = run;
       run += cnt;
     }
+    // run = the tile's count of digit t; its run starts at the exclusive sum
+    s_loc[t] = block_excl_scan(run, nullptr);
   }
   __syncthreads();
 #pragma unroll
@@ -213,10 +228,19 @@ __global__ void __launch_bounds__(RS_THREADS) k_radix_scatter(const K *keys, con
     const long long i = base + r * 32 + lane;
     if (i < n) {
       const unsigned d = (unsigned)(k[r] >> shift) & 0xffu;
-      const unsigned pos = s_base[d] + s_cnt[w][d] + rk[r];
-      okeys[pos] = k[r];
-      ovals[pos] = v[r];
+      const unsigned p = s_loc[d] + s_cnt[w][d] + rk[r];  // < RS_TILE
+      sk[p] = k[r];
+      sv[p] = v[r];
     }
+  }
+  __syncthreads();
+  const unsigned tile_n = (unsigned)min((long long)RS_TILE, n - tile0);
+  for (unsigned j = t; j < tile_n; j += RS_THREADS) {
+    const K key = sk[j];
+    const unsigned d = (unsigned)(key >> shift) & 0xffu;
+    const unsigned pos = s_base[d] + (j - s_loc[d]);
+    okeys[pos] = key;
+    ovals[pos] = sv[j];
   }
 }
 
@@ -263,6 +287,8 @@ int radix_sort_impl(psod_ctx *c, K *keys, unsigned *vals, long long n, int end_b
   if ((st = scratch(c, SLOT_SORT_KEYS, (size_t)n, &tk))) return st;
   if ((st = scratch(c, SLOT_SORT_VALS, (size_t)n, &tv))) return st;
   if ((st = scratch(c, SLOT_SORT_HIST, (size_t)ntiles * RS_RADIX + 1, &hist))) return st;
+  PSOD_CUDA(c, cudaFuncSetAttribute(k_radix_scatter<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)rs_smem_bytes<K>()));
   K *ka = keys, *kb = tk;
   unsigned *va = vals, *vb = tv;
   for (int dgt = 0; dgt < ndigits; dgt++) {
@@ -270,7 +296,8 @@ int radix_sort_impl(psod_ctx *c, K *keys, unsigned *vals, long long n, int end_b
     k_radix_hist<K><<<(unsigned)ntiles, RS_THREADS, 0, c->stream>>>(ka, n, shift, hist, ntiles);
     st = scan_u32(c, hist, hist, ntiles * RS_RADIX, false);
     if (st) break;
-    k_radix_scatter<K><<<(unsigned)ntiles, RS_THREADS, 0, c->stream>>>(ka, va, kb, vb, n, shift, hist, ntiles);
+    k_radix_scatter<K><<<(unsigned)ntiles, RS_THREADS, rs_smem_bytes<K>(), c->stream>>>(ka, va, kb, vb, n, shift,
+                                                                                       hist, ntiles);
     K *tkk = ka;
     ka = kb;
     kb = tkk;
