@@ -172,9 +172,26 @@ __device__ __forceinline__ int wrapi(int a, int nx) {
 // Visit every particle record filed under the cells of the cube of
 // half-width R around (ic,jc,kc): warp per row of cells, lanes stride along
 // the row's contiguous run of records.
+// The records [b, e) of one run, lanes on consecutive records, each lane in
+// increasing order.  Four loads per lane are issued before the first record
+// is used: a CTA that walks a large region alone is bound by the loads it
+// keeps in flight.
+template <typename F>
+__device__ __forceinline__ void run_records(const SodBufs &B, unsigned b, unsigned e, F &f) {
+  unsigned p = b + (threadIdx.x & 31u);
+  for (; p + 96u < e; p += 128u) {
+    const float4 v0 = B.cube[p], v1 = B.cube[p + 32u], v2 = B.cube[p + 64u], v3 = B.cube[p + 96u];
+    f(p, v0);
+    f(p + 32u, v1);
+    f(p + 64u, v2);
+    f(p + 96u, v3);
+  }
+  for (; p < e; p += 32u) f(p, B.cube[p]);
+}
+
 template <typename F>
 __device__ __forceinline__ void for_cube(const SodConst &K, const SodBufs &B, int ic, int jc, int kc, int R, F f) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int w = threadIdx.x >> 5;
   const int side = 2 * R + 1;
   const int nrow = side * side;
   const unsigned nx = (unsigned)K.nx;
@@ -191,11 +208,7 @@ __device__ __forceinline__ void for_cube(const SodConst &K, const SodBufs &B, in
     } else {
       pa[0] = x0; pb[0] = x1; np = 1;
     }
-    for (int q = 0; q < np; q++) {
-      const unsigned b = B.cs[base + (unsigned)pa[q]];
-      const unsigned e = B.cs[base + (unsigned)pb[q] + 1];
-      for (unsigned p = b + lane; p < e; p += 32) f(p, B.cube[p]);
-    }
+    for (int q = 0; q < np; q++) run_records(B, B.cs[base + (unsigned)pa[q]], B.cs[base + (unsigned)pb[q] + 1], f);
   }
 }
 
@@ -224,7 +237,7 @@ __device__ __forceinline__ void for_region(const SodConst &K, const SodBufs &B, 
     for_cube(K, B, G.ic, G.jc, G.kc, K.ncut, f);
     return;
   }
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int w = threadIdx.x >> 5;
   const int R = K.ncut, side = 2 * R + 1, nrow = side * side;
   const unsigned nx = (unsigned)K.nx;
   const double nxd = (double)K.nx;
@@ -260,11 +273,7 @@ __device__ __forceinline__ void for_region(const SodConst &K, const SodBufs &B, 
     } else {
       pa[0] = x0; pb[0] = x1; np = 1;
     }
-    for (int q = 0; q < np; q++) {
-      const unsigned b = B.cs[base + (unsigned)pa[q]];
-      const unsigned e = B.cs[base + (unsigned)pb[q] + 1];
-      for (unsigned p = b + lane; p < e; p += 32) f(p, B.cube[p]);
-    }
+    for (int q = 0; q < np; q++) run_records(B, B.cs[base + (unsigned)pa[q]], B.cs[base + (unsigned)pb[q] + 1], f);
   }
 }
 
@@ -1033,12 +1042,17 @@ __device__ void refine_sum(const SodConst &K, const SodBufs &B, unsigned cp, int
 // (dx,dy,dz) the term is rsqrt(d2e) with d2e = dx^2+dy^2+dz^2+eps^2 formed by
 // three FFMAs.  Each difference of two grid coordinates rounds at most once,
 // and d2e adds three roundings of positive quantities, so d2e is within
-// 3.6e-7 relative and the term, after rsqrtf, within 5e-7.  A pair is counted when d2e <= 1 + eps^2; the lane tracks how close
-// its pairs came to that edge and a tile with a pair within 1e-5 of it is
-// redone with the exact FP64 inclusion test.  Terms are summed in two FP32
+// 3.6e-7 relative and the term, after rsqrtf, within 5e-7.  A pair is
+// counted when d2e <= 1 + eps^2; near that edge d2e is within 3.6e-7 of the
+// exact value, so the FP32 decision is the exact one whenever |d2e - (1 +
+// eps^2)| >= EDGE_MARGIN (5.5 times that bound).  The lane tracks how close
+// its pairs came to the edge and a tile with a pair within EDGE_MARGIN of it
+// is redone with the exact FP64 inclusion test.  Terms are summed in two FP32
 // partials of at most 16 positive terms (relative error below 1e-6) and the
 // partials in FP64, so |S_approx - S| <= 2e-6 S < REF_TOL S.
 // (REF_TOL bounds the gap that sends a candidate to the exact pass.)
+constexpr float EDGE_MARGIN = 2e-6f;
+
 // reciprocal square root of a normal positive float (d2e >= eps^2 here), one
 // MUFU operation, relative error below 2^-22.9 (PTX rsqrt.approx)
 __device__ __forceinline__ float rsqrt_pos(float x) {
@@ -1107,7 +1121,7 @@ __device__ __forceinline__ double tile_terms(const float4 *tile, unsigned nt, fl
       pair_fast<WRAPFREE>(tile[j + u + 1], cx, cy, cz, e2f, limf, K.nxf, p1, edge);
     }
   }
-  if (edge < 1e-5f) return tile_terms_edge<WRAPFREE>(tile, nt, cx, cy, cz, e2f, K.nxf, K.tx, K.rmin2);
+  if (edge < EDGE_MARGIN) return tile_terms_edge<WRAPFREE>(tile, nt, cx, cy, cz, e2f, K.nxf, K.tx, K.rmin2);
   return (double)p0 + (double)p1;
 }
 
@@ -1127,8 +1141,8 @@ __device__ __forceinline__ void tile_terms2(const float4 *tile, unsigned nt, flo
       pair_fast<WRAPFREE>(r1, bx, by, bz, e2f, limf, K.nxf, b1, eb);
     }
   }
-  sa += ea < 1e-5f ? tile_terms_edge<WRAPFREE>(tile, nt, ax, ay, az, e2f, K.nxf, K.tx, K.rmin2) : (double)a0 + (double)a1;
-  sb += eb < 1e-5f ? tile_terms_edge<WRAPFREE>(tile, nt, bx, by, bz, e2f, K.nxf, K.tx, K.rmin2) : (double)b0 + (double)b1;
+  sa += ea < EDGE_MARGIN ? tile_terms_edge<WRAPFREE>(tile, nt, ax, ay, az, e2f, K.nxf, K.tx, K.rmin2) : (double)a0 + (double)a1;
+  sb += eb < EDGE_MARGIN ? tile_terms_edge<WRAPFREE>(tile, nt, bx, by, bz, e2f, K.nxf, K.tx, K.rmin2) : (double)b0 + (double)b1;
 }
 
 // Work item: up to 64 candidates of one candidate cell (two per lane) against
@@ -1241,36 +1255,57 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
       by = to_grid(cv.y, K.nxf);
       bz = to_grid(cv.z, K.nxf);
     }
-    if (lane == 0) {
+    {
       // record runs of the 3x3x3 cells around the candidate cell: 9 rows of a
-      // 3-cell x-run each (two runs when it wraps)
-      int nr = 0;
-      unsigned acc = 0;
-      for (int r = 0; r < 9; r++) {
-        const unsigned yy = (unsigned)wrapi(cyc + r % 3 - 1, K.nx), zz = (unsigned)wrapi(czc + r / 3 - 1, K.nx);
+      // 3-cell x-run each (two runs when it wraps), lane r < 9 on row r; a
+      // warp scan of the run counts and lengths places them in row order
+      int np = 0;
+      unsigned b0 = 0, l0 = 0, b1 = 0, l1 = 0;
+      if (lane < 9) {
+        const unsigned yy = (unsigned)wrapi(cyc + lane % 3 - 1, K.nx), zz = (unsigned)wrapi(czc + lane / 3 - 1, K.nx);
         const unsigned long long base = (unsigned long long)K.nx * (yy + (unsigned long long)K.nx * zz);
         const int x0 = cxc - 1, x1 = cxc + 1;
-        int pa[2], pb[2], np;
-        if (x0 < 0) { pa[0] = x0 + K.nx; pb[0] = K.nx - 1; pa[1] = 0; pb[1] = x1; np = 2; }
-        else if (x1 >= K.nx) { pa[0] = x0; pb[0] = K.nx - 1; pa[1] = 0; pb[1] = x1 - K.nx; np = 2; }
-        else { pa[0] = x0; pb[0] = x1; np = 1; }
-        for (int h = 0; h < np; h++) {
-          const unsigned b = B.cs[base + (unsigned)pa[h]], e = B.cs[base + (unsigned)pb[h] + 1];
-          s_rb[w][nr] = b;
-          s_rp[w][nr] = acc;
-          acc += e - b;
-          nr++;
+        int pa0, pb0, pa1 = 0, pb1 = -1;
+        if (x0 < 0) { pa0 = x0 + K.nx; pb0 = K.nx - 1; pa1 = 0; pb1 = x1; np = 2; }
+        else if (x1 >= K.nx) { pa0 = x0; pb0 = K.nx - 1; pa1 = 0; pb1 = x1 - K.nx; np = 2; }
+        else { pa0 = x0; pb0 = x1; np = 1; }
+        b0 = B.cs[base + (unsigned)pa0];
+        l0 = B.cs[base + (unsigned)pb0 + 1] - b0;
+        if (np == 2) {
+          b1 = B.cs[base + (unsigned)pa1];
+          l1 = B.cs[base + (unsigned)pb1 + 1] - b1;
         }
       }
-      s_rp[w][nr] = acc;
-      s_nr[w] = nr;
-      // the 3-cell coordinate window of each axis stays clear of the box edge
-      auto clear = [&](int c) {
-        double s0 = (double)(c - 1) + K.xs;
-        s0 -= K.tx * floor(s0 / K.tx);
-        return s0 >= 1.0 && s0 + 3.0 <= K.tx - 1.0;
-      };
-      s_wf[w] = clear(cxc) && clear(cyc) && clear(czc);
+      unsigned pc = (unsigned)np, len = l0 + l1;
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned tp = __shfl_up_sync(0xffffffffu, pc, o), tl = __shfl_up_sync(0xffffffffu, len, o);
+        if (lane >= o) {
+          pc += tp;
+          len += tl;
+        }
+      }
+      if (lane < 9) {
+        const unsigned pf = pc - (unsigned)np, lf = len - (l0 + l1);
+        s_rb[w][pf] = b0;
+        s_rp[w][pf] = lf;
+        if (np == 2) {
+          s_rb[w][pf + 1] = b1;
+          s_rp[w][pf + 1] = lf + l0;
+        }
+      }
+      if (lane == 8) {
+        s_rp[w][pc] = len;
+        s_nr[w] = (int)pc;
+      }
+      if (lane == 0) {
+        // the 3-cell coordinate window of each axis stays clear of the box edge
+        auto clear = [&](int c) {
+          double s0 = (double)(c - 1) + K.xs;
+          s0 -= K.tx * floor(s0 / K.tx);
+          return s0 >= 1.0 && s0 + 3.0 <= K.tx - 1.0;
+        };
+        s_wf[w] = clear(cxc) && clear(cyc) && clear(czc);
+      }
     }
     __syncwarp();
     const int nr = s_nr[w];
