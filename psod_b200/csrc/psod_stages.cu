@@ -247,7 +247,7 @@ __global__ void k_cic_interp(const float4 *cube, long long n, CicConst k, const 
 constexpr int CT = 8;                 // SOD cells per tile side
 constexpr int CW = 2 * (CT + 2) + 1;  // window nodes per side
 constexpr int CW3 = CW * CW * CW;
-constexpr unsigned DEP_RUN = 8;      // consecutive particles deposited per thread
+constexpr unsigned DEP_BATCH = 4;    // record loads in flight per thread in the deposit
 
 constexpr int CRNG = 2 * (CT + 2) * (CT + 2);  // record ranges of a tile plus halo (two where x wraps)
 
@@ -311,13 +311,25 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
   range_prefix(s_len, s_pre, CRNG);
   __syncthreads();
   {
-    // Each thread deposits runs of DEP_RUN consecutive particles.  Dense
-    // cells are sub-cell ordered, so consecutive particles mostly share a
-    // fine cell and its 8 nodes: their fixed-point weights are summed in
-    // registers and written with one atomic per node when the fine cell
-    // changes (integer sums, so the grid is the same).
+    // Each thread deposits one contiguous share of the tile's particles
+    // (all threads busy, whatever the tile's count).  Dense cells are
+    // sub-cell ordered, so consecutive particles mostly share a fine cell
+    // and its 8 nodes: their fixed-point weights are summed in registers and
+    // written with one atomic per node when the fine cell changes (integer
+    // sums, so the grid is the same).  Records are loaded DEP_BATCH at a
+    // time before any is used.
     const unsigned total = s_pre[CRNG];
-    int r = 0;
+    const unsigned per = (total + blockDim.x - 1) / blockDim.x;
+    const unsigned f0 = min(total, threadIdx.x * per), f1 = min(total, f0 + per);
+    int r = 0;  // last range with s_pre[r] <= f0
+    {
+      int hi = CRNG;
+      while (hi - r > 1) {
+        const int mid = (r + hi) >> 1;
+        if (s_pre[mid] <= f0) r = mid;
+        else hi = mid;
+      }
+    }
     unsigned long long acc[8];
     int kx = -1, ky = -1, kz = -1;  // fine cell of the accumulated run
     int ncx[2], ncy[2], ncz[2];     // its nodes' window offsets
@@ -331,11 +343,20 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
       }
       kx = -1;
     };
-    for (unsigned f0 = threadIdx.x * DEP_RUN; f0 < total; f0 += blockDim.x * DEP_RUN) {
-      const unsigned f1 = min(total, f0 + DEP_RUN);
-      for (unsigned f = f0; f < f1; f++) {
-        while (s_pre[r + 1] <= f) r++;
-        const float4 v = cube[s_rb[r] + (f - s_pre[r])];
+    for (unsigned fb = f0; fb < f1; fb += DEP_BATCH) {
+      float4 vb[DEP_BATCH];
+#pragma unroll
+      for (unsigned u = 0; u < DEP_BATCH; u++) {
+        const unsigned f = fb + u;
+        if (f < f1) {
+          while (s_pre[r + 1] <= f) r++;
+          vb[u] = cube[s_rb[r] + (f - s_pre[r])];
+        }
+      }
+#pragma unroll
+      for (unsigned u = 0; u < DEP_BATCH; u++) {
+        if (fb + u >= f1) break;
+        const float4 v = vb[u];
         int ix, ixp, iy, iyp, iz, izp;
         double ddx, dex, ddy, dey, ddz, dez;
         cic_axis(v.x, k, ix, ixp, ddx, dex);
@@ -369,8 +390,8 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
           acc[c] += (unsigned long long)__double2ll_rn(dmul(wgt, FIX_ONE));
         }
       }
-      flush();
     }
+    flush();
   }
   __syncthreads();
   // own particles: rho in the reference's term order (main:1368-1383)
@@ -385,10 +406,7 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
   range_prefix(s_len, s_pre, CT * CT);
   __syncthreads();
   const unsigned total = s_pre[CT * CT];
-  int r = 0;
-  for (unsigned f = threadIdx.x; f < total; f += blockDim.x) {
-    while (s_pre[r + 1] <= f) r++;
-    const float4 v = cube[s_rb[r] + (f - s_pre[r])];
+  auto interp = [&](const float4 v) {
     const unsigned idx = __float_as_uint(v.w) & PSOD_IDX_MASK;
     int ix, ixp, iy, iyp, iz, izp;
     double ddx, dex, ddy, dey, ddz, dez;
@@ -412,6 +430,20 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
     }
     if (!ok) atomicOr(bad, 1);
     rho[idx] = rr;
+  };
+  // two records per thread and step, both loaded before either is used
+  int r = 0;
+  for (unsigned fa = threadIdx.x; fa < total; fa += 2 * blockDim.x) {
+    const unsigned fb = fa + blockDim.x;
+    while (s_pre[r + 1] <= fa) r++;
+    const float4 va = cube[s_rb[r] + (fa - s_pre[r])];
+    float4 vb = va;
+    if (fb < total) {
+      while (s_pre[r + 1] <= fb) r++;
+      vb = cube[s_rb[r] + (fb - s_pre[r])];
+    }
+    interp(va);
+    if (fb < total) interp(vb);
   }
 }
 
