@@ -134,8 +134,8 @@ typedef struct psod_run_stats {
   int64_t cross_balls;   /* ball passes of the crossing search */
   int64_t cross_records; /* alive records inside those balls, summed */
   double ms_refine_bound; /* refinement bound pass (part of ms_refine) */
-  int64_t refine_items;   /* refinement work items (64 candidates x one record chunk) */
-  int64_t refine_pruned;  /* of those, skipped because the group's bound is below the best lower bound */
+  int64_t refine_items;   /* refinement work items summed (64 candidates x one record chunk) */
+  int64_t refine_pruned;  /* refinement candidates not summed: their bound is below the best lower bound */
 } psod_run_stats;
 
 typedef struct psod_ctx psod_ctx;

@@ -106,8 +106,8 @@ struct SodBufs {
   // their prefix; per group upper bound U, lower bound L and finished
   // record chunks; per slot the best lower bound (float bits)
   unsigned *cell_groups, *group_pref;
-  float *g_u, *g_l;
-  unsigned *g_done, *s_lmax;
+  float *g_u;  // per 64-candidate group, eight sub-group bounds
+  unsigned *s_lmax;
   unsigned *work_bound;
   int bound_on;
   // per bounded seed the group with the largest upper bound (~0u: none),
@@ -118,6 +118,11 @@ struct SodBufs {
   // offset within the cell, item count, and the prefix sum of the counts
   unsigned *top_ci, *top_rem0, *top_n, *top_pref;
   int ref_phase;
+  // phase 2 runs over the surviving candidates only: per candidate cell
+  // their count and item count, the items' prefix sum, and the candidate
+  // positions (cell by cell, at the cell's candidate offset)
+  unsigned *cnt2, *chunks2, *chunk_pref2, *cand_list;
+  unsigned long long *cand_pruned;
   unsigned *st_big;  // 1: the crossing needs the CTA path (null: CTA for all)
   // scheduler: one bit per seed in block-list order, set once the seed is
   // processed or claimed; list position of each rank and of each cube slot
@@ -1151,20 +1156,28 @@ __device__ __forceinline__ void tile_terms2(const float4 *tile, unsigned nt, flo
 // reads each one by broadcast; warps never wait on one another.  Partial
 // sums of a candidate's neighbour chunks are added into cand_s.
 //
-// BOUND: the same items, but each record adds only to two bounds of its
-// 64-candidate group, from the candidates' box: U = sum of k(d to the box)
-// over records within reach (no candidate of the group can have a larger
-// S) and L = sum of k(d to the farthest corner) over records surely within
-// reach of every candidate (each candidate's S is at least that).  With k
-// decreasing, max_G L(G) <= S of the argmax, so a group with U(G) below it
-// cannot hold the argmax and the pair pass skips it; its sums stay 0, below
-// the select threshold.  U is inflated and L deflated by 1e-3, far above
-// the FP32 error of the sums.
+// BOUND: the same items, but each record adds only to upper bounds of the
+// group's eight sub-groups of 8 candidates (in the cell's candidate order,
+// Morton-compact in dense cells): U(s) = sum over records within reach of
+// k(d to the sub-group's box) for records near the group's box and k(d to
+// the group's box) for the others, so no candidate of s can have a larger
+// S.  Near records are staged in tiles; lane l accumulates sub-group l/4
+// over the tile's records l%4, l%4+4, ...  U is inflated by 1e-3, far above
+// the FP32 error of the sums.  The second pair pass keeps only candidates whose sub-group
+// bound reaches the seed's lower bound; the others cannot hold the argmax
+// and their sums stay 0, below the select threshold.
 constexpr unsigned ITEM_GRAB = 1;  // refinement items claimed per counter update
 
 // Seeds with fewer candidates than this are neither bounded nor pruned: their
 // pair work is small and the bound pass would cost as much as it saves.
 constexpr unsigned BOUND_MIN_CAND = 4096;
+
+// Records nearer than sqrt(NEAR2) cells to a group's box bound its sub-groups
+// through their own boxes; farther ones through the group's box, where the
+// difference is small.  (Measured on NFW halos of 3e4-1e5 particles: the
+// pair work pruned falls from 71 % with every record on the sub-group boxes
+// to 68 % at 0.5 cells, while the sub-box tests fall to a fifth.)
+constexpr float NEAR2 = 0.25f;
 
 template <bool BOUND>
 __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
@@ -1174,12 +1187,14 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const bool phase1 = !BOUND && B.ref_phase == 1;
   const unsigned nready = min(*B.nready, B.cap_ready);
-  const unsigned nitems = phase1 ? B.top_pref[nready] : B.chunk_pref[B.nitems_cells];
+  const bool phase2 = !BOUND && B.ref_phase == 2;
+  const unsigned *cpref = phase2 ? B.chunk_pref2 : B.chunk_pref;
+  const unsigned nitems = phase1 ? B.top_pref[nready] : cpref[B.nitems_cells];
   // pair, slot and staged-record counts: per item in 32 bits, per warp in
   // shared memory (keeps 64-bit totals out of the registers)
-  // (pair pass: also items taken and items pruned by the bound)
-  __shared__ unsigned long long s_count[8][5];
-  if (lane < 5) s_count[w][lane] = 0;
+  // (pair pass: also items taken)
+  __shared__ unsigned long long s_count[8][4];
+  if (lane < 4) s_count[w][lane] = 0;
   // items are claimed ITEM_GRAB at a time (one counter update per group of
   // consecutive items)
   unsigned grab = 0, grab_left = 0;
@@ -1202,14 +1217,14 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
         ci = B.top_ci[lo];
         rem = B.top_rem0[lo] + (item - B.top_pref[lo]);
       } else if (item < nitems) {
-        unsigned lo = 0, hi = B.nitems_cells;  // last ci with chunk_pref[ci] <= item
+        unsigned lo = 0, hi = B.nitems_cells;  // last ci with cpref[ci] <= item
         while (hi - lo > 1) {
           const unsigned mid = (lo + hi) >> 1;
-          if (B.chunk_pref[mid] <= item) lo = mid;
+          if (cpref[mid] <= item) lo = mid;
           else hi = mid;
         }
         ci = lo;
-        rem = item - B.chunk_pref[lo];
+        rem = item - cpref[lo];
       }
     }
     item = __shfl_sync(0xffffffffu, item, 0);
@@ -1222,23 +1237,20 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
     const unsigned grp = B.group_pref[ci] + chunk;
     const bool bounded = B.bound_on && B.st_cn[slot] >= BOUND_MIN_CAND;
     if (BOUND && !bounded) continue;
-    if (!BOUND && B.ref_phase == 2 && bounded && grp == B.s_top[slot]) continue;  // done in phase 1
     if (!BOUND && lane == 0) s_count[w][3]++;
-    if (!BOUND && B.ref_phase != 1 && bounded &&
-        B.g_u[grp] < __uint_as_float(B.s_lmax[slot])) {  // cannot hold the argmax
-      if (lane == 0) s_count[w][4]++;
-      continue;
-    }
     const SeedGeo g = seed_geo(K, B, B.ready[slot]);
     const int di = (int)(o / 9) - 1, dj = (int)((o / 3) % 3) - 1, dk = (int)(o % 3) - 1;
     const int cxc = wrapi(g.ic + di, K.nx), cyc = wrapi(g.jc + dj, K.nx), czc = wrapi(g.kc + dk, K.nx);
-    const unsigned cnt = B.cell_cnt[ci];
-    // candidates k0 = 64*chunk + lane and k1 = k0 + 32 of the cell; items of
-    // at most 32 candidates run one per lane
+    const unsigned cnt = phase2 ? B.cnt2[ci] : B.cell_cnt[ci];
+    // candidates k0 = 64*chunk + lane and k1 = k0 + 32 of the cell (phase 2:
+    // of its surviving candidates); items of at most 32 candidates run one
+    // per lane
     const unsigned k0 = chunk * 64u + (unsigned)lane, k1 = k0 + 32u;
     const bool two = cnt > chunk * 64u + 32u;
     const bool have = k0 < cnt, have1 = k1 < cnt;
-    const unsigned q = B.cell_off[ci] + k0, q1 = q + 32u;
+    const unsigned coff = B.cell_off[ci];
+    const unsigned q = phase2 ? (have ? B.cand_list[coff + k0] : 0u) : coff + k0;
+    const unsigned q1 = phase2 ? (have1 ? B.cand_list[coff + k1] : 0u) : coff + k1;
     const unsigned cp = have ? B.cand_pos[q] : 0u, cp1 = have1 ? B.cand_pos[q1] : 0u;
     const bool quirk = have && K.has_quirk && cp == K.quirk_pos;
     const bool quirk1 = have1 && K.has_quirk && cp1 == K.quirk_pos;
@@ -1333,12 +1345,54 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
       hiz = fmaxf(hiz, __shfl_xor_sync(0xffffffffu, hiz, o));
     }
     const bool any_active = lox <= hix;
+    // BOUND: the box of sub-group lane/4 (candidates 8s..8s+7 of the group:
+    // first candidates of lanes 8s.. for s < 4, second candidates of lanes
+    // 8(s-4).. for s >= 4)
+    float slx = 3e38f, shx = -3e38f, sly = 3e38f, shy = -3e38f, slz = 3e38f, shz = -3e38f;
+    if (BOUND) {
+      float a[6] = {active ? cx : 3e38f, active ? cx : -3e38f, active ? cy : 3e38f,
+                    active ? cy : -3e38f, active ? cz : 3e38f, active ? cz : -3e38f};
+      float b[6] = {active1 ? bx : 3e38f, active1 ? bx : -3e38f, active1 ? by : 3e38f,
+                    active1 ? by : -3e38f, active1 ? bz : 3e38f, active1 ? bz : -3e38f};
+#pragma unroll
+      for (int o = 4; o > 0; o >>= 1)
+#pragma unroll
+        for (int c = 0; c < 6; c += 2) {
+          a[c] = fminf(a[c], __shfl_xor_sync(0xffffffffu, a[c], o));
+          a[c + 1] = fmaxf(a[c + 1], __shfl_xor_sync(0xffffffffu, a[c + 1], o));
+          b[c] = fminf(b[c], __shfl_xor_sync(0xffffffffu, b[c], o));
+          b[c + 1] = fmaxf(b[c + 1], __shfl_xor_sync(0xffffffffu, b[c + 1], o));
+        }
+      const int sg = lane >> 2, src = (sg & 3) << 3;
+      float m[6];
+#pragma unroll
+      for (int c = 0; c < 6; c++) {
+        const float va = __shfl_sync(0xffffffffu, a[c], src), vb = __shfl_sync(0xffffffffu, b[c], src);
+        m[c] = sg < 4 ? va : vb;
+      }
+      slx = m[0]; shx = m[1]; sly = m[2]; shy = m[3]; slz = m[4]; shz = m[5];
+    }
     const unsigned r0 = nchunk * RN_CHUNK, r1 = any_active ? min(total, r0 + RN_CHUNK) : r0;
     const unsigned lt = (1u << lane) - 1u;
     double sum = 0.0, sum1 = 0.0;
     unsigned visits = 0, slots = 0, loaded = 0;
     // tile of 32 kept records: the pair tests of every candidate lane
+    float ub = 0.f;  // BOUND: this lane's share of its sub-group's near-record bound
+    float uf = 0.f;  // BOUND: this lane's far records
+    const float e2b = (float)K.eps2;
     auto consume = [&](unsigned nt) {
+      if (BOUND) {
+        __syncwarp();
+        for (unsigned j = (unsigned)lane & 3u; j < nt; j += 4u) {
+          const float4 rec = s_tile[w][j];
+          const float ex = fmaxf(fmaxf(slx - rec.x, rec.x - shx), 0.f), ey = fmaxf(fmaxf(sly - rec.y, rec.y - shy), 0.f),
+                      ez = fmaxf(fmaxf(slz - rec.z, rec.z - shz), 0.f);
+          const float db2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+          if (db2 <= 1.0001f) ub += rsqrt_pos(db2 + e2b);
+        }
+        __syncwarp();
+        return;
+      }
       // pad to a multiple of 8 with records far from every candidate
       if ((unsigned)lane < ((8u - (nt & 7u)) & 7u)) s_tile[w][nt + lane] = make_float4(1e18f, 1e18f, 1e18f, 0.f);
       __syncwarp();
@@ -1362,10 +1416,10 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
     // 32 is consumed at once and the overflow moves to the front, so no
     // record is loaded twice.
     unsigned fill = 0;
-    float ub = (BOUND && !wf) ? __int_as_float(0x7f800000) : 0.f, lb = 0.f;  // bounds (BOUND)
-    const float e2b = (float)K.eps2;
     int r = 0;
     while (r + 1 < nr && s_rp[w][r + 1] <= r0) r++;
+    // (items near the periodic edge have no box filter: their bound is
+    // infinite and they are not staged by the bound pass)
     for (unsigned pos = (BOUND && !wf) ? r1 : r0; pos < r1; r++) {
       const unsigned run_end = min(s_rp[w][r + 1], r1);
       const unsigned base = s_rb[w][r] - s_rp[w][r];  // cube slot = base + record number
@@ -1381,21 +1435,20 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
             const float ex = fmaxf(fmaxf(lox - rec.x, rec.x - hix), 0.f), ey = fmaxf(fmaxf(loy - rec.y, rec.y - hiy), 0.f),
                         ez = fmaxf(fmaxf(loz - rec.z, rec.z - hiz), 0.f);
             const float db2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-            keep = keep && db2 <= 1.0001f;
-            if (BOUND && keep) {
-              ub += rsqrt_pos(db2 + e2b);
-              const float fx = fmaxf(rec.x - lox, hix - rec.x), fy = fmaxf(rec.y - loy, hiy - rec.y),
-                          fz = fmaxf(rec.z - loz, hiz - rec.z);
-              const float dm2 = fmaf(fx, fx, fmaf(fy, fy, fz * fz));
-              if (dm2 <= 0.9999f) lb += rsqrt_pos(dm2 + e2b);
+            if (BOUND) {
+              // far records add k(d to the group's box) to every sub-group
+              // here; near ones go to the tile for the sub-group boxes
+              if (keep && db2 >= NEAR2 && db2 <= 1.0001f) uf += rsqrt_pos(db2 + e2b);
+              keep = keep && db2 < NEAR2;
+            } else {
+              keep = keep && db2 <= 1.0001f;
             }
           }
         }
-        if (BOUND) continue;
         const unsigned m = __ballot_sync(0xffffffffu, keep);
         if (keep) s_tile[w][fill + __popc(m & lt)] = rec;  // fill < 32: index < 64
         fill += (unsigned)__popc(m);
-        loaded += min(32u, run_end - x0);
+        if (!BOUND) loaded += min(32u, run_end - x0);
         if (fill >= 32u) {
           consume(32u);
           if ((unsigned)lane < fill - 32u) s_tile[w][lane] = s_tile[w][32 + lane];
@@ -1406,22 +1459,17 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
       pos = run_end;
     }
     if (BOUND) {
-      for (int sh = 16; sh > 0; sh >>= 1) {
-        ub += __shfl_xor_sync(0xffffffffu, ub, sh);
-        lb += __shfl_xor_sync(0xffffffffu, lb, sh);
-      }
-      if (lane == 0 && any_active) {
+      if (fill > 0) consume(fill);
+      for (int sh = 16; sh > 0; sh >>= 1) uf += __shfl_xor_sync(0xffffffffu, uf, sh);
+      ub += __shfl_xor_sync(0xffffffffu, ub, 1);
+      ub += __shfl_xor_sync(0xffffffffu, ub, 2);
+      ub += uf;
+      if (!wf) ub = __int_as_float(0x7f800000);
+      if ((lane & 3) == 0 && any_active) {
         // the particle the run scan files under another cell may add up to
         // 1/eps = 64 to any candidate's sum outside these runs
-        atomicAdd(&B.g_u[grp], ub * 1.001f + ((K.has_quirk && nchunk == 0) ? 64.f : 0.f));
-        atomicAdd(&B.g_l[grp], lb * 0.999f);
-        __threadfence();
-        // the group's last record chunk publishes its lower bound
-        if (atomicAdd(&B.g_done[grp], 1u) == nch - 1) {
-          __threadfence();
-          const float L = atomicAdd(&B.g_l[grp], 0.f);
-          atomicMax(&B.s_lmax[slot], __float_as_uint(L));
-        }
+        atomicAdd(&B.g_u[grp * 8u + (unsigned)(lane >> 2)],
+                  ub * 1.001f + ((K.has_quirk && nchunk == 0) ? 64.f : 0.f));
       }
       continue;
     }
@@ -1461,7 +1509,6 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
     if (s_count[w][1]) atomicAdd(B.pair_slots, s_count[w][1]);
     if (s_count[w][2]) atomicAdd(B.pair_slots + 1, s_count[w][2]);
     if (!BOUND && s_count[w][3]) atomicAdd(B.pair_slots + 6, s_count[w][3]);
-    if (!BOUND && s_count[w][4]) atomicAdd(B.pair_slots + 7, s_count[w][4]);
   }
 }
 
@@ -2299,9 +2346,10 @@ __global__ void k_seed_lower(SodConst K, SodBufs B) {
   if ((threadIdx.x & 31) == 0) atomicMax(&B.s_lmax[slot], __float_as_uint((float)(sf * 0.999)));
 }
 
-// The group with the largest finite upper bound of each bounded seed (warp
-// per seed).  Its candidates are the likeliest to hold the maximum, so their
-// sums, computed before all others, give a lower bound close to it.
+// The group holding the sub-group with the largest finite upper bound, per
+// bounded seed (warp per seed).  Its candidates are the likeliest to hold
+// the maximum, so their sums, computed before all others, give a lower bound
+// close to it.  Also the group's item range for the phase-1 pass.
 __global__ void k_top_group(SodConst K, SodBufs B) {
   const unsigned slot = (unsigned)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
   const int lane = threadIdx.x & 31;
@@ -2309,12 +2357,12 @@ __global__ void k_top_group(SodConst K, SodBufs B) {
   float bu = -1.f;
   unsigned best = 0xffffffffu;
   if (B.bound_on && B.st_cn[slot] >= BOUND_MIN_CAND) {
-    const unsigned g0 = B.group_pref[slot * 27u], g1 = B.group_pref[slot * 27u + 27u];
-    for (unsigned gi = g0 + (unsigned)lane; gi < g1; gi += 32u) {
-      const float u = B.g_u[gi];
+    const unsigned g0 = B.group_pref[slot * 27u] * 8u, g1 = B.group_pref[slot * 27u + 27u] * 8u;
+    for (unsigned si = g0 + (unsigned)lane; si < g1; si += 32u) {
+      const float u = B.g_u[si];
       if (u <= 3e38f && u > bu) {  // an infinite bound (item near the periodic edge) says nothing
         bu = u;
-        best = gi;
+        best = si >> 3;
       }
     }
   }
@@ -2361,14 +2409,44 @@ __global__ void k_top_lower(SodConst K, SodBufs B) {
   if (lane == 0 && m > 0.0) atomicMax(&B.s_lmax[slot], __float_as_uint((float)(m * (1.0 - 1e-5))));
 }
 
-// zero the per-group bound arrays of this round (group count on the device)
-__global__ void k_zero_groups(const unsigned *total, float *u, float *l, unsigned *done) {
-  const unsigned n = *total;
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    u[i] = 0.f;
-    l[i] = 0.f;
-    done[i] = 0u;
+// The candidates the second pair pass must still sum (warp per candidate
+// cell, stable): all of an unbounded seed's; of a bounded seed's, those
+// outside the top group whose sub-group bound reaches the seed's lower
+// bound.  Their positions go to cand_list at the cell's candidate offset;
+// the cell's phase-2 item count follows from their number.
+__global__ void k_survivors(SodConst K, SodBufs B) {
+  const unsigned ci = (unsigned)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (ci >= B.nitems_cells) return;
+  const unsigned slot = ci / 27u, cnt = B.cell_cnt[ci], off = B.cell_off[ci], gp = B.group_pref[ci];
+  const bool bounded = B.bound_on && B.st_cn[slot] >= BOUND_MIN_CAND;
+  const float lmax = __uint_as_float(B.s_lmax[slot]);
+  const unsigned top = B.s_top[slot];
+  unsigned n2 = 0, gone = 0;
+  for (unsigned k0 = 0; k0 < cnt; k0 += 32u) {
+    const unsigned k = k0 + (unsigned)lane;
+    bool keep = k < cnt;
+    if (keep && bounded) {
+      const unsigned grp = gp + k / 64u;
+      keep = grp != top && B.g_u[grp * 8u + (k % 64u) / 8u] >= lmax;
+      gone += (!keep && grp != top) ? 1u : 0u;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, keep);
+    if (keep) B.cand_list[off + n2 + __popc(m & ((1u << lane) - 1u))] = off + k;
+    n2 += (unsigned)__popc(m);
   }
+  for (int o = 16; o > 0; o >>= 1) gone += __shfl_xor_sync(0xffffffffu, gone, o);
+  if (lane == 0) {
+    B.cnt2[ci] = n2;
+    B.chunks2[ci] = (n2 + 63u) / 64u * B.cell_nch[ci];
+    if (gone) atomicAdd(B.cand_pruned, (unsigned long long)gone);
+  }
+}
+
+// zero the per-sub-group bounds of this round (group count on the device)
+__global__ void k_zero_groups(const unsigned *total, float *u) {
+  const unsigned n = *total * 8u;
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) u[i] = 0.f;
 }
 
 __global__ void k_clear_dead(float4 *cube, long long n) {
@@ -2716,7 +2794,7 @@ enum {
   SC_HRDELTA, SC_HPOOL, SC_COUNTS, SC_ST_ACTIVE, SC_ST_NA, SC_ST_COFF, SC_ST_CN,
   SC_ST_CENTRE, SC_CAND_POS, SC_CAND_SLOT, SC_CAND_S, SC_ORDER, SC_RKEYS, SC_MASS32, SC_MOFF, SC_TKEY, SC_TIDX,
   SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS, SC_CELLNCH, SC_FEAT, SC_RB0,
-  SC_SBEST, SC_CELLGROUPS, SC_GROUPPREF, SC_GU, SC_GL, SC_GDONE, SC_LMAX, SC_BIG, SC_RESOLVED, SC_BIDXRANK,
+  SC_SBEST, SC_CELLGROUPS, SC_GROUPPREF, SC_GU, SC_CANDLIST, SC_CNT2, SC_LMAX, SC_BIG, SC_RESOLVED, SC_BIDXRANK,
   SC_BIDXCUBE, SC_TOPG
 };
 
@@ -2819,12 +2897,13 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   if ((rc = scratch(c, SC_CELLNCH, (size_t)cap_ready * 27, &cell_nch))) return rc;
   // refinement bound groups: at most cand_cap/64 + 27 per ready seed
   const size_t gcap = (size_t)cand_cap / 64 + (size_t)cap_ready * 27 + 1;
-  unsigned *cell_groups, *group_pref, *g_done, *s_lmax;
-  float *g_u, *g_l;
+  unsigned *cell_groups, *group_pref, *s_lmax, *cand_list, *cnt2;
+  float *g_u;
   if ((rc = scratch(c, SC_CELLGROUPS, (size_t)cap_ready * 27, &cell_groups)) ||
       (rc = scratch(c, SC_GROUPPREF, (size_t)cap_ready * 27 + 1, &group_pref)) ||
-      (rc = scratch(c, SC_GU, gcap, &g_u)) || (rc = scratch(c, SC_GL, gcap, &g_l)) ||
-      (rc = scratch(c, SC_GDONE, gcap, &g_done)) || (rc = scratch(c, SC_LMAX, (size_t)cap_ready, &s_lmax)))
+      (rc = scratch(c, SC_GU, gcap * 8, &g_u)) || (rc = scratch(c, SC_CANDLIST, (size_t)cand_cap, &cand_list)) ||
+      (rc = scratch(c, SC_CNT2, (size_t)cap_ready * 27 * 3 + 1, &cnt2)) ||
+      (rc = scratch(c, SC_LMAX, (size_t)cap_ready, &s_lmax)))
     return rc;
   unsigned *s_top;
   if ((rc = scratch(c, SC_TOPG, (size_t)cap_ready * 5 + 1, &s_top))) return rc;
@@ -2957,9 +3036,12 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.cell_groups = cell_groups;
   B.group_pref = group_pref;
   B.g_u = g_u;
-  B.g_l = g_l;
-  B.g_done = g_done;
   B.s_lmax = s_lmax;
+  B.cand_list = cand_list;
+  B.cnt2 = cnt2;
+  B.chunks2 = cnt2 + (size_t)cap_ready * 27;
+  B.chunk_pref2 = cnt2 + (size_t)cap_ready * 54;
+  B.cand_pruned = u64s + 15;
   B.work_bound = ctrs + 10;
   B.work_top = ctrs + 11;
   B.s_top = s_top;
@@ -3041,7 +3123,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     if ((rc = scan_u32(c, cell_groups, group_pref, (long long)B.nitems_cells, true))) return rc;
     if (B.bound_on) {
       t_bound.start(c->stream);
-      k_zero_groups<<<ref_grid, 256, 0, c->stream>>>(group_pref + B.nitems_cells, g_u, g_l, g_done);
+      k_zero_groups<<<ref_grid, 256, 0, c->stream>>>(group_pref + B.nitems_cells, g_u);
       PSOD_CUDA(c, cudaMemsetAsync(s_lmax, 0, sizeof(unsigned) * nready, c->stream));
       k_seed_lower<<<nblk((long long)nready * 32, 256), 256, 0, c->stream>>>(K, B);
       k_refine_warp<true><<<ref_grid, 256, 0, c->stream>>>(K, B);
@@ -3049,12 +3131,14 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       if ((rc = scan_u32(c, B.top_n, B.top_pref, (long long)nready, true))) return rc;
       t_bound.stop(c->stream);
       // the top groups' sums first, then the lower bound they give, then
-      // every other item against it
+      // the surviving candidates of every cell
       SodBufs Bt = B;
       Bt.ref_phase = 1;
       k_refine_warp<false><<<ref_grid, 256, 0, c->stream>>>(K, Bt);
       k_top_lower<<<nblk((long long)nready * 32, 256), 256, 0, c->stream>>>(K, B);
-      kernels += 6;
+      k_survivors<<<nblk((long long)B.nitems_cells * 32, 256), 256, 0, c->stream>>>(K, B);
+      if ((rc = scan_u32(c, B.chunks2, B.chunk_pref2, (long long)B.nitems_cells, true))) return rc;
+      kernels += 7;
     }
     SodBufs Bp = B;
     Bp.ref_phase = B.bound_on ? 2 : 0;
@@ -3096,7 +3180,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       cudaMemcpy(tv, u64s, sizeof(tv), cudaMemcpyDeviceToHost);
       fprintf(stderr,
               "psod round %lld ready %u active %u cand %u sched %.3f prep %.3f refine %.3f select %.3f cross %.3f "
-              "pairs %llu slots %llu staged %llu bound %.3f items %llu pruned %llu\n",
+              "pairs %llu slots %llu staged %llu bound %.3f items %llu pruned_cand %llu\n",
               rounds, nready, n_active, cu, t_sched.last, t_prep.last, t_ref.last, t_sel.last, t_cross.last, tv[5], tv[8],
               tv[9], B.bound_on ? t_bound.last : 0.0, tv[14], tv[15]);
     }
