@@ -1423,37 +1423,53 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
     for (unsigned pos = (BOUND && !wf) ? r1 : r0; pos < r1; r++) {
       const unsigned run_end = min(s_rp[w][r + 1], r1);
       const unsigned base = s_rb[w][r] - s_rp[w][r];  // cube slot = base + record number
-      for (unsigned x0 = pos; x0 < run_end; x0 += 32u) {
-        const unsigned x = x0 + (unsigned)lane;
-        bool keep = false;
-        float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (x < run_end) {
-          const float4 v = B.cube[base + x];
-          rec = make_float4(to_grid(v.x, K.nxf), to_grid(v.y, K.nxf), to_grid(v.z, K.nxf), 0.f);
-          keep = !(__float_as_uint(v.w) & PSOD_DEAD_BIT);
-          if (wf) {
-            const float ex = fmaxf(fmaxf(lox - rec.x, rec.x - hix), 0.f), ey = fmaxf(fmaxf(loy - rec.y, rec.y - hiy), 0.f),
-                        ez = fmaxf(fmaxf(loz - rec.z, rec.z - hiz), 0.f);
-            const float db2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-            if (BOUND) {
-              // far records add k(d to the group's box) to every sub-group
-              // here; near ones go to the tile for the sub-group boxes
-              if (keep && db2 >= NEAR2 && db2 <= 1.0001f) uf += rsqrt_pos(db2 + e2b);
-              keep = keep && db2 < NEAR2;
-            } else {
-              keep = keep && db2 <= 1.0001f;
+      // SD steps of 32 records per pass: each lane issues its SD loads
+      // before the first is used.  The bound pass has little arithmetic to
+      // hide their latency behind; the pair pass is bound by instruction
+      // issue and runs best with one (measured at 1024^3).
+      constexpr int SD = BOUND ? 4 : 1;
+      for (unsigned xs0 = pos; xs0 < run_end; xs0 += 32u * SD) {
+        float4 vs[SD];
+#pragma unroll
+        for (int u = 0; u < SD; u++) {
+          const unsigned x = xs0 + 32u * (unsigned)u + (unsigned)lane;
+          vs[u] = x < run_end ? B.cube[base + x] : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+#pragma unroll
+        for (int u = 0; u < SD; u++) {
+          const unsigned x0 = xs0 + 32u * (unsigned)u;
+          if (x0 >= run_end) break;  // warp-uniform
+          const unsigned x = x0 + (unsigned)lane;
+          bool keep = false;
+          float4 rec = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (x < run_end) {
+            const float4 v = vs[u];
+            rec = make_float4(to_grid(v.x, K.nxf), to_grid(v.y, K.nxf), to_grid(v.z, K.nxf), 0.f);
+            keep = !(__float_as_uint(v.w) & PSOD_DEAD_BIT);
+            if (wf) {
+              const float ex = fmaxf(fmaxf(lox - rec.x, rec.x - hix), 0.f), ey = fmaxf(fmaxf(loy - rec.y, rec.y - hiy), 0.f),
+                          ez = fmaxf(fmaxf(loz - rec.z, rec.z - hiz), 0.f);
+              const float db2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+              if (BOUND) {
+                // far records add k(d to the group's box) to every sub-group
+                // here; near ones go to the tile for the sub-group boxes
+                if (keep && db2 >= NEAR2 && db2 <= 1.0001f) uf += rsqrt_pos(db2 + e2b);
+                keep = keep && db2 < NEAR2;
+              } else {
+                keep = keep && db2 <= 1.0001f;
+              }
             }
           }
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, keep);
-        if (keep) s_tile[w][fill + __popc(m & lt)] = rec;  // fill < 32: index < 64
-        fill += (unsigned)__popc(m);
-        if (!BOUND) loaded += min(32u, run_end - x0);
-        if (fill >= 32u) {
-          consume(32u);
-          if ((unsigned)lane < fill - 32u) s_tile[w][lane] = s_tile[w][32 + lane];
-          __syncwarp();
-          fill -= 32u;
+          const unsigned m = __ballot_sync(0xffffffffu, keep);
+          if (keep) s_tile[w][fill + __popc(m & lt)] = rec;  // fill < 32: index < 64
+          fill += (unsigned)__popc(m);
+          if (!BOUND) loaded += min(32u, run_end - x0);
+          if (fill >= 32u) {
+            consume(32u);
+            if ((unsigned)lane < fill - 32u) s_tile[w][lane] = s_tile[w][32 + lane];
+            __syncwarp();
+            fill -= 32u;
+          }
         }
       }
       pos = run_end;
