@@ -106,7 +106,7 @@ struct SodBufs {
   // their prefix; per group upper bound U, lower bound L and finished
   // record chunks; per slot the best lower bound (float bits)
   unsigned *cell_groups, *group_pref;
-  float *g_u;  // per 64-candidate group, eight sub-group bounds
+  float *g_u;  // per 64-candidate group, NSUB sub-group bounds
   unsigned *s_lmax;
   unsigned *work_bound;
   int bound_on;
@@ -1157,13 +1157,13 @@ __device__ __forceinline__ void tile_terms2(const float4 *tile, unsigned nt, flo
 // sums of a candidate's neighbour chunks are added into cand_s.
 //
 // BOUND: the same items, but each record adds only to upper bounds of the
-// group's eight sub-groups of 8 candidates (in the cell's candidate order,
-// Morton-compact in dense cells): U(s) = sum over records within reach of
-// k(d to the sub-group's box) for records near the group's box and k(d to
-// the group's box) for the others, so no candidate of s can have a larger
-// S.  Near records are staged in tiles; lane l accumulates sub-group l/4
-// over the tile's records l%4, l%4+4, ...  U is inflated by 1e-3, far above
-// the FP32 error of the sums.  The second pair pass keeps only candidates whose sub-group
+// group's sixteen sub-groups of 4 candidates (in the cell's candidate
+// order, Morton-compact in dense cells): U(s) = sum over records within
+// reach of k(d to the sub-group's box) for records near the group's box and
+// k(d to the group's box) for the others, so no candidate of s can have a
+// larger S.  Near records are staged in tiles; lane l accumulates sub-group
+// l/2 over the tile's records l%2, l%2+2, ...  U is inflated by 1e-3, far
+// above the FP32 error of the sums.  The second pair pass keeps only candidates whose sub-group
 // bound reaches the seed's lower bound; the others cannot hold the argmax
 // and their sums stay 0, below the select threshold.
 constexpr unsigned ITEM_GRAB = 1;  // refinement items claimed per counter update
@@ -1172,12 +1172,15 @@ constexpr unsigned ITEM_GRAB = 1;  // refinement items claimed per counter updat
 // pair work is small and the bound pass would cost as much as it saves.
 constexpr unsigned BOUND_MIN_CAND = 4096;
 
-// Records nearer than sqrt(NEAR2) cells to a group's box bound its sub-groups
-// through their own boxes; farther ones through the group's box, where the
-// difference is small.  (Measured on NFW halos of 3e4-1e5 particles: the
-// pair work pruned falls from 71 % with every record on the sub-group boxes
-// to 68 % at 0.5 cells, while the sub-box tests fall to a fifth.)
-constexpr float NEAR2 = 0.25f;
+// Sub-groups of SUBG candidates (16 per 64-candidate group, two lanes each).
+// Records nearer than sqrt(NEAR2) cells to a group's box bound its
+// sub-groups through their own boxes; farther ones through the group's box,
+// where the difference is small.  (Measured on an NFW halo of 3e4
+// particles, with the exact lower bound: the pair work pruned is 26 % with
+// group boxes only, 79 % with every record on boxes of 4 candidates, 74 %
+// with only records within 0.3 cells, which are a small fraction.)
+constexpr unsigned SUBG = 4, NSUB = 64 / SUBG;
+constexpr float NEAR2 = 0.09f;
 
 template <bool BOUND>
 __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
@@ -1345,9 +1348,9 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
       hiz = fmaxf(hiz, __shfl_xor_sync(0xffffffffu, hiz, o));
     }
     const bool any_active = lox <= hix;
-    // BOUND: the box of sub-group lane/4 (candidates 8s..8s+7 of the group:
-    // first candidates of lanes 8s.. for s < 4, second candidates of lanes
-    // 8(s-4).. for s >= 4)
+    // BOUND: the box of sub-group lane/2 (candidates 4s..4s+3 of the group:
+    // first candidates of lanes 4s.. for s < 8, second candidates of lanes
+    // 4(s-8).. for s >= 8)
     float slx = 3e38f, shx = -3e38f, sly = 3e38f, shy = -3e38f, slz = 3e38f, shz = -3e38f;
     if (BOUND) {
       float a[6] = {active ? cx : 3e38f, active ? cx : -3e38f, active ? cy : 3e38f,
@@ -1355,7 +1358,7 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
       float b[6] = {active1 ? bx : 3e38f, active1 ? bx : -3e38f, active1 ? by : 3e38f,
                     active1 ? by : -3e38f, active1 ? bz : 3e38f, active1 ? bz : -3e38f};
 #pragma unroll
-      for (int o = 4; o > 0; o >>= 1)
+      for (int o = 2; o > 0; o >>= 1)
 #pragma unroll
         for (int c = 0; c < 6; c += 2) {
           a[c] = fminf(a[c], __shfl_xor_sync(0xffffffffu, a[c], o));
@@ -1363,12 +1366,12 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
           b[c] = fminf(b[c], __shfl_xor_sync(0xffffffffu, b[c], o));
           b[c + 1] = fmaxf(b[c + 1], __shfl_xor_sync(0xffffffffu, b[c + 1], o));
         }
-      const int sg = lane >> 2, src = (sg & 3) << 3;
+      const int sg = lane >> 1, src = (sg & 7) << 2;
       float m[6];
 #pragma unroll
       for (int c = 0; c < 6; c++) {
         const float va = __shfl_sync(0xffffffffu, a[c], src), vb = __shfl_sync(0xffffffffu, b[c], src);
-        m[c] = sg < 4 ? va : vb;
+        m[c] = sg < 8 ? va : vb;
       }
       slx = m[0]; shx = m[1]; sly = m[2]; shy = m[3]; slz = m[4]; shz = m[5];
     }
@@ -1383,7 +1386,7 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
     auto consume = [&](unsigned nt) {
       if (BOUND) {
         __syncwarp();
-        for (unsigned j = (unsigned)lane & 3u; j < nt; j += 4u) {
+        for (unsigned j = (unsigned)lane & 1u; j < nt; j += 2u) {
           const float4 rec = s_tile[w][j];
           const float ex = fmaxf(fmaxf(slx - rec.x, rec.x - shx), 0.f), ey = fmaxf(fmaxf(sly - rec.y, rec.y - shy), 0.f),
                       ez = fmaxf(fmaxf(slz - rec.z, rec.z - shz), 0.f);
@@ -1478,13 +1481,12 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
       if (fill > 0) consume(fill);
       for (int sh = 16; sh > 0; sh >>= 1) uf += __shfl_xor_sync(0xffffffffu, uf, sh);
       ub += __shfl_xor_sync(0xffffffffu, ub, 1);
-      ub += __shfl_xor_sync(0xffffffffu, ub, 2);
       ub += uf;
       if (!wf) ub = __int_as_float(0x7f800000);
-      if ((lane & 3) == 0 && any_active) {
+      if ((lane & 1) == 0 && any_active) {
         // the particle the run scan files under another cell may add up to
         // 1/eps = 64 to any candidate's sum outside these runs
-        atomicAdd(&B.g_u[grp * 8u + (unsigned)(lane >> 2)],
+        atomicAdd(&B.g_u[grp * NSUB + (unsigned)(lane >> 1)],
                   ub * 1.001f + ((K.has_quirk && nchunk == 0) ? 64.f : 0.f));
       }
       continue;
@@ -2373,12 +2375,12 @@ __global__ void k_top_group(SodConst K, SodBufs B) {
   float bu = -1.f;
   unsigned best = 0xffffffffu;
   if (B.bound_on && B.st_cn[slot] >= BOUND_MIN_CAND) {
-    const unsigned g0 = B.group_pref[slot * 27u] * 8u, g1 = B.group_pref[slot * 27u + 27u] * 8u;
+    const unsigned g0 = B.group_pref[slot * 27u] * NSUB, g1 = B.group_pref[slot * 27u + 27u] * NSUB;
     for (unsigned si = g0 + (unsigned)lane; si < g1; si += 32u) {
       const float u = B.g_u[si];
       if (u <= 3e38f && u > bu) {  // an infinite bound (item near the periodic edge) says nothing
         bu = u;
-        best = si >> 3;
+        best = si / NSUB;
       }
     }
   }
@@ -2444,7 +2446,7 @@ __global__ void k_survivors(SodConst K, SodBufs B) {
     bool keep = k < cnt;
     if (keep && bounded) {
       const unsigned grp = gp + k / 64u;
-      keep = grp != top && B.g_u[grp * 8u + (k % 64u) / 8u] >= lmax;
+      keep = grp != top && B.g_u[grp * NSUB + (k % 64u) / SUBG] >= lmax;
       gone += (!keep && grp != top) ? 1u : 0u;
     }
     const unsigned m = __ballot_sync(0xffffffffu, keep);
@@ -2461,7 +2463,7 @@ __global__ void k_survivors(SodConst K, SodBufs B) {
 
 // zero the per-sub-group bounds of this round (group count on the device)
 __global__ void k_zero_groups(const unsigned *total, float *u) {
-  const unsigned n = *total * 8u;
+  const unsigned n = *total * NSUB;
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) u[i] = 0.f;
 }
 
@@ -2917,7 +2919,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   float *g_u;
   if ((rc = scratch(c, SC_CELLGROUPS, (size_t)cap_ready * 27, &cell_groups)) ||
       (rc = scratch(c, SC_GROUPPREF, (size_t)cap_ready * 27 + 1, &group_pref)) ||
-      (rc = scratch(c, SC_GU, gcap * 8, &g_u)) || (rc = scratch(c, SC_CANDLIST, (size_t)cand_cap, &cand_list)) ||
+      (rc = scratch(c, SC_GU, gcap * NSUB, &g_u)) || (rc = scratch(c, SC_CANDLIST, (size_t)cand_cap, &cand_list)) ||
       (rc = scratch(c, SC_CNT2, (size_t)cap_ready * 27 * 3 + 1, &cnt2)) ||
       (rc = scratch(c, SC_LMAX, (size_t)cap_ready, &s_lmax)))
     return rc;
