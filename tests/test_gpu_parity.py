@@ -161,6 +161,24 @@ def test_clustered_box_matches_oracle(oracle, nx, nmax, seed, mode):
     assert_same_halos(t, rr, exact_members_order=False)
 
 
+@pytest.mark.parametrize("mode", [0, 1])
+def test_pruned_refinement_matches_oracle(oracle, mode):
+    """A dense cluster: its seeds have far more than 4096 refinement
+    candidates, so the bound pass runs, most candidates are pruned, and the
+    centres, masses and member lists still equal the oracle's."""
+    from psod_b200 import synth
+
+    b = synth.make_box(48, nmax_halo=3000, n_clusters=1, cluster_size=20000, seed=404)
+    pos, ids = b.pos.numpy(), b.ids.numpy()
+    _, _, nn, st, t = gpu_run(48, pos, ids, delta_extra=(500.0, 178.0), mode=mode)
+    assert st["refine_pruned"] > 0
+    rc = oracle.run(oparams(oracle, 48, delta_extra=(500.0, 178.0)), pos, ids, oracle.CANONICAL)
+    assert rc.status == 0 and nn == rc.npart_new
+    assert_same_halos(t, rc)
+    assert np.array_equal(t.halo_profile, rc.halo_profile)
+    assert np.array_equal(t.halo_mextra, rc.halo_mextra)
+
+
 @pytest.mark.parametrize("mode", [1])
 def test_modes_identical_128(mode):
     """plain and batched schedules give bit-identical tables (1-rank 128^3 box)."""
