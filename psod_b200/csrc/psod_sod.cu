@@ -103,16 +103,16 @@ struct SodBufs {
   unsigned long long *learn_n, learn_cap;
   unsigned long long *bracket_hits, *bracket_seeds, *cross_balls, *cross_records;
   // refinement bounds: 64-candidate groups per (slot, candidate cell) and
-  // their prefix; per group upper bound U, lower bound L and finished
-  // record chunks; per slot the best lower bound (float bits)
+  // their prefix; per group the upper bounds U of its sub-groups; per slot
+  // the best lower bound of the maximum sum (float bits)
   unsigned *cell_groups, *group_pref;
   float *g_u;  // per 64-candidate group, NSUB sub-group bounds
   unsigned *s_lmax;
   unsigned *work_bound;
   int bound_on;
   // per bounded seed the group with the largest upper bound (~0u: none),
-  // whose sums run first; pair-pass phase: 0 all items, 1 only those
-  // groups, 2 all other items
+  // whose sums run first; pair-pass phase: 0 all items (no bounds), 1 the
+  // top groups, 2 the surviving candidates
   unsigned *s_top, *work_top;
   // phase-1 items: per seed the top group's candidate cell, first item
   // offset within the cell, item count, and the prefix sum of the counts
