@@ -69,10 +69,11 @@ __device__ __forceinline__ unsigned sub_key(const float *p, float nxf, double xs
 }
 
 // count[c] becomes BIG_FLAG | table index for cells of SUB_MIN or more
-// particles, else 0 (the fill counter of the scatter).  With assign false it
-// only counts them.
+// particles, else the cell's first slot start[c] (the fill cursor of the
+// scatter, so that one atomic gives the slot; start < n < 2^31 keeps the
+// flag bit clear).  With assign false it only counts them.
 __global__ void k_mark_big(unsigned *count, unsigned long long ncell, unsigned *nbig, bool assign,
-                           unsigned *bigcell) {
+                           unsigned *bigcell, const unsigned *start) {
   const unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   const bool big = c < ncell && count[c] >= SUB_MIN;
   const unsigned m = __ballot_sync(0xffffffffu, big);
@@ -86,7 +87,7 @@ __global__ void k_mark_big(unsigned *count, unsigned long long ncell, unsigned *
     bigcell[idx] = (unsigned)c;
     count[c] = BIG_FLAG | idx;
   } else {
-    count[c] = 0;
+    count[c] = start[c];
   }
 }
 
@@ -115,8 +116,8 @@ __global__ void k_sub_scan(unsigned *tab, const unsigned *bigcell, unsigned nbig
   t[2 * lane + 1] = excl + a0;
 }
 
-__global__ void k_cell_scatter(const float *pos, long long n, const unsigned *cell, const unsigned *start,
-                               unsigned *fill, unsigned *tab, float nxf, double xs, float4 *cube, unsigned *inv) {
+__global__ void k_cell_scatter(const float *pos, long long n, const unsigned *cell, unsigned *fill, unsigned *tab,
+                               float nxf, double xs, float4 *cube, unsigned *inv) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned c = i < n ? cell[i] : 0xffffffffu;
   const unsigned v = i < n ? fill[c] : 0u;  // the flag bit never changes under the atomics below
@@ -129,7 +130,7 @@ __global__ void k_cell_scatter(const float *pos, long long n, const unsigned *ce
   const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
   unsigned base = 0;
   if (i < n && lane == leader)
-    base = big ? atomicAdd(&tab[key & ~(1ull << 63)], __popc(peers)) : start[c] + atomicAdd(&fill[c], __popc(peers));
+    base = big ? atomicAdd(&tab[key & ~(1ull << 63)], __popc(peers)) : atomicAdd(&fill[c], __popc(peers));
   base = __shfl_sync(0xffffffffu, base, leader);
   if (i >= n) return;
   const unsigned slot = base + __popc(peers & ((1u << lane) - 1u));
@@ -526,7 +527,7 @@ int stage_cellsort(psod_ctx *c, const float *dpos) {
   if ((st = scan_u32(c, count, c->d_cell_start, (long long)c->ncell, true))) return st;
   unsigned *nbig = reinterpret_cast<unsigned *>(bad + 1);
   const long long ncell = (long long)c->ncell;
-  k_mark_big<<<nblk(ncell, 256), 256, 0, c->stream>>>(count, c->ncell, nbig, false, nullptr);
+  k_mark_big<<<nblk(ncell, 256), 256, 0, c->stream>>>(count, c->ncell, nbig, false, nullptr, nullptr);
   int hflags[2] = {0, 0};
   PSOD_CUDA(c, cudaMemcpyAsync(hflags, bad, sizeof(hflags), cudaMemcpyDeviceToHost, c->stream));
   PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -538,13 +539,13 @@ int stage_cellsort(psod_ctx *c, const float *dpos) {
     if ((st = scratch(c, SLOT_BIG_CELL, (size_t)hnbig + 1, &bigcell))) return st;
     PSOD_CUDA(c, cudaMemsetAsync(nbig, 0, sizeof(unsigned), c->stream));
     PSOD_CUDA(c, cudaMemsetAsync(tab, 0, sizeof(unsigned) * ((size_t)hnbig * SUB_N + 1), c->stream));
-    k_mark_big<<<nblk(ncell, 256), 256, 0, c->stream>>>(count, c->ncell, nbig, true, bigcell);
+    k_mark_big<<<nblk(ncell, 256), 256, 0, c->stream>>>(count, c->ncell, nbig, true, bigcell, c->d_cell_start);
     if (hnbig) {
       k_sub_count<<<nblk(n, 256), 256, 0, c->stream>>>(dpos, n, cell, count, (float)nx, xs, tab);
       k_sub_scan<<<nblk((long long)hnbig * 32, 256), 256, 0, c->stream>>>(tab, bigcell, hnbig, c->d_cell_start);
     }
-    k_cell_scatter<<<nblk(n, 256), 256, 0, c->stream>>>(dpos, n, cell, c->d_cell_start, count, tab, (float)nx, xs,
-                                                        c->d_cube, c->d_inv);
+    k_cell_scatter<<<nblk(n, 256), 256, 0, c->stream>>>(dpos, n, cell, count, tab, (float)nx, xs, c->d_cube,
+                                                        c->d_inv);
     PSOD_CUDA(c, cudaGetLastError());
     PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
   }
