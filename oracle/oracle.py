@@ -51,6 +51,7 @@ class _Result(C.Structure):
         ("fail_rank", C.c_int64),
         ("npart_new", C.c_int64),
         ("nprocessed", C.c_int64),
+        ("cross_touch", C.c_int64),
         ("nhalo", C.c_int64),
         ("nmember", C.c_int64),
         ("halo_id", C.POINTER(C.c_int64)),
@@ -138,6 +139,7 @@ class Result:
     fail_rank: int
     npart_new: int
     nprocessed: int
+    cross_touch: int = 0
     halo_id: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
     halo_mass: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
     halo_rank: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
@@ -209,7 +211,8 @@ def tri_cic(rho_values, mode=REFERENCE) -> tuple[np.ndarray, int]:
 
 
 def _collect(res: _Result, params: Params) -> Result:
-    out = Result(status=res.status, fail_rank=res.fail_rank, npart_new=res.npart_new, nprocessed=res.nprocessed)
+    out = Result(status=res.status, fail_rank=res.fail_rank, npart_new=res.npart_new, nprocessed=res.nprocessed,
+                 cross_touch=res.cross_touch)
     h = int(res.nhalo)
     if res.status == 0:
         def arr(ptr, n, dt):

@@ -376,6 +376,52 @@ static inline double dist2(double xx, double yy, double zz, double xc,
   return (dx * dx + dy * dy) + dz * dz;
 }
 
+/* Records stored in the cells of the preselect cube (half-width ncut around
+ * cell c0) that meet the ball of radius rb around (xc, yc, zc): the
+ * algorithmic read volume of one crossing search.  A cell i of an axis
+ * spans [i + xs, i + xs + 1); the ball meets row (dj, dk) when
+ * rb^2 - gy^2 - gz^2 >= 0 with g the gap from the centre to the row's cells,
+ * and the row's cells t0..t1 around the centre's x offset.  Every operation
+ * is rounded separately, as in the GPU's counter. */
+static double cell_rel(double x, int64_t i, double xs, double nxd) {
+  double d = x - (((double)i + xs) + 0.5);
+  d = d - nxd * floor(d / nxd + 0.5);
+  return d;
+}
+static double cell_gap(double t0, int t, double nxd) {
+  double d = fabs((double)t - t0);
+  d = fmin(d, nxd - d);
+  return fmax(d - 0.5, 0.0);
+}
+static int64_t ball_touch(const int64_t *num, int32_t nx, int32_t ncut, const int64_t c0[3], double xc,
+                          double yc, double zc, double xs, double rb) {
+  const double nxd = (double)nx;
+  const double tx = cell_rel(xc, c0[0], xs, nxd), ty = cell_rel(yc, c0[1], xs, nxd),
+               tz = cell_rel(zc, c0[2], xs, nxd);
+  const double rm2 = rb * rb;
+  int64_t sum = 0;
+  for (int dk = -ncut; dk <= ncut; dk++)
+    for (int dj = -ncut; dj <= ncut; dj++) {
+      const double gy = cell_gap(ty, dj, nxd), gz = cell_gap(tz, dk, nxd);
+      const double gy2 = gy * gy, gz2 = gz * gz;
+      const double rem = (rm2 - gy2) - gz2;
+      if (rem < 0.0) continue;
+      const double wx = sqrt(rem);
+      int t0 = (int)ceil((tx - 0.5) - wx), t1 = (int)floor((tx + 0.5) + wx);
+      if (t0 < -ncut) t0 = -ncut;
+      if (t1 > ncut) t1 = ncut;
+      int64_t jj = (c0[1] + dj) % nx, kk = (c0[2] + dk) % nx;
+      if (jj < 0) jj += nx;
+      if (kk < 0) kk += nx;
+      for (int t = t0; t <= t1; t++) {
+        int64_t ii = (c0[0] + t) % nx;
+        if (ii < 0) ii += nx;
+        sum += num[ii + (int64_t)nx * (jj + (int64_t)nx * kk)];
+      }
+    }
+  return sum;
+}
+
 /* Crossing scan of main:2040-2100 for one threshold.  dist is sorted.
  * Returns i (1-based stop index); *ovd_out gets overdens at exit. */
 static int64_t crossing_scan(const double *dist, int64_t npart_sel,
@@ -636,6 +682,9 @@ int psod_oracle_spherover(const psod_oracle_params *p, int64_t n,
     }
     const double rayon = sqrt(dist.v[i - 2]); /* distance(i-1), 1-based */
     const int64_t masse = i - 1;
+    /* algorithmic reads: the cells meeting the ball out to the stopping
+     * particle (the i-th, 1-based) */
+    res->cross_touch += ball_touch(num, nx, p->ncut, c0, xc, yc, zc, xxmin * scale, sqrt(dist.v[i - 1]));
     const double amass = (double)masse * munit;
 
     /* profile edges and cumulative counts, main:2103-2115 */

@@ -74,6 +74,10 @@ typedef struct psod_oracle_result {
   int64_t fail_rank;      /* 0-based seed rank (ipart-1) that failed, or -1 */
   int64_t npart_new;      /* tri_cic count (includes the first rho<=100) */
   int64_t nprocessed;     /* seeds that passed Mtotsel >= Mmin */
+  int64_t cross_touch;    /* records stored in the preselect-cube cells that
+                             meet each crossing seed's ball out to its
+                             stopping particle, summed (the algorithmic reads
+                             of the crossing search) */
   int64_t nhalo;
   int64_t nmember;
   int64_t *halo_id;       /* iamas */

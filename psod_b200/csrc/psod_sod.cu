@@ -300,7 +300,9 @@ __device__ unsigned region_records(const SodConst &K, const SodBufs &B, const Re
   for (int row = threadIdx.x; row < nrow; row += TPB) {
     const int dj = row % side - R, dk = row / side - R;
     const double gy = cell_gap(ty, dj, nxd), gz = cell_gap(tz, dk, nxd);
-    const double rem = rm2 - gy * gy - gz * gz;
+    // each operation rounded on its own (no contraction): the count is
+    // restated exactly by the oracle
+    const double rem = __dsub_rn(__dsub_rn(rm2, __dmul_rn(gy, gy)), __dmul_rn(gz, gz));
     if (rem < 0.0) continue;
     const double wx = sqrt(rem);
     const int t0 = max((int)ceil(tx - 0.5 - wx), -R), t1 = min((int)floor(tx + 0.5 + wx), R);
@@ -2038,7 +2040,7 @@ __device__ __forceinline__ int ball_row_ranges(const SodConst &K, const SodBufs 
   const int R = K.ncut;
   const double nxd = (double)K.nx;
   const double gy = cell_gap(ty, dj, nxd), gz = cell_gap(tz, dk, nxd);
-  const double rem = rm2 - gy * gy - gz * gz;
+  const double rem = __dsub_rn(__dsub_rn(rm2, __dmul_rn(gy, gy)), __dmul_rn(gz, gz));  // as region_records
   if (rem < 0.0) return 0;
   const double wx = sqrt(rem);
   int t0 = (int)ceil(tx - 0.5 - wx), t1 = (int)floor(tx + 0.5 + wx);

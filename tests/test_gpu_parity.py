@@ -147,6 +147,9 @@ def test_clustered_box_matches_oracle(oracle, nx, nmax, seed, mode):
     assert rc.status == 0 and rc.nhalo > 0
     assert nn == rc.npart_new
     assert st["nprocessed"] == rc.nprocessed
+    # the roofline numerator: records of the cells meeting each crossing
+    # ball out to its stopping particle, counted the same way by both
+    assert st["cross_touch"] == rc.cross_touch
     assert_same_halos(t, rc)
     assert np.array_equal(t.halo_profile, rc.halo_profile)
     assert np.array_equal(t.halo_mass2, rc.halo_mass2)

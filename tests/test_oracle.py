@@ -101,6 +101,46 @@ def test_isolated_ball_exact(oracle, mode):
     assert r.halo_profile[0, -1] <= ball.size
 
 
+def test_isolated_ball_touch_count(oracle):
+    """The algorithmic reads of the crossing (the bench's roofline
+    numerator): the records stored in the preselect-cube cells that meet each
+    crossing ball out to its stopping particle.  The ball seed's share is
+    brute-forced cell by cell; the other processed seed is a lattice
+    particle (the first seed at rho <= 100), whose ball reaches its 27
+    nearest cells at most."""
+    nx = 24
+    pos, ids, balls = hole_ball_box(nx, [(11.3, 12.6, 9.9)], r_hole=3.6, r_ball=0.3)
+    p = oracle.Params(nx=nx)
+    r = oracle.run(p, pos, ids, oracle.CANONICAL)
+    assert r.status == 0 and r.nprocessed == 2 and r.nhalo == 1
+    isort, _ = oracle.tri_cic(oracle.rho(p, pos, oracle.CANONICAL), oracle.CANONICAL)
+    seed = int(isort[r.halo_rank[0]])
+    # the stopping particle is the first one after the N_delta members
+    d2 = np.sort(ref_d2(pos, nx, int(r.halo_cidx[0])))
+    rb = np.sqrt(d2[r.halo_mass[0]])
+    pg = (pos.astype(np.float64) * nx).astype(np.float32).astype(np.float64)
+    cell = np.floor(pg).astype(np.int64) % nx
+    counts = np.zeros((nx, nx, nx), np.int64)
+    np.add.at(counts, (cell[:, 0], cell[:, 1], cell[:, 2]), 1)
+    c = pg[int(r.halo_cidx[0])]
+    s0 = cell[seed]
+    want = 0
+    for dx in range(-p.ncut, p.ncut + 1):
+        for dy in range(-p.ncut, p.ncut + 1):
+            for dz in range(-p.ncut, p.ncut + 1):
+                lo = s0 + np.array([dx, dy, dz])
+                gap = 0.0
+                for a in range(3):
+                    # periodic distance from the centre to the slab [lo, lo + 1)
+                    dd = (c[a] - (lo[a] + 0.5)) % nx
+                    dd = min(dd, nx - dd)
+                    gap += max(dd - 0.5, 0.0) ** 2
+                if gap <= rb * rb:
+                    want += counts[lo[0] % nx, lo[1] % nx, lo[2] % nx]
+    assert want >= r.halo_mass[0] + 1
+    assert want < r.cross_touch <= want + 27
+
+
 def test_ball_across_periodic_boundary(oracle):
     nx = 24
     c = (0.2, 23.9, 12.0)
