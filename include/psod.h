@@ -46,12 +46,14 @@ typedef enum psod_status {
   PSOD_ERR_CUDA = 4,      /* CUDA runtime error or no device */
   PSOD_ERR_ARG = 5,       /* invalid argument or parameter */
   PSOD_ERR_STATE = 6,     /* entry point called out of order */
-  PSOD_ERR_NOMEM = 7      /* device allocation failed */
+  PSOD_ERR_NOMEM = 7,     /* device allocation failed */
+  PSOD_ERR_IO = 8         /* an output file could not be written */
 } psod_status;
 
 typedef enum psod_mode {
   PSOD_MODE_PLAIN = 0,   /* one launch per round, full-cube gather */
-  PSOD_MODE_BATCHED = 1, /* size-classed seeds, graph-captured rounds */
+  PSOD_MODE_BATCHED = 1, /* per-cell alive counts, growing-ball crossing
+                            (warp per small ball, CTA per large one) */
   PSOD_MODE_LEARNED = 2  /* batched + learned first ball of the crossing
                             search (psod_learn_*); batched without a model */
 } psod_mode;
@@ -190,6 +192,28 @@ int psod_get_halos(psod_ctx *ctx, const psod_halo_table *t);
 
 /* Convenience: cic, cicm1, tri_cic and spherover in one call. */
 int psod_run(psod_ctx *ctx, psod_run_stats *stats);
+
+/* The reference's binary halo files, written by spherover when it is built
+ * without HDF5 (main:2230-2259): Fortran unformatted sequential records
+ * (int32 byte length, payload, int32 byte length), from a halo table that
+ * psod_get_halos filled into HOST memory.  Host-only: no context, no device.
+ *   psod_write_masst ("sod_<snap>_masst_<zone>", main:2234-2239): record
+ *     namas (int32); per halo one record: ID (int64), N_delta (int32),
+ *     centre x, y, z (float32, box units).  Reads halo_id, halo_mass,
+ *     halo_center.
+ *   psod_write_strct ("sod_<snap>_strct_<zone>", main:2246-2256): record
+ *     namas (int32); per halo the records N_delta (int32), member positions
+ *     (3 float32 each, box units), velocities (3 float32 each; zeros when
+ *     vel is NULL), IDs (int64), then potential (float32) and force (3
+ *     float32) when pot / force are given, members in ascending distance.
+ *     Reads halo_mass, member_offset, member_index; pos/vel/id/pot/force
+ *     are the zone's particle arrays (n entries, input order, as loaded).
+ * Returns PSOD_ERR_ARG for missing arrays, inconsistent offsets, member
+ * indices outside [0, n) or records of 2^31 bytes or more, PSOD_ERR_IO
+ * when the file cannot be written. */
+int psod_write_masst(const char *path, const psod_halo_table *t, int64_t nhalo);
+int psod_write_strct(const char *path, const psod_halo_table *t, int64_t nhalo, int64_t n, const float *pos,
+                     const float *vel, const int64_t *id, const float *pot, const float *force);
 
 /* CIC density (cic + cicm1, the same fixed-point arithmetic) for a zone of
  * at most 64 cells per side, without any device allocation.  This entry

@@ -11,7 +11,7 @@ module psod_gpu
 
   integer(c_int), parameter :: PSOD_OK = 0, PSOD_ERR_NSEL = 1, &
        PSOD_ERR_SELRADIUS = 2, PSOD_ERR_TIMEOUT = 3, PSOD_ERR_CUDA = 4, &
-       PSOD_ERR_ARG = 5, PSOD_ERR_STATE = 6, PSOD_ERR_NOMEM = 7
+       PSOD_ERR_ARG = 5, PSOD_ERR_STATE = 6, PSOD_ERR_NOMEM = 7, PSOD_ERR_IO = 8
   integer(c_int), parameter :: PSOD_MODE_PLAIN = 0, PSOD_MODE_BATCHED = 1, &
        PSOD_MODE_LEARNED = 2
 
@@ -131,6 +131,23 @@ module psod_gpu
      type(c_ptr) function psod_last_error(ctx) bind(C, name="psod_last_error")
        import :: c_ptr
        type(c_ptr), value :: ctx
+     end function
+     ! binary halo files of a build without HDF5 (main:2230-2259); path is a
+     ! NUL-terminated character array (trim(name)//c_null_char), t a table
+     ! filled into host arrays
+     integer(c_int) function psod_write_masst(path, t, nhalo) bind(C, name="psod_write_masst")
+       import :: c_int, c_char, c_int64_t, psod_halo_table
+       character(kind=c_char), dimension(*), intent(in) :: path
+       type(psod_halo_table), intent(in) :: t
+       integer(c_int64_t), value :: nhalo
+     end function
+     integer(c_int) function psod_write_strct(path, t, nhalo, n, pos, vel, id, pot, force) &
+          bind(C, name="psod_write_strct")
+       import :: c_int, c_char, c_int64_t, c_ptr, psod_halo_table
+       character(kind=c_char), dimension(*), intent(in) :: path
+       type(psod_halo_table), intent(in) :: t
+       integer(c_int64_t), value :: nhalo, n
+       type(c_ptr), value :: pos, vel, id, pot, force
      end function
   end interface
 end module psod_gpu

@@ -22,6 +22,7 @@ ERR_CUDA = 4
 ERR_ARG = 5
 ERR_STATE = 6
 ERR_NOMEM = 7
+ERR_IO = 8
 
 MODE_PLAIN = 0
 MODE_BATCHED = 1
@@ -127,6 +128,8 @@ EXPORTS = [
     "psod_learn_set_margin",
     "psod_learn_forward",
     "psod_learn_gradient",
+    "psod_write_masst",
+    "psod_write_strct",
 ]
 
 LEARN_FEATURES = 10
@@ -181,6 +184,8 @@ def load(build_if_missing: bool = True):
     L.psod_run.argtypes = [vp, P(RunStats)]
     L.psod_halo_count.argtypes = [vp, P(C.c_int64), P(C.c_int64)]
     L.psod_get_halos.argtypes = [vp, P(HaloTable)]
+    L.psod_write_masst.argtypes = [C.c_char_p, P(HaloTable), C.c_int64]
+    L.psod_write_strct.argtypes = [C.c_char_p, P(HaloTable), C.c_int64, C.c_int64, vp, vp, vp, vp, vp]
     L.psod_last_error.argtypes = [vp]
     L.psod_cic_rho_static.argtypes = [C.c_int64, vp, C.c_int32, C.c_int64, C.c_int32, vp, vp, vp]
     L.psod_learn_collect.argtypes = [vp, C.c_int64]

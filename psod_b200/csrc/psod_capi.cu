@@ -90,6 +90,7 @@ const char *psod_status_string(int s) {
     case PSOD_ERR_ARG: return "invalid argument";
     case PSOD_ERR_STATE: return "call out of order or internal check failed";
     case PSOD_ERR_NOMEM: return "device allocation failed";
+    case PSOD_ERR_IO: return "output file could not be written";
     default: return "unknown status";
   }
 }

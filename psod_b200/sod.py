@@ -252,6 +252,57 @@ class SphericalOverdensity:
         return t
 
 
+def _host_table(t: HaloTable) -> tuple[capi.HaloTable, list]:
+    """A C halo table pointing at host numpy copies of ``t``'s arrays (the
+    copies are returned too, to keep them alive during the call)."""
+    keep = []
+    ct = capi.HaloTable()
+    dtypes = dict(halo_center=np.float32, halo_rdelta=np.float64)
+    for f, _ in capi.HaloTable._fields_:
+        a = getattr(t, f)
+        if isinstance(a, torch.Tensor):
+            a = a.detach().cpu().numpy()
+        a = np.ascontiguousarray(np.asarray(a).reshape(-1), dtype=dtypes.get(f, np.int64))
+        keep.append(a)
+        setattr(ct, f, None if a.size == 0 else a.ctypes.data)
+    return ct, keep
+
+
+def write_masst(path: str, table: HaloTable) -> None:
+    """The reference's "masst" file of one zone (main:2234-2239): Fortran
+    unformatted records of namas, then (ID, N_delta, centre) per halo."""
+    lib = capi.load()
+    ct, keep = _host_table(table)
+    st = lib.psod_write_masst(str(path).encode(), C.byref(ct), table.nhalo)
+    if st != capi.OK:
+        raise PsodError(st, f"psod_write_masst({path}) failed")
+
+
+def write_strct(path: str, table: HaloTable, pos, ids, vel=None, pot=None, force=None) -> None:
+    """The reference's "strct" file of one zone (main:2246-2256): per halo
+    N_delta, then its members' positions, velocities, IDs (and potential /
+    force when given), members in ascending distance.  ``pos``/``vel``/
+    ``ids`` are the zone's particle arrays in input order."""
+    lib = capi.load()
+    ct, keep = _host_table(table)
+
+    def host(a, dt, width):
+        if a is None:
+            return None
+        if isinstance(a, torch.Tensor):
+            a = a.detach().cpu().numpy()
+        return np.ascontiguousarray(np.asarray(a, dtype=dt).reshape(-1, width) if width > 1 else
+                                    np.asarray(a, dtype=dt).reshape(-1))
+
+    p, i = host(pos, np.float32, 3), host(ids, np.int64, 1)
+    v, q, fo = host(vel, np.float32, 3), host(pot, np.float32, 1), host(force, np.float32, 3)
+    n = i.shape[0]
+    st = lib.psod_write_strct(str(path).encode(), C.byref(ct), table.nhalo, n, _ptr(p), _ptr(v), _ptr(i), _ptr(q),
+                              _ptr(fo))
+    if st != capi.OK:
+        raise PsodError(st, f"psod_write_strct({path}) failed")
+
+
 def _contig(x, dtype):
     if isinstance(x, torch.Tensor):
         return x.to(dtype).contiguous()
