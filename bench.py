@@ -49,9 +49,64 @@ WORKLOADS = {
 EXTRA_DELTAS = (500.0, 178.0)
 EXTRA_BINS = 48
 
+METRIC = "SOD halos/s (delta=200, N200 exact)"
+
 
 def npu_for(nx):
     return {128: 0, 256: 0, 512: 200000, 1024: 1000000}.get(nx, 0)
+
+
+def inputs_fit_l2(nx):
+    """True when one box's positions and IDs (20 B a particle) would stay in
+    the 126 MB L2 between steps, so that the timed loop must flush it."""
+    return nx**3 * (12 + 8) < (126 << 20) * 2
+
+
+def workload_config(nx, ndelta):
+    """The ``config`` object of both arms: the workload alone (no
+    implementation or measurement keys), so the two lines name the same
+    configuration."""
+    wl = WORKLOADS.get(nx, dict(nmax_halo=20000, box=f"{nx}^3"))
+    return {
+        "workload": wl["box"],
+        "nx": nx,
+        "particles": nx**3,
+        "npu": npu_for(nx),
+        "delta": [200.0, 500.0, 178.0] if ndelta else [200.0],
+        "nbins": EXTRA_BINS if ndelta else 60,
+        "l2": "flushed between steps" if inputs_fit_l2(nx) else "inputs larger than L2",
+    }
+
+
+def table_digest(sod, members):
+    """Checksum of the whole halo table, computed on the device: every field
+    (IDs, masses, ranks, centres, radii, seuil2 and extra-delta masses,
+    profiles, member offsets and member indices) mixed with its position."""
+    import torch
+
+    from psod_b200.sod import HaloTable
+
+    h, m = sod.halo_count()
+    nb, ne = sod.params.nbins, sod.params.ndelta_extra
+    dev = f"cuda:{torch.cuda.current_device()}"
+    sizes = dict(halo_id=h, halo_mass=h, halo_rank=h, halo_center=3 * h, halo_rdelta=h, halo_mass2=h,
+                 halo_mextra=h * ne, halo_profile=h * nb, member_offset=h + 1, member_index=m, member_id=0)
+    dt = dict(halo_center=torch.float32, halo_rdelta=torch.float64)
+    out = HaloTable(**{f: torch.zeros(max(1, k), dtype=dt.get(f, torch.int64), device=dev) for f, k in sizes.items()})
+    t = sod.halos(members=True, out=out)
+    acc = 0
+    for k, f in enumerate(("halo_id", "halo_mass", "halo_rank", "halo_center", "halo_rdelta", "halo_mass2",
+                           "halo_mextra", "halo_profile", "member_offset", "member_index")):
+        a = getattr(t, f).reshape(-1)
+        if a.numel() == 0:
+            continue
+        x = a.view(torch.int32).to(torch.int64) if a.dtype == torch.float32 else a.view(torch.int64)
+        i = torch.arange(x.numel(), dtype=torch.int64, device=dev)
+        y = x * -7046029254386353131 + (i + 1) * -4658895280553007687 + k * 1442695040888963407
+        y = y ^ (y >> 29)
+        acc = (acc * 6364136223846793005 + int(y.sum().item()) + members) & ((1 << 64) - 1)
+    del out
+    return f"{h}:{m}:{acc:016x}"
 
 
 def load_peaks():
@@ -185,7 +240,7 @@ def run_ours(args):
     # L2 flush buffer (used when the inputs are smaller than L2)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
     inputs_bytes = n * (12 + 8)
-    need_flush = inputs_bytes < (126 << 20) * 2
+    need_flush = inputs_fit_l2(nx)
 
     def step_device():
         if need_flush:
@@ -262,7 +317,7 @@ def run_ours(args):
     props = torch.cuda.get_device_properties(dev)
     ceiling = props.multi_processor_count * 4 * sm_mhz * 1e6 * 32 / 12.0
     line = {
-        "metric": "SOD halos/s (delta=200, N200 exact)",
+        "metric": METRIC,
         "value": round(value, 2),
         "unit": "halos/s",
         "n_gpus": world,
@@ -274,13 +329,10 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic NFW-mixture box (seeded); inputs resident in HBM",
-        "config": {
-            "workload": wl["box"],
-            "nx": nx,
-            "particles": n,
-            "mode": args.mode,
-            "npu": params["npu"],
-            "delta": [200.0, 500.0, 178.0] if args.ndelta else [200.0],
+        "mode": args.mode,
+        "parallelism": f"replicas x{world}",
+        "config": workload_config(nx, args.ndelta),
+        "detail": {
             "halos": nhalo_all,
             "members": s["nmember"],
             "seeds": s["npart_new"],
@@ -289,8 +341,6 @@ def run_ours(args):
             "stage_ms": {k: round(v, 2) for k, v in stage_ms.items()},
             "sod_phase_ms": {k: round(s[k], 2) for k in ("ms_setup", "ms_sched", "ms_prep", "ms_refine", "ms_select",
                                                          "ms_cross", "ms_output")},
-            "l2": "flushed between steps" if need_flush else "inputs larger than L2",
-            "parallelism": f"replicas x{world}",
         },
         "e2e": {
             "value": round(nhalo_all / (e2e_ms / 1000.0), 2),
@@ -331,15 +381,23 @@ def run_ours(args):
                        cross_records=int(s["cross_records"]), ms_learn=round(s["ms_learn"], 2))
         line["bracket"] = bracket
     if args.compare_plain and args.mode != "plain" and world == 1:
+        # the same box through the other modes: their tables must be
+        # identical to this one (device checksums of every field)
+        digests = {args.mode: table_digest(sod, 0)}
         if args.mode == "learned":
             line["batched"] = mode_reference(nx, params, pos_d, ids_d, sod, 1)
             line["vs_batched"] = round(line["batched"]["ms_per_step"] / ms, 3)
+            digests["batched"] = line["batched"].pop("digest")
             sod = None
         line["plain"] = mode_reference(nx, params, pos_d, ids_d, sod, 0)
         line["vs_plain"] = round(line["plain"]["ms_per_step"] / ms, 3)
+        digests["plain"] = line["plain"].pop("digest")
         sod = None
+        line["modes_identical"] = len(set(digests.values())) == 1
+        line["table_digests"] = digests
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args, nx, wl, quick=True)
+        cb = cpu_baseline(args, nx, wl, cores=1, boxes_per_core=4 if nx > 128 else 1)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if sod is not None:
         sod.close()
     if world > 1:
@@ -401,11 +459,12 @@ def mode_reference(nx, params, pos_d, ids_d, sod, mode):
     b.record()
     torch.cuda.synchronize()
     msp = a.elapsed_time(b)
+    digest = table_digest(sp, 0)
     sp.close()
     out = {"mode": {0: "plain", 1: "batched"}[mode], "ms_per_step": round(msp, 3), "halos": st["nhalo"],
            "value": round(st["nhalo"] / (msp / 1000.0), 2), "unit": "halos/s",
            "sod_phase_ms": {k: round(st[k], 2) for k in ("ms_setup", "ms_sched", "ms_prep", "ms_refine", "ms_select",
-                                                         "ms_cross", "ms_output")}}
+                                                         "ms_cross", "ms_output")}, "digest": digest}
     if mode == 1:
         out.update(hit_rate=round(st["bracket_hits"] / max(1, st["bracket_seeds"]), 4),
                    cross_balls=int(st["cross_balls"]), cross_records=int(st["cross_records"]))
@@ -441,76 +500,149 @@ def train_bracket(args, dev, thresholds):
                    "train_s": round(time.perf_counter() - t0, 2)}
 
 
-def _cpu_sample(seed, nx, nmax, npu, ndelta):
-    """One sample box through the oracle's reference arithmetic, with the
-    parameters -npu derives (main:211-219) and the workload's thresholds."""
+def sample_nx(nx):
+    """Side of the CPU sample boxes: the workload itself up to 128^3 (the
+    oracle runs a full 128^3 box in about 20 s on one core), else 48^3 boxes
+    drawn with the workload's generator law (1-5 s each on one core, so that
+    a step of one box per core stays bounded)."""
+    return nx if nx <= 128 else 48
+
+
+def _oracle_params(snx, npu, ndelta):
+    """Oracle parameters of one sample box: the ones -npu derives
+    (main:211-219) and the workload's thresholds and bins."""
     import math
 
     from oracle import oracle as O
-    from psod_b200 import synth
 
-    b = synth.make_box(nx, nmax_halo=nmax, seed=seed)
     kw = {}
     if npu > 0:
         ncut = math.ceil(((npu * 2.0 / 200.0) ** (1.0 / 3.0)) / 2.0)
         kw = dict(ncut=ncut, nxbuffer=4 * ncut, nsel=math.ceil((2 * ncut + 1.0) ** 3 * 200.0 * 4.0))
     if ndelta:
         kw.update(delta_extra=EXTRA_DELTAS, nbins=EXTRA_BINS)
-    t0 = time.perf_counter()
-    r = O.run(O.Params(nx=nx, **kw), b.pos, b.ids, O.REFERENCE)
-    return r.nhalo, time.perf_counter() - t0
+    return O.Params(nx=snx, **kw)
 
 
-def cpu_baseline(args, nx, wl, quick=False, cores=None, nsamples=None):
-    """The reference algorithm on host cores: sample boxes of 64^3 cells with
-    the workload's generator law (same halo mass range and -npu), one per core."""
-    import multiprocessing as mp
+def _oracle_worker(seeds, snx, nmax, npu, ndelta, inq, outq):
+    """One host core of the CPU arms.  Builds its sample boxes once, before
+    any clock starts, then runs cic/cicm1/tri_cic/spherover of the oracle
+    (reference arithmetic) on them for every "run" it receives and returns
+    (halos, seconds of oracle work)."""
+    import torch
 
     from oracle import oracle as O
+    from psod_b200 import synth
 
-    O.build()
-    snx = 64
+    torch.set_num_threads(1)
+    boxes = []
+    for sd in seeds:
+        b = synth.make_box(snx, nmax_halo=nmax, seed=sd)
+        boxes.append((b.pos.numpy().copy(), b.ids.numpy().copy()))
+    params = _oracle_params(snx, npu, ndelta)
+    O.lib()
+    outq.put((0, 0.0))
+    while inq.get() == "run":
+        halos, busy = 0, 0.0
+        for pos, ids in boxes:
+            t0 = time.perf_counter()
+            r = O.run(params, pos, ids, O.REFERENCE)
+            busy += time.perf_counter() - t0
+            halos += r.nhalo
+        outq.put((halos, busy))
+
+
+class OracleCores:
+    """``cores`` worker processes (spawned), each holding its own sample
+    boxes.  ``step()`` runs every worker once and returns the halos found,
+    the oracle seconds summed over workers and the step's wall time."""
+
+    def __init__(self, cores, boxes_per_core, seed, snx, nmax, npu, ndelta):
+        import multiprocessing as mp
+
+        from oracle import oracle as O
+
+        O.build()
+        ctx = mp.get_context("spawn")
+        self.out = ctx.Queue()
+        self.ins, self.procs = [], []
+        for c in range(cores):
+            q = ctx.Queue()
+            seeds = [seed + 100 + c * boxes_per_core + j for j in range(boxes_per_core)]
+            pr = ctx.Process(target=_oracle_worker, args=(seeds, snx, nmax, npu, ndelta, q, self.out), daemon=True)
+            pr.start()
+            self.ins.append(q)
+            self.procs.append(pr)
+        for _ in self.procs:
+            self.out.get()
+        self.cores = cores
+
+    def step(self):
+        t0 = time.perf_counter()
+        for q in self.ins:
+            q.put("run")
+        res = [self.out.get() for _ in self.ins]
+        return sum(r[0] for r in res), sum(r[1] for r in res), time.perf_counter() - t0
+
+    def close(self):
+        for q in self.ins:
+            q.put("stop")
+        for pr in self.procs:
+            pr.join(timeout=30)
+
+
+def cpu_baseline(args, nx, wl, cores=1, boxes_per_core=2, steps=1, warmup=0):
+    """The reference algorithm on ``cores`` host cores: the oracle in
+    reference arithmetic on sample boxes built before the clock starts.
+    value = halos / (oracle seconds / cores), i.e. only oracle work is timed;
+    the wall time of the steps is reported beside it."""
+    snx = sample_nx(nx)
     nmax = wl["nmax_halo"]
     npu = npu_for(nx)
-    ncores = 1 if quick else (cores or os.cpu_count() or 1)
-    ns = nsamples or (2 if quick else ncores)
-    ctx = mp.get_context("spawn")
-    t0 = time.perf_counter()
-    with ctx.Pool(ncores) as pool:
-        res = pool.starmap(_cpu_sample, [(args.seed + 100 + i, snx, nmax, npu, args.ndelta) for i in range(ns)])
-    wall = time.perf_counter() - t0
-    halos = sum(r[0] for r in res)
-    busy = sum(r[1] for r in res) / ncores if quick else wall
+    pool = OracleCores(cores, boxes_per_core, args.seed, snx, nmax, npu, args.ndelta)
+    try:
+        for _ in range(warmup):
+            pool.step()
+        halos, busy, wall = 0, 0.0, 0.0
+        vals = []
+        for _ in range(steps):
+            h, b, w = pool.step()
+            halos, busy, wall = halos + h, busy + b, wall + w
+            vals.append(h / (b / cores) if b > 0 else 0.0)
+    finally:
+        pool.close()
+    what = "the workload's own box" if snx == nx else f"box(es) of {snx}^3 cells from the workload's generator law"
     return {
-        "value": round(halos / busy, 3),
+        "value": round(halos / (busy / cores), 3) if busy > 0 else 0.0,
         "unit": "halos/s",
-        "cores": ncores,
+        "cores": cores,
         "kind": "port",
-        "sample": f"{ns} box(es) of {snx}^3 cells from the same generator (halo N in [20, {nmax}], npu {npu}), "
-                  f"{'Delta 200/500/178, 48 bins, ' if args.ndelta else ''}"
-                  f"full cic/cicm1/tri_cic/spherover in reference arithmetic, {halos} halos; wall {wall:.1f}s",
+        "sample": f"{cores * boxes_per_core} {what} (halo N in [20, {nmax}], npu {npu}, seeds from {args.seed + 100}), "
+                  f"{'Delta 200/500/178, 48 bins, ' if args.ndelta else 'Delta 200, 60 bins, '}"
+                  f"cic/cicm1/tri_cic/spherover of the C oracle in reference arithmetic, one core each; "
+                  f"{halos // max(1, steps)} halos and {busy / max(1, steps):.1f} core-seconds of oracle work a step; "
+                  f"boxes built before timing; wall {wall / max(1, steps):.1f} s a step",
+        "step_values": [round(v, 3) for v in vals],
     }
 
 
 def run_reference(args):
+    """The driver's reference arm: the reference's algorithm (the C oracle,
+    reference arithmetic; the Fortran itself cannot be built here) on all
+    host cores, rank 0 only, same metric, unit and config as our arm."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     nx = args.nx
     wl = WORKLOADS.get(nx, dict(nmax_halo=20000, box=f"{nx}^3"))
-    vals = []
-    cb = None
-    for i in range(args.warmup):  # warm-up: one small sample on one core
-        cpu_baseline(args, nx, wl, quick=True, nsamples=1)
-    for i in range(args.steps):
-        cb = cpu_baseline(args, nx, wl, quick=False)
-        vals.append(cb["value"])
-    v = sum(vals) / len(vals)
+    cores = max(1, min(os.cpu_count() or 1, 64))
+    cb = cpu_baseline(args, nx, wl, cores=cores, boxes_per_core=1, steps=args.steps, warmup=args.warmup)
+    v = cb["value"]
     line = {
         "impl": "reference",
-        "metric": "SOD halos/s (delta=200, N200 exact)",
-        "value": round(v, 3),
+        "metric": METRIC,
+        "value": v,
         "unit": "halos/s",
         "n_gpus": world,
         "steps": args.steps,
@@ -520,12 +652,25 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic NFW-mixture boxes (seeded)",
-        "config": {"workload": wl["box"], "nx": nx, "mode": "reference CPU oracle"},
-        "cpu_baseline": {"value": round(v, 3), "unit": "halos/s", "cores": cb["cores"], "kind": "port",
-                         "sample": cb["sample"]},
-        "e2e": {"value": round(v, 3), "unit": "halos/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "mode": "reference CPU oracle",
+        "config": workload_config(nx, args.ndelta),
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": v, "unit": "halos/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def relaunch_with_torchrun(args):
+    """``--gpus N`` without a torchrun environment: start the N ranks here
+    (one process per GPU) with the same arguments, and return their status."""
+    import socket
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
 
 
 def main():
@@ -543,6 +688,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.mode_id = {"plain": 0, "batched": 1, "learned": 2}[args.mode]
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch_with_torchrun(args))
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -217,12 +217,13 @@ int psod_write_strct(const char *path, const psod_halo_table *t, int64_t nhalo, 
 
 /* CIC density (cic + cicm1, the same fixed-point arithmetic) for a zone of
  * at most 64 cells per side, without any device allocation.  This entry
- * point has no counterpart in the reference.  It is for callers that cannot
- * let the library allocate device memory: code recording a stream into a
- * CUDA graph (cudaMalloc is not allowed during capture), and host codes that
- * size all device memory themselves and forbid libraries from allocating.
- * The node grid is a file-scope device array of (2*64)^3 int64 (16 MiB)
- * that every device loading the library holds until exit.
+ * point has no counterpart in the reference.  It is for host codes that
+ * cannot let a library allocate device memory: drivers that size all of the
+ * GPU's memory themselves (several MPI ranks sharing one GPU under fixed
+ * per-rank budgets, or a host whose own pool allocator owns the device) and
+ * forbid libraries from calling cudaMalloc.  The node grid is a file-scope
+ * device array of (2*64)^3 int64 (16 MiB) that every device loading the
+ * library holds until exit.
  *   pos      device, xyz-interleaved float32 box units [0,1], n particles
  *   rho      device, n doubles, input order (as psod_cicm1)
  *   bad_flag device int or NULL: set to 1 when a position lies outside
@@ -230,9 +231,11 @@ int psod_write_strct(const char *path, const psod_halo_table *t, int64_t nhalo, 
  *   stream   cudaStream_t as void* (NULL: legacy default stream)
  * Work is enqueued on the stream and not waited for.  Returns PSOD_ERR_ARG
  * for nx > 64, nxbuffer >= nx or host pointers.  The first call on a device
- * looks up the array's device address (cudaGetSymbolAddress); make that
- * first call before any stream capture.  All calls share the array, so
- * calls that overlap on the GPU race: serialise them. */
+ * looks up the array's device address (cudaGetSymbolAddress, with that
+ * device current); make that first call before any stream capture.  Every
+ * call clears the array before depositing.  All calls share the array, so
+ * calls that overlap on the GPU race and give wrong densities: serialise
+ * them. */
 int psod_cic_rho_static(int64_t n, const float *pos, int32_t nx, int64_t npart_total, int32_t nxbuffer,
                         double *rho, int *bad_flag, void *stream);
 

@@ -53,18 +53,38 @@ bool table_ok(const psod_halo_table *t, int64_t nhalo) {
   return t && nhalo >= 0 && nhalo < ((int64_t)1 << 31) && (nhalo == 0 || (t->halo_mass && t->member_offset));
 }
 
+// Every record is checked before the file is opened, so an invalid table
+// leaves no partly written file behind.
+bool masses_ok(const psod_halo_table *t, int64_t nhalo) {
+  for (int64_t h = 0; h < nhalo; h++)
+    if (t->halo_mass[h] < 0 || t->halo_mass[h] > INT32_MAX) return false;
+  return true;
+}
+
+bool members_ok(const psod_halo_table *t, int64_t nhalo, int64_t n) {
+  for (int64_t h = 0; h < nhalo; h++) {
+    const int64_t m = t->halo_mass[h], o = t->member_offset[h];
+    if (m < 0 || 12 * m >= ((int64_t)1 << 31) || o < 0 || t->member_offset[h + 1] - o != m) return false;
+    for (int64_t j = 0; j < m; j++) {
+      const int64_t q = t->member_index[o + j];
+      if (q < 0 || q >= n) return false;
+    }
+  }
+  return true;
+}
+
 }  // namespace
 
 extern "C" {
 
 int psod_write_masst(const char *path, const psod_halo_table *t, int64_t nhalo) {
   if (!path || !table_ok(t, nhalo) || (nhalo > 0 && (!t->halo_id || !t->halo_center))) return PSOD_ERR_ARG;
+  if (!masses_ok(t, nhalo)) return PSOD_ERR_ARG;
   RecordFile out(path);
   if (!out.ok) return PSOD_ERR_IO;
   const int32_t namas = (int32_t)nhalo;
   out.record({{&namas, 4}});  // main:2235
   for (int64_t h = 0; h < nhalo; h++) {
-    if (t->halo_mass[h] < 0 || t->halo_mass[h] > INT32_MAX) return PSOD_ERR_ARG;
     const int64_t id = t->halo_id[h];
     const int32_t mass = (int32_t)t->halo_mass[h];  // masses(i), default integer
     // int(idtab(i),kind=8), masses(i), xctab(i), yctab(i), zctab(i) (main:2237)
@@ -77,6 +97,7 @@ int psod_write_strct(const char *path, const psod_halo_table *t, int64_t nhalo, 
                      const float *vel, const int64_t *id, const float *pot, const float *force) {
   if (!path || !table_ok(t, nhalo) || n < 0 || (nhalo > 0 && (!t->member_index || !pos || !id)))
     return PSOD_ERR_ARG;
+  if (!members_ok(t, nhalo, n)) return PSOD_ERR_ARG;
   RecordFile out(path);
   if (!out.ok) return PSOD_ERR_IO;
   const int32_t namas = (int32_t)nhalo;
@@ -85,14 +106,12 @@ int psod_write_strct(const char *path, const psod_halo_table *t, int64_t nhalo, 
   std::vector<int64_t> bufi;
   for (int64_t h = 0; h < nhalo; h++) {
     const int64_t m = t->halo_mass[h], o = t->member_offset[h];
-    if (m < 0 || 12 * m >= ((int64_t)1 << 31) || t->member_offset[h + 1] - o != m) return PSOD_ERR_ARG;
     const int32_t mass = (int32_t)m;
     out.record({{&mass, 4}});  // main:2250
     buf3.resize((size_t)(3 * m));
     bufi.resize((size_t)m);
     for (int64_t j = 0; j < m; j++) {
       const int64_t q = t->member_index[o + j];
-      if (q < 0 || q >= n) return PSOD_ERR_ARG;
       std::memcpy(&buf3[3 * j], pos + 3 * q, 12);
       bufi[j] = id[q];
     }

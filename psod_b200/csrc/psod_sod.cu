@@ -2603,6 +2603,16 @@ __global__ void k_ready(const unsigned *active, const unsigned *nactive, const u
   if (at < cap) ready[at] = h;
 }
 
+// seeds among [0, nseed) whose resolved bit is clear
+__global__ void k_count_unresolved(const unsigned *resolved, long long nseed, unsigned long long *out) {
+  const long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (w * 32 >= nseed) return;
+  unsigned open = ~resolved[w];
+  const long long left = nseed - w * 32;
+  if (left < 32) open &= (1u << left) - 1u;
+  if (open) atomicAdd(out, (unsigned long long)__popc(open));
+}
+
 __global__ void k_find_rank(const unsigned *seed_idx, long long nseed, unsigned idx, unsigned *out) {
   long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (r < nseed && seed_idx[r] == idx) *out = (unsigned)r;
@@ -2889,7 +2899,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       (rc = scratch(c, SC_HEAD, (size_t)nblocks, &head)) || (rc = scratch(c, SC_FILT_A, (size_t)nblocks, &filt_a)) ||
       (rc = scratch(c, SC_FILT_B, (size_t)nblocks, &filt_b)) || (rc = scratch(c, SC_READY, (size_t)nblocks + 1, &ready)) ||
       (rc = scratch(c, SC_CTRS, 16, &ctrs)) || (rc = scratch(c, SC_COUNTS, (size_t)nblocks + 1, &counts)) ||
-      (rc = scratch(c, SC_PROCESSED, (size_t)nseed + 1, &processed)) || (rc = scratch(c, SC_U64, 16, &u64s)) ||
+      (rc = scratch(c, SC_PROCESSED, (size_t)nseed + 1, &processed)) || (rc = scratch(c, SC_U64, 32, &u64s)) ||
       (rc = scratch(c, SC_EDGES, (size_t)c->p.nbins, &edge_fac)) || (rc = scratch(c, SC_HRANK, (size_t)hcap, &h_rank)) ||
       (rc = scratch(c, SC_HID, (size_t)hcap, &h_id)) || (rc = scratch(c, SC_HMASS, (size_t)hcap, &h_mass)) ||
       (rc = scratch(c, SC_HMASS2, (size_t)hcap, &h_mass2)) || (rc = scratch(c, SC_HMEXTRA, (size_t)hcap * ne, &h_mextra)) ||
@@ -2945,7 +2955,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   PSOD_CUDA(c, cudaMemcpyAsync(edge_fac, c->edge_fac.data(), sizeof(double) * c->p.nbins, cudaMemcpyHostToDevice,
                                c->stream));
   PSOD_CUDA(c, cudaMemsetAsync(processed, 0, (size_t)nseed + 1, c->stream));
-  PSOD_CUDA(c, cudaMemsetAsync(u64s, 0, sizeof(unsigned long long) * 16, c->stream));
+  PSOD_CUDA(c, cudaMemsetAsync(u64s, 0, sizeof(unsigned long long) * 32, c->stream));
   PSOD_CUDA(c, cudaMemsetAsync(u64s, 0xff, sizeof(unsigned long long), c->stream));  // err = none
   PSOD_CUDA(c, cudaMemsetAsync(ctrs, 0xff, sizeof(unsigned) * 16, c->stream));
 
@@ -3094,10 +3104,6 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   }
 
   long long rounds = 0, seed_launches = 0;
-  // PSOD_TRACE=1: one line per round on stderr (ready seeds, active blocks,
-  // candidates, phase times)
-  const char *trace_env = getenv("PSOD_TRACE");
-  const bool trace = trace_env && trace_env[0] == '1';
   // ctrs[8]: active-block count of the current list, ctrs[9]: of the next
   unsigned n_active = 0;
   if (nseed > 0) {
@@ -3131,7 +3137,12 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     unsigned nready = hc[0];
     n_active = hc[9];
     std::swap(act_a, act_b);
-    if (nready == 0) break;
+    if (nready == 0) {
+      // the lowest-ranked unresolved seed is always ready, so an empty
+      // round with unresolved seeds left is a scheduler fault
+      if (n_active > 0) return set_err(c, PSOD_ERR_STATE, "scheduler stalled with unresolved seeds");
+      break;
+    }
     nready = std::min(nready, cap_ready);
     const unsigned g = std::min<unsigned>(seed_grid, nready);
     t_prep.start(c->stream);
@@ -3193,22 +3204,32 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     t_cross.collect();
     if (B.learn_use) t_learn.collect();
     if (B.bound_on) t_bound.collect();
-    if (trace) {
+#ifdef PSOD_TRACE_ROUNDS
+    {
+      // diagnostic build only (-DPSOD_TRACE_ROUNDS): one line per round on
+      // stderr with the ready seeds, active blocks, candidates and phase times
       unsigned cu = 0;
       unsigned long long tv[16];
-      cudaMemcpy(&cu, cand_used, sizeof(unsigned), cudaMemcpyDeviceToHost);
-      cudaMemcpy(tv, u64s, sizeof(tv), cudaMemcpyDeviceToHost);
+      cudaMemcpyAsync(&cu, cand_used, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream);
+      cudaMemcpyAsync(tv, u64s, sizeof(tv), cudaMemcpyDeviceToHost, c->stream);
+      cudaStreamSynchronize(c->stream);
       fprintf(stderr,
               "psod round %lld ready %u active %u cand %u sched %.3f prep %.3f refine %.3f select %.3f cross %.3f "
               "pairs %llu slots %llu staged %llu bound %.3f items %llu pruned_cand %llu\n",
               rounds, nready, n_active, cu, t_sched.last, t_prep.last, t_ref.last, t_sel.last, t_cross.last, tv[5], tv[8],
               tv[9], B.bound_on ? t_bound.last : 0.0, tv[14], tv[15]);
     }
+#endif
     rounds++;
     seed_launches += 4;
     kernels += 4;
   }
-  unsigned long long hv[16];
+  // every seed must end processed or claimed; u64s[16] counts those that did not
+  if (nseed > 0) {
+    k_count_unresolved<<<nblk(nseed / 32 + 1, 256), 256, 0, c->stream>>>(resolved, nseed, u64s + 16);
+    kernels++;
+  }
+  unsigned long long hv[17];
   PSOD_CUDA(c, cudaMemcpyAsync(hv, u64s, sizeof(hv), cudaMemcpyDeviceToHost, c->stream));
   PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
   st.rounds = rounds;
@@ -3236,6 +3257,12 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   c->nhalo = 0;
   c->nmember = 0;
   c->sod_done = false;
+  if (hv[0] == ~0ull && hv[16] != 0) {
+    st.kernel_launches = kernels;
+    c->last_stats = st;
+    if (out_stats) *out_stats = st;
+    return set_err(c, PSOD_ERR_STATE, std::to_string(hv[16]) + " seeds left unresolved by the scheduler");
+  }
   if (hv[0] != ~0ull) {
     const int code = (int)(hv[0] & 0xff);
     st.fail_rank = (int64_t)(hv[0] >> 8);

@@ -4,16 +4,20 @@
 // psod_cic + psod_cicm1 (fixed-point nodes, the reference's interpolation
 // order), for zones of at most PSOD_STATIC_MAX_NX cells per side, using a
 // node grid that lives in a file-scope __device__ array instead of memory
-// the library allocates.  It exists for callers that cannot let a library
-// allocate device memory: a caller recording a stream into a CUDA graph,
-// where cudaMalloc is not allowed during capture, and host codes that size
-// all device memory themselves (for instance MPI ranks sharing a GPU under
-// fixed per-rank memory budgets) and forbid libraries from allocating.
+// the library allocates.  It exists for host codes that cannot let a library
+// allocate device memory: drivers that size all of the GPU's memory
+// themselves (for instance several MPI ranks sharing a GPU under fixed
+// per-rank budgets, or a host whose own pool allocator owns the device) and
+// forbid libraries from calling cudaMalloc.
 //
 // The array (PSOD_STATIC_MAX_NX = 64: (2*64)^3 int64 nodes, 16 MiB) is held
-// on every device that loads the library until the process exits.  All calls
-// share it: calls whose work overlaps on the GPU (two streams, or two host
-// threads) race and give wrong densities; serialise them.
+// on every device that loads the library until the process exits.  Host code
+// cannot use the array's name as a device address, so the first call on each
+// device looks the address up with cudaGetSymbolAddress (that device current)
+// and keeps it; make that first call before any stream capture.  Every call
+// clears the nodes before depositing.  All calls share the array: calls
+// whose work overlaps on the GPU (two streams, or two host threads) race and
+// give wrong densities; serialise them.
 #include <cuda_runtime.h>
 
 #include <mutex>

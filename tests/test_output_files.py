@@ -101,6 +101,13 @@ def test_writer_errors(tmp_path):
     with pytest.raises(PsodError) as e:
         write_strct(tmp_path / "s", t, pos, ids)
     assert e.value.status == capi.ERR_ARG
+    # the table is checked before the file is opened: nothing is left behind
+    assert not (tmp_path / "s").exists()
+    t = table([0, 1], [1, -3], [[0, 0, 0], [0, 0, 0]], [0, 1, 1], [0])  # negative mass in the last record
+    with pytest.raises(PsodError) as e:
+        write_masst(tmp_path / "m_bad", t)
+    assert e.value.status == capi.ERR_ARG
+    assert not (tmp_path / "m_bad").exists()
     t = table([0], [2], [[0, 0, 0]], [0, 2], [0, 1])
     with pytest.raises(PsodError) as e:
         write_masst(tmp_path / "missing_dir" / "m", t)
