@@ -68,6 +68,17 @@ class _Result(C.Structure):
     ]
 
 
+class _Audit(C.Structure):
+    _fields_ = [
+        ("refine_seeds", C.c_int64),
+        ("refine_flips", C.c_int64),
+        ("refine_near", C.c_int64),
+        ("dist_tie_cut", C.c_int64),
+        ("dist_tie_cut_nmax", C.c_int64),
+        ("dist_tie_members", C.c_int64),
+    ]
+
+
 _lib = None
 
 
@@ -91,6 +102,9 @@ def lib():
         L.psod_oracle_run.argtypes = [P(_Params), C.c_int64, P(C.c_float), P(C.c_int64), C.c_int, P(_Result)]
         L.psod_oracle_spherover.argtypes = [
             P(_Params), C.c_int64, P(C.c_float), P(C.c_int64), P(C.c_int64), C.c_int64, C.c_int, P(_Result)
+        ]
+        L.psod_oracle_audit_spherover.argtypes = [
+            P(_Params), C.c_int64, P(C.c_float), P(C.c_int64), P(C.c_int64), C.c_int64, C.c_int, P(_Result), P(_Audit)
         ]
         L.psod_oracle_free.argtypes = [P(_Result)]
         _lib = L
@@ -261,3 +275,81 @@ def spherover(params: Params, pos, ids, isort, npart_new, mode=REFERENCE) -> Res
         return _collect(res, params)
     finally:
         lib().psod_oracle_free(C.byref(res))
+
+
+def audit_spherover(params: Params, pos, ids, isort, npart_new, mode=REFERENCE) -> tuple[Result, dict]:
+    """spherover in ``mode`` with the refinement evaluated in both
+    arithmetics side by side; returns the result and the audit counters."""
+    p = _as_pos(pos)
+    i = _as_ids(ids)
+    s = np.ascontiguousarray(isort, dtype=np.int64)
+    cp = params.c(p.shape[0])
+    res = _Result()
+    au = _Audit()
+    lib().psod_oracle_audit_spherover(
+        C.byref(cp), p.shape[0], _ptr(p, C.c_float), _ptr(i, C.c_int64), _ptr(s, C.c_int64), npart_new, mode,
+        C.byref(res), C.byref(au)
+    )
+    try:
+        return _collect(res, params), {f: int(getattr(au, f)) for f, _ in _Audit._fields_}
+    finally:
+        lib().psod_oracle_free(C.byref(res))
+
+
+def arithmetic_audit(params: Params, pos, ids) -> dict:
+    """Where the reference's FP64 arithmetic and quicksort tie orders and the
+    canonical arithmetic (int64 fixed point, index tie-breaks) of the GPU
+    part ways on one box, step by step:
+      rho_differ          particles whose rho differs (FP64 file-order sums vs
+                          fixed point; relative gaps ~1e-16)
+      seed_order_moved    seed ranks holding a different particle
+      seed_adjacent_swaps neighbouring seed pairs exchanged
+      seed_exact_ties     neighbouring seeds with exactly equal 1/rho (either
+                          arithmetic)
+      refine_*            from the reference run: seeds whose FP64-sum and
+                          fixed-point-sum argmax differ, seeds whose best two
+                          fixed-point sums are within 1e-9
+      dist_tie_*          crossings with exactly equal distances at the
+                          N_delta cut / among the members
+      halos_*             the two full runs compared halo by halo (matched by
+                          centre particle ID): halos in one run only, equal
+                          centres with a different N_delta, R_delta or member
+                          set."""
+    p = _as_pos(pos)
+    i = _as_ids(ids)
+    r_ref = rho(params, p, REFERENCE)
+    r_can = rho(params, p, CANONICAL)
+    s_ref, n_ref = tri_cic(r_ref, REFERENCE)
+    s_can, n_can = tri_cic(r_can, CANONICAL)
+    nn = min(n_ref, n_can)
+    moved = int(np.count_nonzero(s_ref[:nn] != s_can[:nn]))
+    swaps = int(np.count_nonzero((s_ref[: nn - 1] == s_can[1:nn]) & (s_ref[1:nn] == s_can[: nn - 1])))
+    pd_ref = 1.0 / r_ref[s_ref[:n_ref]]
+    pd_can = 1.0 / r_can[s_can[:n_can]]
+    ties = int(np.count_nonzero(pd_ref[1:] == pd_ref[:-1])) + int(np.count_nonzero(pd_can[1:] == pd_can[:-1]))
+    res_ref, au = audit_spherover(params, p, i, s_ref, n_ref, REFERENCE)
+    res_can = spherover(params, p, i, s_can, n_can, CANONICAL)
+    out = dict(rho_differ=int(np.count_nonzero(r_ref != r_can)),
+               rho_max_rel=float(np.max(np.abs(r_ref - r_can) / np.maximum(np.abs(r_ref), 1e-300))),
+               npart_new=(n_ref, n_can), seed_order_moved=moved, seed_adjacent_swaps=swaps, seed_exact_ties=ties,
+               refine_seeds=au["refine_seeds"], refine_flips=au["refine_flips"], refine_near=au["refine_near"],
+               dist_tie_cut=au["dist_tie_cut"], dist_tie_cut_nmax=au["dist_tie_cut_nmax"],
+               dist_tie_members=au["dist_tie_members"],
+               status=(res_ref.status, res_can.status), nhalo=(res_ref.nhalo, res_can.nhalo))
+    a = {int(h): k for k, h in enumerate(res_ref.halo_id)}
+    b = {int(h): k for k, h in enumerate(res_can.halo_id)}
+    only = len(set(a) ^ set(b))
+    dmass = drad = dset = 0
+    for h in set(a) & set(b):
+        x, y = a[h], b[h]
+        if res_ref.halo_mass[x] != res_can.halo_mass[y]:
+            dmass += 1
+        if res_ref.halo_rdelta[x] != res_can.halo_rdelta[y]:
+            drad += 1
+        mx = res_ref.member_index[res_ref.member_offset[x]: res_ref.member_offset[x + 1]]
+        my = res_can.member_index[res_can.member_offset[y]: res_can.member_offset[y + 1]]
+        if not np.array_equal(np.sort(mx), np.sort(my)):
+            dset += 1
+    out.update(halos_one_run_only=only, halos_mass_differ=dmass, halos_rdelta_differ=drad,
+               halos_members_differ=dset)
+    return out

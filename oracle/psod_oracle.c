@@ -447,11 +447,14 @@ static int64_t crossing_scan(const double *dist, int64_t npart_sel,
   return i;
 }
 
-int psod_oracle_spherover(const psod_oracle_params *p, int64_t n,
+/* spherover; when au is given, the arithmetic audit counters are filled
+ * along the way (see psod_oracle_audit_spherover). */
+static int spherover_impl(const psod_oracle_params *p, int64_t n,
                           const float *pos, const int64_t *ids,
                           const int64_t *isort, int64_t npart_new, int mode,
-                          psod_oracle_result *res) {
+                          psod_oracle_result *res, psod_oracle_audit *au) {
   memset(res, 0, sizeof(*res));
+  if (au) memset(au, 0, sizeof(*au));
   res->fail_rank = -1;
   res->npart_new = npart_new;
   zone_t z;
@@ -606,6 +609,10 @@ int psod_oracle_spherover(const psod_oracle_params *p, int64_t n,
     {
       double smax = 0.0;
       int64_t sqmax = 0;
+      /* audit: the argmax of each arithmetic over the same candidates in
+       * the same scan order, and the runner-up of the fixed-point sums */
+      double a_smax = 0.0;
+      int64_t a_sqmax = 0, a_sq2 = 0, a_cr = -1, a_cc = -1;
       for (int di = -1; di <= 1; di++) {
         int64_t ii = di + c0[0];
         if (ii >= nx) ii -= nx;
@@ -631,10 +638,23 @@ int psod_oracle_spherover(const psod_oracle_params *p, int64_t n,
                                   ycn, zcn, tx, tx, tx);
                 if (d2 <= rmin2) {
                   double t = 1.0 / sqrt(d2 + eps2); /* main:1854-1855 */
-                  if (mode == PSOD_ORACLE_CANONICAL)
+                  if (mode == PSOD_ORACLE_CANONICAL || au)
                     sq += (int64_t)llrint(t * FIX_ONE);
-                  else
+                  if (mode == PSOD_ORACLE_REFERENCE || au)
                     sum = sum + t;
+                }
+              }
+              if (au) {
+                if (sum > a_smax) {
+                  a_smax = sum;
+                  a_cr = q;
+                }
+                if (sq > a_sqmax) {
+                  a_sq2 = a_sqmax;
+                  a_sqmax = sq;
+                  a_cc = q;
+                } else if (sq > a_sq2) {
+                  a_sq2 = sq;
                 }
               }
               int better = (mode == PSOD_ORACLE_CANONICAL) ? (sq > sqmax)
@@ -651,6 +671,11 @@ int psod_oracle_spherover(const psod_oracle_params *p, int64_t n,
             }
           }
         }
+      }
+      if (au) {
+        au->refine_seeds++;
+        if (a_cr != a_cc) au->refine_flips++;
+        if (a_sqmax > 0 && (double)(a_sqmax - a_sq2) < 1e-9 * (double)a_sqmax) au->refine_near++;
       }
     }
 
@@ -682,6 +707,19 @@ int psod_oracle_spherover(const psod_oracle_params *p, int64_t n,
     }
     const double rayon = sqrt(dist.v[i - 2]); /* distance(i-1), 1-based */
     const int64_t masse = i - 1;
+    if (au) {
+      /* the masse-th and (masse+1)-th sorted distances equal: which of the
+       * tied particles become members depends on the sort's tie order */
+      if (masse < npart_sel && dist.v[masse - 1] == dist.v[masse]) {
+        au->dist_tie_cut++;
+        if (masse > au->dist_tie_cut_nmax) au->dist_tie_cut_nmax = masse;
+      }
+      for (int64_t k = 1; k < masse; k++)
+        if (dist.v[k - 1] == dist.v[k]) {
+          au->dist_tie_members++;
+          break;
+        }
+    }
     /* algorithmic reads: the cells meeting the ball out to the stopping
      * particle (the i-th, 1-based) */
     res->cross_touch += ball_touch(num, nx, p->ncut, c0, xc, yc, zc, xxmin * scale, sqrt(dist.v[i - 1]));
@@ -769,6 +807,21 @@ int psod_oracle_spherover(const psod_oracle_params *p, int64_t n,
   free(cell_of);
   free(pg);
   return status;
+}
+
+int psod_oracle_spherover(const psod_oracle_params *p, int64_t n,
+                          const float *pos, const int64_t *ids,
+                          const int64_t *isort, int64_t npart_new, int mode,
+                          psod_oracle_result *res) {
+  return spherover_impl(p, n, pos, ids, isort, npart_new, mode, res, NULL);
+}
+
+int psod_oracle_audit_spherover(const psod_oracle_params *p, int64_t n,
+                                const float *pos, const int64_t *ids,
+                                const int64_t *isort, int64_t npart_new,
+                                int mode, psod_oracle_result *res,
+                                psod_oracle_audit *au) {
+  return spherover_impl(p, n, pos, ids, isort, npart_new, mode, res, au);
 }
 
 int psod_oracle_run(const psod_oracle_params *p, int64_t n, const float *pos,

@@ -123,6 +123,32 @@ int psod_oracle_spherover(const psod_oracle_params *p, int64_t n,
                           const int64_t *isort, int64_t npart_new, int mode,
                           psod_oracle_result *res);
 
+/* Arithmetic audit of one spherover run: how often the reference's FP64
+ * arithmetic and the canonical fixed-point arithmetic would decide a step
+ * differently on the same inputs. */
+typedef struct psod_oracle_audit {
+  int64_t refine_seeds;     /* seeds that ran the centre refinement */
+  int64_t refine_flips;     /* seeds whose FP64-sum argmax (main:1851-1875)
+                               and fixed-point-sum argmax differ */
+  int64_t refine_near;      /* seeds whose two largest fixed-point sums are
+                               within 1e-9 relative */
+  int64_t dist_tie_cut;     /* crossings whose N_Delta-th and next sorted
+                               distances are exactly equal */
+  int64_t dist_tie_cut_nmax; /* the largest N_Delta among those: below 10
+                               whenever the loop's monotonicity holds */
+  int64_t dist_tie_members; /* crossings with an exact distance tie among
+                               the members */
+} psod_oracle_audit;
+
+/* spherover (as psod_oracle_spherover, same outputs for the given mode)
+ * with both arithmetics of the centre refinement evaluated side by side and
+ * the audit counters filled. */
+int psod_oracle_audit_spherover(const psod_oracle_params *p, int64_t n,
+                                const float *pos, const int64_t *ids,
+                                const int64_t *isort, int64_t npart_new,
+                                int mode, psod_oracle_result *res,
+                                psod_oracle_audit *au);
+
 void psod_oracle_free(psod_oracle_result *res);
 
 /* Fixed-point scale of the canonical CIC and refinement sums. */

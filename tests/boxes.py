@@ -118,3 +118,48 @@ def ref_d2(pos_box: np.ndarray, nx: int, centre_idx: int) -> np.ndarray:
     d = np.abs(pg - c)
     d = np.minimum(d, nx - d)
     return (d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]
+
+
+def shell_ball_points(centre, core_h, core_r, outer_h, outer_r):
+    """Points on two nested cubic lattices around ``centre`` (grid units): a
+    fine core (spacing ``core_h`` cells, radius ``core_r``) and a coarser
+    shell region (spacing ``outer_h``, out to ``outer_r``).  With the centre
+    and both spacings powers of two fractions of a cell, every coordinate
+    and every squared distance to the centre is exact in float32 / FP64, so
+    whole shells of points lie at exactly equal distances."""
+    pts = [np.zeros((1, 3))]
+    for h, r0, r1 in ((core_h, 0.0, core_r), (outer_h, core_r, outer_r)):
+        m = int(np.floor(r1 / h))
+        g = np.arange(-m, m + 1, dtype=np.float64) * h
+        zz, yy, xx = np.meshgrid(g, g, g, indexing="ij")
+        p = np.stack([xx, yy, zz], -1).reshape(-1, 3)
+        d2 = (p * p).sum(1)
+        pts.append(p[(d2 > r0 * r0) & (d2 <= r1 * r1)])
+    return np.asarray(centre, np.float64) + np.unique(np.concatenate(pts), axis=0)
+
+
+def tie_ball_box(nx: int, centres, r_hole: float = 3.6, core_h=1 / 32, core_r=0.1, outer_h=1 / 8, outer_r=0.45):
+    """A cell-centred lattice with holes of radius ``r_hole`` around each
+    centre, each hole holding the same exact-lattice ball
+    (``shell_ball_points``).  Particles are listed lattice first, then the
+    balls one after the other in the same order, so that translated copies
+    deposit identical CIC contributions in the same order and their
+    particles get exactly equal densities in both arithmetics.  Returns
+    (pos float32 box units, ids int64, per-ball index arrays)."""
+    lat = lattice_points(nx)
+    keep = np.ones(lat.shape[0], bool)
+    for c in centres:
+        d = lat - np.asarray(c, np.float64)
+        d -= nx * np.round(d / nx)
+        keep &= (d * d).sum(1) > r_hole * r_hole
+    parts = [lat[keep]]
+    balls = []
+    start = int(keep.sum())
+    for c in centres:
+        b = shell_ball_points(c, core_h, core_r, outer_h, outer_r)
+        parts.append(b)
+        balls.append(np.arange(start, start + b.shape[0]))
+        start += b.shape[0]
+    pos = _wrap_f32(np.concatenate(parts, 0), nx)
+    ids = np.arange(pos.shape[0], dtype=np.int64) * 7 + 11
+    return pos, ids, balls

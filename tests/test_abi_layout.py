@@ -23,6 +23,7 @@ PAIRS = [
     ("psod_train_params", capi.TrainParams, "psod.h"),
     ("psod_oracle_params", O._Params, "psod_oracle.h"),
     ("psod_oracle_result", O._Result, "psod_oracle.h"),
+    ("psod_oracle_audit", O._Audit, "psod_oracle.h"),
 ]
 
 

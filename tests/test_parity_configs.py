@@ -1,0 +1,100 @@
+"""GPU parity at the configuration-1 size: the whole 128^3 box (2,097,152
+particles, halo N in [20, 2e4], -nx 128 -min 100 -del 200, 32 profile bins
+over [0.01, 2] R_delta) through the C-ABI in the plain, batched and learned
+modes, against the oracle.
+
+Every output is bit-identical to the oracle's canonical arithmetic.  On
+this box the reference's own arithmetic makes the same decisions at every
+step (tests/test_ties_and_audit.py counts them on the CPU), so every output
+is also identical to the oracle's reference-arithmetic run: same seed
+ranks, centres, N_delta, R_delta, profiles and member lists in the same
+order.  Also a box built of exact ties, where only the order of members at
+equal distance may differ from the reference's quicksort order.
+"""
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("no CUDA device", allow_module_level=True)
+
+from psod_b200 import synth  # noqa: E402
+from psod_b200.sod import SphericalOverdensity  # noqa: E402
+from tests.boxes import tie_ball_box  # noqa: E402
+
+CFG1 = dict(nbins=32, rbin_lo=0.01, rbin_hi=2.0)
+FIELDS = ("halo_id", "halo_mass", "halo_rank", "halo_center", "halo_rdelta", "halo_mass2", "halo_profile",
+          "member_offset", "member_index")
+
+
+@pytest.fixture(scope="module")
+def cfg1_box():
+    b = synth.make_box(128, nmax_halo=20000, seed=20261203)
+    return b.pos.numpy(), b.ids.numpy()
+
+
+@pytest.fixture(scope="module")
+def cfg1_oracle(oracle, cfg1_box):
+    pos, ids = cfg1_box
+    p = oracle.Params(nx=128, **CFG1)
+    return oracle.run(p, pos, ids, oracle.CANONICAL), oracle.run(p, pos, ids, oracle.REFERENCE)
+
+
+def _model(pos, ids):
+    """A bracket network trained on this box's batched-mode samples (the
+    halo table never depends on the model, only the crossing's first ball)."""
+    with SphericalOverdensity(128, mode=1, **CFG1) as s:
+        s.learn_collect(1 << 20)
+        s.load(pos, ids)
+        s.run()
+        s.learn_train(epochs=5, batch=256, lr=1e-3, seed=3)
+        return s.learn_get_model()
+
+
+@pytest.mark.parametrize("mode", [0, 1, 2])
+def test_configuration_1_box_all_modes(cfg1_box, cfg1_oracle, mode):
+    pos, ids = cfg1_box
+    rc, rr = cfg1_oracle
+    assert rc.status == rr.status == 0 and rc.nhalo > 900
+    with SphericalOverdensity(128, mode=mode, **CFG1) as s:
+        if mode == 2:
+            s.learn_set_model(_model(pos, ids))
+        s.load(pos, ids)
+        s.cic()
+        rho = s.cicm1()
+        isort, nn = s.tri_cic()
+        st = s.spherover()
+        t = s.halos()
+    assert nn == rc.npart_new == rr.npart_new
+    assert st["nprocessed"] == rc.nprocessed
+    assert st["cross_touch"] == rc.cross_touch
+    for r in (rc, rr):
+        for f in FIELDS:
+            assert np.array_equal(getattr(t, f), getattr(r, f)), f
+    assert np.array_equal(t.member_id, ids[t.member_index])
+    assert np.all(rho > 0)
+
+
+def test_exact_tie_box_against_both_arithmetics(oracle):
+    pos, ids, balls = tie_ball_box(32, [(15.5, 15.5, 15.5), (31.5, 15.5, 15.5)])
+    p = oracle.Params(nx=32, delta=1000.0, nmin=10)
+    rc = oracle.run(p, pos, ids, oracle.CANONICAL)
+    rr = oracle.run(p, pos, ids, oracle.REFERENCE)
+    for mode in (0, 1):
+        with SphericalOverdensity(32, delta=1000.0, nmin=10, mode=mode) as s:
+            s.load(pos, ids)
+            s.run()
+            t = s.halos()
+        for f in FIELDS:
+            assert np.array_equal(getattr(t, f), getattr(rc, f)), f
+        # the reference's arithmetic: the same halos, masses, radii and member
+        # sets; members at equal distance may be listed in another order
+        for f in ("halo_id", "halo_mass", "halo_rdelta", "halo_profile", "member_offset"):
+            assert np.array_equal(getattr(t, f), getattr(rr, f)), f
+        for h in range(t.nhalo):
+            a = t.member_index[t.member_offset[h] : t.member_offset[h + 1]]
+            b = rr.member_index[rr.member_offset[h] : rr.member_offset[h + 1]]
+            assert np.array_equal(np.sort(a), np.sort(b))
