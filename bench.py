@@ -90,13 +90,13 @@ def table_digest(sod, members):
     nb, ne = sod.params.nbins, sod.params.ndelta_extra
     dev = f"cuda:{torch.cuda.current_device()}"
     sizes = dict(halo_id=h, halo_mass=h, halo_rank=h, halo_center=3 * h, halo_rdelta=h, halo_mass2=h,
-                 halo_mextra=h * ne, halo_profile=h * nb, member_offset=h + 1, member_index=m, member_id=0)
+                 halo_mextra=h * ne, halo_profile=h * nb, member_offset=h + 1, member_index=m, member_id=m)
     dt = dict(halo_center=torch.float32, halo_rdelta=torch.float64)
     out = HaloTable(**{f: torch.zeros(max(1, k), dtype=dt.get(f, torch.int64), device=dev) for f, k in sizes.items()})
     t = sod.halos(members=True, out=out)
     acc = 0
     for k, f in enumerate(("halo_id", "halo_mass", "halo_rank", "halo_center", "halo_rdelta", "halo_mass2",
-                           "halo_mextra", "halo_profile", "member_offset", "member_index")):
+                           "halo_mextra", "halo_profile", "member_offset", "member_index", "member_id")):
         a = getattr(t, f).reshape(-1)
         if a.numel() == 0:
             continue

@@ -46,6 +46,14 @@ int copy_out(psod_ctx *c, void *dst, const void *dsrc, size_t bytes) {
   return PSOD_OK;
 }
 
+int wait_ids(psod_ctx *c) {
+  if (c->ids_pending) {
+    PSOD_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_ids, 0));
+    c->ids_pending = false;
+  }
+  return PSOD_OK;
+}
+
 int copy_in(psod_ctx *c, void *ddst, const void *src, size_t bytes) {
   if (bytes == 0) return PSOD_OK;
   PSOD_CUDA(c, cudaMemcpyAsync(ddst, src, bytes, cudaMemcpyDefault, c->stream));
@@ -182,7 +190,11 @@ int psod_ctx_destroy(psod_ctx *c) {
   if (!c) return PSOD_OK;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->side_stream) cudaStreamSynchronize(c->side_stream);
   free_all(c);
+  if (c->side_stream) cudaStreamDestroy(c->side_stream);
+  if (c->ev_pos) cudaEventDestroy(c->ev_pos);
+  if (c->ev_ids) cudaEventDestroy(c->ev_ids);
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return PSOD_OK;
@@ -191,6 +203,12 @@ int psod_ctx_destroy(psod_ctx *c) {
 int psod_set_stream(psod_ctx *c, void *stream) {
   if (!c) return PSOD_ERR_ARG;
   cudaSetDevice(c->device);
+  // a pending ID copy is ordered before the new stream's work
+  if (c->ids_pending) {
+    if (cudaStreamWaitEvent((cudaStream_t)stream, c->ev_ids, 0) != cudaSuccess)
+      return cuda_check(c, cudaGetLastError(), "cudaStreamWaitEvent");
+    c->ids_pending = false;
+  }
   if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
   c->stream = (cudaStream_t)stream;
   c->own_stream = false;
@@ -219,15 +237,38 @@ int psod_load_particles(psod_ctx *c, int64_t n, const float *pos, const float *v
     dpos = c->d_pos;
   }
   if (!c->d_ids || c->ids_cap < n) {
+    if ((st = wait_ids(c))) return st;  // the old buffer may still be a copy's target
     if ((st = dalloc(c, &c->d_ids, (size_t)n))) return st;
     c->ids_cap = n;
   }
-  if ((st = copy_in(c, c->d_ids, id, sizeof(int64_t) * n))) return st;
   if (vel) {
+    if ((st = wait_ids(c))) return st;
     if ((st = scratch(c, SLOT_VEL, (size_t)n * 3, &c->d_vel))) return st;
-    if ((st = copy_in(c, c->d_vel, vel, sizeof(float) * 3 * n))) return st;
   } else {
     c->d_vel = nullptr;
+  }
+  // IDs and velocities are first read by spherover (halo records): host
+  // arrays go over on a side stream after the positions, so their copy
+  // overlaps the cell sort, the CIC and the seed order.  The side stream
+  // first waits for the context's stream, which may still read the previous
+  // IDs; spherover and psod_get_halos wait for the copy.
+  const bool side = !is_device_ptr(id) || (vel && !is_device_ptr(vel));
+  if (side) {
+    if (!c->side_stream) {
+      PSOD_CUDA(c, cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking));
+      PSOD_CUDA(c, cudaEventCreateWithFlags(&c->ev_pos, cudaEventDisableTiming));
+      PSOD_CUDA(c, cudaEventCreateWithFlags(&c->ev_ids, cudaEventDisableTiming));
+    }
+    if ((st = wait_ids(c))) return st;
+    PSOD_CUDA(c, cudaEventRecord(c->ev_pos, c->stream));
+    PSOD_CUDA(c, cudaStreamWaitEvent(c->side_stream, c->ev_pos, 0));
+    PSOD_CUDA(c, cudaMemcpyAsync(c->d_ids, id, sizeof(int64_t) * n, cudaMemcpyDefault, c->side_stream));
+    if (vel) PSOD_CUDA(c, cudaMemcpyAsync(c->d_vel, vel, sizeof(float) * 3 * n, cudaMemcpyDefault, c->side_stream));
+    PSOD_CUDA(c, cudaEventRecord(c->ev_ids, c->side_stream));
+    c->ids_pending = true;
+  } else {
+    if ((st = copy_in(c, c->d_ids, id, sizeof(int64_t) * n))) return st;
+    if (vel && (st = copy_in(c, c->d_vel, vel, sizeof(float) * 3 * n))) return st;
   }
   return stage_cellsort(c, dpos);
 }
@@ -290,6 +331,8 @@ int psod_get_halos(psod_ctx *c, const psod_halo_table *t) {
   if (!c || !t) return PSOD_ERR_ARG;
   if (!c->sod_done) return set_err(c, PSOD_ERR_STATE, "no halo table: call psod_spherover first");
   cudaSetDevice(c->device);
+  int wst = wait_ids(c);
+  if (wst) return wst;
   const long long nh = c->nhalo, nm = c->nmember;
   int st;
   if (t->halo_id && (st = copy_out(c, t->halo_id, c->d_h_id, sizeof(int64_t) * nh))) return st;

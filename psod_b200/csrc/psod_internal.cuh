@@ -134,6 +134,11 @@ struct psod_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // host IDs and velocities are copied on a side stream (they are first
+  // read by spherover); ev_ids marks that copy's end
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_pos = nullptr, ev_ids = nullptr;
+  bool ids_pending = false;
   std::string err;
 
   // particles
@@ -299,6 +304,8 @@ void learn_sample_buffers(const psod_ctx *c, float **x, float **t, unsigned long
 int learn_predict(psod_ctx *c, const float *feat, unsigned n, float *rb0);
 
 bool is_device_ptr(const void *p);
+// make the context's stream wait for a pending side-stream copy of the IDs
+int wait_ids(psod_ctx *c);
 int copy_out(psod_ctx *c, void *dst, const void *dsrc, size_t bytes);
 int copy_in(psod_ctx *c, void *ddst, const void *src, size_t bytes);
 

@@ -2852,6 +2852,10 @@ struct PhaseTimer {
 
 int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   if (!c->seeds_done) return set_err(c, PSOD_ERR_STATE, "psod_spherover needs psod_tri_cic first");
+  {
+    const int wst = wait_ids(c);  // the halo records read the particle IDs
+    if (wst) return wst;
+  }
   psod_run_stats st{};
   st.fail_rank = -1;
   st.npart_new = c->npart_new;
