@@ -215,6 +215,24 @@ int psod_write_masst(const char *path, const psod_halo_table *t, int64_t nhalo);
 int psod_write_strct(const char *path, const psod_halo_table *t, int64_t nhalo, int64_t n, const float *pos,
                      const float *vel, const int64_t *id, const float *pot, const float *force);
 
+/* The reference's binary particle reader (main:455-534), host-only: the
+ * zone's particles from the FoF step's cube files "<root>_cube_NNNNN", each
+ * Fortran unformatted sequential records of nloc (int32), the writer's rank
+ * (int32), the cube bounds (6 float32), positions (3*nloc float32, box
+ * units), velocities (3*nloc float32) and IDs (nloc int64; int32 when
+ * id_bytes = 4, a build without LONGINT).  ncpu = nxcpu^3 cubes; zone nzone
+ * (0-based, x-major) reads the 27 cubes around it in the reference's order
+ * (x outer, z inner, periodic) and keeps, in file order, the particles
+ * within the zone plus nxbuffer cells (0 means half the zone, main:380-381)
+ * by the reference's FP64 distance test (main:471-479).  With fewer than 3
+ * cubes a side the reference lists some cubes twice and loads their
+ * particles twice; each distinct cube is read once here.  Call with
+ * pos == NULL to get *npart, then with arrays of at least *npart entries
+ * (capacity); vel may be NULL.  Returns PSOD_ERR_IO for a missing or
+ * malformed file, PSOD_ERR_ARG for bad arguments or a short capacity. */
+int psod_read_cube_zone(const char *root, int32_t ncpu, int32_t nzone, int32_t nx, int32_t nxbuffer, int32_t id_bytes,
+                        int64_t capacity, int64_t *npart, float *pos, float *vel, int64_t *id);
+
 /* CIC density (cic + cicm1, the same fixed-point arithmetic) for a zone of
  * at most 64 cells per side, without any device allocation.  This entry
  * point has no counterpart in the reference.  It is for host codes that

@@ -149,5 +149,16 @@ module psod_gpu
        integer(c_int64_t), value :: nhalo, n
        type(c_ptr), value :: pos, vel, id, pot, force
      end function
+     ! the zone's particles from the binary cube files (main:455-534):
+     ! first with pos = c_null_ptr for the count, then with posf/velf/idf
+     integer(c_int) function psod_read_cube_zone(root, ncpu, nzone, nx, nxbuffer, id_bytes, capacity, &
+          npart, pos, vel, id) bind(C, name="psod_read_cube_zone")
+       import :: c_int, c_char, c_int32_t, c_int64_t, c_ptr
+       character(kind=c_char), dimension(*), intent(in) :: root
+       integer(c_int32_t), value :: ncpu, nzone, nx, nxbuffer, id_bytes
+       integer(c_int64_t), value :: capacity
+       integer(c_int64_t), intent(out) :: npart
+       type(c_ptr), value :: pos, vel, id
+     end function
   end interface
 end module psod_gpu

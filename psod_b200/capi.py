@@ -130,6 +130,7 @@ EXPORTS = [
     "psod_learn_gradient",
     "psod_write_masst",
     "psod_write_strct",
+    "psod_read_cube_zone",
 ]
 
 LEARN_FEATURES = 10
@@ -186,6 +187,8 @@ def load(build_if_missing: bool = True):
     L.psod_get_halos.argtypes = [vp, P(HaloTable)]
     L.psod_write_masst.argtypes = [C.c_char_p, P(HaloTable), C.c_int64]
     L.psod_write_strct.argtypes = [C.c_char_p, P(HaloTable), C.c_int64, C.c_int64, vp, vp, vp, vp, vp]
+    L.psod_read_cube_zone.argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64,
+                                      P(C.c_int64), vp, vp, vp]
     L.psod_last_error.argtypes = [vp]
     L.psod_cic_rho_static.argtypes = [C.c_int64, vp, C.c_int32, C.c_int64, C.c_int32, vp, vp, vp]
     L.psod_learn_collect.argtypes = [vp, C.c_int64]

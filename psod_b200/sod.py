@@ -307,3 +307,24 @@ def _contig(x, dtype):
     if isinstance(x, torch.Tensor):
         return x.to(dtype).contiguous()
     return np.ascontiguousarray(x, dtype=torch.empty(0, dtype=dtype).numpy().dtype)
+
+
+def read_cube_zone(root: str, ncpu: int, nzone: int, nx: int, nxbuffer: int = 0, id_bytes: int = 8):
+    """The reference's binary particle reader (main:455-534): the particles
+    of zone ``nzone`` from the cube files ``<root>_cube_NNNNN`` of an
+    ``ncpu``-cube decomposition, as (pos (n, 3) float32 box units, vel (n, 3)
+    float32, ids int64) in the reference's order, ready for ``load``."""
+    lib = capi.load()
+    n = C.c_int64(0)
+    st = lib.psod_read_cube_zone(str(root).encode(), ncpu, nzone, nx, nxbuffer, id_bytes, 0, C.byref(n), None, None,
+                                 None)
+    if st != capi.OK:
+        raise PsodError(st, f"psod_read_cube_zone({root}, zone {nzone}) failed")
+    pos = np.zeros((max(n.value, 1), 3), np.float32)
+    vel = np.zeros((max(n.value, 1), 3), np.float32)
+    ids = np.zeros(max(n.value, 1), np.int64)
+    st = lib.psod_read_cube_zone(str(root).encode(), ncpu, nzone, nx, nxbuffer, id_bytes, pos.shape[0], C.byref(n),
+                                 _ptr(pos), _ptr(vel), _ptr(ids))
+    if st != capi.OK:
+        raise PsodError(st, f"psod_read_cube_zone({root}, zone {nzone}) failed")
+    return pos[: n.value], vel[: n.value], ids[: n.value]
