@@ -290,10 +290,12 @@ def run_ours(args):
 
     s = stats_list[-1]
     peak, peak_kind = load_peaks()
-    # Gather/distance kernel (k_cross): HBM-bound.  Algorithmic bytes: 16 B
-    # per record of the cube cells meeting each ball out to its stopping
-    # particle, plus 12 B per member written (d2 key + index).
-    alg_bytes = 16.0 * s["cross_touch"] + 12.0 * s["nmember"]
+    # Gather/distance kernel (k_cross and its warp form, the rounds the host
+    # launches): HBM-bound.  Algorithmic bytes: 16 B per record of the cube
+    # cells meeting each ball out to its stopping particle, plus 12 B per
+    # member written (d2 key + index).  The device tail loop's crossings are
+    # counted apart (they share a launch with the refinement).
+    alg_bytes = 16.0 * (s["cross_touch"] - s["tail_touch"]) + 12.0 * s["cross_members"]
     cross_s = s["ms_cross"] / 1000.0
     achieved = alg_bytes / cross_s / 1e9 if cross_s > 0 else 0.0
     launches = max(1, s["rounds"])
@@ -340,7 +342,8 @@ def run_ours(args):
             "rounds": s["rounds"],
             "stage_ms": {k: round(v, 2) for k, v in stage_ms.items()},
             "sod_phase_ms": {k: round(s[k], 2) for k in ("ms_setup", "ms_sched", "ms_prep", "ms_refine", "ms_select",
-                                                         "ms_cross", "ms_output")},
+                                                         "ms_cross", "ms_tail", "ms_output")},
+            "tail_rounds": s["tail_rounds"],
         },
         "e2e": {
             "value": round(nhalo_all / (e2e_ms / 1000.0), 2),
@@ -464,7 +467,8 @@ def mode_reference(nx, params, pos_d, ids_d, sod, mode):
     out = {"mode": {0: "plain", 1: "batched"}[mode], "ms_per_step": round(msp, 3), "halos": st["nhalo"],
            "value": round(st["nhalo"] / (msp / 1000.0), 2), "unit": "halos/s",
            "sod_phase_ms": {k: round(st[k], 2) for k in ("ms_setup", "ms_sched", "ms_prep", "ms_refine", "ms_select",
-                                                         "ms_cross", "ms_output")}, "digest": digest}
+                                                         "ms_cross", "ms_tail", "ms_output")}, "digest": digest,
+           "tail_rounds": st["tail_rounds"]}
     if mode == 1:
         out.update(hit_rate=round(st["bracket_hits"] / max(1, st["bracket_seeds"]), 4),
                    cross_balls=int(st["cross_balls"]), cross_records=int(st["cross_records"]))

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define PSOD_ABI_VERSION 1
+#define PSOD_ABI_VERSION 2
 #define PSOD_MAX_EXTRA_DELTA 4
 
 typedef enum psod_status {
@@ -138,6 +138,11 @@ typedef struct psod_run_stats {
   double ms_refine_bound; /* refinement bound pass (part of ms_refine) */
   int64_t refine_items;   /* refinement work items summed (64 candidates x one record chunk) */
   int64_t refine_pruned;  /* refinement candidates not summed: their bound is below the best lower bound */
+  double ms_tail;         /* device tail loop (late rounds run by one cooperative launch) */
+  int64_t tail_rounds;    /* rounds run by the device tail loop (part of rounds) */
+  int64_t tail_touch;     /* part of cross_touch from the tail loop's crossings */
+  int64_t cross_members;  /* members of kept halos written by the crossing kernels (k_cross, k_cross_warp) */
+  int64_t tail_members;   /* members of kept halos written by the tail loop */
 } psod_run_stats;
 
 typedef struct psod_ctx psod_ctx;

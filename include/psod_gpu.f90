@@ -50,6 +50,8 @@ module psod_gpu
      integer(c_int64_t) :: bracket_hits, bracket_seeds, cross_balls, cross_records
      real(c_double) :: ms_refine_bound
      integer(c_int64_t) :: refine_items, refine_pruned
+     real(c_double) :: ms_tail
+     integer(c_int64_t) :: tail_rounds, tail_touch, cross_members, tail_members
   end type psod_run_stats
 
   type, bind(C) :: psod_train_params

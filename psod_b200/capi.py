@@ -97,6 +97,11 @@ class RunStats(C.Structure):
         ("ms_refine_bound", C.c_double),
         ("refine_items", C.c_int64),
         ("refine_pruned", C.c_int64),
+        ("ms_tail", C.c_double),
+        ("tail_rounds", C.c_int64),
+        ("tail_touch", C.c_int64),
+        ("cross_members", C.c_int64),
+        ("tail_members", C.c_int64),
     ]
 
     def as_dict(self):

@@ -44,6 +44,11 @@ constexpr int L1_SHIFT = 45;
 
 enum { ERR_NONE = 0 };
 
+// Seeds with fewer refinement candidates than this are neither bounded nor
+// pruned: their pair work is small and the bound pass would cost as much as
+// it saves.
+constexpr unsigned BOUND_MIN_CAND = 4096;
+
 struct SodBufs {
   float4 *cube;
   const unsigned *cs;        // cell_start
@@ -80,9 +85,14 @@ struct SodBufs {
   double *cand_s;       // approximate refinement sum
   unsigned *cand_used;  // allocator
   unsigned *work;       // [4] work-stealing counters: prep, refine, select, cross
+  unsigned *nbig;       // seeds of this round with BOUND_MIN_CAND candidates or more
+  unsigned *maxcand;    // largest candidate count of a seed this round (or null)
+  unsigned max_cand;    // seeds with more candidates wait (device tail loop), else ~0u
+  unsigned *deferred;   // set when a seed waited for that reason
   unsigned *alive_cnt;  // alive records per cell (batched modes)
   unsigned long long *pairs;       // candidate-neighbour records visited
   unsigned long long *touch;       // records of the balls out to each stop
+  unsigned long long *kept_members; // members of the kept halos written
   unsigned long long *pair_slots;  // lane slots spent on pair tests
   unsigned long long *ncand_total; // candidates over all rounds
   // refinement work: per (ready slot, candidate cell) counts, offsets into
@@ -128,6 +138,12 @@ struct SodBufs {
   // processed or claimed; list position of each rank and of each cube slot
   // (~0 for particles that are not seeds)
   unsigned *resolved, *bidx_of_rank, *bidx_of_cube;
+  // crossing buffer: the entries (d2 bits, input index, cube slot) of large
+  // balls, bucketed by their level-0 histogram bucket, one slice per seed;
+  // xused allocates the slices of a round
+  unsigned long long *xkey;
+  unsigned *xidx, *xpos;
+  unsigned long long *xused, xcap;
 };
 
 __device__ __forceinline__ void mark_resolved(const SodBufs &B, unsigned bi) {
@@ -162,6 +178,7 @@ struct Smem {
   unsigned best_pos;
   unsigned nsorted;
   unsigned long long pool_base;
+  unsigned long long xbase;  // the seed's slice of the crossing buffer (bucketed ball)
   unsigned claim_cnt;
   // last radial_search hit: sorted-buffer index and bucket lower bound
   int res_k;
@@ -285,7 +302,7 @@ __device__ __forceinline__ void for_region(const SodConst &K, const SodBufs &B, 
 // Records filed under the region's cells (alive or not), from the cell
 // offsets alone (no record loads).  For the ball out to the stopping
 // particle this is the algorithmic read volume of the crossing search.
-__device__ unsigned region_records(const SodConst &K, const SodBufs &B, const Region &G) {
+__device__ __forceinline__ unsigned region_records(const SodConst &K, const SodBufs &B, const Region &G) {
   const int R = K.ncut, side = 2 * R + 1, nrow = side * side;
   const unsigned nx = (unsigned)K.nx;
   const double nxd = (double)K.nx;
@@ -382,7 +399,7 @@ __device__ __forceinline__ void block_max_pair(Smem &S, unsigned long long &a, u
 }
 
 // block exclusive scan over S.hist[l] into S.pref (NB = 16 per thread)
-__device__ void hist_prefix(Smem &S, int l) {
+__device__ __forceinline__ void hist_prefix(Smem &S, int l) {
   const int t = threadIdx.x;
   unsigned v[NB / TPB];
   unsigned s = 0;
@@ -451,43 +468,78 @@ __device__ __forceinline__ bool keeps_going(const SodConst &K, long long i, doub
   return ovd > delta && i < na && r < (double)K.ncut;
 }
 
-// fill S.hist[l] with the bucket counts of alive records whose d2 bits lie
-// in [lo, hi]
-__device__ void build_hist(const SodConst &K, const SodBufs &B, Smem &S, int l, const Region &G) {
+// Entry sources of the crossing searches: (d2 bits, input index, cube slot)
+// of the alive records of a region, computed from the records as they are
+// walked, or a contiguous slice of the seed's bucketed crossing buffer
+// (written once per ball by scatter_ball).
+struct RegionSrc {
+  const Region &g;
+  template <typename F>
+  __device__ __forceinline__ void each(const SodConst &K, const SodBufs &B, F &&f) const {
+    for_region(K, B, g, [&](unsigned p, float4 v) {
+      double d2;
+      if (!region_d2(K, g, v, d2)) return;
+      f(dbits(d2), __float_as_uint(v.w) & PSOD_IDX_MASK, p);
+    });
+  }
+};
+
+struct BufSrc {
+  unsigned long long lo, hi;  // entries [lo, hi) of the crossing buffer
+  template <typename F>
+  __device__ __forceinline__ void each(const SodConst &K, const SodBufs &B, F &&f) const {
+    for (unsigned long long e = lo + threadIdx.x; e < hi; e += TPB) f(B.xkey[e], B.xidx[e], B.xpos[e]);
+  }
+};
+
+// fill S.hist[l] with the bucket counts of the source's entries whose d2
+// bits lie in the level's range (level 0: all)
+template <class Src>
+__device__ __forceinline__ void build_hist(const SodConst &K, const SodBufs &B, Smem &S, int l, const Src &src) {
   for (int k = threadIdx.x; k < NB; k += TPB) S.hist[l][k] = 0;
   __syncthreads();
   const Level L = S.lev[l];
-  unsigned inball = 0;
-  for_region(K, B, G, [&](unsigned p, float4 v) {
-    double d2;
-    if (!region_d2(K, G, v, d2)) return;
-    inball++;
-    unsigned long long x = dbits(d2);
+  src.each(K, B, [&](unsigned long long x, unsigned, unsigned) {
     if (l > 0 && (x < L.lo || x > L.hi)) return;
     atomicAdd(&S.hist[l][bucket_of(L, l, x)], 1u);
   });
   __syncthreads();
-  if (l == 0) {
-    const unsigned tot = block_sum_u32(S, inball);
-    if (threadIdx.x == 0) atomicAdd(B.cross_records, (unsigned long long)tot);
-  }
 }
 
-// load alive records with d2 bits in [lo, hi] into S.skey/S.sidx, sort them
-// by (bits, input index); returns the count
-__device__ unsigned extract_sorted(const SodConst &K, const SodBufs &B, Smem &S, const Region &G,
+// level-0 histogram of a ball's alive records (one region walk); returns
+// the ball's entry count and adds it to the ball-record statistic
+__device__ __forceinline__ unsigned ball_hist0(const SodConst &K, const SodBufs &B, Smem &S, const Region &G) {
+  if (threadIdx.x == 0) {
+    S.lev[0].lo = 0;
+    S.lev[0].hi = 0x7fefffffffffffffull;
+    S.lev[0].shift = L1_SHIFT;
+  }
+  for (int k = threadIdx.x; k < NB; k += TPB) S.hist[0][k] = 0;
+  __syncthreads();
+  unsigned inball = 0;
+  RegionSrc{G}.each(K, B, [&](unsigned long long x, unsigned, unsigned) {
+    inball++;
+    atomicAdd(&S.hist[0][bucket_of(S.lev[0], 0, x)], 1u);
+  });
+  __syncthreads();
+  const unsigned tot = block_sum_u32(S, inball);
+  if (threadIdx.x == 0) atomicAdd(B.cross_records, (unsigned long long)tot);
+  return tot;
+}
+
+// load the source's entries with d2 bits in [lo, hi] into S.skey/S.sidx and
+// sort them by (bits, input index); returns the count
+template <class Src>
+__device__ __forceinline__ unsigned extract_sorted(const SodConst &K, const SodBufs &B, Smem &S, const Src &src,
                                    unsigned long long lo, unsigned long long hi) {
   if (threadIdx.x == 0) S.nsorted = 0;
   __syncthreads();
-  for_region(K, B, G, [&](unsigned p, float4 v) {
-    double d2;
-    if (!region_d2(K, G, v, d2)) return;
-    unsigned long long x = dbits(d2);
+  src.each(K, B, [&](unsigned long long x, unsigned ix, unsigned) {
     if (x < lo || x > hi) return;
     unsigned s = atomicAdd(&S.nsorted, 1u);
     if (s < CAP) {
       S.skey[s] = x;
-      S.sidx[s] = __float_as_uint(v.w) & PSOD_IDX_MASK;
+      S.sidx[s] = ix;
     }
   });
   __syncthreads();
@@ -530,7 +582,7 @@ __device__ __forceinline__ unsigned *small_pos(Smem &S) { return S.hist[MAXLEV -
 
 // every alive record of region G, sorted; returns the count, or CAP + 1 when
 // the region holds more than CAP (the list is then unusable)
-__device__ unsigned load_ball_sorted(const SodConst &K, const SodBufs &B, Smem &S, const Region &G) {
+__device__ __forceinline__ unsigned load_ball_sorted(const SodConst &K, const SodBufs &B, Smem &S, const Region &G) {
   unsigned *spos = small_pos(S);
   if (threadIdx.x == 0) S.nsorted = 0;
   __syncthreads();
@@ -582,7 +634,7 @@ __device__ unsigned load_ball_sorted(const SodConst &K, const SodBufs &B, Smem &
 
 // forward crossing search over the sorted list [0, n): the first 1-based
 // position i >= 10 where the reference's loop stops (main:2046); 0 if none
-__device__ long long sorted_stop(const SodConst &K, Smem &S, unsigned n, long long na, double delta) {
+__device__ __forceinline__ long long sorted_stop(const SodConst &K, Smem &S, unsigned n, long long na, double delta) {
   int best = 0x7fffffff;
   for (unsigned k = 9 + threadIdx.x; k < n; k += TPB)
     if (!keeps_going(K, (long long)k + 1, bitsd(S.skey[k]), na, delta)) best = min(best, (int)k);
@@ -590,16 +642,21 @@ __device__ long long sorted_stop(const SodConst &K, Smem &S, unsigned n, long lo
   return best == 0x7fffffff ? 0 : (long long)best + 1;
 }
 
-// Search over the sorted d2 sequence of the cube.
+// Search over the sorted d2 sequence of the ball.
 //  mode 0 (forward): first 1-based position i >= 10 where the reference's
 //                    loop stops for threshold delta.
 //  mode 1 (backward): last position i in [2, imax] with overdensity > delta.
+// The level-0 histogram of the ball is in S.hist[0] (built by the caller).
+// BUF: the ball's entries are bucketed in the crossing buffer from S.xbase
+// (level-0 bucket order), so descents and extractions read the slice of the
+// level-0 bucket under examination; otherwise they walk the region G.
 // Returns 0 if not found, else the position; *d2_out its squared distance.
 // Returns -1 on an unresolvable bucket (more than CAP exact-equal keys).
-__device__ long long radial_search(const SodConst &K, const SodBufs &B, Smem &S, const Region &G, long long na,
+template <bool BUF>
+__device__ __forceinline__ long long radial_search(const SodConst &K, const SodBufs &B, Smem &S, const Region &G, long long na,
                                    double delta, int mode, long long imax, double *d2_out) {
-  // level 0 histogram is built by the caller
   int l = 0;
+  unsigned long long b0lo = 0, b0hi = 0;  // buffer slice of the level-0 bucket being resolved
   if (threadIdx.x == 0) {
     S.lev[0].cum = 0;
     S.lev[0].next = (mode == 0) ? 0 : NB - 1;
@@ -656,8 +713,14 @@ __device__ long long radial_search(const SodConst &K, const SodBufs &B, Smem &S,
     unsigned long long lo, hi;
     bucket_range(L, l, cand, lo, hi);
     const long long c0 = (long long)L.cum + S.pref[cand];
+    if (BUF && l == 0) {
+      b0lo = S.xbase + S.pref[cand];
+      b0hi = b0lo + nb;
+    }
     if (nb <= CAP) {
-      unsigned n = extract_sorted(K, B, S, G, lo, hi);
+      unsigned n;
+      if constexpr (BUF) n = extract_sorted(K, B, S, BufSrc{b0lo, b0hi}, lo, hi);
+      else n = extract_sorted(K, B, S, RegionSrc{G}, lo, hi);
       long long hit;
       if (mode == 0) {
         int best = 0x7fffffff;
@@ -701,21 +764,20 @@ __device__ long long radial_search(const SodConst &K, const SodBufs &B, Smem &S,
     }
     __syncthreads();
     l++;
-    build_hist(K, B, S, l, G);
+    if constexpr (BUF) build_hist(K, B, S, l, BufSrc{b0lo, b0hi});
+    else build_hist(K, B, S, l, RegionSrc{G});
   }
 }
 
 // the pos-th (1-based) element of the sorted sequence when it is the last
 // element below `below_lo`: the maximum (bits, index) under that bound
-__device__ void max_below(const SodConst &K, const SodBufs &B, Smem &S, const Region &G,
+template <class Src>
+__device__ __forceinline__ void max_below(const SodConst &K, const SodBufs &B, Smem &S, const Src &src,
                           unsigned long long below_lo, unsigned long long &kout, unsigned &iout) {
   unsigned long long a = 0, b = 0;
-  for_region(K, B, G, [&](unsigned p, float4 v) {
-    double d2;
-    if (!region_d2(K, G, v, d2)) return;
-    unsigned long long x = dbits(d2);
+  src.each(K, B, [&](unsigned long long x, unsigned ixu, unsigned) {
     if (x >= below_lo) return;
-    unsigned long long ix = __float_as_uint(v.w) & PSOD_IDX_MASK;
+    const unsigned long long ix = ixu;
     if (x > a || (x == a && ix > b)) { a = x; b = ix; }
   });
   block_max_pair(S, a, b);
@@ -723,7 +785,7 @@ __device__ void max_below(const SodConst &K, const SodBufs &B, Smem &S, const Re
   iout = (unsigned)b;
 }
 
-__device__ void record_error(const SodBufs &B, unsigned rank, unsigned code) {
+__device__ __forceinline__ void record_error(const SodBufs &B, unsigned rank, unsigned code) {
   atomicMin(B.err, ((unsigned long long)rank << 8) | code);
 }
 
@@ -752,7 +814,7 @@ __device__ __forceinline__ unsigned next_item(unsigned *ctr) {
 }
 
 // records filed under the cube's cells (alive or not): one run per row
-__device__ unsigned cube_records(const SodConst &K, const SodBufs &B, Smem &S, int ic, int jc, int kc) {
+__device__ __forceinline__ unsigned cube_records(const SodConst &K, const SodBufs &B, Smem &S, int ic, int jc, int kc) {
   const int R = K.ncut, side = 2 * R + 1;
   unsigned sum = 0;
   for (int row = threadIdx.x; row < side * side; row += TPB) {
@@ -777,7 +839,7 @@ __device__ __forceinline__ int zig(int a) { return (a & 1) ? -((a + 1) >> 1) : (
 
 // alive particles of the cube from the per-cell counts, rows nearest the
 // seed first; stops once `need` is reached (returns the running sum)
-__device__ unsigned alive_rows(const SodConst &K, const SodBufs &B, Smem &S, int ic, int jc, int kc, unsigned need) {
+__device__ __forceinline__ unsigned alive_rows(const SodConst &K, const SodBufs &B, Smem &S, int ic, int jc, int kc, unsigned need) {
   const int R = K.ncut, side = 2 * R + 1, nrow = side * side;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   unsigned total = 0;
@@ -800,7 +862,7 @@ __device__ unsigned alive_rows(const SodConst &K, const SodBufs &B, Smem &S, int
 // phase 1: preselect count (main:1657-1716) and the candidate list of the
 // +-1 cells (main:1807-1826)
 // ---------------------------------------------------------------------------
-__device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
+__device__ __forceinline__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
   if (threadIdx.x == 0) {
     B.st_active[slot] = 0;
     B.st_cn[slot] = 0;
@@ -870,21 +932,26 @@ __device__ void prep_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned
       s_coff[o] = tot;
       tot += s_cnt[o];
     }
-    s_base = atomicAdd(B.cand_used, tot);
-    if ((unsigned long long)s_base + tot > B.cand_cap) {
-      // candidate buffer full this round: the seed waits for the next one
+    const bool too_many = tot > B.max_cand;
+    s_base = too_many ? 0u : atomicAdd(B.cand_used, tot);
+    if (B.maxcand) atomicMax(B.maxcand, tot);
+    if (too_many || (unsigned long long)s_base + tot > B.cand_cap) {
+      // candidate buffer full this round, or more candidates than the
+      // device tail loop takes: the seed waits for the next round
       s_base = 0xffffffffu;
       B.processed[rank] = 0;
       {
         const unsigned bi = B.bidx_of_rank[rank];
         atomicAnd(&B.resolved[bi >> 5], ~(1u << (bi & 31)));
       }
-      if (tot > B.cand_cap) record_error(B, rank, PSOD_ERR_STATE);
+      if (too_many) atomicOr(B.deferred, 1u);
+      else if (tot > B.cand_cap) record_error(B, rank, PSOD_ERR_STATE);
     } else {
       B.st_na[slot] = na;  // 0 when unknown (batched modes)
       B.st_coff[slot] = s_base;
       B.st_cn[slot] = tot;
       B.st_active[slot] = 1;
+      if (tot >= BOUND_MIN_CAND) atomicAdd(B.nbig, 1u);
       B.st_centre[slot] = g.sp;  // no candidate: the seed stays the centre
       atomicAdd(B.nprocessed, 1ull);
     }
@@ -974,7 +1041,7 @@ __device__ __forceinline__ bool in_sel2(const SodConst &K, int x, int y, int z, 
 // int64 fixed-point sum of FP64 terms (main:1840-1859); else the FP64 sum of
 // FP32 terms.  Result valid in lane 0.
 template <bool EXACT>
-__device__ void refine_sum(const SodConst &K, const SodBufs &B, unsigned cp, int ic, int jc, int kc,
+__device__ __forceinline__ void refine_sum(const SodConst &K, const SodBufs &B, unsigned cp, int ic, int jc, int kc,
                            unsigned long long &sq_out, double &sf_out, unsigned *visits = nullptr) {
   const int lane = threadIdx.x & 31;
   const float4 cv = B.cube[cp];
@@ -1068,18 +1135,24 @@ __device__ __forceinline__ float rsqrt_pos(float x) {
   return y;
 }
 
+// A warp's staged records, one array per coordinate (grid units), so that
+// one 16-byte shared load gives one coordinate of four consecutive records.
+struct __align__(16) RecTile {
+  float x[64], y[64], z[64];
+};
+
 template <bool WRAPFREE>
-__device__ __forceinline__ void pair_fast(const float4 nb, float cx, float cy, float cz, float e2f, float limf,
-                                          float nxf, float &acc, float &edge) {
+__device__ __forceinline__ void pair_fast(float rx, float ry, float rz, float cx, float cy, float cz, float e2f,
+                                          float limf, float nxf, float &acc, float &edge) {
   float dx, dy, dz;
   if (WRAPFREE) {
-    dx = __fsub_rn(nb.x, cx);
-    dy = __fsub_rn(nb.y, cy);
-    dz = __fsub_rn(nb.z, cz);
+    dx = __fsub_rn(rx, cx);
+    dy = __fsub_rn(ry, cy);
+    dz = __fsub_rn(rz, cz);
   } else {
-    dx = mi_dx(nb.x, cx, nxf);
-    dy = mi_dx(nb.y, cy, nxf);
-    dz = mi_dx(nb.z, cz, nxf);
+    dx = mi_dx(rx, cx, nxf);
+    dy = mi_dx(ry, cy, nxf);
+    dz = mi_dx(rz, cz, nxf);
   }
   const float d2e = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmaf_rn(dz, dz, e2f)));
   // e has the sign of d2e - limf (a rounded difference never changes sign)
@@ -1092,23 +1165,23 @@ __device__ __forceinline__ void pair_fast(const float4 nb, float cx, float cy, f
 // a tile whose lane met a pair near the inclusion edge: the same FP32 terms,
 // with the inclusion decided by the FP64 minimum-image distance
 template <bool WRAPFREE>
-__device__ __noinline__ double tile_terms_edge(const float4 *tile, unsigned nt, float cx, float cy, float cz,
+__device__ __noinline__ double tile_terms_edge(const RecTile &tile, unsigned nt, float cx, float cy, float cz,
                                                float e2f, float nxf, double tx, double rmin2) {
   double sum = 0.0;
   for (unsigned j = 0; j < nt; j++) {
-    const float4 nb = tile[j];
+    const float rx = tile.x[j], ry = tile.y[j], rz = tile.z[j];
     float dx, dy, dz;
     if (WRAPFREE) {
-      dx = __fsub_rn(nb.x, cx);
-      dy = __fsub_rn(nb.y, cy);
-      dz = __fsub_rn(nb.z, cz);
+      dx = __fsub_rn(rx, cx);
+      dy = __fsub_rn(ry, cy);
+      dz = __fsub_rn(rz, cz);
     } else {
-      dx = mi_dx(nb.x, cx, nxf);
-      dy = mi_dx(nb.y, cy, nxf);
-      dz = mi_dx(nb.z, cz, nxf);
+      dx = mi_dx(rx, cx, nxf);
+      dy = mi_dx(ry, cy, nxf);
+      dz = mi_dx(rz, cz, nxf);
     }
     const float d2e = __fmaf_rn(dx, dx, __fmaf_rn(dy, dy, __fmaf_rn(dz, dz, e2f)));
-    if (min_image_d2((double)nb.x, (double)nb.y, (double)nb.z, (double)cx, (double)cy, (double)cz, tx) <= rmin2)
+    if (min_image_d2((double)rx, (double)ry, (double)rz, (double)cx, (double)cy, (double)cz, tx) <= rmin2)
       sum += (double)rsqrt_pos(d2e);
   }
   return sum;
@@ -1117,39 +1190,118 @@ __device__ __noinline__ double tile_terms_edge(const float4 *tile, unsigned nt, 
 // sum of the terms of nt staged records; the tile is padded with far
 // records up to a multiple of 8
 template <bool WRAPFREE>
-__device__ __forceinline__ double tile_terms(const float4 *tile, unsigned nt, float cx, float cy, float cz,
+__device__ __forceinline__ double tile_terms(const RecTile &tile, unsigned nt, float cx, float cy, float cz,
                                              const SodConst &K) {
   const float e2f = (float)K.eps2, limf = (float)(1.0 + K.eps2);
   float p0 = 0.f, p1 = 0.f, edge = 1.f;
   for (unsigned j = 0; j < nt; j += 8) {
 #pragma unroll
     for (int u = 0; u < 8; u += 2) {
-      pair_fast<WRAPFREE>(tile[j + u], cx, cy, cz, e2f, limf, K.nxf, p0, edge);
-      pair_fast<WRAPFREE>(tile[j + u + 1], cx, cy, cz, e2f, limf, K.nxf, p1, edge);
+      pair_fast<WRAPFREE>(tile.x[j + u], tile.y[j + u], tile.z[j + u], cx, cy, cz, e2f, limf, K.nxf, p0, edge);
+      pair_fast<WRAPFREE>(tile.x[j + u + 1], tile.y[j + u + 1], tile.z[j + u + 1], cx, cy, cz, e2f, limf, K.nxf, p1,
+                          edge);
     }
   }
   if (edge < EDGE_MARGIN) return tile_terms_edge<WRAPFREE>(tile, nt, cx, cy, cz, e2f, K.nxf, K.tx, K.rmin2);
   return (double)p0 + (double)p1;
 }
 
-// the same for two candidates per lane: each staged record serves both
+// Packed FP32 pairs (the f32x2 operations of sm_100): two floats in one
+// 64-bit register pair, both halves rounded exactly as the scalar operation.
+__device__ __forceinline__ unsigned long long f2_pack(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(unsigned long long r, float &lo, float &hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(r));
+}
+__device__ __forceinline__ unsigned long long f2_add(unsigned long long a, unsigned long long b) {
+  unsigned long long d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+  unsigned long long d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+// 1.0f where x <= 0, else 0.0f
+__device__ __forceinline__ float le0(float x) {
+  float m;
+  asm("set.le.f32.f32 %0, %1, 0f00000000;" : "=f"(m) : "f"(x));
+  return m;
+}
+
+// One candidate against records (j, j+1) held packed in (px, py, pz): the
+// same operations as pair_fast on each half.  The accumulator's low half
+// sums the even records and its high half the odd ones, as tile_terms does;
+// t * 1.0 + acc rounds as acc + t, and t * 0.0 + acc is acc.
+__device__ __forceinline__ void pair_packed(unsigned long long px, unsigned long long py, unsigned long long pz,
+                                            unsigned long long ncx, unsigned long long ncy, unsigned long long ncz,
+                                            unsigned long long e2, unsigned long long nlim, unsigned long long &acc,
+                                            float &edge) {
+  const unsigned long long dx = f2_add(px, ncx), dy = f2_add(py, ncy), dz = f2_add(pz, ncz);
+  const unsigned long long d2e = f2_fma(dx, dx, f2_fma(dy, dy, f2_fma(dz, dz, e2)));
+  const unsigned long long e = f2_add(d2e, nlim);
+  float d0, d1, e0, e1;
+  f2_unpack(d2e, d0, d1);
+  f2_unpack(e, e0, e1);
+  edge = fminf(edge, fminf(fabsf(e0), fabsf(e1)));
+  acc = f2_fma(f2_pack(rsqrt_pos(d0), rsqrt_pos(d1)), f2_pack(le0(e0), le0(e1)), acc);
+}
+
+// the same for two candidates per lane: each staged record serves both.
+// Wrap-free tiles use the packed form: four records a step, one 16-byte
+// load per coordinate, two packed records per operation.
 template <bool WRAPFREE>
-__device__ __forceinline__ void tile_terms2(const float4 *tile, unsigned nt, float ax, float ay, float az, float bx,
+__device__ __forceinline__ void tile_terms2(const RecTile &tile, unsigned nt, float ax, float ay, float az, float bx,
                                             float by, float bz, const SodConst &K, double &sa, double &sb) {
   const float e2f = (float)K.eps2, limf = (float)(1.0 + K.eps2);
-  float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f, ea = 1.f, eb = 1.f;
-  for (unsigned j = 0; j < nt; j += 8) {
+  float ea = 1.f, eb = 1.f;
+  double ra, rb;
+  if (WRAPFREE) {
+    const unsigned long long nax = f2_pack(-ax, -ax), nay = f2_pack(-ay, -ay), naz = f2_pack(-az, -az);
+    const unsigned long long nbx = f2_pack(-bx, -bx), nby = f2_pack(-by, -by), nbz = f2_pack(-bz, -bz);
+    const unsigned long long e2 = f2_pack(e2f, e2f), nlim = f2_pack(-limf, -limf);
+    unsigned long long acca = f2_pack(0.f, 0.f), accb = f2_pack(0.f, 0.f);
+    const ulonglong2 *tx = reinterpret_cast<const ulonglong2 *>(tile.x);
+    const ulonglong2 *ty = reinterpret_cast<const ulonglong2 *>(tile.y);
+    const ulonglong2 *tz = reinterpret_cast<const ulonglong2 *>(tile.z);
+    for (unsigned j = 0; j < nt; j += 8) {
 #pragma unroll
-    for (int u = 0; u < 8; u += 2) {
-      const float4 r0 = tile[j + u], r1 = tile[j + u + 1];
-      pair_fast<WRAPFREE>(r0, ax, ay, az, e2f, limf, K.nxf, a0, ea);
-      pair_fast<WRAPFREE>(r0, bx, by, bz, e2f, limf, K.nxf, b0, eb);
-      pair_fast<WRAPFREE>(r1, ax, ay, az, e2f, limf, K.nxf, a1, ea);
-      pair_fast<WRAPFREE>(r1, bx, by, bz, e2f, limf, K.nxf, b1, eb);
+      for (unsigned u = 0; u < 8; u += 4) {
+        const ulonglong2 X = tx[(j + u) >> 2], Y = ty[(j + u) >> 2], Z = tz[(j + u) >> 2];
+        pair_packed(X.x, Y.x, Z.x, nax, nay, naz, e2, nlim, acca, ea);
+        pair_packed(X.x, Y.x, Z.x, nbx, nby, nbz, e2, nlim, accb, eb);
+        pair_packed(X.y, Y.y, Z.y, nax, nay, naz, e2, nlim, acca, ea);
+        pair_packed(X.y, Y.y, Z.y, nbx, nby, nbz, e2, nlim, accb, eb);
+      }
     }
+    float a0, a1, b0, b1;
+    f2_unpack(acca, a0, a1);
+    f2_unpack(accb, b0, b1);
+    ra = (double)a0 + (double)a1;
+    rb = (double)b0 + (double)b1;
+  } else {
+    float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
+    for (unsigned j = 0; j < nt; j += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; u += 2) {
+        const float x0 = tile.x[j + u], y0 = tile.y[j + u], z0 = tile.z[j + u];
+        const float x1 = tile.x[j + u + 1], y1 = tile.y[j + u + 1], z1 = tile.z[j + u + 1];
+        pair_fast<false>(x0, y0, z0, ax, ay, az, e2f, limf, K.nxf, a0, ea);
+        pair_fast<false>(x0, y0, z0, bx, by, bz, e2f, limf, K.nxf, b0, eb);
+        pair_fast<false>(x1, y1, z1, ax, ay, az, e2f, limf, K.nxf, a1, ea);
+        pair_fast<false>(x1, y1, z1, bx, by, bz, e2f, limf, K.nxf, b1, eb);
+      }
+    }
+    ra = (double)a0 + (double)a1;
+    rb = (double)b0 + (double)b1;
   }
-  sa += ea < EDGE_MARGIN ? tile_terms_edge<WRAPFREE>(tile, nt, ax, ay, az, e2f, K.nxf, K.tx, K.rmin2) : (double)a0 + (double)a1;
-  sb += eb < EDGE_MARGIN ? tile_terms_edge<WRAPFREE>(tile, nt, bx, by, bz, e2f, K.nxf, K.tx, K.rmin2) : (double)b0 + (double)b1;
+  sa += ea < EDGE_MARGIN ? tile_terms_edge<WRAPFREE>(tile, nt, ax, ay, az, e2f, K.nxf, K.tx, K.rmin2) : ra;
+  sb += eb < EDGE_MARGIN ? tile_terms_edge<WRAPFREE>(tile, nt, bx, by, bz, e2f, K.nxf, K.tx, K.rmin2) : rb;
 }
 
 // Work item: up to 64 candidates of one candidate cell (two per lane) against
@@ -1170,9 +1322,6 @@ __device__ __forceinline__ void tile_terms2(const float4 *tile, unsigned nt, flo
 // and their sums stay 0, below the select threshold.
 constexpr unsigned ITEM_GRAB = 1;  // refinement items claimed per counter update
 
-// Seeds with fewer candidates than this are neither bounded nor pruned: their
-// pair work is small and the bound pass would cost as much as it saves.
-constexpr unsigned BOUND_MIN_CAND = 4096;
 
 // Sub-groups of SUBG candidates (16 per 64-candidate group, two lanes each).
 // Records nearer than sqrt(NEAR2) cells to a group's box bound its
@@ -1186,7 +1335,7 @@ constexpr float NEAR2 = 0.09f;
 
 template <bool BOUND>
 __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
-  __shared__ float4 s_tile[8][64];
+  __shared__ RecTile s_tile[8];
   __shared__ unsigned s_rb[8][18], s_rp[8][19];
   __shared__ int s_nr[8], s_wf[8];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1389,7 +1538,7 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
       if (BOUND) {
         __syncwarp();
         for (unsigned j = (unsigned)lane & 1u; j < nt; j += 2u) {
-          const float4 rec = s_tile[w][j];
+          const float4 rec = make_float4(s_tile[w].x[j], s_tile[w].y[j], s_tile[w].z[j], 0.f);
           const float ex = fmaxf(fmaxf(slx - rec.x, rec.x - shx), 0.f), ey = fmaxf(fmaxf(sly - rec.y, rec.y - shy), 0.f),
                       ez = fmaxf(fmaxf(slz - rec.z, rec.z - shz), 0.f);
           const float db2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
@@ -1399,7 +1548,11 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
         return;
       }
       // pad to a multiple of 8 with records far from every candidate
-      if ((unsigned)lane < ((8u - (nt & 7u)) & 7u)) s_tile[w][nt + lane] = make_float4(1e18f, 1e18f, 1e18f, 0.f);
+      if ((unsigned)lane < ((8u - (nt & 7u)) & 7u)) {
+        s_tile[w].x[nt + lane] = 1e18f;
+        s_tile[w].y[nt + lane] = 1e18f;
+        s_tile[w].z[nt + lane] = 1e18f;
+      }
       __syncwarp();
       if (two) {
         if (active || active1) {
@@ -1466,12 +1619,21 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
             }
           }
           const unsigned m = __ballot_sync(0xffffffffu, keep);
-          if (keep) s_tile[w][fill + __popc(m & lt)] = rec;  // fill < 32: index < 64
+          if (keep) {  // fill < 32: index < 64
+            const unsigned at = fill + __popc(m & lt);
+            s_tile[w].x[at] = rec.x;
+            s_tile[w].y[at] = rec.y;
+            s_tile[w].z[at] = rec.z;
+          }
           fill += (unsigned)__popc(m);
           if (!BOUND) loaded += min(32u, run_end - x0);
           if (fill >= 32u) {
             consume(32u);
-            if ((unsigned)lane < fill - 32u) s_tile[w][lane] = s_tile[w][32 + lane];
+            if ((unsigned)lane < fill - 32u) {
+              s_tile[w].x[lane] = s_tile[w].x[32 + lane];
+              s_tile[w].y[lane] = s_tile[w].y[32 + lane];
+              s_tile[w].z[lane] = s_tile[w].z[32 + lane];
+            }
             __syncwarp();
             fill -= 32u;
           }
@@ -1537,7 +1699,7 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
 // largest sum wins, equal sums go to the first candidate in the reference's
 // scan order (listed cell offset x-outer/z-inner, then input index)
 // ---------------------------------------------------------------------------
-__device__ void select_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
+__device__ __forceinline__ void select_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
   if (!B.st_active[slot]) return;
   const unsigned off = B.st_coff[slot], n = B.st_cn[slot];
   if (n == 0) {
@@ -1605,7 +1767,7 @@ __device__ void select_seed(const SodConst &K, const SodBufs &B, Smem &S, unsign
 // covers every seed.
 constexpr unsigned LEARN_MIN_CAND = 256;
 
-__device__ void seed_features(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
+__device__ __forceinline__ void seed_features(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
   float *f = B.st_feat + (size_t)slot * 16;
   if (!B.st_active[slot] || (!B.learn_collect && B.st_cn[slot] < LEARN_MIN_CAND)) {
     if (threadIdx.x < 16) f[threadIdx.x] = threadIdx.x == 15 ? 1.f : 0.f;
@@ -1668,7 +1830,7 @@ __global__ void __launch_bounds__(TPB) k_select(SodConst K, SodBufs B) {
 // (main:2118-2141) and claims (main:2148-2166)
 // ---------------------------------------------------------------------------
 // exact alive count of the whole cube (the reference's npart_sel)
-__device__ unsigned count_alive_cube(const SodConst &K, const SodBufs &B, Smem &S, int ic, int jc, int kc) {
+__device__ __forceinline__ unsigned count_alive_cube(const SodConst &K, const SodBufs &B, Smem &S, int ic, int jc, int kc) {
   unsigned cnt = 0;
   for_cube(K, B, ic, jc, kc, K.ncut, [&](unsigned p, float4 v) {
     if (!(__float_as_uint(v.w) & PSOD_DEAD_BIT)) cnt++;
@@ -1686,9 +1848,10 @@ __device__ __forceinline__ unsigned listed_cell(const SodConst &K, unsigned p, f
 }
 
 // Forward crossing search for threshold delta over a region that grows from
-// rb0 (cells) until the stop is proven inside it.  The plain mode starts from
-// the whole cube.  Returns the stop position; G is left at the region used.
-__device__ long long bracketed_stop(const SodConst &K, const SodBufs &B, Smem &S, Region &G, double rb0,
+// rb0 (cells) until the stop is proven inside it, walking the region for
+// every histogram level.  The plain mode starts from the whole cube.
+// Returns the stop position; G is left at the region used.
+__device__ __forceinline__ long long bracketed_stop(const SodConst &K, const SodBufs &B, Smem &S, Region &G, double rb0,
                                     unsigned &na, bool &na_known, double delta, double *d2stop) {
   double rb = rb0;
   while (true) {
@@ -1699,23 +1862,85 @@ __device__ long long bracketed_stop(const SodConst &K, const SodBufs &B, Smem &S
       na = count_alive_cube(K, B, S, G.ic, G.jc, G.kc);
       na_known = true;
     }
-    if (threadIdx.x == 0) {
-      S.lev[0].lo = 0;
-      S.lev[0].hi = 0x7fefffffffffffffull;
-      S.lev[0].shift = L1_SHIFT;
-    }
-    __syncthreads();
-    build_hist(K, B, S, 0, G);
+    ball_hist0(K, B, S, G);
     if (threadIdx.x == 0) atomicAdd(B.cross_balls, 1ull);
     // inside a partial ball the cube's count is not reached: i < npart_sel holds
     const long long na_eff = full ? (long long)na : 0x7fffffffffffffffll;
-    const long long i = radial_search(K, B, S, G, na_eff, delta, 0, 0, d2stop);
+    const long long i = radial_search<false>(K, B, S, G, na_eff, delta, 0, 0, d2stop);
     if (i != 0 || full) return i;
     rb *= 2.0;
   }
 }
 
-__device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
+// Does some level-0 bucket of the ball (S.hist[0]) possibly hold the stop for
+// threshold delta?  (the forward test of radial_search at level 0)
+__device__ __forceinline__ bool stop_may_lie_inside(const SodConst &K, Smem &S, long long na, double delta) {
+  hist_prefix(S, 0);
+  const Level L = S.lev[0];
+  int any = 0;
+  for (int k = 0; k < NB / TPB; k++) {
+    const int b = threadIdx.x * (NB / TPB) + k;
+    const unsigned nb = S.hist[0][b];
+    if (nb == 0) continue;
+    unsigned long long lo, hi;
+    bucket_range(L, 0, b, lo, hi);
+    const long long ilo = (long long)S.pref[b] + 1, ihi = (long long)S.pref[b] + nb;
+    if (ihi < 10) continue;
+    const long long i0 = ilo < 10 ? 10 : ilo;
+    const double hd = bitsd(hi);
+    if (!(overdens(K, i0, hd) > delta && ihi < na && dsqrt(hd) < (double)K.ncut)) any = 1;
+  }
+  return block_max_i(S, any) > 0;
+}
+
+// Bucketed ball: grow the ball (one histogram walk per size) until every
+// threshold's stop may lie inside it, then scatter its entries into a slice
+// of the crossing buffer in level-0 bucket order (one more walk).  Returns
+// the entry count, or -1 when the buffer has no room this round (the caller
+// then walks the region for every search).
+__device__ __forceinline__ long long bucket_ball(const SodConst &K, const SodBufs &B, Smem &S, Region &G, double rb0, unsigned &na,
+                                 bool &na_known) {
+  double rb = rb0;
+  unsigned nball = 0;
+  while (true) {
+    const bool full = !(rb > 0.0) || rb >= (double)K.ncut;
+    G.rb = full ? -1.0 : rb;
+    G.rb2 = full ? -1.0 : rb * rb;
+    if (full && !na_known) {
+      na = count_alive_cube(K, B, S, G.ic, G.jc, G.kc);
+      na_known = true;
+    }
+    nball = ball_hist0(K, B, S, G);
+    if (threadIdx.x == 0) atomicAdd(B.cross_balls, 1ull);
+    if (full) break;
+    bool inside = stop_may_lie_inside(K, S, 0x7fffffffffffffffll, K.delta);
+    for (int e = 0; e < K.ndx && inside; e++) inside = stop_may_lie_inside(K, S, 0x7fffffffffffffffll, K.dx_extra[e]);
+    if (inside) break;
+    rb *= 2.0;
+  }
+  if (threadIdx.x == 0) {
+    const unsigned long long at = atomicAdd(B.xused, (unsigned long long)nball);
+    S.xbase = (at + nball <= B.xcap) ? at : ~0ull;
+  }
+  __syncthreads();
+  if (S.xbase == ~0ull) return -1;
+  // cursors: the level-0 bucket starts
+  hist_prefix(S, 0);
+  unsigned *cur = S.hist[1];
+  for (int k = threadIdx.x; k < NB; k += TPB) cur[k] = S.pref[k];
+  __syncthreads();
+  const unsigned long long base = S.xbase;
+  RegionSrc{G}.each(K, B, [&](unsigned long long x, unsigned ix, unsigned p) {
+    const unsigned slot = atomicAdd(&cur[bucket_of(S.lev[0], 0, x)], 1u);
+    B.xkey[base + slot] = x;
+    B.xidx[base + slot] = ix;
+    B.xpos[base + slot] = p;
+  });
+  __syncthreads();
+  return (long long)nball;
+}
+
+__device__ __forceinline__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
   if (!B.st_active[slot]) return;
   const SeedGeo g = seed_geo(K, B, rank);
   unsigned na = B.st_na[slot];
@@ -1741,12 +1966,16 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
     if (r > 0.f) rb0 = fmin(fmax((double)r, BALL0), (double)K.ncut);
   }
 
-  // 3. crossing (main:2040-2100).  Balls of at most CAP alive records are
-  // sorted whole (small path); larger ones go through the histogram search
-  // from the first ball that overflowed.
+  // 3. crossing (main:2040-2100), in one of three forms:
+  //  SMALL  the ball holds at most CAP alive records: sorted whole in shared
+  //         memory; every later step reads the sorted list;
+  //  BUF    a larger ball bucketed into the crossing buffer (bucket_ball):
+  //         searches, profile and claims read bucket slices;
+  //  REGION the buffer is full: every search level walks the region.
+  enum { SMALL, BUF, REGION };
+  int form = REGION;
   double d2stop = 0;
   long long istop = 0;
-  bool small = false;
   unsigned nball = 0;
   {
     double rb = rb0;
@@ -1765,13 +1994,30 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
       if (i != 0 || full) {
         istop = i;
         if (i > 0) d2stop = bitsd(S.skey[i - 1]);
-        small = true;
+        form = SMALL;
         nball = n;
         break;
       }
       rb *= 2.0;
     }
-    if (!small) istop = bracketed_stop(K, B, S, G, G.rb2 < 0.0 ? -1.0 : G.rb, na, na_known, K.delta, &d2stop);
+    if (form != SMALL) {
+      // the ball that overflowed CAP is where the large forms start
+      double rb = G.rb2 < 0.0 ? -1.0 : G.rb;
+      while (true) {
+        const long long nb = bucket_ball(K, B, S, G, rb, na, na_known);
+        if (nb < 0) {
+          form = REGION;
+          istop = bracketed_stop(K, B, S, G, G.rb2 < 0.0 ? -1.0 : G.rb, na, na_known, K.delta, &d2stop);
+          break;
+        }
+        form = BUF;
+        nball = (unsigned)nb;
+        const long long na_eff = G.rb2 < 0.0 ? (long long)na : 0x7fffffffffffffffll;
+        istop = radial_search<true>(K, B, S, G, na_eff, K.delta, 0, 0, &d2stop);
+        if (istop != 0 || G.rb2 < 0.0) break;
+        rb = 2.0 * G.rb;  // no stop in this ball after all: a larger one
+      }
+    }
   }
   if (istop <= 0) {
     if (threadIdx.x == 0) record_error(B, rank, PSOD_ERR_STATE);
@@ -1782,6 +2028,7 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
     return;
   }
   const long long masse = istop - 1;
+  const BufSrc ball_buf{S.xbase, S.xbase + nball};  // BUF: the whole ball
   {
     // algorithmic read volume: records of the cube cells that meet the ball
     // out to the stopping particle
@@ -1794,7 +2041,7 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
   // the masse-th element closes the member set (main:2090-2100, 2148)
   unsigned long long thr_key;
   unsigned thr_idx;
-  if (small) {
+  if (form == SMALL) {
     thr_key = S.skey[masse - 1];
     thr_idx = S.sidx[masse - 1];
   } else {
@@ -1804,8 +2051,10 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
     if (hk > 0) {
       thr_key = S.skey[hk - 1];
       thr_idx = S.sidx[hk - 1];
+    } else if (form == BUF) {
+      max_below(K, B, S, ball_buf, blo, thr_key, thr_idx);
     } else {
-      max_below(K, B, S, G, blo, thr_key, thr_idx);
+      max_below(K, B, S, RegionSrc{G}, blo, thr_key, thr_idx);
     }
   }
   const double rayon = dsqrt(bitsd(thr_key));
@@ -1813,7 +2062,7 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
   // seuil2 capture (main:2062-2069): last step i in [2, istop] above seuil2;
   // every such step lies inside the region that held the stop
   long long masse2 = 0;
-  if (small) {
+  if (form == SMALL) {
     int best = -1;
     for (unsigned k = 1 + threadIdx.x; k < (unsigned)istop; k += TPB)
       if (overdens(K, (long long)k + 1, bitsd(S.skey[k])) > K.delta2) best = max(best, (int)k);
@@ -1822,23 +2071,31 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
   } else {
     double dd;
     const long long na_eff = G.rb2 < 0.0 ? (long long)na : 0x7fffffffffffffffll;
-    long long i2 = radial_search(K, B, S, G, na_eff, K.delta2, 1, istop, &dd);
+    const long long i2 = form == BUF ? radial_search<true>(K, B, S, G, na_eff, K.delta2, 1, istop, &dd)
+                                     : radial_search<false>(K, B, S, G, na_eff, K.delta2, 1, istop, &dd);
     if (i2 > 0) masse2 = i2;
   }
   // extra thresholds: the same stop rule, -1 when not crossed
   long long mext[PSOD_MAX_EXTRA_DELTA];
   double d2far = d2stop;  // farthest stop over the thresholds
+  bool list_ok = form == SMALL;  // the sorted list still holds the ball
+  bool buf_ok = form == BUF;     // S.hist[0] still describes the bucketed ball
   for (int e = 0; e < K.ndx; e++) {
     double dd = 0.0;
     long long ie = 0;
-    if (small) {
-      ie = sorted_stop(K, S, nball, G.rb2 < 0.0 ? (long long)na : 0x7fffffffffffffffll, K.dx_extra[e]);
+    const long long na_eff = G.rb2 < 0.0 ? (long long)na : 0x7fffffffffffffffll;
+    if (list_ok) {
+      ie = sorted_stop(K, S, nball, na_eff, K.dx_extra[e]);
       if (ie > 0) dd = bitsd(S.skey[ie - 1]);
+    } else if (buf_ok) {
+      ie = radial_search<true>(K, B, S, G, na_eff, K.dx_extra[e], 0, 0, &dd);
     }
-    if (!small || (ie == 0 && G.rb2 >= 0.0)) {
-      // the stop lies outside the sorted ball: the histogram search takes
-      // over, and the list is no longer valid
-      small = false;
+    if ((!list_ok && !buf_ok) || (ie == 0 && G.rb2 >= 0.0)) {
+      // the stop lies outside this ball (or nothing is cached): the region
+      // search takes over from this ball's size; it rebuilds S.hist[0] and
+      // the sort buffer for another ball
+      list_ok = false;
+      buf_ok = false;
       Region Ge = G;
       const double rbe = G.rb2 < 0.0 ? -1.0 : G.rb;
       ie = bracketed_stop(K, B, S, Ge, rbe, na, na_known, K.dx_extra[e], &dd);
@@ -1846,6 +2103,7 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
     mext[e] = (ie <= 0 || overdens(K, ie, dd) > K.dx_extra[e]) ? -1 : ie - 1;
     if (ie > 0) d2far = fmax(d2far, dd);
   }
+  const bool small = form == SMALL && list_ok;
   // bracket bookkeeping: did the first ball hold every stop; samples for
   // training the bracket (this seed's features, log stop radius, log N)
   if (threadIdx.x == 0 && rb0 > 0.0) {
@@ -1873,7 +2131,19 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
     for (int j = threadIdx.x; j <= K.nbins; j += TPB) S.phist[j] = 0;
     __syncthreads();
     const double emax = S.edges[K.nbins - 1];
-    if (small && (G.rb2 < 0.0 || emax * (1.0 + 1e-9) < G.rb)) {
+    const bool ball_holds = G.rb2 < 0.0 || emax * (1.0 + 1e-9) < G.rb;
+    auto bin_entry = [&](unsigned long long x) {
+      const double r = dsqrt(bitsd(x));
+      if (!(r < emax)) return;
+      int lo = 0, hi = K.nbins - 1;  // first edge with r < edge
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (r < S.edges[mid]) hi = mid;
+        else lo = mid + 1;
+      }
+      atomicAdd(&S.phist[lo], 1u);
+    };
+    if (small && ball_holds) {
       // every particle closer than the last edge is in the sorted list:
       // cumulative counts by binary search, one bin per thread
       for (int j = threadIdx.x; j < K.nbins; j += TPB) {
@@ -1888,32 +2158,23 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
       __syncthreads();
       for (int j = threadIdx.x; j < K.nbins; j += TPB) S.phist[j] = S.pref[j] - (j > 0 ? S.pref[j - 1] : 0u);
       __syncthreads();
+    } else if (form == BUF && ball_holds) {
+      ball_buf.each(K, B, [&](unsigned long long x, unsigned, unsigned) { bin_entry(x); });
+      __syncthreads();
     } else {
-    Region Gp = G;
-    if (Gp.rb2 >= 0.0 && !(emax * (1.0 + 1e-9) < Gp.rb)) {
-      const double r = emax * 1.01 + 0.01;
-      if (r >= (double)K.ncut) {
-        Gp.rb = -1.0;
-        Gp.rb2 = -1.0;
-      } else {
-        Gp.rb = r;
-        Gp.rb2 = r * r;
+      Region Gp = G;
+      if (Gp.rb2 >= 0.0 && !ball_holds) {
+        const double r = emax * 1.01 + 0.01;
+        if (r >= (double)K.ncut) {
+          Gp.rb = -1.0;
+          Gp.rb2 = -1.0;
+        } else {
+          Gp.rb = r;
+          Gp.rb2 = r * r;
+        }
       }
-    }
-    for_region(K, B, Gp, [&](unsigned p, float4 v) {
-      double d2;
-      if (!region_d2(K, Gp, v, d2)) return;
-      double r = dsqrt(d2);
-      if (!(r < emax)) return;
-      int lo = 0, hi = K.nbins - 1;  // first edge with r < edge
-      while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if (r < S.edges[mid]) hi = mid;
-        else lo = mid + 1;
-      }
-      atomicAdd(&S.phist[lo], 1u);
-    });
-    __syncthreads();
+      RegionSrc{Gp}.each(K, B, [&](unsigned long long x, unsigned, unsigned) { bin_entry(x); });
+      __syncthreads();
     }
     if (threadIdx.x == 0) {
       S.pool_base = atomicAdd(B.pool_used, (unsigned long long)masse);
@@ -1927,6 +2188,18 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
 
   // 4b. claims (main:2148-2166): the masse nearest die, kept or not
   const unsigned long long pool_base = S.pool_base;
+  auto claim = [&](unsigned long long x, unsigned ix, unsigned p) {
+    if (!(x < thr_key || (x == thr_key && ix <= thr_idx))) return;
+    const float4 v = B.cube[p];
+    B.cube[p].w = __uint_as_float(__float_as_uint(v.w) | PSOD_DEAD_BIT);
+    mark_resolved(B, B.bidx_of_cube[p]);
+    if (B.alive_cnt) atomicSub(&B.alive_cnt[listed_cell(K, p, v)], 1u);
+    const unsigned slot2 = atomicAdd(&S.claim_cnt, 1u);
+    if (keep && slot2 < (unsigned)masse) {
+      B.pool_key[pool_base + slot2] = x;
+      B.pool_idx[pool_base + slot2] = ix;
+    }
+  };
   if (small) {
     // the first masse entries of the sorted list
     const unsigned *spos = small_pos(S);
@@ -1942,24 +2215,11 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
       }
     }
     if (threadIdx.x == 0) S.claim_cnt = (unsigned)masse;
-  } else
-  for_region(K, B, G, [&](unsigned p, float4 v) {
-    double d2;
-    if (!region_d2(K, G, v, d2)) return;
-    const unsigned wv = __float_as_uint(v.w);
-    const unsigned long long x = dbits(d2);
-    const unsigned ix = wv & PSOD_IDX_MASK;
-    if (x < thr_key || (x == thr_key && ix <= thr_idx)) {
-      B.cube[p].w = __uint_as_float(wv | PSOD_DEAD_BIT);
-      mark_resolved(B, B.bidx_of_cube[p]);
-      if (B.alive_cnt) atomicSub(&B.alive_cnt[listed_cell(K, p, v)], 1u);
-      const unsigned slot2 = atomicAdd(&S.claim_cnt, 1u);
-      if (keep && slot2 < (unsigned)masse) {
-        B.pool_key[pool_base + slot2] = x;
-        B.pool_idx[pool_base + slot2] = ix;
-      }
-    }
-  });
+  } else if (form == BUF) {
+    ball_buf.each(K, B, claim);
+  } else {
+    RegionSrc{G}.each(K, B, claim);
+  }
   __syncthreads();
   if (S.claim_cnt != (unsigned)masse) {
     if (threadIdx.x == 0) record_error(B, rank, PSOD_ERR_STATE);
@@ -1969,6 +2229,7 @@ __device__ void cross_seed(const SodConst &K, const SodBufs &B, Smem &S, unsigne
 
   // 5. halo record
   if (threadIdx.x == 0) {
+    atomicAdd(B.kept_members, (unsigned long long)masse);
     const unsigned long long hs = atomicAdd(B.nhalo, 1ull);
     B.h_rank[hs] = rank;
     B.h_id[hs] = B.ids[cidx];
@@ -2070,7 +2331,7 @@ __device__ __forceinline__ int ball_row_ranges(const SodConst &K, const SodBufs 
 
 // load the ball's alive records into the slice, sorted; returns the count
 // (above WCAP: overflow, slice unusable)
-__device__ unsigned warp_load_ball(const SodConst &K, const SodBufs &B, WSlice &W, const Region &G) {
+__device__ __forceinline__ unsigned warp_load_ball(const SodConst &K, const SodBufs &B, WSlice &W, const Region &G) {
   const int lane = threadIdx.x & 31;
   const double nxd = (double)K.nx;
   auto rel = [&](double x, int i) {
@@ -2140,7 +2401,7 @@ __device__ unsigned warp_load_ball(const SodConst &K, const SodBufs &B, WSlice &
 
 // first 1-based i >= 10 of the sorted slice where the loop stops (partial
 // ball: i < npart_sel always holds); 0 if none
-__device__ long long warp_stop(const SodConst &K, const WSlice &W, unsigned n, double delta) {
+__device__ __forceinline__ long long warp_stop(const SodConst &K, const WSlice &W, unsigned n, double delta) {
   const int lane = threadIdx.x & 31;
   int best = 0x7fffffff;
   for (unsigned k = 9 + lane; k < n; k += 32)
@@ -2153,7 +2414,7 @@ __device__ long long warp_stop(const SodConst &K, const WSlice &W, unsigned n, d
 }
 
 // records of the cube cells meeting the ball of radius rb (the touch count)
-__device__ unsigned warp_ball_records(const SodConst &K, const SodBufs &B, const Region &G) {
+__device__ __forceinline__ unsigned warp_ball_records(const SodConst &K, const SodBufs &B, const Region &G) {
   const int lane = threadIdx.x & 31;
   const double nxd = (double)K.nx;
   auto rel = [&](double x, int i) {
@@ -2298,6 +2559,7 @@ __global__ void __launch_bounds__(256) k_cross_warp(SodConst K, SodBufs B) {
     if (keep) {
       pool_base = atomicAdd(B.pool_used, (unsigned long long)masse);
       hs = atomicAdd(B.nhalo, 1ull);
+      atomicAdd(B.kept_members, (unsigned long long)masse);
     }
   }
   pool_base = __shfl_sync(0xffffffffu, pool_base, 0);
@@ -2613,6 +2875,297 @@ __global__ void k_count_unresolved(const unsigned *resolved, long long nseed, un
   if (open) atomicAdd(out, (unsigned long long)__popc(open));
 }
 
+// Per-round counters back to their start values in one launch: nready, the
+// four work counters, the bound/top-group pass counters, the candidate and
+// crossing-buffer allocators, the next active count, the bounded-seed count
+// and the global minimum head.
+__global__ void k_round_reset(unsigned *ctrs, unsigned long long *xused) {
+  const int t = threadIdx.x;
+  if (t < 5) ctrs[t] = 0;                   // nready, work[4]
+  if (t == 5) ctrs[5] = 0xffffffffu;        // gmin
+  if (t == 7) ctrs[7] = 0;                  // cand_used
+  if (t >= 9 && t <= 13) ctrs[t] = 0;       // next active count, bound / top work, nbig, max candidates
+  if (t == 0) *xused = 0ull;
+}
+
+// Readiness of each active block's head by a direct look at the heads of
+// its window (Chebyshev radius rb blocks, periodic; the whole axis when the
+// window covers it): ready when no head there is lower.  The same set as the
+// separable min filter + k_ready, for rounds with few active blocks.
+__global__ void k_ready_direct(const unsigned *active, const unsigned *nactive, const unsigned *head, int nb, int rb,
+                               unsigned quirk_rank, const unsigned *gmin, unsigned *ready, unsigned *nready,
+                               unsigned cap) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= *nactive) return;
+  const unsigned b = active[i];
+  const unsigned h = head[b];
+  if (h == PSOD_INF_RANK) return;
+  const int bx = (int)(b % (unsigned)nb), by = (int)((b / (unsigned)nb) % (unsigned)nb),
+            bz = (int)(b / ((unsigned)nb * nb));
+  const bool full = 2 * rb + 1 >= nb;
+  const int lo = full ? 0 : -rb, hi = full ? nb - 1 : rb;
+  for (int dz = lo; dz <= hi; dz++) {
+    int z = full ? dz : bz + dz;
+    if (z < 0) z += nb;
+    if (z >= nb) z -= nb;
+    for (int dy = lo; dy <= hi; dy++) {
+      int y = full ? dy : by + dy;
+      if (y < 0) y += nb;
+      if (y >= nb) y -= nb;
+      const unsigned row = (unsigned)nb * ((unsigned)y + (unsigned)nb * (unsigned)z);
+      for (int dx = lo; dx <= hi; dx++) {
+        int x = full ? dx : bx + dx;
+        if (x < 0) x += nb;
+        if (x >= nb) x -= nb;
+        if (head[row + (unsigned)x] < h) return;
+      }
+    }
+  }
+  // the particle filed under another cell waits until it is the global minimum
+  if (h == quirk_rank && h != *gmin) return;
+  const unsigned at = atomicAdd(nready, 1u);
+  if (at < cap) ready[at] = h;
+}
+
+// ---------------------------------------------------------------------------
+// Device tail loop.  Late rounds hold few, small seeds; run as separate
+// launches with a host read per round they cost more in launch and
+// synchronisation latency than in work.  One cooperative launch (all CTAs
+// resident) runs round after round on the device: the heads of the active
+// blocks, their readiness (the direct window test, or the separable min
+// filter when many blocks are active) and every ready seed's preselect,
+// refinement (FP32 approximate sums, a warp per candidate, then the exact
+// sums of the contenders and the argmax, as k_select does) and crossing by
+// one CTA, with a grid-wide barrier between the steps.  A seed with more
+// than max_cand candidates waits; the launch ends after its round and the
+// host runs the next rounds with the batched kernels.  The learned first
+// ball is not used here (the crossing starts from BALL0; the halo table does
+// not depend on it).  Every barrier wait is bounded: a wait that runs out
+// records PSOD_ERR_TIMEOUT and every CTA leaves at its next barrier.
+// ---------------------------------------------------------------------------
+enum : unsigned { TAIL_RUNNING = 0, TAIL_DONE = 1, TAIL_DEFERRED = 2, TAIL_STALLED = 3, TAIL_TIMEOUT = 4 };
+
+struct TailState {
+  unsigned nact[2];       // active-block count of list act[p]
+  unsigned nready[2];     // per round parity
+  unsigned work[2];
+  unsigned cand_used[2];
+  unsigned gmin[2];
+  unsigned deferred;
+  unsigned status;
+  unsigned rounds;        // rounds completed by the launch
+  unsigned parity;        // parity of the next round (its live list is act[parity])
+  unsigned bar_count, bar_gen;
+  unsigned long long xused[2];
+};
+
+constexpr unsigned long long BARRIER_POLLS = 1ull << 24;  // about 2-4 s of polling
+
+// Grid-wide barrier of the cooperative launch (generation counting).  The
+// fences make every write before the barrier visible to every read after
+// it.  Returns false when the wait ran out or another CTA's did.
+__device__ bool grid_barrier(TailState *ts) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    volatile unsigned *gen = &ts->bar_gen;
+    volatile unsigned *status = &ts->status;
+    const unsigned g0 = *gen;
+    __threadfence();
+    if (atomicAdd(&ts->bar_count, 1u) == gridDim.x - 1) {
+      ts->bar_count = 0;
+      __threadfence();
+      atomicAdd(&ts->bar_gen, 1u);
+    } else {
+      unsigned long long polls = 0;
+      while (*gen == g0) {
+        if (*status == TAIL_TIMEOUT || ++polls > BARRIER_POLLS) {
+          ok = 0;
+          break;
+        }
+        __nanosleep(128);
+      }
+      if (!ok) atomicExch(&ts->status, TAIL_TIMEOUT);
+    }
+    __threadfence();
+    if (*status == TAIL_TIMEOUT) ok = 0;
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// value written by another CTA before the last barrier
+__device__ __forceinline__ unsigned ld_shared_state(const unsigned *p) { return *(volatile const unsigned *)p; }
+
+__global__ void __launch_bounds__(TPB) k_tail_rounds(SodConst K, SodBufs B, TailState *ts, unsigned *act0,
+                                                    unsigned *act1, const unsigned *bbegin, unsigned *cursor,
+                                                    const unsigned *blist, unsigned *head, int nb, int rb,
+                                                    unsigned quirk_rank, unsigned *ready) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Smem &S = *reinterpret_cast<Smem *>(smem_raw);
+  __shared__ unsigned s_cnt, s_next, s_nready;
+  const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  // the round parity: every CTA flips its own copy once per round
+  unsigned q = ts->parity;
+  while (true) {
+    // this round's active count was written (heads of the previous round,
+    // or the host) before the last barrier
+    if (threadIdx.x == 0) s_cnt = ld_shared_state(&ts->nact[q]);
+    __syncthreads();
+    const unsigned cnt = s_cnt;
+    unsigned *cur = q ? act1 : act0, *nxt = q ? act0 : act1;
+    // heads (k_heads): warp-uniform strides over the active list
+    for (unsigned base = gtid - (unsigned)lane; base < cnt; base += gthreads) {
+      const unsigned i = base + (unsigned)lane;
+      const bool have = i < cnt;
+      unsigned b = 0, h = PSOD_INF_RANK, cu = 0;
+      if (have) {
+        b = cur[i];
+        const unsigned end = bbegin[b + 1];
+        cu = first_unresolved(B.resolved, cursor[b], end);
+        if (cu < end) h = blist[cu];
+      }
+      const bool live = have && h != PSOD_INF_RANK;
+      const unsigned lm = __ballot_sync(0xffffffffu, live);
+      unsigned at = 0;
+      if (lane == 0 && lm) at = atomicAdd(&ts->nact[q ^ 1u], (unsigned)__popc(lm));
+      at = __shfl_sync(0xffffffffu, at, 0);
+      unsigned hmin = live ? h : PSOD_INF_RANK;
+      for (int o = 16; o > 0; o >>= 1) hmin = min(hmin, __shfl_xor_sync(0xffffffffu, hmin, o));
+      if (lane == 0 && hmin != PSOD_INF_RANK) atomicMin(&ts->gmin[q], hmin);
+      if (have) {
+        cursor[b] = cu;
+        head[b] = h;
+        if (live) nxt[at + __popc(lm & ((1u << lane) - 1u))] = b;
+      }
+    }
+    if (!grid_barrier(ts)) return;
+    // the next round's counters (parity q^1) are free now: reset them
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      ts->nact[q] = 0;
+      ts->gmin[q ^ 1u] = PSOD_INF_RANK;
+      ts->nready[q ^ 1u] = 0;
+      ts->work[q ^ 1u] = 0;
+      ts->cand_used[q ^ 1u] = 0;
+      ts->xused[q ^ 1u] = 0;
+    }
+    if (threadIdx.x == 0) s_next = ld_shared_state(&ts->nact[q ^ 1u]);
+    __syncthreads();
+    const unsigned next = s_next;
+    const unsigned gmin = ld_shared_state(&ts->gmin[q]);
+    // readiness: the direct window test (the launch is used only while few
+    // blocks are active)
+    for (unsigned i = gtid; i < next; i += gthreads) {
+      const unsigned b = nxt[i];
+      const unsigned h = head[b];
+      if (h == PSOD_INF_RANK) continue;
+      const int bx = (int)(b % (unsigned)nb), by = (int)((b / (unsigned)nb) % (unsigned)nb),
+                bz = (int)(b / ((unsigned)nb * nb));
+      const bool full = 2 * rb + 1 >= nb;
+      const int lo = full ? 0 : -rb, hi = full ? nb - 1 : rb;
+      bool is_ready = true;
+      for (int dz = lo; dz <= hi && is_ready; dz++) {
+        int z = full ? dz : bz + dz;
+        if (z < 0) z += nb;
+        if (z >= nb) z -= nb;
+        for (int dy = lo; dy <= hi && is_ready; dy++) {
+          int y = full ? dy : by + dy;
+          if (y < 0) y += nb;
+          if (y >= nb) y -= nb;
+          const unsigned row = (unsigned)nb * ((unsigned)y + (unsigned)nb * (unsigned)z);
+          for (int dx = lo; dx <= hi; dx++) {
+            int x = full ? dx : bx + dx;
+            if (x < 0) x += nb;
+            if (x >= nb) x -= nb;
+            if (head[row + (unsigned)x] < h) {
+              is_ready = false;
+              break;
+            }
+          }
+        }
+      }
+      if (!is_ready || (h == quirk_rank && h != gmin)) continue;
+      const unsigned at = atomicAdd(&ts->nready[q], 1u);
+      if (at < B.cap_ready) ready[at] = h;
+    }
+    if (!grid_barrier(ts)) return;
+    if (threadIdx.x == 0) s_nready = ld_shared_state(&ts->nready[q]);
+    __syncthreads();
+    const unsigned nready = min(s_nready, B.cap_ready);
+    if (nready == 0) {
+      // the lowest-ranked unresolved seed is always ready: an empty round
+      // with active blocks left is a scheduler fault
+      if (blockIdx.x == 0 && threadIdx.x == 0) {
+        ts->status = next > 0 ? TAIL_STALLED : TAIL_DONE;
+        ts->parity = q ^ 1u;
+      }
+      return;
+    }
+    // the round's seeds, a CTA each
+    SodBufs Br = B;
+    Br.nready = &ts->nready[q];
+    Br.cand_used = &ts->cand_used[q];
+    Br.xused = &ts->xused[q];
+    Br.deferred = &ts->deferred;
+    Br.maxcand = nullptr;
+    Br.learn_use = 0;
+    while (true) {
+      const unsigned item = next_item(&ts->work[q]);
+      if (item >= nready) break;
+      const unsigned rank = B.ready[item];
+      prep_seed(K, Br, S, item, rank);
+      __syncthreads();
+      if (!Br.st_active[item]) continue;
+      const unsigned off = Br.st_coff[item], ncand = Br.st_cn[item];
+      const SeedGeo g = seed_geo(K, Br, rank);
+      for (unsigned k = (unsigned)w; k < ncand; k += NWARP) {
+        unsigned long long sq;
+        double sf;
+        refine_sum<false>(K, Br, Br.cand_pos[off + k], g.ic, g.jc, g.kc, sq, sf);
+        // the particle the run scan files under another cell is marked for
+        // the exact pass (an infinite entry)
+        if (lane == 0 && !isinf(Br.cand_s[off + k])) Br.cand_s[off + k] = sf;
+      }
+      __syncthreads();
+      select_seed(K, Br, S, item, rank);
+      if (Br.learn_collect) seed_features(K, Br, S, item, rank);
+      __syncthreads();
+      cross_seed(K, Br, S, item, rank);
+    }
+    if (!grid_barrier(ts)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      ts->rounds++;
+      ts->parity = q ^ 1u;
+    }
+    if (threadIdx.x == 0) s_nready = ld_shared_state(&ts->deferred);
+    __syncthreads();
+    if (s_nready) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) ts->status = TAIL_DEFERRED;
+      return;
+    }
+    q ^= 1u;
+  }
+}
+
+__global__ void k_tail_init(TailState *ts, unsigned n_active) {
+  ts->nact[0] = n_active;
+  ts->nact[1] = 0;
+  ts->nready[0] = ts->nready[1] = 0;
+  ts->work[0] = ts->work[1] = 0;
+  ts->cand_used[0] = ts->cand_used[1] = 0;
+  ts->gmin[0] = ts->gmin[1] = PSOD_INF_RANK;
+  ts->xused[0] = ts->xused[1] = 0;
+  ts->deferred = 0;
+  ts->status = TAIL_RUNNING;
+  ts->rounds = 0;
+  ts->parity = 0;
+  ts->bar_count = 0;
+  ts->bar_gen = 0;
+}
+
 __global__ void k_find_rank(const unsigned *seed_idx, long long nseed, unsigned idx, unsigned *out) {
   long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (r < nseed && seed_idx[r] == idx) *out = (unsigned)r;
@@ -2825,8 +3378,17 @@ enum {
   SC_ST_CENTRE, SC_CAND_POS, SC_CAND_SLOT, SC_CAND_S, SC_ORDER, SC_RKEYS, SC_MASS32, SC_MOFF, SC_TKEY, SC_TIDX,
   SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS, SC_CELLNCH, SC_FEAT, SC_RB0,
   SC_SBEST, SC_CELLGROUPS, SC_GROUPPREF, SC_GU, SC_CANDLIST, SC_CNT2, SC_LMAX, SC_BIG, SC_RESOLVED, SC_BIDXRANK,
-  SC_BIDXCUBE, SC_TOPG
+  SC_BIDXCUBE, SC_TOPG, SC_XKEY, SC_XIDX, SC_XPOS, SC_TAIL
 };
+
+// Rounds go to the device tail loop once the last host round had no seed
+// for the bound pass, no seed with more than TAIL_MAX_CAND candidates, at
+// most TAIL_MAX_READY ready seeds and few enough active blocks for the
+// direct readiness test; after a launch that ended on a larger seed, the
+// host runs at least TAIL_REST rounds before the next launch.
+constexpr unsigned TAIL_MAX_CAND = 1024;
+constexpr unsigned TAIL_MAX_READY = 1024;
+constexpr int TAIL_REST = 8;
 
 struct PhaseTimer {
   cudaEvent_t a, b;
@@ -2859,7 +3421,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   psod_run_stats st{};
   st.fail_rank = -1;
   st.npart_new = c->npart_new;
-  PhaseTimer t_all, t_sched, t_prep, t_ref, t_sel, t_cross, t_setup, t_out, t_learn, t_bound;
+  PhaseTimer t_all, t_sched, t_prep, t_ref, t_sel, t_cross, t_setup, t_out, t_learn, t_bound, t_tail;
   t_all.start(c->stream);
   int rc = PSOD_OK;
   const SodConst K = make_sod_const(c);
@@ -2948,12 +3510,20 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       (rc = scratch(c, SC_BIDXRANK, (size_t)nseed + 1, &bidx_of_rank)) ||
       (rc = scratch(c, SC_BIDXCUBE, (size_t)n, &bidx_of_cube)))
     return rc;
+  // crossing buffer of the bucketed balls, shared by the seeds of a round
+  const long long xcap = std::min<long long>(n, 256ll << 20);
+  unsigned long long *xkey;
+  unsigned *xidx, *xpos;
+  if ((rc = scratch(c, SC_XKEY, (size_t)xcap, &xkey)) || (rc = scratch(c, SC_XIDX, (size_t)xcap, &xidx)) ||
+      (rc = scratch(c, SC_XPOS, (size_t)xcap, &xpos)))
+    return rc;
   float *st_feat, *st_rb0;
   unsigned long long *st_sbest;
   if ((rc = scratch(c, SC_FEAT, (size_t)cap_ready * 16, &st_feat)) || (rc = scratch(c, SC_RB0, (size_t)cap_ready, &st_rb0)) ||
       (rc = scratch(c, SC_SBEST, (size_t)cap_ready, &st_sbest)))
     return rc;
-  // ctrs: 0 nready, 1..4 work counters, 5 gmin, 6 quirk rank, 7 cand_used
+  // ctrs: 0 nready, 1..4 work counters, 5 gmin, 6 quirk rank, 7 cand_used,
+  // 8/9 active-block counts, 10/11 bound and top-group pass work, 12 nbig
   unsigned *nready_d = ctrs, *work = ctrs + 1, *gmin = ctrs + 5, *qrank_d = ctrs + 6, *cand_used = ctrs + 7;
 
   PSOD_CUDA(c, cudaMemcpyAsync(edge_fac, c->edge_fac.data(), sizeof(double) * c->p.nbins, cudaMemcpyHostToDevice,
@@ -3053,9 +3623,14 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.cand_s = cand_s;
   B.cand_used = cand_used;
   B.work = work;
+  B.nbig = ctrs + 12;
+  B.maxcand = ctrs + 13;
+  B.max_cand = ~0u;
+  B.deferred = ctrs + 14;
   B.alive_cnt = nullptr;
   B.pairs = u64s + 5;
   B.touch = u64s + 7;
+  B.kept_members = u64s + 18;
   B.pair_slots = u64s + 8;
   B.ncand_total = u64s + 6;
   B.mode = c->p.mode;
@@ -3090,6 +3665,11 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.resolved = resolved;
   B.bidx_of_rank = bidx_of_rank;
   B.bidx_of_cube = bidx_of_cube;
+  B.xkey = xkey;
+  B.xidx = xidx;
+  B.xpos = xpos;
+  B.xused = u64s + 17;
+  B.xcap = (unsigned long long)xcap;
   const size_t wsmem = 8 * sizeof(WSlice);
   PSOD_CUDA(c, cudaFuncSetAttribute(k_cross_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wsmem));
   // the learned bracket needs the per-cell alive counts of the batched modes
@@ -3117,29 +3697,73 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     PSOD_CUDA(c, cudaMemcpyAsync(&n_active, ctrs + 8, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
     PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
   }
+  // Each round launches the counter reset, the heads, the readiness test and
+  // the preselect back to back; the host then reads the round's counters
+  // (its only synchronisation per round) and launches the refinement,
+  // select and crossing kernels sized by them, the bound pipeline only when
+  // some seed has BOUND_MIN_CAND candidates.  Phase timers of the refinement
+  // onwards are read one round later, when their events have completed.
+  const long long window = (long long)std::min(2 * rb + 1, nb);
+  const long long direct_cost_per_block = window * window * window, filter_cost = 3 * nblocks * window;
+  bool pending = false, pend_learn = false, pend_bound = false;
+  // device tail loop: one CTA per seed slot resident on every SM
+  int tail_grid = 0, rest = 0;
+  long long tail_rounds = 0;
+  TailState *tail = nullptr;
+  {
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, c->device);
+    int per_sm_tail = 0;
+    if (coop && (rc = scratch(c, SC_TAIL, 1, &tail)) == PSOD_OK &&
+        cudaFuncSetAttribute(k_tail_rounds, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_tail, k_tail_rounds, TPB, smem) == cudaSuccess &&
+        per_sm_tail > 0)
+      tail_grid = dev_sms * per_sm_tail;
+    if (rc) return rc;
+    cudaGetLastError();
+  }
+  auto collect_pending = [&]() {
+    if (!pending) return;
+    t_ref.collect();
+    t_sel.collect();
+    t_cross.collect();
+    if (pend_learn) t_learn.collect();
+    if (pend_bound) t_bound.collect();
+    pending = false;
+  };
   while (nseed > 0 && n_active > 0) {
     t_sched.start(c->stream);
-    PSOD_CUDA(c, cudaMemsetAsync(ctrs, 0, sizeof(unsigned) * 5, c->stream));  // nready, work[4]
-    PSOD_CUDA(c, cudaMemsetAsync(ctrs + 10, 0, sizeof(unsigned) * 2, c->stream));  // bound and top-group pass work
-    PSOD_CUDA(c, cudaMemsetAsync(gmin, 0xff, sizeof(unsigned), c->stream));
-    PSOD_CUDA(c, cudaMemsetAsync(cand_used, 0, sizeof(unsigned), c->stream));
-    PSOD_CUDA(c, cudaMemsetAsync(ctrs + 9, 0, sizeof(unsigned), c->stream));
+    k_round_reset<<<1, 32, 0, c->stream>>>(ctrs, u64s + 17);
     k_heads<<<nblk((long long)n_active, 256), 256, 0, c->stream>>>(
         act_a, n_active, bbegin, cursor, blist, resolved, head,
         quirk_rank != PSOD_INF_RANK ? gmin : nullptr, act_b, ctrs + 9);
-    k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(head, filt_a, nb, 0, rb);
-    k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(filt_a, filt_b, nb, 1, rb);
-    k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(filt_b, filt_a, nb, 2, rb);
-    k_ready<<<nblk(n_active, 256), 256, 0, c->stream>>>(act_b, ctrs + 9, head, filt_a, quirk_rank, gmin, ready,
-                                                         nready_d, cap_ready);
+    if ((long long)n_active * direct_cost_per_block <= filter_cost) {
+      k_ready_direct<<<nblk(n_active, 256), 256, 0, c->stream>>>(act_b, ctrs + 9, head, nb, rb, quirk_rank, gmin,
+                                                                 ready, nready_d, cap_ready);
+      kernels += 3;
+    } else {
+      k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(head, filt_a, nb, 0, rb);
+      k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(filt_a, filt_b, nb, 1, rb);
+      k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(filt_b, filt_a, nb, 2, rb);
+      k_ready<<<nblk(n_active, 256), 256, 0, c->stream>>>(act_b, ctrs + 9, head, filt_a, quirk_rank, gmin, ready,
+                                                           nready_d, cap_ready);
+      kernels += 6;
+    }
     t_sched.stop(c->stream);
-    kernels += 5;
-    unsigned hc[10];
+    // preselect over a persistent grid: the ready count is read on the device
+    t_prep.start(c->stream);
+    k_prep<<<seed_grid, TPB, smem, c->stream>>>(K, B);
+    t_prep.stop(c->stream);
+    kernels++;
+    unsigned hc[14];
     PSOD_CUDA(c, cudaMemcpyAsync(hc, ctrs, sizeof(hc), cudaMemcpyDeviceToHost, c->stream));
     PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
     t_sched.collect();
+    t_prep.collect();
+    collect_pending();
     unsigned nready = hc[0];
     n_active = hc[9];
+    const unsigned nbig = hc[12], maxcand = hc[13];
     std::swap(act_a, act_b);
     if (nready == 0) {
       // the lowest-ranked unresolved seed is always ready, so an empty
@@ -3149,14 +3773,12 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     }
     nready = std::min(nready, cap_ready);
     const unsigned g = std::min<unsigned>(seed_grid, nready);
-    t_prep.start(c->stream);
-    k_prep<<<g, TPB, smem, c->stream>>>(K, B);
-    t_prep.stop(c->stream);
+    B.bound_on = nbig > 0 ? 1 : 0;
     t_ref.start(c->stream);
     B.nitems_cells = 27u * nready;
     if ((rc = scan_u32(c, cell_chunks, chunk_pref, (long long)B.nitems_cells, true))) return rc;
-    if ((rc = scan_u32(c, cell_groups, group_pref, (long long)B.nitems_cells, true))) return rc;
     if (B.bound_on) {
+      if ((rc = scan_u32(c, cell_groups, group_pref, (long long)B.nitems_cells, true))) return rc;
       t_bound.start(c->stream);
       k_zero_groups<<<ref_grid, 256, 0, c->stream>>>(group_pref + B.nitems_cells, g_u);
       PSOD_CUDA(c, cudaMemsetAsync(s_lmax, 0, sizeof(unsigned) * nready, c->stream));
@@ -3202,38 +3824,72 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     k_cross<<<g, TPB, smem, c->stream>>>(K, Bc);
     t_cross.stop(c->stream);
     PSOD_CUDA(c, cudaGetLastError());
-    t_prep.collect();
-    t_ref.collect();
-    t_sel.collect();
-    t_cross.collect();
-    if (B.learn_use) t_learn.collect();
-    if (B.bound_on) t_bound.collect();
+    pending = true;
+    pend_learn = B.learn_use;
+    pend_bound = B.bound_on;
 #ifdef PSOD_TRACE_ROUNDS
     {
       // diagnostic build only (-DPSOD_TRACE_ROUNDS): one line per round on
       // stderr with the ready seeds, active blocks, candidates and phase times
+      collect_pending();
       unsigned cu = 0;
       unsigned long long tv[16];
       cudaMemcpyAsync(&cu, cand_used, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream);
       cudaMemcpyAsync(tv, u64s, sizeof(tv), cudaMemcpyDeviceToHost, c->stream);
       cudaStreamSynchronize(c->stream);
       fprintf(stderr,
-              "psod round %lld ready %u active %u cand %u sched %.3f prep %.3f refine %.3f select %.3f cross %.3f "
+              "psod round %lld ready %u active %u cand %u nbig %u sched %.3f prep %.3f refine %.3f select %.3f cross %.3f "
               "pairs %llu slots %llu staged %llu bound %.3f items %llu pruned_cand %llu\n",
-              rounds, nready, n_active, cu, t_sched.last, t_prep.last, t_ref.last, t_sel.last, t_cross.last, tv[5], tv[8],
-              tv[9], B.bound_on ? t_bound.last : 0.0, tv[14], tv[15]);
+              rounds, nready, n_active, cu, nbig, t_sched.last, t_prep.last, t_ref.last, t_sel.last, t_cross.last,
+              tv[5], tv[8], tv[9], B.bound_on ? t_bound.last : 0.0, tv[14], tv[15]);
     }
 #endif
     rounds++;
     seed_launches += 4;
     kernels += 4;
+    rest++;
+    if (tail_grid > 0 && nbig == 0 && maxcand <= TAIL_MAX_CAND && nready <= TAIL_MAX_READY && rest >= TAIL_REST &&
+        n_active > 0 && (long long)n_active * direct_cost_per_block <= filter_cost) {
+      // the following rounds on the device, until a larger seed or the end
+      k_tail_init<<<1, 1, 0, c->stream>>>(tail, n_active);
+      SodBufs Bt = B;
+      Bt.max_cand = TAIL_MAX_CAND;
+      Bt.st_big = nullptr;
+      Bt.touch = u64s + 19;  // the tail's crossings counted apart from k_cross
+      Bt.kept_members = u64s + 20;
+      void *args[] = {(void *)&K,     (void *)&Bt,   (void *)&tail, (void *)&act_a,      (void *)&act_b,
+                      (void *)&bbegin, (void *)&cursor, (void *)&blist, (void *)&head, (void *)&nb,
+                      (void *)&rb,    (void *)&quirk_rank, (void *)&ready};
+      t_tail.start(c->stream);
+      PSOD_CUDA(c, cudaLaunchCooperativeKernel((const void *)k_tail_rounds, dim3(tail_grid), dim3(TPB), args, smem,
+                                               c->stream));
+      t_tail.stop(c->stream);
+      kernels += 2;
+      TailState ts;
+      PSOD_CUDA(c, cudaMemcpyAsync(&ts, tail, sizeof(ts), cudaMemcpyDeviceToHost, c->stream));
+      PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+      t_tail.collect();
+      collect_pending();
+      rounds += ts.rounds;
+      tail_rounds += ts.rounds;
+      if (ts.status == TAIL_TIMEOUT)
+        return set_err(c, PSOD_ERR_TIMEOUT, "device tail loop: a grid barrier wait ran out");
+      if (ts.status == TAIL_STALLED) return set_err(c, PSOD_ERR_STATE, "scheduler stalled with unresolved seeds");
+      if (ts.status != TAIL_DONE && ts.status != TAIL_DEFERRED)
+        return set_err(c, PSOD_ERR_STATE, "device tail loop ended in an unknown state");
+      // the live list and its count for the host's next round
+      if (ts.parity) std::swap(act_a, act_b);
+      n_active = ts.status == TAIL_DONE ? 0u : ts.nact[ts.parity];
+      rest = 0;
+    }
   }
+  collect_pending();
   // every seed must end processed or claimed; u64s[16] counts those that did not
   if (nseed > 0) {
     k_count_unresolved<<<nblk(nseed / 32 + 1, 256), 256, 0, c->stream>>>(resolved, nseed, u64s + 16);
     kernels++;
   }
-  unsigned long long hv[17];
+  unsigned long long hv[21];
   PSOD_CUDA(c, cudaMemcpyAsync(hv, u64s, sizeof(hv), cudaMemcpyDeviceToHost, c->stream));
   PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
   st.rounds = rounds;
@@ -3248,7 +3904,10 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   st.sod_launches = seed_launches;
   st.ncandidates = (int64_t)hv[6];
   st.refine_pairs = (int64_t)hv[5];
-  st.cross_touch = (int64_t)hv[7];
+  st.cross_touch = (int64_t)(hv[7] + hv[19]);
+  st.tail_touch = (int64_t)hv[19];
+  st.cross_members = (int64_t)hv[18];
+  st.tail_members = (int64_t)hv[20];
   st.refine_slots = (int64_t)hv[8];
   st.ms_learn = t_learn.total;
   st.bracket_hits = (int64_t)hv[10];
@@ -3258,6 +3917,8 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   st.ms_refine_bound = t_bound.total;
   st.refine_items = (int64_t)hv[14];
   st.refine_pruned = (int64_t)hv[15];
+  st.ms_tail = t_tail.total;
+  st.tail_rounds = tail_rounds;
   c->nhalo = 0;
   c->nmember = 0;
   c->sod_done = false;

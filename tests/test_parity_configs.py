@@ -70,6 +70,8 @@ def test_configuration_1_box_all_modes(cfg1_box, cfg1_oracle, mode):
         t = s.halos()
     assert nn == rc.npart_new == rr.npart_new
     assert st["nprocessed"] == rc.nprocessed
+    # the late rounds ran in the device tail loop
+    assert 0 < st["tail_rounds"] < st["rounds"]
     assert st["cross_touch"] == rc.cross_touch
     for r in (rc, rr):
         for f in FIELDS:
