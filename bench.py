@@ -43,6 +43,11 @@ WORKLOADS = {
     512: dict(nmax_halo=200000, box="512^3, 656.25 Mpc/h, halo N in [20, 2e5]"),
     1024: dict(nmax_halo=1000000, box="1024^3, 1312.5 Mpc/h, halo N in [20, 1e6]"),
 }
+# the heavy-tail stress box: the 1024^3 law plus 16 clusters of 5e6 particles
+# (NFW c = 4, axis ratios 1:0.8:0.6), -npu 1e7, Delta 200 and 500, 64 bins
+HEAVY = dict(nx=1024, nmax_halo=1000000, n_clusters=16, cluster_size=5_000_000, npu=10_000_000,
+             delta_extra=(500.0,), nbins=64,
+             box="1024^3 + 16 clusters of 5e6 (c=4, axes 1:0.8:0.6), halo N in [20, 1e6], Delta 200/500, 64 bins")
 
 
 # the 1024^3 workload computes three thresholds in one pass, with 48 bins
@@ -62,10 +67,13 @@ def inputs_fit_l2(nx):
     return nx**3 * (12 + 8) < (126 << 20) * 2
 
 
-def workload_config(nx, ndelta):
+def workload_config(nx, ndelta, heavy=False):
     """The ``config`` object of both arms: the workload alone (no
     implementation or measurement keys), so the two lines name the same
     configuration."""
+    if heavy:
+        return {"workload": HEAVY["box"], "nx": HEAVY["nx"], "particles": HEAVY["nx"] ** 3, "npu": HEAVY["npu"],
+                "delta": [200.0, 500.0], "nbins": HEAVY["nbins"], "l2": "inputs larger than L2"}
     wl = WORKLOADS.get(nx, dict(nmax_halo=20000, box=f"{nx}^3"))
     return {
         "workload": wl["box"],
@@ -222,18 +230,21 @@ def run_ours(args):
     world, rank, local = dist_setup()
     dev = local if world > 1 else 0
     torch.cuda.set_device(dev)
-    nx = args.nx
+    nx = HEAVY["nx"] if args.heavy else args.nx
     wl = WORKLOADS.get(nx, dict(nmax_halo=20000, box=f"{nx}^3"))
     thresholds = dict(delta_extra=EXTRA_DELTAS, nbins=EXTRA_BINS) if args.ndelta else {}
+    if args.heavy:
+        thresholds = dict(delta_extra=HEAVY["delta_extra"], nbins=HEAVY["nbins"])
     model, bracket = None, None
     if args.mode == "learned":
         model, bracket = train_bracket(args, dev, thresholds)
-    box = synth.make_box(nx, nmax_halo=wl["nmax_halo"], seed=args.seed + rank, device=f"cuda:{dev}")
+    clusters = dict(n_clusters=HEAVY["n_clusters"], cluster_size=HEAVY["cluster_size"]) if args.heavy else {}
+    box = synth.make_box(nx, nmax_halo=wl["nmax_halo"], seed=args.seed + rank, device=f"cuda:{dev}", **clusters)
     pos_d, ids_d = box.pos, box.ids
     del box
     torch.cuda.empty_cache()  # hand the generator's temporaries back before the engine allocates
     n = int(pos_d.shape[0])
-    params = dict(npu=npu_for(nx), mode=args.mode_id, **thresholds)
+    params = dict(npu=HEAVY["npu"] if args.heavy else npu_for(nx), mode=args.mode_id, **thresholds)
     sod = SphericalOverdensity(nx, device=dev, **params)
     if model is not None:
         sod.learn_set_model(model)
@@ -333,7 +344,7 @@ def run_ours(args):
         "data": "synthetic NFW-mixture box (seeded); inputs resident in HBM",
         "mode": args.mode,
         "parallelism": f"replicas x{world}",
-        "config": workload_config(nx, args.ndelta),
+        "config": workload_config(nx, args.ndelta, args.heavy),
         "detail": {
             "halos": nhalo_all,
             "members": s["nmember"],
@@ -690,6 +701,8 @@ def main():
     ap.add_argument("--delta200-only", dest="ndelta", action="store_false",
                     help="Delta = 200 and 60 bins only (default: 200, 500 and 178 in one pass, 48 bins)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--heavy", action="store_true",
+                    help="the heavy-tail stress box (1024^3 + 16 clusters of 5e6, -npu 1e7, Delta 200/500, 64 bins)")
     args = ap.parse_args()
     args.mode_id = {"plain": 0, "batched": 1, "learned": 2}[args.mode]
     if args.gpus > 1 and "WORLD_SIZE" not in os.environ:

@@ -292,7 +292,9 @@ enum : int {
   SLOT_LEARN_Y,         // learned bracket: outputs / raw targets of an API call
   SLOT_LEARN_XB,        // learned bracket: standardised bf16 inputs
   SLOT_LEARN_TS,        // learned bracket: standardised targets
-  SLOT_LEARN_PERM       // learned bracket: batch order
+  SLOT_LEARN_PERM,      // learned bracket: batch order
+  SLOT_SLAB_REC,        // load: particle records grouped by slab (n float4)
+  SLOT_SLABS            // load: slab counts and write cursors
 };
 
 // learned radius bracket (psod_learn.cu)

@@ -1040,6 +1040,59 @@ __device__ __forceinline__ bool in_sel2(const SodConst &K, int x, int y, int z, 
 // Refinement sum of one candidate, warp-cooperative.  exact: canonical
 // int64 fixed-point sum of FP64 terms (main:1840-1859); else the FP64 sum of
 // FP32 terms.  Result valid in lane 0.
+// The alive records of the 3x3x3 cells around cell (cx, cy, cz) that lie
+// within +-2 cells of the seed cell (ic, jc, kc), as one list: lane l < 27
+// holds cell l's record range (begin, exclusive prefix of the lengths);
+// `at` maps a list position to its cube slot.  One warp; all lanes call.
+struct NbrList {
+  unsigned beg, pre, total;  // this lane's cell (lanes < 27), the list length
+  __device__ __forceinline__ unsigned at(unsigned t) const {
+    // the last cell whose prefix is <= t (cells 0..26 held by lanes 0..26):
+    // five halvings cover 27 cells; every lane takes all five steps, so
+    // every shuffle has the whole warp
+    int lo = 0, hi = 26;
+#pragma unroll
+    for (int step = 0; step < 5; step++) {
+      const int mid = (lo + hi + 1) >> 1;
+      const unsigned pm = __shfl_sync(0xffffffffu, pre, mid);
+      if (lo < hi) {
+        if (pm <= t) lo = mid;
+        else hi = mid - 1;
+      }
+    }
+    return __shfl_sync(0xffffffffu, beg, lo) + (t - __shfl_sync(0xffffffffu, pre, lo));
+  }
+};
+
+__device__ __forceinline__ NbrList nbr_list(const SodConst &K, const SodBufs &B, int cx, int cy, int cz, int ic,
+                                            int jc, int kc) {
+  const int lane = threadIdx.x & 31;
+  unsigned beg = 0, len = 0;
+  if (lane < 27) {
+    const int xx = wrapi(cx + lane % 3 - 1, K.nx), yy = wrapi(cy + (lane / 3) % 3 - 1, K.nx),
+              zz = wrapi(cz + lane / 9 - 1, K.nx);
+    if (abs(pdiff(xx, ic, K.nx)) <= 2 && abs(pdiff(yy, jc, K.nx)) <= 2 && abs(pdiff(zz, kc, K.nx)) <= 2) {
+      const unsigned long long c = (unsigned long long)xx + (unsigned long long)K.nx * ((unsigned)yy + (unsigned long long)K.nx * (unsigned)zz);
+      beg = B.cs[c];
+      len = B.cs[c + 1] - beg;
+    }
+  }
+  unsigned inc = len;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  NbrList L;
+  L.beg = beg;
+  L.pre = inc - len;
+  L.total = __shfl_sync(0xffffffffu, inc, 26);
+  return L;
+}
+
+// Refinement sum of one candidate, warp-cooperative.  exact: canonical
+// int64 fixed-point sum of FP64 terms (main:1840-1859); else the FP64 sum of
+// FP32 terms.  Result valid in lane 0.  The 27 neighbour cells are walked
+// as one list, 32 records a step.
 template <bool EXACT>
 __device__ __forceinline__ void refine_sum(const SodConst &K, const SodBufs &B, unsigned cp, int ic, int jc, int kc,
                            unsigned long long &sq_out, double &sf_out, unsigned *visits = nullptr) {
@@ -1052,36 +1105,30 @@ __device__ __forceinline__ void refine_sum(const SodConst &K, const SodBufs &B, 
   const float e2f = (float)K.eps2;
   unsigned long long sq = 0;
   double sf = 0.0;
-  for (int nrow = 0; nrow < 9; nrow++) {
-    const int ny = wrapi(pcy + nrow % 3 - 1, K.nx), nz = wrapi(pcz + nrow / 3 - 1, K.nx);
-    if (abs(pdiff(ny, jc, K.nx)) > 2 || abs(pdiff(nz, kc, K.nx)) > 2) continue;
-    const unsigned long long nbase = (unsigned long long)K.nx * ((unsigned)ny + (unsigned long long)K.nx * (unsigned)nz);
-    for (int ndi = -1; ndi <= 1; ndi++) {
-      const int nxc = wrapi(pcx + ndi, K.nx);
-      if (abs(pdiff(nxc, ic, K.nx)) > 2) continue;
-      const unsigned nb = B.cs[nbase + (unsigned)nxc], ne = B.cs[nbase + (unsigned)nxc + 1];
-      if (visits && lane == 0) *visits += ne - nb;
-      for (unsigned q = nb + lane; q < ne; q += 32) {
-        const float4 nv = B.cube[q];
-        if (__float_as_uint(nv.w) & PSOD_DEAD_BIT) continue;
-        const float nxg = to_grid(nv.x, K.nxf), nyg = to_grid(nv.y, K.nxf), nzg = to_grid(nv.z, K.nxf);
-        if (EXACT) {
-          const double d2 = min_image_d2((double)nxg, (double)nyg, (double)nzg, cx, cy, cz, K.tx);
-          if (d2 <= K.rmin2) {
-            const double t = ddiv(1.0, dsqrt(dadd(d2, K.eps2)));
-            sq += (unsigned long long)__double2ll_rn(dmul(t, 1099511627776.0));
-          }
-        } else {
-          const float dx = mi_dx(nxg, cxg, K.nxf), dy = mi_dx(nyg, cyg, K.nxf), dz = mi_dx(nzg, czg, K.nxf);
-          const float d2f = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-          bool in = d2f <= 0.99999f;
-          if (!in && d2f <= 1.00001f) {
-            const double d2 = min_image_d2((double)nxg, (double)nyg, (double)nzg, cx, cy, cz, K.tx);
-            in = d2 <= K.rmin2;
-          }
-          if (in) sf += (double)rsqrtf(__fadd_rn(d2f, e2f));
-        }
+  const NbrList L = nbr_list(K, B, pcx, pcy, pcz, ic, jc, kc);
+  if (visits && lane == 0) *visits += L.total;
+  for (unsigned t0 = 0; t0 < L.total; t0 += 32) {
+    const unsigned t = t0 + (unsigned)lane;
+    const unsigned q = L.at(t < L.total ? t : L.total - 1);
+    if (t >= L.total) continue;
+    const float4 nv = B.cube[q];
+    if (__float_as_uint(nv.w) & PSOD_DEAD_BIT) continue;
+    const float nxg = to_grid(nv.x, K.nxf), nyg = to_grid(nv.y, K.nxf), nzg = to_grid(nv.z, K.nxf);
+    if (EXACT) {
+      const double d2 = min_image_d2((double)nxg, (double)nyg, (double)nzg, cx, cy, cz, K.tx);
+      if (d2 <= K.rmin2) {
+        const double tt = ddiv(1.0, dsqrt(dadd(d2, K.eps2)));
+        sq += (unsigned long long)__double2ll_rn(dmul(tt, 1099511627776.0));
       }
+    } else {
+      const float dx = mi_dx(nxg, cxg, K.nxf), dy = mi_dx(nyg, cyg, K.nxf), dz = mi_dx(nzg, czg, K.nxf);
+      const float d2f = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+      bool in = d2f <= 0.99999f;
+      if (!in && d2f <= 1.00001f) {
+        const double d2 = min_image_d2((double)nxg, (double)nyg, (double)nzg, cx, cy, cz, K.tx);
+        in = d2 <= K.rmin2;
+      }
+      if (in) sf += (double)rsqrtf(__fadd_rn(d2f, e2f));
     }
   }
   // the particle the run scan files under another cell
@@ -1097,9 +1144,9 @@ __device__ __forceinline__ void refine_sum(const SodConst &K, const SodBufs &B, 
         const double d2 = min_image_d2((double)to_grid(qv.x, K.nxf), (double)to_grid(qv.y, K.nxf),
                                        (double)to_grid(qv.z, K.nxf), cx, cy, cz, K.tx);
         if (d2 <= K.rmin2) {
-          const double t = ddiv(1.0, dsqrt(dadd(d2, K.eps2)));
-          if (EXACT) sq += (unsigned long long)__double2ll_rn(dmul(t, 1099511627776.0));
-          else sf += t;
+          const double tt = ddiv(1.0, dsqrt(dadd(d2, K.eps2)));
+          if (EXACT) sq += (unsigned long long)__double2ll_rn(dmul(tt, 1099511627776.0));
+          else sf += tt;
         }
       }
     }
@@ -2888,43 +2935,48 @@ __global__ void k_round_reset(unsigned *ctrs, unsigned long long *xused) {
   if (t == 0) *xused = 0ull;
 }
 
-// Readiness of each active block's head by a direct look at the heads of
-// its window (Chebyshev radius rb blocks, periodic; the whole axis when the
+// Readiness of an active block's head by a direct look at the heads of its
+// window (Chebyshev radius rb blocks, periodic; the whole axis when the
 // window covers it): ready when no head there is lower.  The same set as the
-// separable min filter + k_ready, for rounds with few active blocks.
-__global__ void k_ready_direct(const unsigned *active, const unsigned *nactive, const unsigned *head, int nb, int rb,
-                               unsigned quirk_rank, const unsigned *gmin, unsigned *ready, unsigned *nready,
-                               unsigned cap) {
-  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= *nactive) return;
-  const unsigned b = active[i];
+// separable min filter + k_ready, for rounds with few active blocks.  One
+// warp per block: the lanes read the window's heads side by side.
+__device__ __forceinline__ void ready_test_warp(unsigned b, const unsigned *head, int nb, int rb, unsigned quirk_rank,
+                                                unsigned gmin, unsigned *ready, unsigned *nready, unsigned cap) {
+  const int lane = threadIdx.x & 31;
   const unsigned h = head[b];
   if (h == PSOD_INF_RANK) return;
   const int bx = (int)(b % (unsigned)nb), by = (int)((b / (unsigned)nb) % (unsigned)nb),
             bz = (int)(b / ((unsigned)nb * nb));
   const bool full = 2 * rb + 1 >= nb;
-  const int lo = full ? 0 : -rb, hi = full ? nb - 1 : rb;
-  for (int dz = lo; dz <= hi; dz++) {
-    int z = full ? dz : bz + dz;
+  const int side = full ? nb : 2 * rb + 1, lo = full ? 0 : -rb;
+  const int nwin = side * side * side;
+  bool lower = false;
+  for (int e = lane; e < nwin; e += 32) {
+    const int dx = e % side + lo, dy = (e / side) % side + lo, dz = e / (side * side) + lo;
+    int x = full ? dx : bx + dx, y = full ? dy : by + dy, z = full ? dz : bz + dz;
+    if (x < 0) x += nb;
+    if (x >= nb) x -= nb;
+    if (y < 0) y += nb;
+    if (y >= nb) y -= nb;
     if (z < 0) z += nb;
     if (z >= nb) z -= nb;
-    for (int dy = lo; dy <= hi; dy++) {
-      int y = full ? dy : by + dy;
-      if (y < 0) y += nb;
-      if (y >= nb) y -= nb;
-      const unsigned row = (unsigned)nb * ((unsigned)y + (unsigned)nb * (unsigned)z);
-      for (int dx = lo; dx <= hi; dx++) {
-        int x = full ? dx : bx + dx;
-        if (x < 0) x += nb;
-        if (x >= nb) x -= nb;
-        if (head[row + (unsigned)x] < h) return;
-      }
-    }
+    lower |= head[(unsigned)x + (unsigned)nb * ((unsigned)y + (unsigned)nb * (unsigned)z)] < h;
   }
+  if (__any_sync(0xffffffffu, lower)) return;
   // the particle filed under another cell waits until it is the global minimum
-  if (h == quirk_rank && h != *gmin) return;
-  const unsigned at = atomicAdd(nready, 1u);
-  if (at < cap) ready[at] = h;
+  if (h == quirk_rank && h != gmin) return;
+  if (lane == 0) {
+    const unsigned at = atomicAdd(nready, 1u);
+    if (at < cap) ready[at] = h;
+  }
+}
+
+__global__ void k_ready_direct(const unsigned *active, const unsigned *nactive, const unsigned *head, int nb, int rb,
+                               unsigned quirk_rank, const unsigned *gmin, unsigned *ready, unsigned *nready,
+                               unsigned cap) {
+  const unsigned wi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (wi >= *nactive) return;
+  ready_test_warp(active[wi], head, nb, rb, quirk_rank, *gmin, ready, nready, cap);
 }
 
 // ---------------------------------------------------------------------------
@@ -2943,12 +2995,118 @@ __global__ void k_ready_direct(const unsigned *active, const unsigned *nactive, 
 // not depend on it).  Every barrier wait is bounded: a wait that runs out
 // records PSOD_ERR_TIMEOUT and every CTA leaves at its next barrier.
 // ---------------------------------------------------------------------------
+// Approximate refinement sums of the candidates of one candidate cell (o of
+// the 27 around the seed) by one warp (the device tail loop): 32 candidates
+// a pass, the alive records of the cell's 3x3x3 neighbourhood staged 32 at
+// a time in the warp's tile and summed by tile_terms, i.e. the same FP32
+// terms and partial sums as k_refine_warp and the same error bound.
+__device__ __forceinline__ void tail_refine_cell(const SodConst &K, const SodBufs &B, unsigned slot, int o,
+                                                 const SeedGeo &g, RecTile &T) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  auto clear = [&](int c) {  // the 3-cell coordinate window stays clear of the box edge
+    double s0 = (double)(c - 1) + K.xs;
+    s0 -= K.tx * floor(s0 / K.tx);
+    return s0 >= 1.0 && s0 + 3.0 <= K.tx - 1.0;
+  };
+  {
+    const unsigned ci = slot * 27u + (unsigned)o;
+    const unsigned cnt = B.cell_cnt[ci];
+    if (cnt == 0) return;
+    const unsigned coff = B.cell_off[ci];
+    const int cxc = wrapi(g.ic + o / 9 - 1, K.nx), cyc = wrapi(g.jc + (o / 3) % 3 - 1, K.nx),
+              czc = wrapi(g.kc + o % 3 - 1, K.nx);
+    const bool wf = clear(cxc) && clear(cyc) && clear(czc);
+    const NbrList L = nbr_list(K, B, cxc, cyc, czc, g.ic, g.jc, g.kc);
+    for (unsigned c0 = 0; c0 < cnt; c0 += 32) {
+      const unsigned k = c0 + (unsigned)lane;
+      const bool have = k < cnt;
+      const unsigned cp = have ? B.cand_pos[coff + k] : 0u;
+      const bool active = have && !(K.has_quirk && cp == K.quirk_pos);  // that one goes exact
+      float cx = 1e18f, cy = 1e18f, cz = 1e18f;
+      if (active) {
+        const float4 cv = B.cube[cp];
+        cx = to_grid(cv.x, K.nxf);
+        cy = to_grid(cv.y, K.nxf);
+        cz = to_grid(cv.z, K.nxf);
+      }
+      double sum = 0.0;
+      unsigned fill = 0;
+      for (unsigned t0 = 0; t0 < L.total; t0 += 32) {
+        const unsigned t = t0 + (unsigned)lane;
+        const unsigned q = L.at(t < L.total ? t : L.total - 1);
+        bool keep = false;
+        float rx = 0.f, ry = 0.f, rz = 0.f;
+        if (t < L.total) {
+          const float4 v = B.cube[q];
+          keep = !(__float_as_uint(v.w) & PSOD_DEAD_BIT);
+          rx = to_grid(v.x, K.nxf);
+          ry = to_grid(v.y, K.nxf);
+          rz = to_grid(v.z, K.nxf);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        if (keep) {  // fill < 32: index < 64
+          const unsigned at = fill + __popc(m & lt);
+          T.x[at] = rx;
+          T.y[at] = ry;
+          T.z[at] = rz;
+        }
+        fill += (unsigned)__popc(m);
+        __syncwarp();
+        if (fill >= 32u) {
+          if (active) sum += wf ? tile_terms<true>(T, 32u, cx, cy, cz, K) : tile_terms<false>(T, 32u, cx, cy, cz, K);
+          __syncwarp();
+          if ((unsigned)lane < fill - 32u) {
+            T.x[lane] = T.x[32 + lane];
+            T.y[lane] = T.y[32 + lane];
+            T.z[lane] = T.z[32 + lane];
+          }
+          __syncwarp();
+          fill -= 32u;
+        }
+      }
+      if (fill > 0) {
+        // pad to a multiple of 8 with records far from every candidate
+        if ((unsigned)lane < ((8u - (fill & 7u)) & 7u)) {
+          T.x[fill + lane] = 1e18f;
+          T.y[fill + lane] = 1e18f;
+          T.z[fill + lane] = 1e18f;
+        }
+        __syncwarp();
+        if (active) sum += wf ? tile_terms<true>(T, fill, cx, cy, cz, K) : tile_terms<false>(T, fill, cx, cy, cz, K);
+        __syncwarp();
+      }
+      if (active && K.has_quirk) {
+        // the particle the run scan files under another cell: counted if
+        // that cell is in x_sel2 but outside this candidate cell's 27
+        // neighbours (as k_refine_warp does)
+        const int ax = (int)(K.quirk_listed % K.nx), ay = (int)((K.quirk_listed / K.nx) % K.nx),
+                  az = (int)(K.quirk_listed / ((unsigned)K.nx * K.nx));
+        const bool listed_in_sel2 = in_sel2(K, ax, ay, az, g.ic, g.jc, g.kc);
+        const bool seen = abs(pdiff(ax, cxc, K.nx)) <= 1 && abs(pdiff(ay, cyc, K.nx)) <= 1 && abs(pdiff(az, czc, K.nx)) <= 1;
+        if (listed_in_sel2 && !seen) {
+          const float4 qv = B.cube[K.quirk_pos];
+          if (!(__float_as_uint(qv.w) & PSOD_DEAD_BIT)) {
+            const double d2 = min_image_d2((double)to_grid(qv.x, K.nxf), (double)to_grid(qv.y, K.nxf),
+                                           (double)to_grid(qv.z, K.nxf), (double)cx, (double)cy, (double)cz, K.tx);
+            if (d2 <= K.rmin2) sum += ddiv(1.0, dsqrt(dadd(d2, K.eps2)));
+          }
+        }
+      }
+      if (active) B.cand_s[coff + k] = sum;
+    }
+  }
+}
+
 enum : unsigned { TAIL_RUNNING = 0, TAIL_DONE = 1, TAIL_DEFERRED = 2, TAIL_STALLED = 3, TAIL_TIMEOUT = 4 };
 
 struct TailState {
   unsigned nact[2];       // active-block count of list act[p]
   unsigned nready[2];     // per round parity
-  unsigned work[2];
+  unsigned work[2];       // work counters of the seed steps: preselect,
+  unsigned work_r[2];     // refinement (candidate cells), select, crossing
+  unsigned work_s[2];
+  unsigned work_c[2];
   unsigned cand_used[2];
   unsigned gmin[2];
   unsigned deferred;
@@ -2957,7 +3115,16 @@ struct TailState {
   unsigned parity;        // parity of the next round (its live list is act[parity])
   unsigned bar_count, bar_gen;
   unsigned long long xused[2];
+  // time spent by the launch in each step (ns, block 0's clock, each step
+  // up to the barrier that ends it)
+  unsigned long long t_heads, t_ready, t_seeds;
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 constexpr unsigned long long BARRIER_POLLS = 1ull << 24;  // about 2-4 s of polling
 
@@ -3006,8 +3173,9 @@ __global__ void __launch_bounds__(TPB) k_tail_rounds(SodConst K, SodBufs B, Tail
   extern __shared__ __align__(16) unsigned char smem_raw[];
   Smem &S = *reinterpret_cast<Smem *>(smem_raw);
   __shared__ unsigned s_cnt, s_next, s_nready;
+  __shared__ RecTile t_tiles[NWARP];
   const unsigned gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   // the round parity: every CTA flips its own copy once per round
   unsigned q = ts->parity;
   while (true) {
@@ -3016,6 +3184,8 @@ __global__ void __launch_bounds__(TPB) k_tail_rounds(SodConst K, SodBufs B, Tail
     if (threadIdx.x == 0) s_cnt = ld_shared_state(&ts->nact[q]);
     __syncthreads();
     const unsigned cnt = s_cnt;
+    const bool timer = blockIdx.x == 0 && threadIdx.x == 0;
+    unsigned long long tk = timer ? global_ns() : 0ull;
     unsigned *cur = q ? act1 : act0, *nxt = q ? act0 : act1;
     // heads (k_heads): warp-uniform strides over the active list
     for (unsigned base = gtid - (unsigned)lane; base < cnt; base += gthreads) {
@@ -3043,12 +3213,20 @@ __global__ void __launch_bounds__(TPB) k_tail_rounds(SodConst K, SodBufs B, Tail
       }
     }
     if (!grid_barrier(ts)) return;
+    if (timer) {
+      const unsigned long long now = global_ns();
+      ts->t_heads += now - tk;
+      tk = now;
+    }
     // the next round's counters (parity q^1) are free now: reset them
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       ts->nact[q] = 0;
       ts->gmin[q ^ 1u] = PSOD_INF_RANK;
       ts->nready[q ^ 1u] = 0;
       ts->work[q ^ 1u] = 0;
+      ts->work_r[q ^ 1u] = 0;
+      ts->work_s[q ^ 1u] = 0;
+      ts->work_c[q ^ 1u] = 0;
       ts->cand_used[q ^ 1u] = 0;
       ts->xused[q ^ 1u] = 0;
     }
@@ -3057,41 +3235,15 @@ __global__ void __launch_bounds__(TPB) k_tail_rounds(SodConst K, SodBufs B, Tail
     const unsigned next = s_next;
     const unsigned gmin = ld_shared_state(&ts->gmin[q]);
     // readiness: the direct window test (the launch is used only while few
-    // blocks are active)
-    for (unsigned i = gtid; i < next; i += gthreads) {
-      const unsigned b = nxt[i];
-      const unsigned h = head[b];
-      if (h == PSOD_INF_RANK) continue;
-      const int bx = (int)(b % (unsigned)nb), by = (int)((b / (unsigned)nb) % (unsigned)nb),
-                bz = (int)(b / ((unsigned)nb * nb));
-      const bool full = 2 * rb + 1 >= nb;
-      const int lo = full ? 0 : -rb, hi = full ? nb - 1 : rb;
-      bool is_ready = true;
-      for (int dz = lo; dz <= hi && is_ready; dz++) {
-        int z = full ? dz : bz + dz;
-        if (z < 0) z += nb;
-        if (z >= nb) z -= nb;
-        for (int dy = lo; dy <= hi && is_ready; dy++) {
-          int y = full ? dy : by + dy;
-          if (y < 0) y += nb;
-          if (y >= nb) y -= nb;
-          const unsigned row = (unsigned)nb * ((unsigned)y + (unsigned)nb * (unsigned)z);
-          for (int dx = lo; dx <= hi; dx++) {
-            int x = full ? dx : bx + dx;
-            if (x < 0) x += nb;
-            if (x >= nb) x -= nb;
-            if (head[row + (unsigned)x] < h) {
-              is_ready = false;
-              break;
-            }
-          }
-        }
-      }
-      if (!is_ready || (h == quirk_rank && h != gmin)) continue;
-      const unsigned at = atomicAdd(&ts->nready[q], 1u);
-      if (at < B.cap_ready) ready[at] = h;
-    }
+    // blocks are active), a warp per active block
+    for (unsigned wi = gtid >> 5; wi < next; wi += gthreads >> 5)
+      ready_test_warp(nxt[wi], head, nb, rb, quirk_rank, gmin, ready, &ts->nready[q], B.cap_ready);
     if (!grid_barrier(ts)) return;
+    if (timer) {
+      const unsigned long long now = global_ns();
+      ts->t_ready += now - tk;
+      tk = now;
+    }
     if (threadIdx.x == 0) s_nready = ld_shared_state(&ts->nready[q]);
     __syncthreads();
     const unsigned nready = min(s_nready, B.cap_ready);
@@ -3112,33 +3264,46 @@ __global__ void __launch_bounds__(TPB) k_tail_rounds(SodConst K, SodBufs B, Tail
     Br.deferred = &ts->deferred;
     Br.maxcand = nullptr;
     Br.learn_use = 0;
+    // preselect: a CTA per seed
     while (true) {
       const unsigned item = next_item(&ts->work[q]);
       if (item >= nready) break;
-      const unsigned rank = B.ready[item];
-      prep_seed(K, Br, S, item, rank);
-      __syncthreads();
-      if (!Br.st_active[item]) continue;
-      const unsigned off = Br.st_coff[item], ncand = Br.st_cn[item];
-      const SeedGeo g = seed_geo(K, Br, rank);
-      for (unsigned k = (unsigned)w; k < ncand; k += NWARP) {
-        unsigned long long sq;
-        double sf;
-        refine_sum<false>(K, Br, Br.cand_pos[off + k], g.ic, g.jc, g.kc, sq, sf);
-        // the particle the run scan files under another cell is marked for
-        // the exact pass (an infinite entry)
-        if (lane == 0 && !isinf(Br.cand_s[off + k])) Br.cand_s[off + k] = sf;
+      prep_seed(K, Br, S, item, B.ready[item]);
+    }
+    if (!grid_barrier(ts)) return;
+    // refinement: a warp per (seed, candidate cell) over the whole grid
+    {
+      const int w = threadIdx.x >> 5;
+      while (true) {
+        unsigned it = 0;
+        if (lane == 0) it = atomicAdd(&ts->work_r[q], 1u);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= nready * 27u) break;
+        const unsigned slot = it / 27u;
+        if (!Br.st_active[slot]) continue;
+        tail_refine_cell(K, Br, slot, (int)(it % 27u), seed_geo(K, Br, B.ready[slot]), t_tiles[w]);
       }
-      __syncthreads();
-      select_seed(K, Br, S, item, rank);
-      if (Br.learn_collect) seed_features(K, Br, S, item, rank);
-      __syncthreads();
-      cross_seed(K, Br, S, item, rank);
+    }
+    if (!grid_barrier(ts)) return;
+    // exact sums of the contenders and the argmax: a CTA per seed
+    while (true) {
+      const unsigned item = next_item(&ts->work_s[q]);
+      if (item >= nready) break;
+      select_seed(K, Br, S, item, B.ready[item]);
+      if (Br.learn_collect) seed_features(K, Br, S, item, B.ready[item]);
+    }
+    if (!grid_barrier(ts)) return;
+    // crossing, profile and claims: a CTA per seed
+    while (true) {
+      const unsigned item = next_item(&ts->work_c[q]);
+      if (item >= nready) break;
+      cross_seed(K, Br, S, item, B.ready[item]);
     }
     if (!grid_barrier(ts)) return;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
       ts->rounds++;
       ts->parity = q ^ 1u;
+      ts->t_seeds += global_ns() - tk;
     }
     if (threadIdx.x == 0) s_nready = ld_shared_state(&ts->deferred);
     __syncthreads();
@@ -3155,6 +3320,9 @@ __global__ void k_tail_init(TailState *ts, unsigned n_active) {
   ts->nact[1] = 0;
   ts->nready[0] = ts->nready[1] = 0;
   ts->work[0] = ts->work[1] = 0;
+  ts->work_r[0] = ts->work_r[1] = 0;
+  ts->work_s[0] = ts->work_s[1] = 0;
+  ts->work_c[0] = ts->work_c[1] = 0;
   ts->cand_used[0] = ts->cand_used[1] = 0;
   ts->gmin[0] = ts->gmin[1] = PSOD_INF_RANK;
   ts->xused[0] = ts->xused[1] = 0;
@@ -3164,6 +3332,7 @@ __global__ void k_tail_init(TailState *ts, unsigned n_active) {
   ts->parity = 0;
   ts->bar_count = 0;
   ts->bar_gen = 0;
+  ts->t_heads = ts->t_ready = ts->t_seeds = 0;
 }
 
 __global__ void k_find_rank(const unsigned *seed_idx, long long nseed, unsigned idx, unsigned *out) {
@@ -3738,8 +3907,9 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
         act_a, n_active, bbegin, cursor, blist, resolved, head,
         quirk_rank != PSOD_INF_RANK ? gmin : nullptr, act_b, ctrs + 9);
     if ((long long)n_active * direct_cost_per_block <= filter_cost) {
-      k_ready_direct<<<nblk(n_active, 256), 256, 0, c->stream>>>(act_b, ctrs + 9, head, nb, rb, quirk_rank, gmin,
-                                                                 ready, nready_d, cap_ready);
+      k_ready_direct<<<nblk((long long)n_active * 32, 256), 256, 0, c->stream>>>(act_b, ctrs + 9, head, nb, rb,
+                                                                                  quirk_rank, gmin, ready, nready_d,
+                                                                                  cap_ready);
       kernels += 3;
     } else {
       k_minfilter<<<nblk(nblocks, 256), 256, 0, c->stream>>>(head, filt_a, nb, 0, rb);
@@ -3872,6 +4042,10 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       collect_pending();
       rounds += ts.rounds;
       tail_rounds += ts.rounds;
+#ifdef PSOD_TRACE_ROUNDS
+      fprintf(stderr, "psod tail launch rounds %u status %u heads %.3f ready %.3f seeds %.3f ms total %.3f ms grid %d\n",
+              ts.rounds, ts.status, ts.t_heads * 1e-6, ts.t_ready * 1e-6, ts.t_seeds * 1e-6, t_tail.last, tail_grid);
+#endif
       if (ts.status == TAIL_TIMEOUT)
         return set_err(c, PSOD_ERR_TIMEOUT, "device tail loop: a grid barrier wait ran out");
       if (ts.status == TAIL_STALLED) return set_err(c, PSOD_ERR_STATE, "scheduler stalled with unresolved seeds");

@@ -25,22 +25,126 @@ constexpr double FIX_ONE = 1099511627776.0;  // 2^40
 // ---------------------------------------------------------------------------
 // cell sort
 // ---------------------------------------------------------------------------
-__global__ void k_cell_count(const float *pos, long long n, float nxf, double xs, int nx, unsigned *cell,
-                             unsigned *count, int *bad) {
+// Slab partition.  The particles arrive in random order, so a direct
+// counting sort into nx^3 cells spreads its atomics and its record writes
+// over the whole cube.  A first pass groups them by slab (a run of z-planes
+// of cells, at most SLAB_MAX slabs) with coalesced writes: each CTA orders a
+// tile of SLAB_TILE particles by slab in shared memory and writes one run
+// per slab.  The counting sort then reads the records slab after slab, so at
+// any moment its atomics and record writes fall into the few slabs that the
+// running CTAs hold, which stay in L2.
+constexpr int SLAB_MAX = 512;
+constexpr int SLAB_TILE = 4096;
+constexpr int SLAB_THREADS = 256;
+constexpr int SLAB_PER = SLAB_TILE / SLAB_THREADS;
+
+__device__ __forceinline__ bool in_unit_box(float x, float y, float z) {
+  return x >= 0.f && x <= 1.f && y >= 0.f && y <= 1.f && z >= 0.f && z <= 1.f;
+}
+
+// slab of a position: its z cell scaled to the slab count (slabs are runs of
+// whole z-planes, so runs of cell indices)
+__device__ __forceinline__ unsigned slab_of(float z, float nxf, double xs, int nx, int nslab) {
+  const int k = sod_cell_axis(to_grid(z, nxf), xs, nx);
+  return (unsigned)(((long long)k * nslab) / nx);
+}
+
+__global__ void __launch_bounds__(SLAB_THREADS) k_slab_count(const float *pos, long long n, float nxf, double xs,
+                                                             int nx, int nslab, unsigned *hist, int *bad) {
+  __shared__ unsigned h[SLAB_MAX];
+  for (int k = threadIdx.x; k < nslab; k += SLAB_THREADS) h[k] = 0;
+  __syncthreads();
+  const long long base = (long long)blockIdx.x * SLAB_TILE;
+  int badl = 0;
+  for (int u = 0; u < SLAB_PER; u++) {
+    const long long i = base + (long long)u * SLAB_THREADS + threadIdx.x;
+    if (i >= n) break;
+    const float x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
+    if (!in_unit_box(x, y, z)) badl = 1;
+    atomicAdd(&h[slab_of(z, nxf, xs, nx, nslab)], 1u);
+  }
+  if (badl) atomicOr(bad, 1);
+  __syncthreads();
+  for (int k = threadIdx.x; k < nslab; k += SLAB_THREADS)
+    if (h[k]) atomicAdd(&hist[k], h[k]);
+}
+
+// exclusive scan of the slab counts into the write cursors (one CTA)
+__global__ void k_slab_scan(const unsigned *hist, int nslab, unsigned *cursor) {
+  __shared__ unsigned s[SLAB_MAX];
+  for (int k = threadIdx.x; k < SLAB_MAX; k += blockDim.x) s[k] = k < nslab ? hist[k] : 0u;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned run = 0;
+    for (int k = 0; k < nslab; k++) {
+      const unsigned v = s[k];
+      cursor[k] = run;
+      run += v;
+    }
+  }
+}
+
+// records (x, y, z, input index) grouped by slab; the order inside a slab
+// carries no meaning
+__global__ void __launch_bounds__(SLAB_THREADS) k_slab_scatter(const float *pos, long long n, float nxf, double xs,
+                                                               int nx, int nslab, unsigned *cursor, float4 *rec) {
+  __shared__ unsigned cnt[SLAB_MAX], start[SLAB_MAX], gbase[SLAB_MAX];
+  extern __shared__ __align__(16) unsigned char slab_smem[];
+  float4 *stage = reinterpret_cast<float4 *>(slab_smem);                                // SLAB_TILE records
+  unsigned short *sdig = reinterpret_cast<unsigned short *>(stage + SLAB_TILE);          // their slabs
+  for (int k = threadIdx.x; k < nslab; k += SLAB_THREADS) cnt[k] = 0;
+  __syncthreads();
+  const long long base = (long long)blockIdx.x * SLAB_TILE;
+  const int m = (int)min((long long)SLAB_TILE, n - base);
+  unsigned d[SLAB_PER], r[SLAB_PER];
+#pragma unroll
+  for (int u = 0; u < SLAB_PER; u++) {
+    const int j = u * SLAB_THREADS + threadIdx.x;
+    if (j < m) {
+      d[u] = slab_of(pos[3 * (base + j) + 2], nxf, xs, nx, nslab);
+      r[u] = atomicAdd(&cnt[d[u]], 1u);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned run = 0;
+    for (int k = 0; k < nslab; k++) {
+      start[k] = run;
+      run += cnt[k];
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nslab; k += SLAB_THREADS)
+    if (cnt[k]) gbase[k] = atomicAdd(&cursor[k], cnt[k]);
+#pragma unroll
+  for (int u = 0; u < SLAB_PER; u++) {
+    const int j = u * SLAB_THREADS + threadIdx.x;
+    if (j < m) {
+      const long long i = base + j;
+      const unsigned at = start[d[u]] + r[u];
+      stage[at] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], __uint_as_float((unsigned)i));
+      sdig[at] = (unsigned short)d[u];
+    }
+  }
+  __syncthreads();
+  // consecutive threads write consecutive records of each slab's run
+  for (int j = threadIdx.x; j < m; j += SLAB_THREADS) {
+    const unsigned k = sdig[j];
+    rec[gbase[k] + (j - start[k])] = stage[j];
+  }
+}
+
+__global__ void k_cell_count(const float4 *rec, long long n, float nxf, double xs, int nx, unsigned *cell,
+                             unsigned *count) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned c = 0xffffffffu;
   if (i < n) {
-    const float x = pos[3 * i], y = pos[3 * i + 1], z = pos[3 * i + 2];
-    if (!(x >= 0.f && x <= 1.f && y >= 0.f && y <= 1.f && z >= 0.f && z <= 1.f)) {
-      atomicOr(bad, 1);
-      cell[i] = 0;
-    } else {
-      const int ci = sod_cell_axis(to_grid(x, nxf), xs, nx);
-      const int cj = sod_cell_axis(to_grid(y, nxf), xs, nx);
-      const int ck = sod_cell_axis(to_grid(z, nxf), xs, nx);
-      c = (unsigned)ci + (unsigned)nx * ((unsigned)cj + (unsigned)nx * (unsigned)ck);
-      cell[i] = c;
-    }
+    const float4 v = rec[i];
+    const int ci = sod_cell_axis(to_grid(v.x, nxf), xs, nx);
+    const int cj = sod_cell_axis(to_grid(v.y, nxf), xs, nx);
+    const int ck = sod_cell_axis(to_grid(v.z, nxf), xs, nx);
+    c = (unsigned)ci + (unsigned)nx * ((unsigned)cj + (unsigned)nx * (unsigned)ck);
+    cell[i] = c;
   }
   // one atomic per distinct cell in the warp
   const unsigned peers = __match_any_sync(0xffffffffu, c);
@@ -62,9 +166,9 @@ __device__ __forceinline__ unsigned sub_axis(float xg, double xs) {
   return (unsigned)min(max(s, 0), 3);
 }
 
-__device__ __forceinline__ unsigned sub_key(const float *p, float nxf, double xs) {
-  const unsigned a = sub_axis(to_grid(p[0], nxf), xs), b = sub_axis(to_grid(p[1], nxf), xs),
-                 c = sub_axis(to_grid(p[2], nxf), xs);
+__device__ __forceinline__ unsigned sub_key(const float4 &p, float nxf, double xs) {
+  const unsigned a = sub_axis(to_grid(p.x, nxf), xs), b = sub_axis(to_grid(p.y, nxf), xs),
+                 c = sub_axis(to_grid(p.z, nxf), xs);
   return (a & 1u) | ((b & 1u) << 1) | ((c & 1u) << 2) | ((a >> 1) << 3) | ((b >> 1) << 4) | ((c >> 1) << 5);
 }
 
@@ -91,12 +195,12 @@ __global__ void k_mark_big(unsigned *count, unsigned long long ncell, unsigned *
   }
 }
 
-__global__ void k_sub_count(const float *pos, long long n, const unsigned *cell, const unsigned *count, float nxf,
+__global__ void k_sub_count(const float4 *rec, long long n, const unsigned *cell, const unsigned *count, float nxf,
                             double xs, unsigned *tab) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const unsigned v = count[cell[i]];
-  if (v & BIG_FLAG) atomicAdd(&tab[(unsigned long long)(v & ~BIG_FLAG) * SUB_N + sub_key(pos + 3 * i, nxf, xs)], 1u);
+  if (v & BIG_FLAG) atomicAdd(&tab[(unsigned long long)(v & ~BIG_FLAG) * SUB_N + sub_key(rec[i], nxf, xs)], 1u);
 }
 
 // one warp per dense cell: sub-cell counts -> absolute start slots
@@ -116,15 +220,16 @@ __global__ void k_sub_scan(unsigned *tab, const unsigned *bigcell, unsigned nbig
   t[2 * lane + 1] = excl + a0;
 }
 
-__global__ void k_cell_scatter(const float *pos, long long n, const unsigned *cell, unsigned *fill, unsigned *tab,
+__global__ void k_cell_scatter(const float4 *rec, long long n, const unsigned *cell, unsigned *fill, unsigned *tab,
                                float nxf, double xs, float4 *cube, unsigned *inv) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned c = i < n ? cell[i] : 0xffffffffu;
   const unsigned v = i < n ? fill[c] : 0u;  // the flag bit never changes under the atomics below
   const bool big = (v & BIG_FLAG) != 0;
+  const float4 r = i < n ? rec[i] : make_float4(0.f, 0.f, 0.f, 0.f);
   const unsigned long long key =
       i >= n ? ~0ull
-      : big  ? (1ull << 63) | ((unsigned long long)(v & ~BIG_FLAG) * SUB_N + sub_key(pos + 3 * i, nxf, xs))
+      : big  ? (1ull << 63) | ((unsigned long long)(v & ~BIG_FLAG) * SUB_N + sub_key(r, nxf, xs))
              : (unsigned long long)c;
   const unsigned peers = __match_any_sync(0xffffffffu, key);
   const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
@@ -134,8 +239,8 @@ __global__ void k_cell_scatter(const float *pos, long long n, const unsigned *ce
   base = __shfl_sync(0xffffffffu, base, leader);
   if (i >= n) return;
   const unsigned slot = base + __popc(peers & ((1u << lane) - 1u));
-  cube[slot] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], __uint_as_float((unsigned)i));
-  inv[i] = slot;
+  cube[slot] = r;
+  inv[__float_as_uint(r.w)] = slot;
 }
 
 __global__ void k_set_range(unsigned *a, unsigned long long lo, unsigned long long hi, unsigned v) {
@@ -512,9 +617,12 @@ int stage_cellsort(psod_ctx *c, const float *dpos) {
   const int nx = c->nx;
   c->ncell = (unsigned long long)nx * nx * nx;
   int st;
-  unsigned *cell = nullptr, *count = nullptr;
+  unsigned *cell = nullptr, *count = nullptr, *slabs = nullptr;
+  float4 *rec = nullptr;
   int *bad = nullptr;
   if ((st = scratch(c, SLOT_PART_U32, (size_t)n, &cell))) return st;
+  if ((st = scratch(c, SLOT_SLAB_REC, (size_t)n, &rec))) return st;
+  if ((st = scratch(c, SLOT_SLABS, 2 * SLAB_MAX, &slabs))) return st;
   if ((st = scratch(c, SLOT_CELL_U32, (size_t)c->ncell + 1, &count))) return st;
   if ((st = scratch(c, SLOT_LOAD_FLAGS, 2, &bad))) return st;
   if ((st = ensure(c, &c->d_cell_start, &c->cs_cap, (size_t)c->ncell + 1))) return st;
@@ -523,7 +631,17 @@ int stage_cellsort(psod_ctx *c, const float *dpos) {
   PSOD_CUDA(c, cudaMemsetAsync(count, 0, sizeof(unsigned) * (c->ncell + 1), c->stream));
   PSOD_CUDA(c, cudaMemsetAsync(bad, 0, 2 * sizeof(int), c->stream));
   const double xs = c->xxmin * c->scale;  // main:1565
-  k_cell_count<<<nblk(n, 256), 256, 0, c->stream>>>(dpos, n, (float)nx, xs, nx, cell, count, bad);
+  // records grouped by slab first (see k_slab_scatter)
+  const int nslab = std::min(nx, SLAB_MAX);
+  PSOD_CUDA(c, cudaMemsetAsync(slabs, 0, sizeof(unsigned) * SLAB_MAX, c->stream));
+  const unsigned ntile = nblk(n, SLAB_TILE);
+  k_slab_count<<<ntile, SLAB_THREADS, 0, c->stream>>>(dpos, n, (float)nx, xs, nx, nslab, slabs, bad);
+  k_slab_scan<<<1, 32, 0, c->stream>>>(slabs, nslab, slabs + SLAB_MAX);
+  const int slab_smem = SLAB_TILE * (int)(sizeof(float4) + sizeof(unsigned short));
+  PSOD_CUDA(c, cudaFuncSetAttribute(k_slab_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, slab_smem));
+  k_slab_scatter<<<ntile, SLAB_THREADS, slab_smem, c->stream>>>(dpos, n, (float)nx, xs, nx, nslab, slabs + SLAB_MAX,
+                                                                rec);
+  k_cell_count<<<nblk(n, 256), 256, 0, c->stream>>>(rec, n, (float)nx, xs, nx, cell, count);
   if ((st = scan_u32(c, count, c->d_cell_start, (long long)c->ncell, true))) return st;
   unsigned *nbig = reinterpret_cast<unsigned *>(bad + 1);
   const long long ncell = (long long)c->ncell;
@@ -541,10 +659,10 @@ int stage_cellsort(psod_ctx *c, const float *dpos) {
     PSOD_CUDA(c, cudaMemsetAsync(tab, 0, sizeof(unsigned) * ((size_t)hnbig * SUB_N + 1), c->stream));
     k_mark_big<<<nblk(ncell, 256), 256, 0, c->stream>>>(count, c->ncell, nbig, true, bigcell, c->d_cell_start);
     if (hnbig) {
-      k_sub_count<<<nblk(n, 256), 256, 0, c->stream>>>(dpos, n, cell, count, (float)nx, xs, tab);
+      k_sub_count<<<nblk(n, 256), 256, 0, c->stream>>>(rec, n, cell, count, (float)nx, xs, tab);
       k_sub_scan<<<nblk((long long)hnbig * 32, 256), 256, 0, c->stream>>>(tab, bigcell, hnbig, c->d_cell_start);
     }
-    k_cell_scatter<<<nblk(n, 256), 256, 0, c->stream>>>(dpos, n, cell, count, tab, (float)nx, xs, c->d_cube,
+    k_cell_scatter<<<nblk(n, 256), 256, 0, c->stream>>>(rec, n, cell, count, tab, (float)nx, xs, c->d_cube,
                                                         c->d_inv);
     PSOD_CUDA(c, cudaGetLastError());
     PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
