@@ -675,6 +675,98 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+FOF_METRIC = "FoF particles/s (b=0.2, Mmin=20, one rank, periodic)"
+
+
+def run_fof(args):
+    """The friends-of-friends stage (psod_fof) on the workload's box: one
+    step = linking-cell sort, union-find, labels, member lists, centres and
+    radii over all particles.  value: particles per second with the particles
+    resident in HBM; e2e: host positions/IDs/velocities in, the catalogue
+    (halo table and member IDs) out, through the public API."""
+    import numpy as np
+    import torch
+
+    from psod_b200 import synth
+    from psod_b200.sod import SphericalOverdensity
+
+    nx = args.nx
+    wl = WORKLOADS.get(nx, dict(nmax_halo=20000, box=f"{nx}^3"))
+    torch.cuda.set_device(0)
+    box = synth.make_box(nx, nmax_halo=wl["nmax_halo"], seed=args.seed, device="cuda:0")
+    pos_d, ids_d = box.pos, box.ids
+    del box
+    gen = torch.Generator(device="cuda:0")
+    gen.manual_seed(args.seed + 7)
+    vel_d = torch.randn(pos_d.shape, generator=gen, device="cuda:0", dtype=torch.float32) * 300.0
+    torch.cuda.empty_cache()
+    n = int(pos_d.shape[0])
+    sod = SphericalOverdensity(nx, device=0)
+    sod.load(pos_d, ids_d, vel=vel_d)
+    for _ in range(args.warmup):
+        st = sod.fof(percolation=0.2, mmin=20)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    with ClockSampler(0) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            stats.append(sod.fof(percolation=0.2, mmin=20))
+        ev1.record()
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    st = stats[-1]
+    # e2e through the public API: pinned host arrays in, catalogue out
+    pos_h, ids_h, vel_h = (x.cpu().pin_memory() for x in (pos_d, ids_d, vel_d))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sod.load(pos_h, ids_h, vel=vel_h)
+        sod.fof(percolation=0.2, mmin=20)
+        cat = sod.fof_halos()
+    e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
+    d2h = sum(getattr(cat, f).nbytes for f in cat.__dataclass_fields__)
+    sod.close()
+    peak, peak_kind = load_peaks()
+    # union-find linking: each record's position (16 B) read and its parent
+    # (4 B) written once per launch is the algorithmic floor of the kernel
+    link_s = st["ms_link"] / 1000.0
+    alg = 20.0 * n
+    achieved = alg / link_s / 1e9 if link_s > 0 else 0.0
+    line = {
+        "metric": FOF_METRIC, "value": round(n / (ms / 1000.0), 1), "unit": "particles/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (friend test), f64 (centres, radii)",
+        "data": "synthetic NFW-mixture box (seeded); inputs resident in HBM",
+        "config": {"workload": wl["box"] + ", FoF b=0.2, Mmin=20", "nx": nx, "particles": n,
+                   "l2": "inputs larger than L2" if n * 16 > 126e6 else "inputs fit in L2 (no flush)"},
+        "detail": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()},
+        "e2e": {"value": round(n / (e2e_ms / 1000.0), 1), "unit": "particles/s",
+                "h2d_bytes_per_step": int(n * (12 + 8 + 12)), "d2h_bytes_per_step": int(d2h),
+                "ms_per_step": round(e2e_ms, 3)},
+        "roofline": {"bound": "hbm", "kernel": "k_fof_link_thread + k_fof_link_warp (union-find over linking cells)",
+                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "peak_kind": peak_kind, "traffic": None, "alg_bytes_per_launch": int(alg),
+                     "kernel_ms": round(st["ms_link"], 3)},
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        # the oracle's sequential pFoF on the 128^3 box of the same law
+        from oracle import oracle as O
+
+        snx = min(nx, 128)
+        b = synth.make_box(snx, nmax_halo=WORKLOADS.get(snx, wl)["nmax_halo"], seed=args.seed + 100)
+        p, i = b.pos.numpy(), b.ids.numpy()
+        t0 = time.perf_counter()
+        r = O.fof(p, i, percolation=0.2, nres=snx, mmin=20)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(len(p) / dt, 1), "unit": "particles/s", "cores": 1, "kind": "port",
+                                "sample": f"one {snx}^3 box of the workload's law ({len(p)} particles, {r.nhalo} "
+                                          f"halos), the C oracle's sequential pFoF scan + merge + observables, "
+                                          f"{dt:.2f} s"}
+    print(json.dumps(line), flush=True)
+
+
 def relaunch_with_torchrun(args):
     """``--gpus N`` without a torchrun environment: start the N ranks here
     (one process per GPU) with the same arguments, and return their status."""
@@ -701,6 +793,8 @@ def main():
     ap.add_argument("--delta200-only", dest="ndelta", action="store_false",
                     help="Delta = 200 and 60 bins only (default: 200, 500 and 178 in one pass, 48 bins)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fof", action="store_true",
+                    help="time the friends-of-friends stage (psod_fof) instead of SOD; one GPU")
     ap.add_argument("--heavy", action="store_true",
                     help="the heavy-tail stress box (1024^3 + 16 clusters of 5e6, -npu 1e7, Delta 200/500, 64 bins)")
     args = ap.parse_args()
@@ -709,6 +803,8 @@ def main():
         sys.exit(relaunch_with_torchrun(args))
     if args.impl == "reference":
         run_reference(args)
+    elif args.fof:
+        run_fof(args)
     else:
         run_ours(args)
 

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define PSOD_ABI_VERSION 2
+#define PSOD_ABI_VERSION 3
 #define PSOD_MAX_EXTRA_DELTA 4
 
 typedef enum psod_status {
@@ -305,6 +305,78 @@ int psod_learn_set_model(psod_ctx *ctx, const float *model, int64_t nfloats);
 int psod_learn_set_margin(psod_ctx *ctx, float margin);
 int psod_learn_forward(psod_ctx *ctx, int64_t n, const float *x, float *y);
 int psod_learn_gradient(psod_ctx *ctx, int64_t n, const float *x, const float *t, float *grad, float *loss);
+
+/* ---- Friends-of-friends (pFoF on one rank) -----------------------------
+ * The halo finder that writes the catalogue and cube files the SOD stage
+ * reads: pFoF's fofpara (Pfof/trunk/pfof_snap/src/modfofpara.f90:31-296)
+ * with the periodic merge of Pfof/trunk/common/src/modfofmpi.f90 (:37-649),
+ * then selecthaloes, computecom and computeradius (sod/modhalo.f90:253-376,
+ * 381-441, 445-488), on the particles of psod_load_particles (the periodic
+ * unit box).  psod_fof replaces that sequence for one MPI rank.
+ *
+ * Two particles are friends when their squared distance, evaluated in FP32
+ * as the reference evaluates it, is <= r2 = (percolation / nres)^2 (FP32):
+ * |x1 - x2| per axis for pairs within half a box on every axis (the local
+ * scan, modfofpara.f90:234-238); min(d, 1 - d) per axis for pairs across the
+ * periodic boundary whose particles lie within percolation / nres of
+ * opposite faces of one axis (the bridges, modfofmpi.f90:226-233).
+ * Positions equal to 1.0 count as 0.0.  A halo is a connected group of at
+ * least mmin particles.
+ *
+ * Labels and order: a halo's ID is the ID of its member with the lowest
+ * input index, and halos come in ascending ID; members in ascending input
+ * index.  The reference labels a group with the ID of the particle its
+ * sequential scan started the group from (the front of its in-place queue),
+ * merged across the boundary to the smallest such label, and keeps members
+ * in heap order; that label follows from the scan order and has no
+ * parallel counterpart.  Member sets, masses, centres and radii are the
+ * reference's.
+ *
+ * Centre of mass: FP64 mean of the member positions, each unwrapped by one
+ * box against the halo's first member where they lie more than half a box
+ * apart (the reference unwraps against the running mean: the same for
+ * halos smaller than a quarter box), wrapped into [0,1].  Mean velocity
+ * (zeros when no velocities were loaded).  Radius: the largest member
+ * distance from the centre, per axis |d| > 0.5 -> 1 - |d| (computeradius).
+ *
+ * The linking length percolation * nx / nres must lie between about 0.06
+ * and 0.5 SOD cells (PSOD_ERR_ARG otherwise); percolation < 0.5 as the
+ * reference requires (modfofpara.f90:101-117). */
+typedef struct psod_fof_params {
+  float percolation; /* param%percolation_length, in mean inter-particle spacings (0.2) */
+  int32_t reserved;  /* 0 */
+  int64_t nres;      /* particles per side (nres); 0: cube root of the loaded count, rounded */
+  int64_t mmin;      /* param%Mmin: smallest halo kept */
+} psod_fof_params;
+
+typedef struct psod_fof_stats {
+  int64_t nhalo;      /* groups of at least mmin particles */
+  int64_t nmember;    /* their particles */
+  int64_t ngroups;    /* all groups, single particles included */
+  int64_t fine_cells; /* non-empty linking cells */
+  int64_t pair_tests; /* particle pairs tested */
+  int64_t cell_pairs; /* neighbouring linking-cell pairs examined */
+  double ms_total;    /* device time of psod_fof */
+  double ms_sort;     /* linking-cell sort */
+  double ms_link;     /* union-find over the linking cells */
+  double ms_label;    /* groups, labels, member lists */
+  double ms_props;    /* centres, velocities, radii */
+} psod_fof_stats;
+
+typedef struct psod_fof_table {
+  int64_t *halo_id;       /* [nhalo] ID of the lowest-index member, ascending */
+  int64_t *halo_mass;     /* [nhalo] particle count */
+  double *halo_com;       /* [3*nhalo] centre of mass, box units */
+  double *halo_vel;       /* [3*nhalo] mean velocity */
+  double *halo_radius;    /* [nhalo] largest member distance from the centre, box units */
+  int64_t *member_offset; /* [nhalo+1] */
+  int64_t *member_index;  /* [nmember] input indices, ascending inside a halo */
+  int64_t *member_id;     /* [nmember] particle IDs */
+} psod_fof_table;
+
+int psod_fof(psod_ctx *ctx, const psod_fof_params *p, psod_fof_stats *stats);
+int psod_fof_halo_count(psod_ctx *ctx, int64_t *nhalo, int64_t *nmember);
+int psod_fof_get_halos(psod_ctx *ctx, const psod_fof_table *t);
 
 const char *psod_last_error(const psod_ctx *ctx);
 const char *psod_status_string(int status);

@@ -60,6 +60,26 @@ module psod_gpu
      integer(c_int64_t) :: seed
   end type psod_train_params
 
+  ! friends-of-friends (pFoF fofpara on one rank): param%percolation_length,
+  ! nres (0: cube root of the particle count), param%Mmin
+  type, bind(C) :: psod_fof_params
+     real(c_float)      :: percolation
+     integer(c_int32_t) :: reserved
+     integer(c_int64_t) :: nres, mmin
+  end type psod_fof_params
+
+  type, bind(C) :: psod_fof_stats
+     integer(c_int64_t) :: nhalo, nmember, ngroups, fine_cells, pair_tests, cell_pairs
+     real(c_double)     :: ms_total, ms_sort, ms_link, ms_label, ms_props
+  end type psod_fof_stats
+
+  ! haloID, haloMass, halocomPos, halocomVel, haloRadius of modhalo, and the
+  ! member lists (0-based input indices and IDs)
+  type, bind(C) :: psod_fof_table
+     type(c_ptr) :: halo_id, halo_mass, halo_com, halo_vel, halo_radius
+     type(c_ptr) :: member_offset, member_index, member_id
+  end type psod_fof_table
+
   interface
      subroutine psod_params_default(p) bind(C, name="psod_params_default")
        import :: psod_params
@@ -161,6 +181,25 @@ module psod_gpu
        integer(c_int64_t), value :: capacity
        integer(c_int64_t), intent(out) :: npart
        type(c_ptr), value :: pos, vel, id
+     end function
+     ! friends-of-friends on the loaded particles (replaces fofpara's local
+     ! scan, mergehaloes, gatherhaloes, selecthaloes, computecom and
+     ! computeradius for one rank)
+     integer(c_int) function psod_fof(ctx, p, stats) bind(C, name="psod_fof")
+       import :: c_int, c_ptr, psod_fof_params, psod_fof_stats
+       type(c_ptr), value :: ctx
+       type(psod_fof_params), intent(in) :: p
+       type(psod_fof_stats), intent(out) :: stats
+     end function
+     integer(c_int) function psod_fof_halo_count(ctx, nhalo, nmember) bind(C, name="psod_fof_halo_count")
+       import :: c_int, c_ptr, c_int64_t
+       type(c_ptr), value :: ctx
+       integer(c_int64_t), intent(out) :: nhalo, nmember
+     end function
+     integer(c_int) function psod_fof_get_halos(ctx, t) bind(C, name="psod_fof_get_halos")
+       import :: c_int, c_ptr, psod_fof_table
+       type(c_ptr), value :: ctx
+       type(psod_fof_table), intent(in) :: t
      end function
   end interface
 end module psod_gpu

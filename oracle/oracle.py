@@ -353,3 +353,95 @@ def arithmetic_audit(params: Params, pos, ids) -> dict:
     out.update(halos_one_run_only=only, halos_mass_differ=dmass, halos_rdelta_differ=drad,
                halos_members_differ=dset)
     return out
+
+
+# ---------------------------------------------------------------------------
+# friends-of-friends (pFoF fofpara + periodic merge + sod/modhalo.f90
+# selecthaloes, computecom, computeradius; psod_oracle_fof.c)
+# ---------------------------------------------------------------------------
+class _FofParams(C.Structure):
+    _fields_ = [("percolation", C.c_float), ("nres", C.c_int64), ("mmin", C.c_int64)]
+
+
+class _FofResult(C.Structure):
+    _fields_ = [
+        ("status", C.c_int32),
+        ("ngroups_local", C.c_int64),
+        ("nbridges", C.c_int64),
+        ("nhalo", C.c_int64),
+        ("nmember", C.c_int64),
+        ("halo_id", C.POINTER(C.c_int64)),
+        ("halo_mass", C.POINTER(C.c_int64)),
+        ("halo_com", C.POINTER(C.c_double)),
+        ("halo_vel", C.POINTER(C.c_double)),
+        ("halo_radius", C.POINTER(C.c_double)),
+        ("member_offset", C.POINTER(C.c_int64)),
+        ("member_index", C.POINTER(C.c_int64)),
+        ("structure", C.POINTER(C.c_int64)),
+    ]
+
+
+@dataclass
+class FofResult:
+    """The reference's FoF catalogue: halos in ascending label, members in
+    heap order inside a halo, plus every particle's final label."""
+
+    status: int
+    ngroups_local: int = 0
+    nbridges: int = 0
+    halo_id: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    halo_mass: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    halo_com: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.float64))
+    halo_vel: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), np.float64))
+    halo_radius: np.ndarray = field(default_factory=lambda: np.zeros(0, np.float64))
+    member_offset: np.ndarray = field(default_factory=lambda: np.zeros(1, np.int64))
+    member_index: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    structure: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+
+    @property
+    def nhalo(self) -> int:
+        return int(self.halo_id.shape[0])
+
+    def members(self, h: int) -> np.ndarray:
+        return self.member_index[self.member_offset[h]: self.member_offset[h + 1]]
+
+
+def fof(pos, ids, vel=None, percolation: float = 0.2, nres: int | None = None, mmin: int = 20) -> FofResult:
+    """pFoF on one rank over the periodic unit box (modfofpara.f90:31-296,
+    modfofmpi.f90:37-649, sod/modhalo.f90:253-488)."""
+    L = lib()
+    if not hasattr(L, "_fof_ready"):
+        L.psod_oracle_fof.argtypes = [C.POINTER(_FofParams), C.c_int64, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                      C.POINTER(C.c_int64), C.POINTER(_FofResult)]
+        L.psod_oracle_fof_free.argtypes = [C.POINTER(_FofResult)]
+        L._fof_ready = True
+    p = _as_pos(pos)
+    i = _as_ids(ids)
+    n = p.shape[0]
+    if nres is None:
+        nres = int(round(n ** (1.0 / 3.0)))
+    v = None if vel is None else np.ascontiguousarray(
+        vel.cpu().numpy() if hasattr(vel, "cpu") else vel, dtype=np.float32).reshape(-1, 3)
+    cp = _FofParams(percolation, nres, mmin)
+    r = _FofResult()
+    st = L.psod_oracle_fof(C.byref(cp), n, _ptr(p, C.c_float), None if v is None else _ptr(v, C.c_float),
+                           _ptr(i, C.c_int64), C.byref(r))
+    if st != 0:
+        L.psod_oracle_fof_free(C.byref(r))
+        return FofResult(status=st)
+    nh, nm = r.nhalo, r.nmember
+
+    def take(ptr, count, dtype, shape=None):
+        a = np.ctypeslib.as_array(ptr, shape=(max(count, 1),))[:count].astype(dtype, copy=True)
+        return a.reshape(shape) if shape else a
+
+    out = FofResult(status=0, ngroups_local=r.ngroups_local, nbridges=r.nbridges,
+                    halo_id=take(r.halo_id, nh, np.int64), halo_mass=take(r.halo_mass, nh, np.int64),
+                    halo_com=take(r.halo_com, 3 * nh, np.float64, (nh, 3)),
+                    halo_vel=take(r.halo_vel, 3 * nh, np.float64, (nh, 3)),
+                    halo_radius=take(r.halo_radius, nh, np.float64),
+                    member_offset=take(r.member_offset, nh + 1, np.int64),
+                    member_index=take(r.member_index, nm, np.int64),
+                    structure=take(r.structure, n, np.int64))
+    L.psod_oracle_fof_free(C.byref(r))
+    return out

@@ -11,7 +11,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libpsod.so")
 SOURCES = ["psod_capi.cu", "psod_stages.cu", "psod_sod.cu", "psod_sort.cu", "psod_static.cu", "psod_learn.cu",
-           "psod_output.cu", "psod_input.cu"]
+           "psod_output.cu", "psod_input.cu", "psod_fof.cu"]
 HEADERS = ["psod_internal.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--extended-lambda", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]

@@ -108,6 +108,42 @@ class RunStats(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class FofParams(C.Structure):
+    _fields_ = [("percolation", C.c_float), ("reserved", C.c_int32), ("nres", C.c_int64), ("mmin", C.c_int64)]
+
+
+class FofStats(C.Structure):
+    _fields_ = [
+        ("nhalo", C.c_int64),
+        ("nmember", C.c_int64),
+        ("ngroups", C.c_int64),
+        ("fine_cells", C.c_int64),
+        ("pair_tests", C.c_int64),
+        ("cell_pairs", C.c_int64),
+        ("ms_total", C.c_double),
+        ("ms_sort", C.c_double),
+        ("ms_link", C.c_double),
+        ("ms_label", C.c_double),
+        ("ms_props", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+class FofTable(C.Structure):
+    _fields_ = [
+        ("halo_id", C.c_void_p),
+        ("halo_mass", C.c_void_p),
+        ("halo_com", C.c_void_p),
+        ("halo_vel", C.c_void_p),
+        ("halo_radius", C.c_void_p),
+        ("member_offset", C.c_void_p),
+        ("member_index", C.c_void_p),
+        ("member_id", C.c_void_p),
+    ]
+
+
 EXPORTS = [
     "psod_abi_version",
     "psod_status_string",
@@ -136,6 +172,9 @@ EXPORTS = [
     "psod_write_masst",
     "psod_write_strct",
     "psod_read_cube_zone",
+    "psod_fof",
+    "psod_fof_halo_count",
+    "psod_fof_get_halos",
 ]
 
 LEARN_FEATURES = 10
@@ -194,6 +233,9 @@ def load(build_if_missing: bool = True):
     L.psod_write_strct.argtypes = [C.c_char_p, P(HaloTable), C.c_int64, C.c_int64, vp, vp, vp, vp, vp]
     L.psod_read_cube_zone.argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64,
                                       P(C.c_int64), vp, vp, vp]
+    L.psod_fof.argtypes = [vp, P(FofParams), P(FofStats)]
+    L.psod_fof_halo_count.argtypes = [vp, P(C.c_int64), P(C.c_int64)]
+    L.psod_fof_get_halos.argtypes = [vp, P(FofTable)]
     L.psod_last_error.argtypes = [vp]
     L.psod_cic_rho_static.argtypes = [C.c_int64, vp, C.c_int32, C.c_int64, C.c_int32, vp, vp, vp]
     L.psod_learn_collect.argtypes = [vp, C.c_int64]

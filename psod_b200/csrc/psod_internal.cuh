@@ -183,6 +183,10 @@ struct psod_ctx {
 
   // learned radius bracket (model, optimiser state, collected samples)
   psod::LearnState *learn = nullptr;
+
+  // friends-of-friends catalogue (psod_fof; arrays in the SLOT_F_* slots)
+  bool fof_done = false;
+  long long fof_nhalo = 0, fof_nmember = 0;
 };
 
 namespace psod {
@@ -294,7 +298,30 @@ enum : int {
   SLOT_LEARN_TS,        // learned bracket: standardised targets
   SLOT_LEARN_PERM,      // learned bracket: batch order
   SLOT_SLAB_REC,        // load: particle records grouped by slab (n float4)
-  SLOT_SLABS            // load: slab counts and write cursors
+  SLOT_SLABS,           // load: slab counts and write cursors
+  SLOT_FOF_KEY,         // fof: linking-cell keys in cube order
+  SLOT_FOF_SKEY,        // fof: keys in FoF order
+  SLOT_FOF_PERM,        // fof: FoF order -> cube slot; later halo-root flags
+  SLOT_FOF_PAR,         // fof: union-find parents
+  SLOT_FOF_INV,         // fof: input index -> FoF position
+  SLOT_FOF_AUX1,        // fof: head flags, then component sizes
+  SLOT_FOF_AUX2,        // fof: large cells and head scan, then lowest index / halo rank
+  SLOT_FOF_HEADS,       // fof: run heads (+ end)
+  SLOT_FOF_BIGRUN,      // fof: runs linked by a warp
+  SLOT_FOF_HPOS,        // fof: flag scans
+  SLOT_FOF_HKEY,        // fof: halo labels (sort keys)
+  SLOT_FOF_HROOT,       // fof: halo roots
+  SLOT_FOF_MKEY,        // fof: member halo ranks
+  SLOT_FOF_MCOUNT,      // fof: halo masses, then their exclusive scan
+  SLOT_FOF_CNT,         // fof: list counters
+  SLOT_FOF_CTR,         // fof: test counters
+  SLOT_F_ID,            // fof catalogue (kept until the next psod_fof)
+  SLOT_F_MASS,
+  SLOT_F_OFF,
+  SLOT_F_COM,
+  SLOT_F_VEL,
+  SLOT_F_RAD,
+  SLOT_F_MEM
 };
 
 // learned radius bracket (psod_learn.cu)

@@ -3556,7 +3556,7 @@ enum {
 // direct readiness test; after a launch that ended on a larger seed, the
 // host runs at least TAIL_REST rounds before the next launch.
 constexpr unsigned TAIL_MAX_CAND = 1024;
-constexpr unsigned TAIL_MAX_READY = 1024;
+constexpr unsigned TAIL_MAX_READY = 256;
 constexpr int TAIL_REST = 8;
 
 struct PhaseTimer {
@@ -4003,15 +4003,15 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
       // stderr with the ready seeds, active blocks, candidates and phase times
       collect_pending();
       unsigned cu = 0;
-      unsigned long long tv[16];
+      unsigned long long tv[21];
       cudaMemcpyAsync(&cu, cand_used, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream);
       cudaMemcpyAsync(tv, u64s, sizeof(tv), cudaMemcpyDeviceToHost, c->stream);
       cudaStreamSynchronize(c->stream);
       fprintf(stderr,
               "psod round %lld ready %u active %u cand %u nbig %u sched %.3f prep %.3f refine %.3f select %.3f cross %.3f "
-              "pairs %llu slots %llu staged %llu bound %.3f items %llu pruned_cand %llu\n",
+              "pairs %llu slots %llu staged %llu bound %.3f items %llu pruned_cand %llu touch %llu kept %llu\n",
               rounds, nready, n_active, cu, nbig, t_sched.last, t_prep.last, t_ref.last, t_sel.last, t_cross.last,
-              tv[5], tv[8], tv[9], B.bound_on ? t_bound.last : 0.0, tv[14], tv[15]);
+              tv[5], tv[8], tv[9], B.bound_on ? t_bound.last : 0.0, tv[14], tv[15], tv[7], tv[18]);
     }
 #endif
     rounds++;

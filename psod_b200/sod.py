@@ -44,6 +44,28 @@ class HaloTable:
         return int(self.halo_id.shape[0])
 
 
+@dataclass
+class FofTable:
+    """Friends-of-friends catalogue (psod_fof_get_halos): halos in ascending
+    ID (the ID of the lowest-index member), members in ascending input index."""
+
+    halo_id: np.ndarray
+    halo_mass: np.ndarray
+    halo_com: np.ndarray
+    halo_vel: np.ndarray
+    halo_radius: np.ndarray
+    member_offset: np.ndarray
+    member_index: np.ndarray
+    member_id: np.ndarray
+
+    @property
+    def nhalo(self) -> int:
+        return int(self.halo_id.shape[0])
+
+    def members(self, h: int) -> np.ndarray:
+        return self.member_index[self.member_offset[h]: self.member_offset[h + 1]]
+
+
 def _ptr(t):
     if t is None:
         return None
@@ -249,6 +271,36 @@ class SphericalOverdensity:
             else:
                 setattr(ct, f, a.ctypes.data)
         self._check(self.lib.psod_get_halos(self.ctx, C.byref(ct)))
+        return t
+
+
+    # ---- friends-of-friends (pFoF fofpara + merge + modhalo observables) ----
+    def fof(self, percolation: float = 0.2, mmin: int = 20, nres: int = 0) -> dict:
+        """pFoF's halo finder on the loaded particles (one rank, periodic
+        box): modfofpara.f90 fofpara with the modfofmpi.f90 merge, then
+        selecthaloes / computecom / computeradius.  ``percolation`` is
+        param%percolation_length, ``mmin`` param%Mmin, ``nres`` the
+        particles per side (0: cube root of the count).  Returns the
+        counters; the catalogue comes from fof_halos()."""
+        p = capi.FofParams(percolation, 0, nres, mmin)
+        st = capi.FofStats()
+        self._check(self.lib.psod_fof(self.ctx, C.byref(p), C.byref(st)))
+        return st.as_dict()
+
+    def fof_halos(self, members: bool = True) -> FofTable:
+        nh, nm = C.c_int64(0), C.c_int64(0)
+        self._check(self.lib.psod_fof_halo_count(self.ctx, C.byref(nh), C.byref(nm)))
+        h, m = int(nh.value), int(nm.value)
+        t = FofTable(halo_id=np.zeros(h, np.int64), halo_mass=np.zeros(h, np.int64),
+                     halo_com=np.zeros((h, 3), np.float64), halo_vel=np.zeros((h, 3), np.float64),
+                     halo_radius=np.zeros(h, np.float64), member_offset=np.zeros(h + 1, np.int64),
+                     member_index=np.zeros(m if members else 0, np.int64),
+                     member_id=np.zeros(m if members else 0, np.int64))
+        ct = capi.FofTable()
+        for f, _ in capi.FofTable._fields_:
+            a = getattr(t, f)
+            setattr(ct, f, None if a.size == 0 else a.ctypes.data)
+        self._check(self.lib.psod_fof_get_halos(self.ctx, C.byref(ct)))
         return t
 
 

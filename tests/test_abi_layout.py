@@ -21,15 +21,20 @@ PAIRS = [
     ("psod_halo_table", capi.HaloTable, "psod.h"),
     ("psod_run_stats", capi.RunStats, "psod.h"),
     ("psod_train_params", capi.TrainParams, "psod.h"),
+    ("psod_fof_params", capi.FofParams, "psod.h"),
+    ("psod_fof_stats", capi.FofStats, "psod.h"),
+    ("psod_fof_table", capi.FofTable, "psod.h"),
     ("psod_oracle_params", O._Params, "psod_oracle.h"),
     ("psod_oracle_result", O._Result, "psod_oracle.h"),
     ("psod_oracle_audit", O._Audit, "psod_oracle.h"),
+    ("psod_oracle_fof_params", O._FofParams, "psod_oracle_fof.h"),
+    ("psod_oracle_fof_result", O._FofResult, "psod_oracle_fof.h"),
 ]
 
 
 def _probe_source() -> str:
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "psod.h"', '#include "psod_oracle.h"',
-             "int main(void) {"]
+             '#include "psod_oracle_fof.h"', "int main(void) {"]
     for cname, py, _ in PAIRS:
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
         for fname, *_ in py._fields_:
