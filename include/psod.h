@@ -355,7 +355,7 @@ typedef struct psod_fof_stats {
   int64_t ngroups;    /* all groups, single particles included */
   int64_t fine_cells; /* non-empty linking cells */
   int64_t pair_tests; /* particle pairs tested */
-  int64_t cell_pairs; /* neighbouring linking-cell pairs examined */
+  int64_t cell_pairs; /* neighbour look-ups (linking-cell rows or cells) */
   double ms_total;    /* device time of psod_fof */
   double ms_sort;     /* linking-cell sort */
   double ms_link;     /* union-find over the linking cells */

@@ -21,7 +21,7 @@
 //      of neighbouring runs (each unordered pair once: offsets in a half
 //      space) the particle pairs are tested until one pair are friends, and
 //      then the two components are joined (lock-free: the larger root is
-//      hooked under the smaller with atomicCAS).  Runs of up to 8 records are
+//      hooked under the smaller with atomicCAS).  Runs of up to 4 records are
 //      handled by a thread, larger ones by a warp.
 //   3. labels, masses, members, centres and radii as the reference computes
 //      them, per halo.
@@ -47,7 +47,7 @@ namespace {
 
 constexpr int FOF_TPB = 256;
 constexpr unsigned FOF_SMALL_CELL = 16;  // records a thread sorts itself
-constexpr unsigned FOF_THREAD_RUN = 8;   // runs a thread links; longer ones go to a warp
+constexpr unsigned FOF_THREAD_RUN = 4;   // runs a thread links; longer ones go to a warp
 constexpr int FOF_MAX_OFF = 171;         // half of the 7^3 - 1 neighbour offsets
 constexpr unsigned FOF_WARP_HALO = 2048; // halos whose observables a warp computes; larger: a CTA
 
@@ -58,6 +58,7 @@ struct FofGeo {
   float nxf;
   double xs;   // SOD grid shift (grid units)
   int k;       // linking cells per SOD cell and axis
+  int R;       // reach in linking cells per axis
   double reach2;  // squared reach, in linking-cell units, for the box filter
   int noff;    // neighbour offsets in c_fof_off
   float r2, rT;
@@ -338,14 +339,22 @@ __device__ __forceinline__ float box_gap2(const RunGeo &u, int ox, int oy, int o
 constexpr int FOF_SAMPLE = 2;
 
 // A thread per run of up to FOF_THREAD_RUN records; longer runs are listed
-// (in the first pass) for k_fof_link_warp.
+// (in the first pass) for k_fof_link_warp.  The neighbour cells are walked
+// row by row: for each (dy, dz) of the half space whose row of linking
+// cells comes within reach of the run's records, the cells of the row that
+// do form one key range inside each SOD cell the row crosses, found with
+// one search; every record of the range is then tested.  A friend joins the
+// two components; in the full pass a record whose parent is the run's
+// parent (both compressed) needs no test.
 template <bool FULL>
-__global__ void __launch_bounds__(FOF_TPB) k_fof_link_thread(const unsigned *heads, long long nrun, FofGeo G,
+__global__ void __launch_bounds__(FOF_TPB, 3) k_fof_link_thread(const unsigned *heads, long long nrun, FofGeo G,
                                                              const unsigned *cs, const unsigned short *skey,
                                                              const unsigned *perm, const float4 *cube,
                                                              unsigned *par, unsigned *bigrun, unsigned *nbigrun,
                                                              unsigned long long *counters) {
   unsigned long long tests = 0, pairs = 0;
+  const int R = G.R;
+  const float reach2 = (float)G.reach2;
   for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < nrun;
        q += (long long)gridDim.x * blockDim.x) {
     const unsigned h = heads[q], e = heads[q + 1];
@@ -353,47 +362,96 @@ __global__ void __launch_bounds__(FOF_TPB) k_fof_link_thread(const unsigned *hea
       if (!FULL) bigrun[atomicAdd(nbigrun, 1u)] = (unsigned)q;
       continue;
     }
+    const unsigned m = e - h;
     float4 ur[FOF_THREAD_RUN];
     float lo[3], hi[3];
     ur[0] = cube[perm[h]];
     const RunGeo u = run_geo(ur[0], G, lo, hi);
-    for (unsigned j = 1; j < e - h; j++) {
-      ur[j] = cube[perm[h + j]];
-      int c, f;
-      float p;
-      fof_axis(ur[j].x, G, c, f, p);
-      lo[0] = fminf(lo[0], p);
-      hi[0] = fmaxf(hi[0], p);
-      fof_axis(ur[j].y, G, c, f, p);
-      lo[1] = fminf(lo[1], p);
-      hi[1] = fmaxf(hi[1], p);
-      fof_axis(ur[j].z, G, c, f, p);
-      lo[2] = fminf(lo[2], p);
-      hi[2] = fmaxf(hi[2], p);
+#pragma unroll
+    for (unsigned j = 1; j < FOF_THREAD_RUN; j++) {
+      if (j < m) {
+        ur[j] = cube[perm[h + j]];
+        int c, f;
+        float pp;
+        fof_axis(ur[j].x, G, c, f, pp);
+        lo[0] = fminf(lo[0], pp);
+        hi[0] = fmaxf(hi[0], pp);
+        fof_axis(ur[j].y, G, c, f, pp);
+        lo[1] = fminf(lo[1], pp);
+        hi[1] = fmaxf(hi[1], pp);
+        fof_axis(ur[j].z, G, c, f, pp);
+        lo[2] = fminf(lo[2], pp);
+        hi[2] = fmaxf(hi[2], pp);
+      }
     }
-    const unsigned m = e - h;
-    int sampled = 0;
-    for (int o = 0; o < G.noff; o++) {
-      const int ox = c_fof_off[3 * o], oy = c_fof_off[3 * o + 1], oz = c_fof_off[3 * o + 2];
-      if (box_gap2(u, ox, oy, oz, lo, hi) > (float)G.reach2) continue;
-      unsigned vlo, vhi;
-      if (!find_run(u, ox, oy, oz, G, cs, skey, vlo, vhi)) continue;
-      if (vlo == h) continue;  // the run itself (a box of few cells wraps onto itself)
-      if (!FULL && sampled++ == FOF_SAMPLE) break;
-      pairs++;
-      if (FULL && __ldcg(par + h) == __ldcg(par + vlo)) continue;
-      bool hit = false;
-      for (unsigned v = vlo; v < vhi && !hit; v++) {
-        const float4 bv = cube[perm[v]];
-        for (unsigned j = 0; j < m; j++) {
-          tests++;
-          if (fof_friends(ur[j], bv, G.r2, G.rT)) {
-            hit = true;
-            break;
+    const unsigned myroot = FULL ? __ldcg(par + h) : 0u;
+    int found = 0;
+    for (int oz = 0; oz <= R && found <= FOF_SAMPLE; oz++) {
+      const float bz = (float)(u.fz + oz);
+      const float gz = fmaxf(fmaxf(bz - hi[2], lo[2] - (bz + 1.f)), 0.f);
+      if (gz * gz > reach2) continue;
+      for (int oy = (oz == 0 ? 0 : -R); oy <= R && found <= FOF_SAMPLE; oy++) {
+        const float by = (float)(u.fy + oy);
+        const float gy = fmaxf(fmaxf(by - hi[1], lo[1] - (by + 1.f)), 0.f);
+        const float left = reach2 - gz * gz - gy * gy;
+        if (left < 0.f) continue;
+        const float rx = sqrtf(left);
+        // cells of the row within reach, in the run's SOD-cell frame
+        int xa = (int)floorf(lo[0] - rx), xb = (int)floorf(hi[0] + rx);
+        xa = max(xa, u.fx - R);
+        xb = min(xb, u.fx + R);
+        if (oz == 0 && oy == 0) xa = max(xa, u.fx + 1);  // own row: cells after the run's
+        if (xa > xb) continue;
+        // the row's SOD cells in y and z
+        int ty = u.fy + oy, tz = u.fz + oz;
+        const int dcy = ty < 0 ? -1 : (ty >= G.k ? 1 : 0), dcz = tz < 0 ? -1 : (tz >= G.k ? 1 : 0);
+        ty -= dcy * G.k;
+        tz -= dcz * G.k;
+        int cy = u.cy + dcy, cz = u.cz + dcz;
+        cy = cy < 0 ? cy + G.nx : (cy >= G.nx ? cy - G.nx : cy);
+        cz = cz < 0 ? cz + G.nx : (cz >= G.nx ? cz - G.nx : cz);
+        // up to three SOD cells along x
+        for (int dcx = -1; dcx <= 1 && found <= FOF_SAMPLE; dcx++) {
+          const int s0 = max(xa, dcx * G.k), s1 = min(xb, dcx * G.k + G.k - 1);
+          if (s0 > s1) continue;
+          int cx = u.cx + dcx;
+          cx = cx < 0 ? cx + G.nx : (cx >= G.nx ? cx - G.nx : cx);
+          const unsigned long long c = (unsigned long long)cx +
+                                       (unsigned long long)G.nx * ((unsigned long long)cy + (unsigned long long)G.nx * cz);
+          const unsigned clo = __ldg(cs + c), chi = __ldg(cs + c + 1);
+          if (clo == chi) continue;
+          const unsigned rowkey = (unsigned)(G.k * (ty + G.k * tz));
+          const unsigned k0 = rowkey + (unsigned)(s0 - dcx * G.k), k1 = rowkey + (unsigned)(s1 - dcx * G.k);
+          unsigned v = clo;
+          if (chi - clo <= 16) {
+            while (v < chi && __ldg(skey + v) < k0) v++;
+          } else {
+            unsigned b2 = chi;
+            while (v < b2) {
+              const unsigned mid = (v + b2) >> 1;
+              if (__ldg(skey + mid) < k0) v = mid + 1;
+              else b2 = mid;
+            }
+          }
+          pairs++;
+          for (; v < chi && __ldg(skey + v) <= k1; v++) {
+            if (FULL && __ldcg(par + v) == myroot) continue;
+            const float4 bv = cube[perm[v]];
+            bool hit = false;
+#pragma unroll
+            for (unsigned j = 0; j < FOF_THREAD_RUN; j++) {
+              if (j < m && !hit) {
+                tests++;
+                hit = fof_friends(ur[j], bv, G.r2, G.rT);
+              }
+            }
+            if (hit) {
+              uf_union(par, h, v);
+              if (!FULL && ++found > FOF_SAMPLE) break;
+            }
           }
         }
       }
-      if (hit) uf_union(par, h, vlo);
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -773,6 +831,7 @@ int psod_fof(psod_ctx *c, const psod_fof_params *p, psod_fof_stats *stats) {
   G.nxf = (float)c->nx;
   G.xs = c->xxmin * c->scale;
   G.k = k;
+  G.R = R;
   G.reach2 = reach2;
   G.noff = (int)(offs.size() / 3);
   G.rT = p->percolation / (float)nres;  // FP32, as rT = r / size
