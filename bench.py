@@ -767,6 +767,87 @@ def run_fof(args):
     print(json.dumps(line), flush=True)
 
 
+PROPS_METRIC = "halo properties halos/s (haloanalyzer halo_properties on the SOD table)"
+# units of a RAMSES run of this box size: 100 Mpc/h per 128 cells, z = 0
+PROPS_UNITS = dict(unit_d=2.7e-30, unit_t=4.4e17, aexp=1.0, h0=70.0, hz=1.0, delta_vir=178.0)
+
+
+def run_props(args):
+    """The halo-properties stage (psod_halo_properties) on the SOD table of
+    the workload's box: one step = every halo's moments, potential energy,
+    profiles, R178 and inertia eigen solve.  value: halos per second with the
+    particles and the table resident in HBM; e2e adds the copy of every
+    output to host memory."""
+    import numpy as np
+    import torch
+
+    from psod_b200 import synth
+    from psod_b200.sod import SphericalOverdensity
+
+    nx = args.nx
+    wl = WORKLOADS.get(nx, dict(nmax_halo=20000, box=f"{nx}^3"))
+    torch.cuda.set_device(0)
+    box = synth.make_box(nx, nmax_halo=wl["nmax_halo"], seed=args.seed, device="cuda:0")
+    pos_d, ids_d = box.pos, box.ids
+    del box
+    gen = torch.Generator(device="cuda:0")
+    gen.manual_seed(args.seed + 7)
+    vel_d = torch.randn(pos_d.shape, generator=gen, device="cuda:0", dtype=torch.float32) * 0.3
+    torch.cuda.empty_cache()
+    units = dict(PROPS_UNITS, unit_l=3.08568e24 * 100 / 0.7 * nx / 128, levelmin=int(round(np.log2(nx))))
+    sod = SphericalOverdensity(nx, device=0, npu=npu_for(nx), mode=1)
+    sod.load(pos_d, ids_d, vel=vel_d)
+    sst = sod.run()
+    for _ in range(args.warmup):
+        sod.halo_properties(**units, source="sod")
+    torch.cuda.synchronize()
+    stats = []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            stats.append(sod.halo_properties(**units, source="sod")[1])
+    ms = sum(s["ms_total"] for s in stats) / len(stats)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        out, st = sod.halo_properties(**units, source="sod")
+    e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
+    nh = int(st["nhalo"])
+    line = {
+        "metric": PROPS_METRIC, "value": round(nh / (ms / 1000.0), 1), "unit": "halos/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (sums), f32 (pair terms, outputs)",
+        "data": "synthetic NFW-mixture box (seeded), random velocities; SOD table resident in HBM",
+        "config": {"workload": wl["box"] + ", SOD batched, then halo_properties", "nx": nx, "halos": nh,
+                   "members": int(st["nmember"])},
+        "detail": {"potential_items": int(st["potential_items"]), "sod_ms": round(sst["ms_total"], 1)},
+        "e2e": {"value": round(nh / (e2e_ms / 1000.0), 1), "unit": "halos/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": int(sum(a.nbytes for a in out.values())), "ms_per_step": round(e2e_ms, 3)},
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        t = sod.halos()
+        pos_h = pos_d.cpu().numpy()
+        vel_h = vel_d.cpu().numpy()
+        # a bounded sample: every k-th halo, about 20 s of one core at most
+        k = max(1, nh // 4000)
+        sel = np.arange(0, nh, k)
+        off = [0]
+        mem = []
+        for hh in sel:
+            m = t.member_index[t.member_offset[hh]: t.member_offset[hh + 1]]
+            mem.append(m)
+            off.append(off[-1] + len(m))
+        t0 = time.perf_counter()
+        O.halo_properties(np.array(off), np.concatenate(mem), pos_h, vel_h, **units)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": round(len(sel) / dt, 2), "unit": "halos/s", "cores": 1, "kind": "port",
+                                "sample": f"every {k}th halo of the same table ({len(sel)} halos, "
+                                          f"{off[-1]} members), the C oracle's halo_properties, {dt:.2f} s"}
+    sod.close()
+    print(json.dumps(line), flush=True)
+
+
 def relaunch_with_torchrun(args):
     """``--gpus N`` without a torchrun environment: start the N ranks here
     (one process per GPU) with the same arguments, and return their status."""
@@ -793,6 +874,8 @@ def main():
     ap.add_argument("--delta200-only", dest="ndelta", action="store_false",
                     help="Delta = 200 and 60 bins only (default: 200, 500 and 178 in one pass, 48 bins)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--props", action="store_true",
+                    help="time the halo-properties stage (psod_halo_properties) on the SOD table; one GPU")
     ap.add_argument("--fof", action="store_true",
                     help="time the friends-of-friends stage (psod_fof) instead of SOD; one GPU")
     ap.add_argument("--heavy", action="store_true",
@@ -805,6 +888,8 @@ def main():
         run_reference(args)
     elif args.fof:
         run_fof(args)
+    elif args.props:
+        run_props(args)
     else:
         run_ours(args)
 

@@ -378,6 +378,74 @@ int psod_fof(psod_ctx *ctx, const psod_fof_params *p, psod_fof_stats *stats);
 int psod_fof_halo_count(psod_ctx *ctx, int64_t *nhalo, int64_t *nmember);
 int psod_fof_get_halos(psod_ctx *ctx, const psod_fof_table *t);
 
+/* ---- Halo properties (haloanalyzer's halo_properties) -------------------
+ * haloanalyzer_new/src/modfunctions.f90:47-808 for every halo of the last
+ * SOD table (psod_spherover) or FoF catalogue (psod_fof) of the context,
+ * members in the table's order, at a fixed redshift (no lightcone) and
+ * without the volume estimate (which the reference leaves off): virial mass,
+ * radius and velocity from the particle count, centre of mass and mean
+ * velocity, R_max, V_max, the position and velocity dispersions, kinetic
+ * and potential energy and the most bound member, the density,
+ * integrated-density and circular-velocity profiles in 100 log bins of
+ * radius (1 kpc, dlnR 0.1) and 30 of R/R178 (0.01, dlnR 0.2) around the
+ * potential minimum (or the centre of mass), the circular-velocity maximum,
+ * the interpolated R178/M178, the angular momentum's two spin parameters,
+ * the inertia tensor's sorted eigenvalues (cyclic Jacobi) and minor axis,
+ * and the cosine between that axis and the angular momentum.  Values are
+ * the reference's, in its units and precision: real(4) where it stores
+ * real(4) (the float arrays below), real(8) for the four virial values and
+ * cos_alpha.  The halo's particles are the loaded positions (box units)
+ * and velocities (zeros when none were loaded), in the units of the
+ * simulation (unit_l / unit_t per velocity unit).
+ * One departure: for a halo of at least epot_threshold particles the
+ * reference estimates the potential from epot_threshold/10 members drawn
+ * with random_number; here the members at positions floor(k*n/m), k = 0 ..
+ * m-1 (m = epot_threshold/10), form the sample. */
+#define PSOD_PROPS_NBIN1 100
+#define PSOD_PROPS_NBIN2 30
+#define PSOD_PROPS_FROM_SOD 0
+#define PSOD_PROPS_FROM_FOF 1
+
+typedef struct psod_props_params {
+  double unit_l, unit_d, unit_t; /* simu_info%unit_l/_d/_t (cgs) */
+  double aexp;                   /* simu_info%aexp */
+  double h0;                     /* simu_info%h0 (km/s/Mpc) */
+  double hz;                     /* a^2 H(a)/H0 as the reference interpolates it (modanalyzeengines.f90:305-313) */
+  double delta_vir;              /* simu_info%delta_vir (Delta_matter) */
+  int32_t levelmin;              /* simu_info%levelmin: mass_part = 2^-3 levelmin, smoothing 2^-levelmin / 64 */
+  int32_t center_on_mass;        /* do_center_mass: profiles around the centre of mass (1) or the most bound member (0) */
+  int32_t periodic;              /* do_periodic_boundary */
+  int32_t source;                /* PSOD_PROPS_FROM_SOD or PSOD_PROPS_FROM_FOF */
+  int32_t epot_threshold;        /* 30000 (modfunctions.f90:336) */
+  int32_t reserved;              /* 0 */
+} psod_props_params;
+
+typedef struct psod_props_stats {
+  int64_t nhalo, nmember;
+  int64_t potential_items; /* (halo, 256-member) work items of the potential pass */
+  double ms_total;         /* device time of psod_halo_properties */
+} psod_props_stats;
+
+/* per halo; [k] marks k values per halo, halo-major */
+typedef struct psod_props_table {
+  int64_t *npart;
+  double *mvir, *rvir, *rvircom, *vvir;    /* Msun/h, kpc/h physical, kpc/h comoving, km/s */
+  float *com, *comv;                       /* [3] Mpc/h comoving, km/s */
+  float *rmax, *vmax, *dispx, *dispv;      /* over R_vir or V_vir */
+  float *ekin, *epot;                      /* over M_vir V_vir^2 / 2 */
+  float *lambda, *lambda_prime;            /* [3] */
+  float *eig_val, *eig_vec;                /* [3] a, b, c over R_vir; minor axis */
+  double *cos_alpha;
+  float *center_pot;                       /* [3] Mpc/h comoving */
+  float *circ;                             /* [4] M_circ_max, R_circ_max, V_circ_max, Rho_circ_max */
+  float *delta_vals;                       /* [2] M178 (Msun/h), R178 (kpc/h physical) */
+  float *dens, *dens_int, *vcirc;          /* [PSOD_PROPS_NBIN1] */
+  float *dens178, *dens_int178;            /* [PSOD_PROPS_NBIN2] */
+} psod_props_table;
+
+int psod_halo_properties(psod_ctx *ctx, const psod_props_params *p, psod_props_stats *stats);
+int psod_props_get(psod_ctx *ctx, const psod_props_table *t);
+
 const char *psod_last_error(const psod_ctx *ctx);
 const char *psod_status_string(int status);
 int psod_abi_version(void);

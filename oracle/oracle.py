@@ -445,3 +445,60 @@ def fof(pos, ids, vel=None, percolation: float = 0.2, nres: int | None = None, m
                     structure=take(r.structure, n, np.int64))
     L.psod_oracle_fof_free(C.byref(r))
     return out
+
+
+# ---------------------------------------------------------------------------
+# halo properties (haloanalyzer halo_properties; psod_oracle_props.c)
+# ---------------------------------------------------------------------------
+PROPS_NBIN1 = 100
+PROPS_NBIN2 = 30
+
+
+class _PropsParams(C.Structure):
+    _fields_ = [("unit_l", C.c_double), ("unit_d", C.c_double), ("unit_t", C.c_double), ("aexp", C.c_double),
+                ("h0", C.c_double), ("hz", C.c_double), ("delta_vir", C.c_double), ("levelmin", C.c_int32),
+                ("center_on_mass", C.c_int32), ("periodic", C.c_int32), ("epot_threshold", C.c_int32)]
+
+
+_PROPS_OUT = [
+    ("npart", 1, np.int64), ("mvir", 1, np.float64), ("rvir", 1, np.float64), ("rvircom", 1, np.float64),
+    ("vvir", 1, np.float64), ("com", 3, np.float32), ("comv", 3, np.float32), ("rmax", 1, np.float32),
+    ("vmax", 1, np.float32), ("dispx", 1, np.float32), ("dispv", 1, np.float32), ("ekin", 1, np.float32),
+    ("epot", 1, np.float32), ("lambda", 3, np.float32), ("lambda_prime", 3, np.float32),
+    ("eig_val", 3, np.float32), ("eig_vec", 3, np.float32), ("cos_alpha", 1, np.float64),
+    ("center_pot", 3, np.float32), ("circ", 4, np.float32), ("delta_vals", 2, np.float32),
+    ("dens", PROPS_NBIN1, np.float32), ("dens_int", PROPS_NBIN1, np.float32), ("vcirc", PROPS_NBIN1, np.float32),
+    ("dens178", PROPS_NBIN2, np.float32), ("dens_int178", PROPS_NBIN2, np.float32),
+]
+
+
+class _PropsOut(C.Structure):
+    _fields_ = [(f, C.c_void_p) for f, _, _ in _PROPS_OUT]
+
+
+def halo_properties(offset, member, pos, vel=None, *, unit_l, unit_d, unit_t, aexp, h0, hz, delta_vir, levelmin,
+                    center_on_mass=False, periodic=True, epot_threshold=30000) -> dict:
+    """haloanalyzer_new/src/modfunctions.f90 halo_properties (:47-808) for
+    halos given as member lists (offset[h]..offset[h+1] into member, input
+    indices into pos / vel), in the reference's statement order."""
+    L = lib()
+    if not hasattr(L, "_props_ready"):
+        L.psod_oracle_halo_properties.argtypes = [C.POINTER(_PropsParams), C.c_int64, C.POINTER(C.c_int64),
+                                                  C.POINTER(C.c_int64), C.POINTER(C.c_float),
+                                                  C.POINTER(C.c_float), C.POINTER(_PropsOut)]
+        L._props_ready = True
+    off = np.ascontiguousarray(offset, np.int64)
+    mem = np.ascontiguousarray(member, np.int64)
+    p = _as_pos(pos)
+    v = None if vel is None else np.ascontiguousarray(
+        vel.cpu().numpy() if hasattr(vel, "cpu") else vel, dtype=np.float32).reshape(-1, 3)
+    nh = off.shape[0] - 1
+    out = {f: np.zeros((nh, k) if k > 1 else nh, dtype=dt) for f, k, dt in _PROPS_OUT}
+    co = _PropsOut(*[out[f].ctypes.data if out[f].size else None for f, _, _ in _PROPS_OUT])
+    cp = _PropsParams(unit_l, unit_d, unit_t, aexp, h0, hz, delta_vir, levelmin, int(center_on_mass), int(periodic),
+                      epot_threshold)
+    st = L.psod_oracle_halo_properties(C.byref(cp), nh, _ptr(off, C.c_int64), _ptr(mem, C.c_int64),
+                                       _ptr(p, C.c_float), None if v is None else _ptr(v, C.c_float), C.byref(co))
+    if st != 0:
+        raise ValueError(f"psod_oracle_halo_properties status {st}")
+    return out

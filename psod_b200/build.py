@@ -11,8 +11,11 @@ CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libpsod.so")
 SOURCES = ["psod_capi.cu", "psod_stages.cu", "psod_sod.cu", "psod_sort.cu", "psod_static.cu", "psod_learn.cu",
-           "psod_output.cu", "psod_input.cu", "psod_fof.cu"]
+           "psod_output.cu", "psod_input.cu", "psod_fof.cu", "psod_props.cu"]
 HEADERS = ["psod_internal.cuh"]
+# the halo-properties arithmetic follows the reference statement by
+# statement: no multiply-add contraction in that file
+FILE_FLAGS = {"psod_props.cu": ["--fmad=false"]}
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--extended-lambda", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2"]
 
@@ -42,7 +45,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     for s in SOURCES:
         src = os.path.join(CSRC, s)
         obj = os.path.join(OUT_DIR, s.replace(".cu", ".o"))
-        cmd = [nvcc, *ARCH, *FLAGS, "-I", os.path.join(HERE, "..", "include"), "-c", src, "-o", obj]
+        cmd = [nvcc, *ARCH, *FLAGS, *FILE_FLAGS.get(s, []), "-I", os.path.join(HERE, "..", "include"), "-c", src,
+               "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)

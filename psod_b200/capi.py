@@ -144,6 +144,54 @@ class FofTable(C.Structure):
     ]
 
 
+PROPS_NBIN1 = 100
+PROPS_NBIN2 = 30
+PROPS_FROM_SOD = 0
+PROPS_FROM_FOF = 1
+
+
+class PropsParams(C.Structure):
+    _fields_ = [
+        ("unit_l", C.c_double),
+        ("unit_d", C.c_double),
+        ("unit_t", C.c_double),
+        ("aexp", C.c_double),
+        ("h0", C.c_double),
+        ("hz", C.c_double),
+        ("delta_vir", C.c_double),
+        ("levelmin", C.c_int32),
+        ("center_on_mass", C.c_int32),
+        ("periodic", C.c_int32),
+        ("source", C.c_int32),
+        ("epot_threshold", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class PropsStats(C.Structure):
+    _fields_ = [("nhalo", C.c_int64), ("nmember", C.c_int64), ("potential_items", C.c_int64),
+                ("ms_total", C.c_double)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+# (field, values per halo, numpy dtype) in psod_props_table order
+PROPS_FIELDS = [
+    ("npart", 1, "int64"), ("mvir", 1, "float64"), ("rvir", 1, "float64"), ("rvircom", 1, "float64"),
+    ("vvir", 1, "float64"), ("com", 3, "float32"), ("comv", 3, "float32"), ("rmax", 1, "float32"),
+    ("vmax", 1, "float32"), ("dispx", 1, "float32"), ("dispv", 1, "float32"), ("ekin", 1, "float32"),
+    ("epot", 1, "float32"), ("lambda", 3, "float32"), ("lambda_prime", 3, "float32"), ("eig_val", 3, "float32"),
+    ("eig_vec", 3, "float32"), ("cos_alpha", 1, "float64"), ("center_pot", 3, "float32"), ("circ", 4, "float32"),
+    ("delta_vals", 2, "float32"), ("dens", PROPS_NBIN1, "float32"), ("dens_int", PROPS_NBIN1, "float32"),
+    ("vcirc", PROPS_NBIN1, "float32"), ("dens178", PROPS_NBIN2, "float32"), ("dens_int178", PROPS_NBIN2, "float32"),
+]
+
+
+class PropsTable(C.Structure):
+    _fields_ = [(f, C.c_void_p) for f, _, _ in PROPS_FIELDS]
+
+
 EXPORTS = [
     "psod_abi_version",
     "psod_status_string",
@@ -175,6 +223,8 @@ EXPORTS = [
     "psod_fof",
     "psod_fof_halo_count",
     "psod_fof_get_halos",
+    "psod_halo_properties",
+    "psod_props_get",
 ]
 
 LEARN_FEATURES = 10
@@ -236,6 +286,8 @@ def load(build_if_missing: bool = True):
     L.psod_fof.argtypes = [vp, P(FofParams), P(FofStats)]
     L.psod_fof_halo_count.argtypes = [vp, P(C.c_int64), P(C.c_int64)]
     L.psod_fof_get_halos.argtypes = [vp, P(FofTable)]
+    L.psod_halo_properties.argtypes = [vp, P(PropsParams), P(PropsStats)]
+    L.psod_props_get.argtypes = [vp, P(PropsTable)]
     L.psod_last_error.argtypes = [vp]
     L.psod_cic_rho_static.argtypes = [C.c_int64, vp, C.c_int32, C.c_int64, C.c_int32, vp, vp, vp]
     L.psod_learn_collect.argtypes = [vp, C.c_int64]

@@ -187,6 +187,13 @@ struct psod_ctx {
   // friends-of-friends catalogue (psod_fof; arrays in the SLOT_F_* slots)
   bool fof_done = false;
   long long fof_nhalo = 0, fof_nmember = 0;
+
+  // halo properties (psod_halo_properties; arrays in the SLOT_PO_* slots)
+  bool props_done = false;
+  long long props_nhalo = 0;
+  struct {
+    void *npart, *vir, *f32, *cos;
+  } props_out{};
 };
 
 namespace psod {
@@ -321,7 +328,17 @@ enum : int {
   SLOT_F_COM,
   SLOT_F_VEL,
   SLOT_F_RAD,
-  SLOT_F_MEM
+  SLOT_F_MEM,
+  SLOT_PR_POS,          // props: member positions after the periodic shifts
+  SLOT_PR_EPI,          // props: per-member potential sums
+  SLOT_PR_WORK,         // props: per-halo sums
+  SLOT_PR_CNT,          // props: potential items per halo, then their scan
+  SLOT_PR_PREF,         // props: the scan as int64
+  SLOT_PR_IHALO,        // props: halo of each potential item
+  SLOT_PO_NPART,        // props outputs (kept until the next call)
+  SLOT_PO_VIR,
+  SLOT_PO_F32,
+  SLOT_PO_COS
 };
 
 // learned radius bracket (psod_learn.cu)

@@ -304,6 +304,29 @@ class SphericalOverdensity:
         return t
 
 
+    # ---- halo properties (haloanalyzer's halo_properties) ----
+    def halo_properties(self, unit_l: float, unit_d: float, unit_t: float, aexp: float, h0: float, hz: float,
+                        delta_vir: float, levelmin: int, source: str = "sod", center_on_mass: bool = False,
+                        periodic: bool = True, epot_threshold: int = 30000) -> tuple[dict, dict]:
+        """haloanalyzer_new/src/modfunctions.f90 halo_properties for every
+        halo of the last SOD table (``source="sod"``) or FoF catalogue
+        (``source="fof"``).  Returns (properties, counters): each property an
+        array of shape (nhalo,) or (nhalo, k) in the reference's units and
+        precision."""
+        p = capi.PropsParams(unit_l, unit_d, unit_t, aexp, h0, hz, delta_vir, levelmin, int(center_on_mass),
+                             int(periodic), capi.PROPS_FROM_FOF if source == "fof" else capi.PROPS_FROM_SOD,
+                             epot_threshold, 0)
+        st = capi.PropsStats()
+        self._check(self.lib.psod_halo_properties(self.ctx, C.byref(p), C.byref(st)))
+        nh = int(st.nhalo)
+        out = {f: np.zeros((nh, k) if k > 1 else nh, dtype=dt) for f, k, dt in capi.PROPS_FIELDS}
+        ct = capi.PropsTable()
+        for f, _, _ in capi.PROPS_FIELDS:
+            setattr(ct, f, None if out[f].size == 0 else out[f].ctypes.data)
+        self._check(self.lib.psod_props_get(self.ctx, C.byref(ct)))
+        return out, st.as_dict()
+
+
 def _host_table(t: HaloTable) -> tuple[capi.HaloTable, list]:
     """A C halo table pointing at host numpy copies of ``t``'s arrays (the
     copies are returned too, to keep them alive during the call)."""

@@ -24,17 +24,22 @@ PAIRS = [
     ("psod_fof_params", capi.FofParams, "psod.h"),
     ("psod_fof_stats", capi.FofStats, "psod.h"),
     ("psod_fof_table", capi.FofTable, "psod.h"),
+    ("psod_props_params", capi.PropsParams, "psod.h"),
+    ("psod_props_stats", capi.PropsStats, "psod.h"),
+    ("psod_props_table", capi.PropsTable, "psod.h"),
     ("psod_oracle_params", O._Params, "psod_oracle.h"),
     ("psod_oracle_result", O._Result, "psod_oracle.h"),
     ("psod_oracle_audit", O._Audit, "psod_oracle.h"),
     ("psod_oracle_fof_params", O._FofParams, "psod_oracle_fof.h"),
     ("psod_oracle_fof_result", O._FofResult, "psod_oracle_fof.h"),
+    ("psod_oracle_props_params", O._PropsParams, "psod_oracle_props.h"),
+    ("psod_oracle_props_out", O._PropsOut, "psod_oracle_props.h"),
 ]
 
 
 def _probe_source() -> str:
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "psod.h"', '#include "psod_oracle.h"',
-             '#include "psod_oracle_fof.h"', "int main(void) {"]
+             '#include "psod_oracle_fof.h"', '#include "psod_oracle_props.h"', "int main(void) {"]
     for cname, py, _ in PAIRS:
         lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
         for fname, *_ in py._fields_:
