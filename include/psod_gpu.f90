@@ -80,6 +80,28 @@ module psod_gpu
      type(c_ptr) :: member_offset, member_index, member_id
   end type psod_fof_table
 
+  ! haloanalyzer's halo_properties on the SOD table or the FoF catalogue
+  integer(c_int32_t), parameter :: PSOD_PROPS_FROM_SOD = 0, PSOD_PROPS_FROM_FOF = 1
+  integer(c_int32_t), parameter :: PSOD_PROPS_NBIN1 = 100, PSOD_PROPS_NBIN2 = 30
+  type, bind(C) :: psod_props_params
+     real(c_double)     :: unit_l, unit_d, unit_t, aexp, h0, hz, delta_vir
+     integer(c_int32_t) :: levelmin, center_on_mass, periodic, source, epot_threshold, reserved
+  end type psod_props_params
+
+  type, bind(C) :: psod_props_stats
+     integer(c_int64_t) :: nhalo, nmember, potential_items
+     real(c_double)     :: ms_total
+  end type psod_props_stats
+
+  ! haloNpart, haloMvir, haloRvir, haloRvircom, haloVvir, haloCOMX, haloCOMV,
+  ! ..., the five profiles (psod.h lists the sizes per halo)
+  type, bind(C) :: psod_props_table
+     type(c_ptr) :: npart, mvir, rvir, rvircom, vvir, com, comv
+     type(c_ptr) :: rmax, vmax, dispx, dispv, ekin, epot, lambda, lambda_prime
+     type(c_ptr) :: eig_val, eig_vec, cos_alpha, center_pot, circ, delta_vals
+     type(c_ptr) :: dens, dens_int, vcirc, dens178, dens_int178
+  end type psod_props_table
+
   interface
      subroutine psod_params_default(p) bind(C, name="psod_params_default")
        import :: psod_params
@@ -200,6 +222,17 @@ module psod_gpu
        import :: c_int, c_ptr, psod_fof_table
        type(c_ptr), value :: ctx
        type(psod_fof_table), intent(in) :: t
+     end function
+     integer(c_int) function psod_halo_properties(ctx, p, stats) bind(C, name="psod_halo_properties")
+       import :: c_int, c_ptr, psod_props_params, psod_props_stats
+       type(c_ptr), value :: ctx
+       type(psod_props_params), intent(in) :: p
+       type(psod_props_stats), intent(out) :: stats
+     end function
+     integer(c_int) function psod_props_get(ctx, t) bind(C, name="psod_props_get")
+       import :: c_int, c_ptr, psod_props_table
+       type(c_ptr), value :: ctx
+       type(psod_props_table), intent(in) :: t
      end function
   end interface
 end module psod_gpu

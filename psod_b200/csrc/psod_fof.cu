@@ -330,13 +330,16 @@ __device__ __forceinline__ float box_gap2(const RunGeo &u, int ox, int oy, int o
 }
 
 // Linking runs in two passes (the sampling scheme of Afforest, Sutton et
-// al. 2018).  The first pass joins each run to at most FOF_SAMPLE
-// neighbouring runs, which already builds most of every large group; after
+// al. 2018).  The first pass joins each short run to at most FOF_SAMPLE
+// friends and each long run to the friends among FOF_SAMPLE_WARP
+// neighbouring runs, which already builds most of every large group (one
+// friend per run, or six, measured slower at 512^3 and 1024^3); after
 // a compression every position points at its root, so in the full pass a
 // neighbour run with the same parent is skipped with two loads instead of
 // two path walks.  Both passes test the same pairs' friendship, so the
 // components are the same as without sampling.
-constexpr int FOF_SAMPLE = 2;
+constexpr int FOF_SAMPLE = 3;       // friends a thread's run joins in the first pass
+constexpr int FOF_SAMPLE_WARP = 2;  // neighbour runs a warp's run examines in the first pass
 
 // A thread per run of up to FOF_THREAD_RUN records; longer runs are listed
 // (in the first pass) for k_fof_link_warp.  The neighbour cells are walked
@@ -386,11 +389,11 @@ __global__ void __launch_bounds__(FOF_TPB, 3) k_fof_link_thread(const unsigned *
     }
     const unsigned myroot = FULL ? __ldcg(par + h) : 0u;
     int found = 0;
-    for (int oz = 0; oz <= R && found <= FOF_SAMPLE; oz++) {
+    for (int oz = 0; oz <= R && found < FOF_SAMPLE; oz++) {
       const float bz = (float)(u.fz + oz);
       const float gz = fmaxf(fmaxf(bz - hi[2], lo[2] - (bz + 1.f)), 0.f);
       if (gz * gz > reach2) continue;
-      for (int oy = (oz == 0 ? 0 : -R); oy <= R && found <= FOF_SAMPLE; oy++) {
+      for (int oy = (oz == 0 ? 0 : -R); oy <= R && found < FOF_SAMPLE; oy++) {
         const float by = (float)(u.fy + oy);
         const float gy = fmaxf(fmaxf(by - hi[1], lo[1] - (by + 1.f)), 0.f);
         const float left = reach2 - gz * gz - gy * gy;
@@ -411,7 +414,7 @@ __global__ void __launch_bounds__(FOF_TPB, 3) k_fof_link_thread(const unsigned *
         cy = cy < 0 ? cy + G.nx : (cy >= G.nx ? cy - G.nx : cy);
         cz = cz < 0 ? cz + G.nx : (cz >= G.nx ? cz - G.nx : cz);
         // up to three SOD cells along x
-        for (int dcx = -1; dcx <= 1 && found <= FOF_SAMPLE; dcx++) {
+        for (int dcx = -1; dcx <= 1 && found < FOF_SAMPLE; dcx++) {
           const int s0 = max(xa, dcx * G.k), s1 = min(xb, dcx * G.k + G.k - 1);
           if (s0 > s1) continue;
           int cx = u.cx + dcx;
@@ -447,7 +450,7 @@ __global__ void __launch_bounds__(FOF_TPB, 3) k_fof_link_thread(const unsigned *
             }
             if (hit) {
               uf_union(par, h, v);
-              if (!FULL && ++found > FOF_SAMPLE) break;
+              if (!FULL && ++found >= FOF_SAMPLE) break;
             }
           }
         }
@@ -489,14 +492,14 @@ __global__ void __launch_bounds__(FOF_TPB) k_fof_link_warp(const unsigned *heads
     hi[1] = (float)(u.fy + 1);
     lo[2] = (float)u.fz;
     hi[2] = (float)(u.fz + 1);
-    int sampled = 0;
-    for (int o = 0; o < G.noff; o++) {
+    int sampled = 0;  // neighbour runs examined (warp-uniform)
+    for (int o = 0; o < G.noff && (FULL || sampled < FOF_SAMPLE_WARP); o++) {
       const int ox = c_fof_off[3 * o], oy = c_fof_off[3 * o + 1], oz = c_fof_off[3 * o + 2];
       if (box_gap2(u, ox, oy, oz, lo, hi) > (float)G.reach2) continue;
       unsigned vlo, vhi;
       if (!find_run(u, ox, oy, oz, G, cs, skey, vlo, vhi)) continue;
       if (vlo == h) continue;
-      if (!FULL && sampled++ == FOF_SAMPLE) break;
+      sampled++;
       if (lane == 0) pairs++;
       if (FULL && __ldcg(par + h) == __ldcg(par + vlo)) continue;
       bool hit = false;
