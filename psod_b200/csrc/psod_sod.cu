@@ -150,6 +150,18 @@ __device__ __forceinline__ void mark_resolved(const SodBufs &B, unsigned bi) {
   if (bi != 0xffffffffu) atomicOr(&B.resolved[bi >> 5], 1u << (bi & 31));
 }
 
+// Bitonic stages of a block-wide sort: thread k of a stage compares the
+// pair (a, a + stride), a = 2k - (k mod stride), for k = threadIdx.x + j *
+// blockDim.x.  For strides of at most 16 the pairs of warp w lie in its own
+// 64-element blocks (a in [64w + 2j*blockDim.x, +64)), so consecutive stages
+// with such strides need only a warp barrier; a stage with a wider stride
+// (or the end of the sort) needs the block barrier.
+__device__ __forceinline__ void bitonic_stage_sync(unsigned size, unsigned stride, unsigned m) {
+  const unsigned next = stride > 1 ? (stride >> 1) : ((size << 1) <= m ? size : 0u);
+  if (next != 0u && next <= 16u) __syncwarp();
+  else __syncthreads();
+}
+
 struct Level {
   unsigned long long lo, hi;  // bit range of the level
   unsigned long long cum;     // elements below lo
@@ -566,7 +578,7 @@ __device__ __forceinline__ unsigned extract_sorted(const SodConst &K, const SodB
           S.sidx[a] = ib; S.sidx[bb] = ia;
         }
       }
-      __syncthreads();
+      bitonic_stage_sync(size, stride, m);
     }
   }
   return n;
@@ -626,7 +638,7 @@ __device__ __forceinline__ unsigned load_ball_sorted(const SodConst &K, const So
           spos[bb] = pa;
         }
       }
-      __syncthreads();
+      bitonic_stage_sync(size, stride, m);
     }
   }
   return n;
@@ -3418,7 +3430,7 @@ __global__ void __launch_bounds__(256) k_member_sort(const unsigned *order, long
               unsigned ti = si[a]; si[a] = si[bb]; si[bb] = ti;
             }
           }
-          __syncthreads();
+          bitonic_stage_sync(size, stride, p2);
         }
       }
       for (unsigned k = threadIdx.x; k < n; k += blockDim.x) {
