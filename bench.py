@@ -261,6 +261,13 @@ def run_ours(args):
 
     for _ in range(args.warmup):
         st = step_device()
+    tuning = None
+    if args.autotune and args.mode != "plain":
+        # scheduling thresholds picked on this box (untimed; the table does
+        # not depend on them)
+        tuning = sod.autotune()
+    else:
+        tuning = sod.get_tuning()
     torch.cuda.synchronize()
     barrier(world)
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -355,6 +362,7 @@ def run_ours(args):
             "sod_phase_ms": {k: round(s[k], 2) for k in ("ms_setup", "ms_sched", "ms_prep", "ms_refine", "ms_select",
                                                          "ms_cross", "ms_tail", "ms_output")},
             "tail_rounds": s["tail_rounds"],
+            "tuning": tuning,
         },
         "e2e": {
             "value": round(nhalo_all / (e2e_ms / 1000.0), 2),
@@ -399,11 +407,11 @@ def run_ours(args):
         # identical to this one (device checksums of every field)
         digests = {args.mode: table_digest(sod, 0)}
         if args.mode == "learned":
-            line["batched"] = mode_reference(nx, params, pos_d, ids_d, sod, 1)
+            line["batched"] = mode_reference(nx, params, pos_d, ids_d, sod, 1, tuning)
             line["vs_batched"] = round(line["batched"]["ms_per_step"] / ms, 3)
             digests["batched"] = line["batched"].pop("digest")
             sod = None
-        line["plain"] = mode_reference(nx, params, pos_d, ids_d, sod, 0)
+        line["plain"] = mode_reference(nx, params, pos_d, ids_d, sod, 0, tuning)
         line["vs_plain"] = round(line["plain"]["ms_per_step"] / ms, 3)
         digests["plain"] = line["plain"].pop("digest")
         sod = None
@@ -449,7 +457,7 @@ def time_stages(sod, pos, ids):
     return out
 
 
-def mode_reference(nx, params, pos_d, ids_d, sod, mode):
+def mode_reference(nx, params, pos_d, ids_d, sod, mode, tuning=None):
     """The same box through another GPU mode (0 plain: full-cube gathers; 1
     batched: growing balls from 1.5 cells, no network), one untimed and one
     timed step.  Closes ``sod`` first to free its memory."""
@@ -463,6 +471,11 @@ def mode_reference(nx, params, pos_d, ids_d, sod, mode):
     p = dict(params)
     p["mode"] = mode
     sp = SphericalOverdensity(nx, device=torch.cuda.current_device(), **p)
+    if tuning:
+        # the main run's scheduling thresholds, so that the modes compare
+        # on the same settings
+        sp.set_tuning(**{k: tuning[k] for k in ("warp_cross_min_ready", "bound_min_cand", "tail_max_ready",
+                                                 "tail_max_cand")})
     sp.load(pos_d, ids_d)
     sp.run()
     torch.cuda.synchronize()
@@ -874,6 +887,8 @@ def main():
     ap.add_argument("--delta200-only", dest="ndelta", action="store_false",
                     help="Delta = 200 and 60 bins only (default: 200, 500 and 178 in one pass, 48 bins)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default scheduling thresholds instead of psod_autotune in the warm-up")
     ap.add_argument("--props", action="store_true",
                     help="time the halo-properties stage (psod_halo_properties) on the SOD table; one GPU")
     ap.add_argument("--fof", action="store_true",

@@ -306,6 +306,31 @@ int psod_learn_set_margin(psod_ctx *ctx, float margin);
 int psod_learn_forward(psod_ctx *ctx, int64_t n, const float *x, float *y);
 int psod_learn_gradient(psod_ctx *ctx, int64_t n, const float *x, const float *t, float *grad, float *loss);
 
+/* ---- Scheduling thresholds and their autotuner ---------------------------
+ * psod_spherover's size classes and round handling depend on four
+ * thresholds.  None of them changes the halo table (each only chooses which
+ * kernel or pass does a piece of work); they change its speed.  Defaults
+ * are the values measured best on the 1024^3 workload: 2048, 4096, 256,
+ * 1024.  No counterpart in the reference. */
+typedef struct psod_tuning {
+  int32_t warp_cross_min_ready; /* rounds with at least this many ready seeds cross small balls a warp per seed */
+  int32_t bound_min_cand;       /* seeds with at least this many candidates get the refinement bound pass */
+  int32_t tail_max_ready;       /* the device tail loop takes rounds of at most this many ready seeds (0: never) */
+  int32_t tail_max_cand;        /* ... whose seeds have at most this many candidates (<= bound_min_cand) */
+} psod_tuning;
+
+int psod_get_tuning(psod_ctx *ctx, psod_tuning *t);
+/* PSOD_ERR_ARG unless warp_cross_min_ready >= 1, 256 <= bound_min_cand,
+ * tail_max_ready >= 0 and 1 <= tail_max_cand <= bound_min_cand. */
+int psod_set_tuning(psod_ctx *ctx, const psod_tuning *t);
+/* Picks the thresholds by timing psod_spherover on the loaded particles
+ * (after psod_tri_cic): starting from the current values, one threshold at a
+ * time over a few candidates each (coordinate descent, a change kept when it
+ * is at least 0.5 % faster), about a dozen spherover runs.  Leaves the best
+ * thresholds set and the halo table of its last run (the same table as any
+ * run).  chosen / ms_best / runs may be NULL. */
+int psod_autotune(psod_ctx *ctx, psod_tuning *chosen, double *ms_best, int32_t *runs);
+
 /* ---- Friends-of-friends (pFoF on one rank) -----------------------------
  * The halo finder that writes the catalogue and cube files the SOD stage
  * reads: pFoF's fofpara (Pfof/trunk/pfof_snap/src/modfofpara.f90:31-296)

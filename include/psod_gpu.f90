@@ -60,6 +60,11 @@ module psod_gpu
      integer(c_int64_t) :: seed
   end type psod_train_params
 
+  ! scheduling thresholds of psod_spherover (no effect on any result)
+  type, bind(C) :: psod_tuning
+     integer(c_int32_t) :: warp_cross_min_ready, bound_min_cand, tail_max_ready, tail_max_cand
+  end type psod_tuning
+
   ! friends-of-friends (pFoF fofpara on one rank): param%percolation_length,
   ! nres (0: cube root of the particle count), param%Mmin
   type, bind(C) :: psod_fof_params
@@ -222,6 +227,18 @@ module psod_gpu
        import :: c_int, c_ptr, psod_fof_table
        type(c_ptr), value :: ctx
        type(psod_fof_table), intent(in) :: t
+     end function
+     integer(c_int) function psod_autotune(ctx, chosen, ms_best, runs) bind(C, name="psod_autotune")
+       import :: c_int, c_ptr, c_double, c_int32_t, psod_tuning
+       type(c_ptr), value :: ctx
+       type(psod_tuning), intent(out) :: chosen
+       real(c_double), intent(out) :: ms_best
+       integer(c_int32_t), intent(out) :: runs
+     end function
+     integer(c_int) function psod_set_tuning(ctx, t) bind(C, name="psod_set_tuning")
+       import :: c_int, c_ptr, psod_tuning
+       type(c_ptr), value :: ctx
+       type(psod_tuning), intent(in) :: t
      end function
      integer(c_int) function psod_halo_properties(ctx, p, stats) bind(C, name="psod_halo_properties")
        import :: c_int, c_ptr, psod_props_params, psod_props_stats

@@ -108,6 +108,14 @@ class RunStats(C.Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class Tuning(C.Structure):
+    _fields_ = [("warp_cross_min_ready", C.c_int32), ("bound_min_cand", C.c_int32), ("tail_max_ready", C.c_int32),
+                ("tail_max_cand", C.c_int32)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class FofParams(C.Structure):
     _fields_ = [("percolation", C.c_float), ("reserved", C.c_int32), ("nres", C.c_int64), ("mmin", C.c_int64)]
 
@@ -225,6 +233,9 @@ EXPORTS = [
     "psod_fof_get_halos",
     "psod_halo_properties",
     "psod_props_get",
+    "psod_get_tuning",
+    "psod_set_tuning",
+    "psod_autotune",
 ]
 
 LEARN_FEATURES = 10
@@ -286,6 +297,9 @@ def load(build_if_missing: bool = True):
     L.psod_fof.argtypes = [vp, P(FofParams), P(FofStats)]
     L.psod_fof_halo_count.argtypes = [vp, P(C.c_int64), P(C.c_int64)]
     L.psod_fof_get_halos.argtypes = [vp, P(FofTable)]
+    L.psod_get_tuning.argtypes = [vp, P(Tuning)]
+    L.psod_set_tuning.argtypes = [vp, P(Tuning)]
+    L.psod_autotune.argtypes = [vp, P(Tuning), P(C.c_double), P(C.c_int32)]
     L.psod_halo_properties.argtypes = [vp, P(PropsParams), P(PropsStats)]
     L.psod_props_get.argtypes = [vp, P(PropsTable)]
     L.psod_last_error.argtypes = [vp]

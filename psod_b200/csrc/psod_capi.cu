@@ -371,6 +371,77 @@ int psod_get_halos(psod_ctx *c, const psod_halo_table *t) {
   return PSOD_OK;
 }
 
+int psod_get_tuning(psod_ctx *c, psod_tuning *t) {
+  if (!c || !t) return PSOD_ERR_ARG;
+  *t = c->tune;
+  return PSOD_OK;
+}
+
+int psod_set_tuning(psod_ctx *c, const psod_tuning *t) {
+  if (!c || !t) return PSOD_ERR_ARG;
+  if (t->warp_cross_min_ready < 1 || t->bound_min_cand < 256 || t->tail_max_ready < 0 || t->tail_max_cand < 1 ||
+      t->tail_max_cand > t->bound_min_cand)
+    return set_err(c, PSOD_ERR_ARG,
+                   "psod_set_tuning: warp_cross_min_ready >= 1, bound_min_cand >= 256, tail_max_ready >= 0, "
+                   "1 <= tail_max_cand <= bound_min_cand");
+  c->tune = *t;
+  return PSOD_OK;
+}
+
+int psod_autotune(psod_ctx *c, psod_tuning *chosen, double *ms_best, int32_t *runs) {
+  if (!c) return PSOD_ERR_ARG;
+  if (!c->seeds_done) return set_err(c, PSOD_ERR_STATE, "psod_autotune: call psod_tri_cic first");
+  int nrun = 0;
+  auto time_run = [&](double *ms) {
+    psod_run_stats st{};
+    const int s = psod_spherover(c, &st);
+    nrun++;
+    *ms = st.ms_total;
+    return s;
+  };
+  double best_ms = 0.0;
+  int st = time_run(&best_ms);
+  if (st) return st;
+  psod_tuning best = c->tune;
+  // candidates per threshold; 1 << 30 turns the warp pass off
+  const int32_t warp_c[] = {512, 1024, 2048, 4096, 1 << 30};
+  const int32_t bound_c[] = {2048, 4096, 8192};
+  const int32_t tail_c[] = {0, 128, 256, 512, 1024};
+  const int32_t tcand_c[] = {256, 1024, 2048};
+  auto sweep = [&](int32_t psod_tuning::*field, const int32_t *vals, int nv) -> int {
+    for (int k = 0; k < nv; k++) {
+      psod_tuning t = best;
+      t.*field = vals[k];
+      if (t.*field == best.*field || t.tail_max_cand > t.bound_min_cand) continue;
+      c->tune = t;
+      double ms = 0.0;
+      const int s = time_run(&ms);
+      if (s) {
+        c->tune = best;
+        return s;
+      }
+      if (ms < best_ms * 0.995) {
+        best_ms = ms;
+        best = t;
+      }
+    }
+    c->tune = best;
+    return PSOD_OK;
+  };
+  if ((st = sweep(&psod_tuning::warp_cross_min_ready, warp_c, 5))) return st;
+  if ((st = sweep(&psod_tuning::bound_min_cand, bound_c, 3))) return st;
+  if ((st = sweep(&psod_tuning::tail_max_ready, tail_c, 5))) return st;
+  if ((st = sweep(&psod_tuning::tail_max_cand, tcand_c, 3))) return st;
+  // the table of the last run came from the last candidate tried: run once
+  // more with the chosen thresholds so that every counter matches them
+  double last = 0.0;
+  if ((st = time_run(&last))) return st;
+  if (chosen) *chosen = best;
+  if (ms_best) *ms_best = best_ms;
+  if (runs) *runs = nrun;
+  return PSOD_OK;
+}
+
 const char *psod_last_error(const psod_ctx *c) { return c ? c->err.c_str() : "null context"; }
 
 }  // extern "C"

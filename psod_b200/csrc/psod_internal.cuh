@@ -184,6 +184,10 @@ struct psod_ctx {
   // learned radius bracket (model, optimiser state, collected samples)
   psod::LearnState *learn = nullptr;
 
+  // scheduling thresholds of psod_spherover (psod_set_tuning / psod_autotune);
+  // none of them changes a result
+  psod_tuning tune{2048, 4096, 256, 1024};
+
   // friends-of-friends catalogue (psod_fof; arrays in the SLOT_F_* slots)
   bool fof_done = false;
   long long fof_nhalo = 0, fof_nmember = 0;

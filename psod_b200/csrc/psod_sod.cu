@@ -47,7 +47,6 @@ enum { ERR_NONE = 0 };
 // Seeds with fewer refinement candidates than this are neither bounded nor
 // pruned: their pair work is small and the bound pass would cost as much as
 // it saves.
-constexpr unsigned BOUND_MIN_CAND = 4096;
 
 struct SodBufs {
   float4 *cube;
@@ -85,7 +84,8 @@ struct SodBufs {
   double *cand_s;       // approximate refinement sum
   unsigned *cand_used;  // allocator
   unsigned *work;       // [4] work-stealing counters: prep, refine, select, cross
-  unsigned *nbig;       // seeds of this round with BOUND_MIN_CAND candidates or more
+  unsigned *nbig;       // seeds of this round with bound_min candidates or more
+  unsigned bound_min;   // seeds with this many candidates or more get the bound pass
   unsigned *maxcand;    // largest candidate count of a seed this round (or null)
   unsigned max_cand;    // seeds with more candidates wait (device tail loop), else ~0u
   unsigned *deferred;   // set when a seed waited for that reason
@@ -963,7 +963,7 @@ __device__ __forceinline__ void prep_seed(const SodConst &K, const SodBufs &B, S
       B.st_coff[slot] = s_base;
       B.st_cn[slot] = tot;
       B.st_active[slot] = 1;
-      if (tot >= BOUND_MIN_CAND) atomicAdd(B.nbig, 1u);
+      if (tot >= B.bound_min) atomicAdd(B.nbig, 1u);
       B.st_centre[slot] = g.sp;  // no candidate: the seed stays the centre
       atomicAdd(B.nprocessed, 1ull);
     }
@@ -1448,7 +1448,7 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
     const unsigned chunk = rem / nch, nchunk = rem % nch;
     const unsigned slot = ci / 27, o = ci % 27;
     const unsigned grp = B.group_pref[ci] + chunk;
-    const bool bounded = B.bound_on && B.st_cn[slot] >= BOUND_MIN_CAND;
+    const bool bounded = B.bound_on && B.st_cn[slot] >= B.bound_min;
     if (BOUND && !bounded) continue;
     if (!BOUND && lane == 0) s_count[w][3]++;
     const SeedGeo g = seed_geo(K, B, B.ready[slot]);
@@ -2321,7 +2321,6 @@ __device__ __forceinline__ void cross_seed(const SodConst &K, const SodBufs &B, 
 // (st_big), which then processes it from scratch in the same round.
 // ---------------------------------------------------------------------------
 constexpr int WCAP = 512;  // records per warp slice
-constexpr unsigned WARP_CROSS_MIN_READY = 2048;  // rounds with fewer seeds use the CTA kernel only
 struct WSlice {
   unsigned long long key[WCAP];
   unsigned idx[WCAP];
@@ -2679,7 +2678,7 @@ __global__ void __launch_bounds__(TPB) k_cross(SodConst K, SodBufs B) {
 // deflated by 1e-3, is at most the maximum.  Warp per seed.
 __global__ void k_seed_lower(SodConst K, SodBufs B) {
   const unsigned slot = (unsigned)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
-  if (slot >= min(*B.nready, B.cap_ready) || !B.st_active[slot] || B.st_cn[slot] < BOUND_MIN_CAND) return;
+  if (slot >= min(*B.nready, B.cap_ready) || !B.st_active[slot] || B.st_cn[slot] < B.bound_min) return;
   const SeedGeo g = seed_geo(K, B, B.ready[slot]);
   unsigned long long sq = 0;
   double sf = 0.0;
@@ -2697,7 +2696,7 @@ __global__ void k_top_group(SodConst K, SodBufs B) {
   if (slot >= min(*B.nready, B.cap_ready)) return;
   float bu = -1.f;
   unsigned best = 0xffffffffu;
-  if (B.bound_on && B.st_cn[slot] >= BOUND_MIN_CAND) {
+  if (B.bound_on && B.st_cn[slot] >= B.bound_min) {
     const unsigned g0 = B.group_pref[slot * 27u] * NSUB, g1 = B.group_pref[slot * 27u + 27u] * NSUB;
     for (unsigned si = g0 + (unsigned)lane; si < g1; si += 32u) {
       const float u = B.g_u[si];
@@ -2760,7 +2759,7 @@ __global__ void k_survivors(SodConst K, SodBufs B) {
   const int lane = threadIdx.x & 31;
   if (ci >= B.nitems_cells) return;
   const unsigned slot = ci / 27u, cnt = B.cell_cnt[ci], off = B.cell_off[ci], gp = B.group_pref[ci];
-  const bool bounded = B.bound_on && B.st_cn[slot] >= BOUND_MIN_CAND;
+  const bool bounded = B.bound_on && B.st_cn[slot] >= B.bound_min;
   const float lmax = __uint_as_float(B.s_lmax[slot]);
   const unsigned top = B.s_top[slot];
   unsigned n2 = 0, gone = 0;
@@ -3563,12 +3562,10 @@ enum {
 };
 
 // Rounds go to the device tail loop once the last host round had no seed
-// for the bound pass, no seed with more than TAIL_MAX_CAND candidates, at
-// most TAIL_MAX_READY ready seeds and few enough active blocks for the
-// direct readiness test; after a launch that ended on a larger seed, the
-// host runs at least TAIL_REST rounds before the next launch.
-constexpr unsigned TAIL_MAX_CAND = 1024;
-constexpr unsigned TAIL_MAX_READY = 256;
+// for the bound pass, no seed with more than tail_max_cand candidates, at
+// most tail_max_ready ready seeds (psod_tuning) and few enough active blocks
+// for the direct readiness test; after a launch that ended on a larger
+// seed, the host runs at least TAIL_REST rounds before the next launch.
 constexpr int TAIL_REST = 8;
 
 struct PhaseTimer {
@@ -3805,6 +3802,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.cand_used = cand_used;
   B.work = work;
   B.nbig = ctrs + 12;
+  B.bound_min = (unsigned)c->tune.bound_min_cand;
   B.maxcand = ctrs + 13;
   B.max_cand = ~0u;
   B.deferred = ctrs + 14;
@@ -3882,7 +3880,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   // the preselect back to back; the host then reads the round's counters
   // (its only synchronisation per round) and launches the refinement,
   // select and crossing kernels sized by them, the bound pipeline only when
-  // some seed has BOUND_MIN_CAND candidates.  Phase timers of the refinement
+  // some seed has bound_min_cand candidates.  Phase timers of the refinement
   // onwards are read one round later, when their events have completed.
   const long long window = (long long)std::min(2 * rb + 1, nb);
   const long long direct_cost_per_block = window * window * window, filter_cost = 3 * nblocks * window;
@@ -3998,7 +3996,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     // a round lasts as long as its slowest seed, and a CTA handles one seed
     // with eight warps.
     SodBufs Bc = B;
-    if (!(B.st_big && nready >= WARP_CROSS_MIN_READY)) Bc.st_big = nullptr;
+    if (!(B.st_big && nready >= (unsigned)c->tune.warp_cross_min_ready)) Bc.st_big = nullptr;
     if (Bc.st_big) {
       k_cross_warp<<<nblk((long long)nready * 32, 256), 256, wsmem, c->stream>>>(K, Bc);
       kernels++;
@@ -4030,12 +4028,13 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     seed_launches += 4;
     kernels += 4;
     rest++;
-    if (tail_grid > 0 && nbig == 0 && maxcand <= TAIL_MAX_CAND && nready <= TAIL_MAX_READY && rest >= TAIL_REST &&
+    if (tail_grid > 0 && nbig == 0 && maxcand <= (unsigned)c->tune.tail_max_cand &&
+        nready <= (unsigned)c->tune.tail_max_ready && rest >= TAIL_REST &&
         n_active > 0 && (long long)n_active * direct_cost_per_block <= filter_cost) {
       // the following rounds on the device, until a larger seed or the end
       k_tail_init<<<1, 1, 0, c->stream>>>(tail, n_active);
       SodBufs Bt = B;
-      Bt.max_cand = TAIL_MAX_CAND;
+      Bt.max_cand = (unsigned)c->tune.tail_max_cand;
       Bt.st_big = nullptr;
       Bt.touch = u64s + 19;  // the tail's crossings counted apart from k_cross
       Bt.kept_members = u64s + 20;

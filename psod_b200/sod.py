@@ -274,6 +274,23 @@ class SphericalOverdensity:
         return t
 
 
+    # ---- scheduling thresholds (no effect on any result) ----
+    def get_tuning(self) -> dict:
+        t = capi.Tuning()
+        self._check(self.lib.psod_get_tuning(self.ctx, C.byref(t)))
+        return t.as_dict()
+
+    def set_tuning(self, **kw):
+        t = capi.Tuning(**{**self.get_tuning(), **kw})
+        self._check(self.lib.psod_set_tuning(self.ctx, C.byref(t)))
+
+    def autotune(self) -> dict:
+        """Time psod_spherover over a few threshold candidates on the loaded
+        particles (after tri_cic) and keep the fastest (psod_autotune)."""
+        t, ms, n = capi.Tuning(), C.c_double(0.0), C.c_int32(0)
+        self._check(self.lib.psod_autotune(self.ctx, C.byref(t), C.byref(ms), C.byref(n)))
+        return dict(t.as_dict(), ms_best=ms.value, runs=n.value)
+
     # ---- friends-of-friends (pFoF fofpara + merge + modhalo observables) ----
     def fof(self, percolation: float = 0.2, mmin: int = 20, nres: int = 0) -> dict:
         """pFoF's halo finder on the loaded particles (one rank, periodic

@@ -21,6 +21,7 @@ PAIRS = [
     ("psod_halo_table", capi.HaloTable, "psod.h"),
     ("psod_run_stats", capi.RunStats, "psod.h"),
     ("psod_train_params", capi.TrainParams, "psod.h"),
+    ("psod_tuning", capi.Tuning, "psod.h"),
     ("psod_fof_params", capi.FofParams, "psod.h"),
     ("psod_fof_stats", capi.FofStats, "psod.h"),
     ("psod_fof_table", capi.FofTable, "psod.h"),
