@@ -247,7 +247,13 @@ def run_ours(args):
     params = dict(npu=HEAVY["npu"] if args.heavy else npu_for(nx), mode=args.mode_id, **thresholds)
     sod = SphericalOverdensity(nx, device=dev, **params)
     if model is not None:
+        sod.learn_set_features("fof")
         sod.learn_set_model(model)
+        # the FoF catalogue the SOD stage starts from (the previous stage of
+        # the reference's pipeline; untimed), then its working arrays freed
+        sod.load(pos_d, ids_d)
+        sod.fof(percolation=0.2, mmin=20)
+        sod.fof_release()
     # L2 flush buffer (used when the inputs are smaller than L2)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{dev}")
     inputs_bytes = n * (12 + 8)
@@ -399,6 +405,7 @@ def run_ours(args):
     }
     if bracket is not None:
         bracket.update(hit_rate=round(s["bracket_hits"] / max(1, s["bracket_seeds"]), 4),
+                       fallback_rate=round(1.0 - s["bracket_hits"] / max(1, s["bracket_seeds"]), 4),
                        seeds=int(s["bracket_seeds"]), cross_balls=int(s["cross_balls"]),
                        cross_records=int(s["cross_records"]), ms_learn=round(s["ms_learn"], 2))
         line["bracket"] = bracket
@@ -511,10 +518,14 @@ def train_bracket(args, dev, thresholds):
     nbox = 32
     t0 = time.perf_counter()
     with SphericalOverdensity(128, device=dev, mode=1, **thresholds) as s:
+        # the FoF features of the learned-seed configuration: each box's
+        # FoF catalogue (b = 0.2, 20 particles) before its SOD run
+        s.learn_set_features("fof")
         s.learn_collect(1 << 21)
         for i in range(nbox):
             b = synth.make_box(128, nmax_halo=20000, seed=args.seed + 1000 + i, device=f"cuda:{dev}")
             s.load(b.pos, b.ids)
+            s.fof(percolation=0.2, mmin=20)
             s.run()
             del b
         x, _ = s.learn_samples()
@@ -523,6 +534,9 @@ def train_bracket(args, dev, thresholds):
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
     return model, {"trained_on": f"{nbox} boxes of 128^3 (halo N in [20, 2e4]), batched-mode samples",
+                   "features": "FoF group of the seed: log N_FoF, inertia axis ratios, log peak overdensity, "
+                               "peak - centre-of-mass offset, R_FoF, RMS radius; targets log(R_stop/R_FoF), "
+                               "centre offset",
                    "samples": int(x.shape[0]), "epochs": 20, "batch": 4096, "lr": 1e-3,
                    "loss_first_last": [round(float(loss[0]), 4), round(float(loss[-1]), 4)],
                    "train_s": round(time.perf_counter() - t0, 2)}

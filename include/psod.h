@@ -297,6 +297,26 @@ typedef struct psod_train_params {
   uint64_t seed;   /* weight initialisation and batch order */
 } psod_train_params;
 
+/* Feature sets of the learned bracket (both: PSOD_LEARN_FEATURES inputs):
+ *   PSOD_LEARN_FEATURES_SEED (default): seed-local quantities (log rho of
+ *     the seed and the centre, log alive records in cubes of half-width
+ *     0..4 cells, log refinement sum, centre offset, log candidates);
+ *     targets log stop radius (cells) and log N_delta; first ball
+ *     exp(y0) * margin.
+ *   PSOD_LEARN_FEATURES_FOF: from the FoF group of the seed particle, as
+ *     the learned-seed configuration of the task names them: log N_FoF, the
+ *     three inertia axis ratios (b/a, c/a, c/b), log rho(seed) (the CIC peak
+ *     overdensity), seed - FoF centre of mass (3, cells), R_FoF and the RMS
+ *     radius (cells); targets log(R_stop / R_FoF) and the centre offset
+ *     |centre - seed| (cells); first ball exp(y0) * margin * R_FoF.  Needs
+ *     psod_fof on the loaded particles before psod_spherover (else
+ *     PSOD_ERR_STATE); seeds outside the FoF halos get no prediction.
+ * A model is tied to the set it was trained with; the halo table never
+ * depends on either. */
+#define PSOD_LEARN_FEATURES_SEED 0
+#define PSOD_LEARN_FEATURES_FOF 1
+int psod_learn_set_features(psod_ctx *ctx, int32_t set);
+
 int psod_learn_collect(psod_ctx *ctx, int64_t capacity);
 int psod_learn_samples(psod_ctx *ctx, int64_t *n, float *x_out, float *t_out);
 int psod_learn_train(psod_ctx *ctx, const psod_train_params *tp, float *loss_per_epoch);
@@ -400,6 +420,10 @@ typedef struct psod_fof_table {
 } psod_fof_table;
 
 int psod_fof(psod_ctx *ctx, const psod_fof_params *p, psod_fof_stats *stats);
+/* Frees psod_fof's working arrays (about 26 bytes per particle); the
+ * catalogue and the per-particle group codes the learned features read stay.
+ * The next psod_fof allocates them again. */
+int psod_fof_release(psod_ctx *ctx);
 int psod_fof_halo_count(psod_ctx *ctx, int64_t *nhalo, int64_t *nmember);
 int psod_fof_get_halos(psod_ctx *ctx, const psod_fof_table *t);
 

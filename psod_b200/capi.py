@@ -28,6 +28,9 @@ MODE_PLAIN = 0
 MODE_BATCHED = 1
 MODE_LEARNED = 2
 
+LEARN_FEATURES_SEED = 0
+LEARN_FEATURES_FOF = 1
+
 
 class Params(C.Structure):
     _fields_ = [
@@ -233,6 +236,8 @@ EXPORTS = [
     "psod_fof_get_halos",
     "psod_halo_properties",
     "psod_props_get",
+    "psod_learn_set_features",
+    "psod_fof_release",
     "psod_get_tuning",
     "psod_set_tuning",
     "psod_autotune",
@@ -297,6 +302,8 @@ def load(build_if_missing: bool = True):
     L.psod_fof.argtypes = [vp, P(FofParams), P(FofStats)]
     L.psod_fof_halo_count.argtypes = [vp, P(C.c_int64), P(C.c_int64)]
     L.psod_fof_get_halos.argtypes = [vp, P(FofTable)]
+    L.psod_learn_set_features.argtypes = [vp, C.c_int32]
+    L.psod_fof_release.argtypes = [vp]
     L.psod_get_tuning.argtypes = [vp, P(Tuning)]
     L.psod_set_tuning.argtypes = [vp, P(Tuning)]
     L.psod_autotune.argtypes = [vp, P(Tuning), P(C.c_double), P(C.c_int32)]

@@ -371,6 +371,14 @@ int psod_get_halos(psod_ctx *c, const psod_halo_table *t) {
   return PSOD_OK;
 }
 
+int psod_learn_set_features(psod_ctx *c, int32_t set) {
+  if (!c) return PSOD_ERR_ARG;
+  if (set != PSOD_LEARN_FEATURES_SEED && set != PSOD_LEARN_FEATURES_FOF)
+    return set_err(c, PSOD_ERR_ARG, "psod_learn_set_features: PSOD_LEARN_FEATURES_SEED or PSOD_LEARN_FEATURES_FOF");
+  c->learn_features = set;
+  return PSOD_OK;
+}
+
 int psod_get_tuning(psod_ctx *c, psod_tuning *t) {
   if (!c || !t) return PSOD_ERR_ARG;
   *t = c->tune;

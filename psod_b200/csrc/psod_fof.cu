@@ -624,7 +624,7 @@ __global__ void k_fof_offsets(const unsigned *excl, long long nh, long long nm, 
 template <int NT>
 __device__ __forceinline__ void halo_observables(const unsigned *mem, long long b, long long e, const float4 *cube,
                                                  const unsigned *inv, const float *vel, double *com, double *hvel,
-                                                 double *rad, double *red) {
+                                                 double *rad, double *red, float4 *feat) {
   const int t = threadIdx.x % NT;
   const float4 first = cube[inv[mem[b]]];
   const double f0 = fof_wrap1(first.x), f1 = fof_wrap1(first.y), f2 = fof_wrap1(first.z);
@@ -681,10 +681,23 @@ __device__ __forceinline__ void halo_observables(const unsigned *mem, long long 
   else __syncwarp();
   const double c0 = s_c[slot][0], c1 = s_c[slot][1], c2 = s_c[slot][2];
   double rmax2 = 0.0;
+  // shape sums for the learned bracket's features: squared distances and
+  // the inertia tensor of the minimum-image offsets from the centre
+  double sh[7] = {0, 0, 0, 0, 0, 0, 0};
   for (long long k = b + t; k < e; k += NT) {
     const float4 v = cube[inv[mem[k]]];
     double d0 = dsub((double)fof_wrap1(v.x), c0), d1 = dsub((double)fof_wrap1(v.y), c1),
            d2 = dsub((double)fof_wrap1(v.z), c2);
+    const double s0 = d0 > 0.5 ? d0 - 1.0 : (d0 < -0.5 ? d0 + 1.0 : d0);
+    const double s1 = d1 > 0.5 ? d1 - 1.0 : (d1 < -0.5 ? d1 + 1.0 : d1);
+    const double s2 = d2 > 0.5 ? d2 - 1.0 : (d2 < -0.5 ? d2 + 1.0 : d2);
+    sh[0] += s0 * s0 + s1 * s1 + s2 * s2;
+    sh[1] += s0 * s0;
+    sh[2] += s0 * s1;
+    sh[3] += s0 * s2;
+    sh[4] += s1 * s1;
+    sh[5] += s1 * s2;
+    sh[6] += s2 * s2;
     if (fabs(d0) > 0.5) d0 = dsub(1.0, fabs(d0));
     if (fabs(d1) > 0.5) d1 = dsub(1.0, fabs(d1));
     if (fabs(d2) > 0.5) d2 = dsub(1.0, fabs(d2));
@@ -692,27 +705,51 @@ __device__ __forceinline__ void halo_observables(const unsigned *mem, long long 
     rmax2 = fmax(rmax2, q);
   }
   for (int o = 16; o > 0; o >>= 1) rmax2 = fmax(rmax2, __shfl_down_sync(0xffffffffu, rmax2, o));
+#pragma unroll
+  for (int a = 0; a < 7; a++)
+    for (int o = 16; o > 0; o >>= 1) sh[a] += __shfl_down_sync(0xffffffffu, sh[a], o);
   if (NT > 32) {
     const int w = t >> 5, lane = t & 31;
-    if (lane == 0) red[w] = rmax2;
+    if (lane == 0) {
+      red[w] = rmax2;
+      for (int a = 0; a < 7; a++) red[NT / 32 + 7 * w + a] = sh[a];
+    }
     __syncthreads();
-    if (t == 0)
+    if (t == 0) {
       for (int q = 1; q < NT / 32; q++) rmax2 = fmax(rmax2, red[q]);
+      for (int a = 0; a < 7; a++) {
+        double acc = red[NT / 32 + a];
+        for (int q = 1; q < NT / 32; q++) acc += red[NT / 32 + 7 * q + a];
+        sh[a] = acc;
+      }
+    }
     __syncthreads();
   }
-  if (t == 0) *rad = dsqrt(rmax2);
+  if (t == 0) {
+    *rad = dsqrt(rmax2);
+    const double n = (double)(e - b);
+    double A[3][3] = {{sh[1] / n, sh[2] / n, sh[3] / n}, {sh[2] / n, sh[4] / n, sh[5] / n},
+                      {sh[3] / n, sh[5] / n, sh[6] / n}};
+    double dv[3], vv[3][3];
+    jacobi3(A, dv, vv);
+    eigsort3(dv, vv);
+    const double ea = sqrt(fmax(dv[0], 0.0)), eb = sqrt(fmax(dv[1], 0.0)), ec = sqrt(fmax(dv[2], 0.0));
+    *feat = make_float4((float)sqrt(sh[0] / n), ea > 0.0 ? (float)(eb / ea) : 1.f, ea > 0.0 ? (float)(ec / ea) : 1.f,
+                        eb > 0.0 ? (float)(ec / eb) : 1.f);
+  }
 }
 
 __global__ void __launch_bounds__(FOF_TPB) k_fof_observables_warp(const long long *off, const long long *hmass,
                                                                   long long nh, const unsigned *mem,
                                                                   const float4 *cube, const unsigned *inv,
                                                                   const float *vel, double *com, double *hvel,
-                                                                  double *rad) {
+                                                                  double *rad, float4 *feat) {
   const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nwarp = ((long long)gridDim.x * blockDim.x) >> 5;
   for (long long q = warp; q < nh; q += nwarp) {
     if (hmass[q] > FOF_WARP_HALO) continue;  // warp-uniform
-    halo_observables<32>(mem, off[q], off[q + 1], cube, inv, vel, com + 3 * q, hvel + 3 * q, rad + q, nullptr);
+    halo_observables<32>(mem, off[q], off[q + 1], cube, inv, vel, com + 3 * q, hvel + 3 * q, rad + q, nullptr,
+                         feat + q);
   }
 }
 
@@ -720,12 +757,23 @@ __global__ void __launch_bounds__(FOF_TPB) k_fof_observables_cta(const long long
                                                                  long long nh, const unsigned *mem,
                                                                  const float4 *cube, const unsigned *inv,
                                                                  const float *vel, double *com, double *hvel,
-                                                                 double *rad) {
-  __shared__ double red[6 * (FOF_TPB / 32)];
+                                                                 double *rad, float4 *feat) {
+  __shared__ double red[6 * (FOF_TPB / 32) + 7 * (FOF_TPB / 32)];
   for (long long q = blockIdx.x; q < nh; q += gridDim.x) {
     if (hmass[q] <= FOF_WARP_HALO) continue;  // block-uniform
-    halo_observables<FOF_TPB>(mem, off[q], off[q + 1], cube, inv, vel, com + 3 * q, hvel + 3 * q, rad + q, red);
+    halo_observables<FOF_TPB>(mem, off[q], off[q + 1], cube, inv, vel, com + 3 * q, hvel + 3 * q, rad + q, red,
+                              feat + q);
   }
+}
+
+// per input particle: its halo's rank, or (top bit) the size of its group
+// when that group is smaller than mmin (the learned bracket's features)
+__global__ void k_fof_codes(const unsigned *finv, const unsigned *par, const unsigned *size, const unsigned *rank,
+                            long long n, unsigned mmin, unsigned *code) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned r = par[finv[i]], sz = size[r];
+  code[i] = sz >= mmin ? rank[r] : (0x80000000u | sz);
 }
 
 __global__ void k_fof_member_ids(const unsigned *mem, long long nm, const long long *ids, long long *out_idx,
@@ -964,15 +1012,21 @@ int psod_fof(psod_ctx *c, const psod_fof_params *p, psod_fof_stats *stats) {
   PSOD_CUDA(c, cudaGetLastError());
   S.ms_label = tm.stop();
 
-  // 4. observables
+  // 4. observables, and each particle's group code
+  float4 *hfeat = nullptr;
+  unsigned *pcode = nullptr;
+  if ((st = scratch(c, SLOT_F_FEAT, (size_t)nh + 1, &hfeat))) return st;
+  if ((st = scratch(c, SLOT_F_CODE, (size_t)n, &pcode))) return st;
   if (nh > 0) {
     const float *vel = c->d_vel;
     k_fof_observables_warp<<<148 * 8, FOF_TPB, 0, c->stream>>>(hoff, hmass, nh, mem, c->d_cube, c->d_inv, vel, hcom,
-                                                               hvel, hrad);
+                                                               hvel, hrad, hfeat);
     k_fof_observables_cta<<<148 * 2, FOF_TPB, 0, c->stream>>>(hoff, hmass, nh, mem, c->d_cube, c->d_inv, vel, hcom,
-                                                              hvel, hrad);
+                                                              hvel, hrad, hfeat);
     PSOD_CUDA(c, cudaGetLastError());
   }
+  k_fof_codes<<<grid_for(n), FOF_TPB, 0, c->stream>>>(finv, par, aux1, aux2, n, (unsigned)p->mmin, pcode);
+  PSOD_CUDA(c, cudaGetLastError());
   S.ms_props = tm.stop();
   unsigned long long hc[2] = {0, 0};
   PSOD_CUDA(c, cudaMemcpyAsync(hc, ctr, sizeof(hc), cudaMemcpyDeviceToHost, c->stream));
@@ -984,10 +1038,21 @@ int psod_fof(psod_ctx *c, const psod_fof_params *p, psod_fof_stats *stats) {
   S.nmember = nm;
   c->fof_nhalo = nh;
   c->fof_nmember = nm;
+  c->fof_n = n;
   c->fof_done = true;
   // the working arrays stay with the context (repeated calls allocate
   // nothing), like the other stages' slots
   if (stats) *stats = S;
+  return PSOD_OK;
+}
+
+int psod_fof_release(psod_ctx *c) {
+  if (!c) return PSOD_ERR_ARG;
+  cudaSetDevice(c->device);
+  for (int s : {SLOT_FOF_KEY, SLOT_FOF_SKEY, SLOT_FOF_PERM, SLOT_FOF_PAR, SLOT_FOF_INV, SLOT_FOF_AUX1, SLOT_FOF_AUX2,
+                SLOT_FOF_HEADS, SLOT_FOF_BIGRUN, SLOT_FOF_HPOS, SLOT_FOF_HKEY, SLOT_FOF_HROOT, SLOT_FOF_MKEY,
+                SLOT_FOF_MCOUNT})
+    free_scratch_slot(c, s);
   return PSOD_OK;
 }
 

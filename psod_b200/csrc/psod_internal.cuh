@@ -191,6 +191,8 @@ struct psod_ctx {
   // friends-of-friends catalogue (psod_fof; arrays in the SLOT_F_* slots)
   bool fof_done = false;
   long long fof_nhalo = 0, fof_nmember = 0;
+  long long fof_n = 0;  // particles the catalogue was built on
+  int learn_features = 0;  // PSOD_LEARN_FEATURES_SEED or _FOF
 
   // halo properties (psod_halo_properties; arrays in the SLOT_PO_* slots)
   bool props_done = false;
@@ -333,6 +335,8 @@ enum : int {
   SLOT_F_VEL,
   SLOT_F_RAD,
   SLOT_F_MEM,
+  SLOT_F_FEAT,          // fof: per halo RMS radius and inertia axis ratios (float4)
+  SLOT_F_CODE,          // fof: per input particle, its halo rank or (top bit) group size
   SLOT_PR_POS,          // props: member positions after the periodic shifts
   SLOT_PR_EPI,          // props: per-member potential sums
   SLOT_PR_WORK,         // props: per-halo sums
@@ -344,6 +348,102 @@ enum : int {
   SLOT_PO_F32,
   SLOT_PO_COS
 };
+
+// Eigen decomposition of a symmetric 3x3 matrix by the cyclic Jacobi
+// method with thresholds (Rutishauser's, as published in Numerical Recipes'
+// jacobi; haloanalyzer's diag, modfunctions.f90:840-933, follows it): d gets
+// the eigenvalues, v the eigenvectors as columns.  eigsort3 orders them by
+// descending eigenvalue, a later equal value moving first (eigsrt :812-837).
+__device__ inline void jacobi3(double a[3][3], double d[3], double v[3][3]) {
+  double bb[3], z[3];
+  for (int i = 0; i < 3; i++) {
+    for (int j = 0; j < 3; j++) v[i][j] = 0.0;
+    v[i][i] = 1.0;
+    bb[i] = d[i] = a[i][i];
+    z[i] = 0.0;
+  }
+  for (int sweep = 1; sweep <= 50; sweep++) {
+    double sm = 0.0;
+    for (int p = 0; p < 2; p++)
+      for (int q = p + 1; q < 3; q++) sm += fabs(a[p][q]);
+    if (sm == 0.0) return;
+    const double tresh = sweep < 4 ? (double)0.2f * sm / 9.0 : 0.0;
+    for (int p = 0; p < 2; p++)
+      for (int q = p + 1; q < 3; q++) {
+        double g = 100.0 * fabs(a[p][q]);
+        if (sweep > 4 && fabs(d[p]) + g == fabs(d[p]) && fabs(d[q]) + g == fabs(d[q])) {
+          a[p][q] = 0.0;
+        } else if (fabs(a[p][q]) > tresh) {
+          double hh = d[q] - d[p], t;
+          if (fabs(hh) + g == fabs(hh)) {
+            t = a[p][q] / hh;
+          } else {
+            const double theta = 0.5 * hh / a[p][q];
+            t = 1.0 / (fabs(theta) + sqrt(1.0 + theta * theta));
+            if (theta < 0.0) t = -t;
+          }
+          const double c = 1.0 / sqrt(1 + t * t), s = t * c, tau = s / (1.0 + c);
+          hh = t * a[p][q];
+          z[p] -= hh;
+          z[q] += hh;
+          d[p] -= hh;
+          d[q] += hh;
+          a[p][q] = 0.0;
+          for (int j = 0; j < p; j++) {
+            g = a[j][p];
+            hh = a[j][q];
+            a[j][p] = g - s * (hh + g * tau);
+            a[j][q] = hh + s * (g - hh * tau);
+          }
+          for (int j = p + 1; j < q; j++) {
+            g = a[p][j];
+            hh = a[j][q];
+            a[p][j] = g - s * (hh + g * tau);
+            a[j][q] = hh + s * (g - hh * tau);
+          }
+          for (int j = q + 1; j < 3; j++) {
+            g = a[p][j];
+            hh = a[q][j];
+            a[p][j] = g - s * (hh + g * tau);
+            a[q][j] = hh + s * (g - hh * tau);
+          }
+          for (int j = 0; j < 3; j++) {
+            g = v[j][p];
+            hh = v[j][q];
+            v[j][p] = g - s * (hh + g * tau);
+            v[j][q] = hh + s * (g - hh * tau);
+          }
+        }
+      }
+    for (int p = 0; p < 3; p++) {
+      bb[p] += z[p];
+      d[p] = bb[p];
+      z[p] = 0.0;
+    }
+  }
+}
+
+__device__ inline void eigsort3(double d[3], double v[3][3]) {
+  for (int i = 0; i < 2; i++) {
+    int k = i;
+    double p = d[i];
+    for (int j = i + 1; j < 3; j++)
+      if (d[j] >= p) {
+        k = j;
+        p = d[j];
+      }
+    if (k != i) {
+      d[k] = d[i];
+      d[i] = p;
+      for (int j = 0; j < 3; j++) {
+        const double t = v[j][i];
+        v[j][i] = v[j][k];
+        v[j][k] = t;
+      }
+    }
+  }
+}
+
 
 // learned radius bracket (psod_learn.cu)
 void learn_free(psod_ctx *c);

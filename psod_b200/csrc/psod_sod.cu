@@ -109,6 +109,13 @@ struct SodBufs {
   float *st_feat;                  // [slot][16] raw features
   float *st_rb0;                   // first ball radius (cells) when learn_use
   int learn_use, learn_collect;
+  // FoF features (learn_fof): per input particle its halo rank or group
+  // size (top bit), per FoF halo its mass, centre, radius and shape
+  int learn_fof;
+  const unsigned *fof_code;
+  const long long *fof_mass;
+  const double *fof_com, *fof_rad;
+  const float4 *fof_feat;
   float *learn_x, *learn_t;        // collected samples
   unsigned long long *learn_n, learn_cap;
   unsigned long long *bracket_hits, *bracket_seeds, *cross_balls, *cross_records;
@@ -1826,10 +1833,80 @@ __device__ __forceinline__ void select_seed(const SodConst &K, const SodBufs &B,
 // covers every seed.
 constexpr unsigned LEARN_MIN_CAND = 256;
 
+// The FoF feature set (the configuration the task names for the learned
+// seed), from the FoF group holding the seed particle:
+//   0 log N_FoF      1..3 inertia axis ratios b/a, c/a, c/b
+//   4 log rho(seed), the CIC peak overdensity
+//   5..7 seed - FoF centre of mass (cells, minimum image)
+//   8 R_FoF (cells)  9 RMS radius (cells)
+// Targets: log(R_stop / R_FoF), the farthest threshold's stop over the FoF
+// radius, and the centre offset |centre - seed| (cells); the first ball is
+// exp(y0) * margin * R_FoF.  A seed outside the FoF halos (a group below
+// Mmin) has no R_FoF: it gets no prediction and no sample.
+__device__ __forceinline__ void fof_features(const SodConst &K, const SodBufs &B, unsigned slot, unsigned rank,
+                                             float *f) {
+  const unsigned i = B.seed_idx[rank];
+  const unsigned code = B.fof_code[i];
+  const SeedGeo g = seed_geo(K, B, rank);
+  const float4 sv = B.cube[g.sp];
+  for (int k = 0; k < 16; k++) f[k] = 0.f;
+  f[4] = (float)log(fmax(B.rho[i], 1e-30));
+  if (code & 0x80000000u) {
+    f[0] = (float)log((double)max(code & 0x7fffffffu, 1u));
+    f[1] = f[2] = f[3] = 1.f;
+    f[15] = 1.f;
+    return;
+  }
+  const float4 q = B.fof_feat[code];
+  f[0] = (float)log((double)B.fof_mass[code]);
+  f[1] = q.y;
+  f[2] = q.z;
+  f[3] = q.w;
+  const double x[3] = {(double)sv.x, (double)sv.y, (double)sv.z};
+  for (int a = 0; a < 3; a++) {
+    double d = x[a] - B.fof_com[3ull * code + a];
+    d -= floor(d + 0.5);  // minimum image in box units
+    f[5 + a] = (float)(d * K.nxf);
+  }
+  f[8] = (float)(B.fof_rad[code] * K.nxf);
+  f[9] = q.x * K.nxf;
+  if (!(f[8] > 0.f)) f[15] = 1.f;
+}
+
+// the two training targets of a crossing sample; false: no sample
+__device__ __forceinline__ bool learn_targets(const SodConst &K, const SodBufs &B, unsigned slot, double d2far,
+                                              long long masse, unsigned seed_pos, unsigned centre_pos, float &t0,
+                                              float &t1) {
+  if (!B.learn_fof) {
+    t0 = (float)(0.5 * log(fmax(d2far, 1e-12)));
+    t1 = (float)log((double)masse);
+    return true;
+  }
+  const float *f = B.st_feat + (size_t)slot * 16;
+  if (f[15] != 0.f || !(f[8] > 0.f)) return false;
+  const float4 a = B.cube[seed_pos], b = B.cube[centre_pos];
+  const double d2 = min_image_d2((double)to_grid(a.x, K.nxf), (double)to_grid(a.y, K.nxf),
+                                 (double)to_grid(a.z, K.nxf), (double)to_grid(b.x, K.nxf),
+                                 (double)to_grid(b.y, K.nxf), (double)to_grid(b.z, K.nxf), K.tx);
+  t0 = (float)(0.5 * log(fmax(d2far, 1e-12)) - log((double)f[8]));
+  t1 = (float)sqrt(d2);
+  return true;
+}
+
+// the learned first ball (cells) of a ready seed, 0 when none
+__device__ __forceinline__ float learned_ball(const SodBufs &B, unsigned slot) {
+  const float r = B.st_rb0[slot];
+  return B.learn_fof ? r * B.st_feat[(size_t)slot * 16 + 8] : r;
+}
+
 __device__ __forceinline__ void seed_features(const SodConst &K, const SodBufs &B, Smem &S, unsigned slot, unsigned rank) {
   float *f = B.st_feat + (size_t)slot * 16;
   if (!B.st_active[slot] || (!B.learn_collect && B.st_cn[slot] < LEARN_MIN_CAND)) {
     if (threadIdx.x < 16) f[threadIdx.x] = threadIdx.x == 15 ? 1.f : 0.f;
+    return;
+  }
+  if (B.learn_fof) {
+    if (threadIdx.x == 0) fof_features(K, B, slot, rank, f);
     return;
   }
   const SeedGeo g = seed_geo(K, B, rank);
@@ -2021,7 +2098,7 @@ __device__ __forceinline__ void cross_seed(const SodConst &K, const SodBufs &B, 
     // at ncut).  A smaller ball saves records but not time: a pass costs
     // mostly its fixed walk and sort, and a miss adds a pass.  Starting at
     // or above BALL0, the doubling never needs more passes than from BALL0.
-    const float r = B.st_rb0[slot];
+    const float r = learned_ball(B, slot);
     if (r > 0.f) rb0 = fmin(fmax((double)r, BALL0), (double)K.ncut);
   }
 
@@ -2170,11 +2247,14 @@ __device__ __forceinline__ void cross_seed(const SodConst &K, const SodBufs &B, 
     if (d2far <= rb0 * rb0) atomicAdd(B.bracket_hits, 1ull);
   }
   if (threadIdx.x == 0 && B.learn_collect) {
-    const unsigned long long q = atomicAdd(B.learn_n, 1ull);
-    if (q < B.learn_cap) {
-      for (int k = 0; k < PSOD_LEARN_FEATURES; k++) B.learn_x[q * PSOD_LEARN_FEATURES + k] = B.st_feat[slot * 16 + k];
-      B.learn_t[2 * q] = (float)(0.5 * log(fmax(d2far, 1e-12)));
-      B.learn_t[2 * q + 1] = (float)log((double)masse);
+    float t0, t1;
+    if (learn_targets(K, B, slot, d2far, masse, g.sp, cpos, t0, t1)) {
+      const unsigned long long q = atomicAdd(B.learn_n, 1ull);
+      if (q < B.learn_cap) {
+        for (int k = 0; k < PSOD_LEARN_FEATURES; k++) B.learn_x[q * PSOD_LEARN_FEATURES + k] = B.st_feat[slot * 16 + k];
+        B.learn_t[2 * q] = t0;
+        B.learn_t[2 * q + 1] = t1;
+      }
     }
   }
 
@@ -2517,7 +2597,7 @@ __global__ void __launch_bounds__(256) k_cross_warp(SodConst K, SodBufs B) {
   const unsigned cidx = __float_as_uint(cvv.w) & PSOD_IDX_MASK;
   double rb0 = BALL0;
   if (B.learn_use) {
-    const float r = B.st_rb0[slot];
+    const float r = learned_ball(B, slot);
     if (r > 0.f) rb0 = fmin(fmax((double)r, BALL0), (double)K.ncut);
   }
   auto to_cta = [&]() {
@@ -2604,11 +2684,14 @@ __global__ void __launch_bounds__(256) k_cross_warp(SodConst K, SodBufs B) {
     }
   }
   if (lane == 0 && B.learn_collect) {
-    const unsigned long long q = atomicAdd(B.learn_n, 1ull);
-    if (q < B.learn_cap) {
-      for (int k = 0; k < PSOD_LEARN_FEATURES; k++) B.learn_x[q * PSOD_LEARN_FEATURES + k] = B.st_feat[slot * 16 + k];
-      B.learn_t[2 * q] = (float)(0.5 * log(fmax(d2far, 1e-12)));
-      B.learn_t[2 * q + 1] = (float)log((double)masse);
+    float t0, t1;
+    if (learn_targets(K, B, slot, d2far, masse, g.sp, cpos, t0, t1)) {
+      const unsigned long long q = atomicAdd(B.learn_n, 1ull);
+      if (q < B.learn_cap) {
+        for (int k = 0; k < PSOD_LEARN_FEATURES; k++) B.learn_x[q * PSOD_LEARN_FEATURES + k] = B.st_feat[slot * 16 + k];
+        B.learn_t[2 * q] = t0;
+        B.learn_t[2 * q + 1] = t1;
+      }
     }
   }
   unsigned long long pool_base = 0;
@@ -3854,6 +3937,21 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   // the learned bracket needs the per-cell alive counts of the batched modes
   B.learn_use = (c->p.mode == PSOD_MODE_LEARNED && learn_ready(c)) ? 1 : 0;
   B.learn_collect = (c->p.mode != PSOD_MODE_PLAIN && learn_collecting(c)) ? 1 : 0;
+  B.learn_fof = 0;
+  B.fof_code = nullptr;
+  B.fof_mass = nullptr;
+  B.fof_com = B.fof_rad = nullptr;
+  B.fof_feat = nullptr;
+  if ((B.learn_use || B.learn_collect) && c->learn_features == PSOD_LEARN_FEATURES_FOF) {
+    if (!c->fof_done || c->fof_n != c->n)
+      return set_err(c, PSOD_ERR_STATE, "learned FoF features: call psod_fof on the loaded particles first");
+    B.learn_fof = 1;
+    B.fof_code = static_cast<const unsigned *>(c->scratch[SLOT_F_CODE].first);
+    B.fof_mass = static_cast<const long long *>(c->scratch[SLOT_F_MASS].first);
+    B.fof_com = static_cast<const double *>(c->scratch[SLOT_F_COM].first);
+    B.fof_rad = static_cast<const double *>(c->scratch[SLOT_F_RAD].first);
+    B.fof_feat = static_cast<const float4 *>(c->scratch[SLOT_F_FEAT].first);
+  }
   B.learn_x = B.learn_t = nullptr;
   B.learn_n = nullptr;
   B.learn_cap = 0;

@@ -304,6 +304,16 @@ class SphericalOverdensity:
         self._check(self.lib.psod_fof(self.ctx, C.byref(p), C.byref(st)))
         return st.as_dict()
 
+    def fof_release(self):
+        """Free the FoF stage's working arrays (the catalogue stays)."""
+        self._check(self.lib.psod_fof_release(self.ctx))
+
+    def learn_set_features(self, which: str):
+        """The learned bracket's feature set: "seed" (seed-local) or "fof"
+        (from the seed's FoF group; needs fof() on the loaded particles)."""
+        self._check(self.lib.psod_learn_set_features(
+            self.ctx, capi.LEARN_FEATURES_FOF if which == "fof" else capi.LEARN_FEATURES_SEED))
+
     def fof_halos(self, members: bool = True) -> FofTable:
         nh, nm = C.c_int64(0), C.c_int64(0)
         self._check(self.lib.psod_fof_halo_count(self.ctx, C.byref(nh), C.byref(nm)))

@@ -125,3 +125,50 @@ def test_learned_bracket_trains_and_keeps_results():
           f"batched {st_b['cross_balls']}, learned {st_l['cross_balls']}")
     assert st_l["cross_balls"] < st_b["cross_balls"]
     assert hit_l >= hit_b
+
+
+@pytest.mark.gpu
+def test_learned_bracket_with_fof_features():
+    """The configuration the task names: inputs from the seed's FoF group
+    (log N_FoF, inertia axis ratios, log peak overdensity, peak - centre of
+    mass offset, R_FoF, RMS radius), targets log(R_stop / R_FoF) and the
+    centre offset.  Same halo table as the batched mode."""
+    SO = _gpu()
+    from psod_b200 import synth
+
+    box = synth.make_box(128, nmax_halo=20000, seed=7, device="cuda")
+    with SO(128, mode=1) as s:
+        s.load(box.pos, box.ids)
+        s.fof(percolation=0.2, mmin=20)
+        s.fof_release()
+        s.learn_set_features("fof")
+        s.learn_collect(1 << 20)
+        st_b = s.run()
+        tb = s.halos()
+        x, t = s.learn_samples()
+        # samples only for seeds inside FoF halos, with finite features
+        assert 100 < x.shape[0] <= st_b["bracket_seeds"]
+        assert np.all(np.isfinite(x)) and np.all(np.isfinite(t))
+        assert np.all(x[:, 8] > 0) and np.all(x[:, 0] >= np.log(20) - 1e-6)
+        assert np.all((x[:, 1:4] > 0) & (x[:, 1:4] <= 1.0 + 1e-6))
+        assert np.all(t[:, 1] >= 0)  # centre offsets (cells)
+        loss = s.learn_train(epochs=20, batch=256, lr=1e-3, seed=1)
+        model = s.learn_get_model()
+    assert loss[-1] < loss[0], loss
+    with SO(128, mode=2) as s:
+        s.learn_set_features("fof")
+        s.learn_set_model(model)
+        s.load(box.pos, box.ids)
+        from psod_b200.sod import PsodError
+
+        with pytest.raises(PsodError):  # no FoF catalogue yet
+            s.run()
+        s.fof(percolation=0.2, mmin=20)
+        st_l = s.run()
+        tl = s.halos()
+    for f in ("halo_id", "halo_mass", "halo_rank", "halo_center", "halo_rdelta", "halo_mass2", "halo_profile",
+              "member_offset", "member_index", "member_id"):
+        assert np.array_equal(getattr(tl, f), getattr(tb, f)), f
+    print(f"FoF features: bracket hits batched {st_b['bracket_hits'] / st_b['bracket_seeds']:.3f}, "
+          f"learned {st_l['bracket_hits'] / max(1, st_l['bracket_seeds']):.3f}; ball passes batched "
+          f"{st_b['cross_balls']}, learned {st_l['cross_balls']}")
