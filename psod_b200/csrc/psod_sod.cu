@@ -3463,131 +3463,140 @@ __global__ void k_widen(const unsigned *in, long long n, long long *out) {
 }
 
 constexpr int MS_CHUNK = 2048;
-constexpr unsigned MS_TILE = 2048;  // merge outputs staged per step (<= MS_CHUNK)
 
 __device__ __forceinline__ bool pair_less(unsigned long long ka, unsigned ia, unsigned long long kb, unsigned ib) {
   return ka < kb || (ka == kb && ia < ib);
 }
 
-// sort each halo's members by (d2 bits, input index) and write the input
-// indices at the halo's output offset; one CTA per halo
+// Members leave in (d2 bits, input index) order, written as input indices at
+// the halo's output offset.  Halos claimed from a sorted list are copied;
+// the others hold members in claim order.  Those of at most MS_CHUNK members
+// are sorted by one CTA each in shared memory (k_member_sort); the larger
+// ones, a few thousand halos holding most of the members, are sorted
+// together by one device-wide radix sort on (halo, top 32 bits of d2)
+// (k_big_keys), after which the rare runs of equal truncated keys are put
+// in full-key order (k_big_ties) and scattered to the output (k_big_out).
 __global__ void __launch_bounds__(256) k_member_sort(const unsigned *order, long long nh, const unsigned long long *h_pool,
                                                      const long long *h_mass_sorted, const unsigned *moff,
-                                                     unsigned long long *pkey, unsigned *pidx,
-                                                     unsigned long long *tkey, unsigned *tidx, unsigned *m_index) {
+                                                     const unsigned long long *pkey, const unsigned *pidx,
+                                                     unsigned *m_index) {
   __shared__ unsigned long long sk[MS_CHUNK];
   __shared__ unsigned si[MS_CHUNK];
-  __shared__ unsigned s_split[2];
   for (long long h = blockIdx.x; h < nh; h += gridDim.x) {
     const unsigned slot = order[h];
     const unsigned long long base = h_pool[slot] & ~POOL_SORTED;
     const unsigned m = (unsigned)h_mass_sorted[h];
+    const unsigned o = moff[h];
     if (h_pool[slot] & POOL_SORTED) {
       // claimed from a sorted list: already in (d2, index) order
-      const unsigned o = moff[h];
       for (unsigned k = threadIdx.x; k < m; k += blockDim.x) m_index[o + k] = pidx[base + k];
       continue;
     }
-    unsigned long long *ka = pkey + base, *kb = tkey + base;
-    unsigned *ia = pidx + base, *ib = tidx + base;
-    // 1. sort chunks in shared memory
-    for (unsigned c0 = 0; c0 < m; c0 += MS_CHUNK) {
-      const unsigned n = min((unsigned)MS_CHUNK, m - c0);
-      unsigned p2 = 1;
-      while (p2 < n) p2 <<= 1;
-      for (unsigned k = threadIdx.x; k < p2; k += blockDim.x) {
-        sk[k] = k < n ? ka[c0 + k] : ~0ull;
-        si[k] = k < n ? ia[c0 + k] : 0xffffffffu;
-      }
-      __syncthreads();
-      for (unsigned size = 2; size <= p2; size <<= 1) {
-        for (unsigned stride = size >> 1; stride > 0; stride >>= 1) {
-          for (unsigned k = threadIdx.x; k < p2 / 2; k += blockDim.x) {
-            unsigned a = 2 * k - (k & (stride - 1));
-            unsigned bb = a + stride;
-            bool up = ((a & size) == 0);
-            bool gt = pair_less(sk[bb], si[bb], sk[a], si[a]);
-            if (gt == up) {
-              unsigned long long t = sk[a]; sk[a] = sk[bb]; sk[bb] = t;
-              unsigned ti = si[a]; si[a] = si[bb]; si[bb] = ti;
-            }
-          }
-          bitonic_stage_sync(size, stride, p2);
-        }
-      }
-      for (unsigned k = threadIdx.x; k < n; k += blockDim.x) {
-        ka[c0 + k] = sk[k];
-        ia[c0 + k] = si[k];
-      }
-      __syncthreads();
+    if (m > (unsigned)MS_CHUNK) continue;  // the device-wide pass
+    unsigned p2 = 1;
+    while (p2 < m) p2 <<= 1;
+    for (unsigned k = threadIdx.x; k < p2; k += blockDim.x) {
+      sk[k] = k < m ? pkey[base + k] : ~0ull;
+      si[k] = k < m ? pidx[base + k] : 0xffffffffu;
     }
-    // 2. merge runs pairwise, MS_TILE outputs at a time: the tile's split
-    // of the two runs is found by binary search on its diagonals (merge
-    // path), both pieces are staged in shared memory and each thread
-    // merges MS_TILE / 256 outputs there.  Keys (d2 bits, index) are
-    // unique, so the merge is exact.
-    for (unsigned w = MS_CHUNK; w < m; w <<= 1) {
-      for (unsigned s0 = 0; s0 < m; s0 += 2 * w) {
-        const unsigned na = min(w, m - s0), nb = min(w, m - min(m, s0 + w));
-        const unsigned long long *A = ka + s0, *Bk = ka + s0 + na;
-        const unsigned *Ai = ia + s0, *Bi = ia + s0 + na;
-        for (unsigned o0 = 0; o0 < na + nb; o0 += MS_TILE) {
-          const unsigned o1 = min(o0 + MS_TILE, na + nb);
-          if (threadIdx.x < 2) {
-            const unsigned d = threadIdx.x == 0 ? o0 : o1;  // diagonal
-            unsigned lo = d > nb ? d - nb : 0u, hi = min(d, na);
-            while (lo < hi) {
-              const unsigned mid = (lo + hi) >> 1;
-              if (pair_less(Bk[d - mid - 1], Bi[d - mid - 1], A[mid], Ai[mid])) hi = mid;
-              else lo = mid + 1;
-            }
-            s_split[threadIdx.x] = lo;
+    __syncthreads();
+    for (unsigned size = 2; size <= p2; size <<= 1) {
+      for (unsigned stride = size >> 1; stride > 0; stride >>= 1) {
+        for (unsigned k = threadIdx.x; k < p2 / 2; k += blockDim.x) {
+          unsigned a = 2 * k - (k & (stride - 1));
+          unsigned bb = a + stride;
+          bool up = ((a & size) == 0);
+          bool gt = pair_less(sk[bb], si[bb], sk[a], si[a]);
+          if (gt == up) {
+            unsigned long long t = sk[a]; sk[a] = sk[bb]; sk[bb] = t;
+            unsigned ti = si[a]; si[a] = si[bb]; si[bb] = ti;
           }
-          __syncthreads();
-          const unsigned a0 = s_split[0], a1 = s_split[1];
-          const unsigned b0 = o0 - a0, b1 = o1 - a1;
-          const unsigned la = a1 - a0, lb = b1 - b0;
-          for (unsigned k = threadIdx.x; k < la; k += blockDim.x) {
-            sk[k] = A[a0 + k];
-            si[k] = Ai[a0 + k];
-          }
-          for (unsigned k = threadIdx.x; k < lb; k += blockDim.x) {
-            sk[la + k] = Bk[b0 + k];
-            si[la + k] = Bi[b0 + k];
-          }
-          __syncthreads();
-          // thread t: outputs [t*PER, t*PER + PER) of the tile
-          const unsigned per = MS_TILE / 256u, t0 = threadIdx.x * per;
-          if (t0 < la + lb) {
-            unsigned lo = t0 > lb ? t0 - lb : 0u, hi = min(t0, la);
-            while (lo < hi) {
-              const unsigned mid = (lo + hi) >> 1;
-              if (pair_less(sk[la + t0 - mid - 1], si[la + t0 - mid - 1], sk[mid], si[mid])) hi = mid;
-              else lo = mid + 1;
-            }
-            unsigned x = lo, y = t0 - lo;
-            const unsigned tend = min(t0 + per, la + lb);
-            for (unsigned q = t0; q < tend; q++) {
-              bool take_a;
-              if (x >= la) take_a = false;
-              else if (y >= lb) take_a = true;
-              else take_a = !pair_less(sk[la + y], si[la + y], sk[x], si[x]);
-              const unsigned src = take_a ? x++ : la + y++;
-              kb[s0 + o0 + q] = sk[src];
-              ib[s0 + o0 + q] = si[src];
-            }
-          }
-          __syncthreads();
         }
+        bitonic_stage_sync(size, stride, p2);
       }
-      __syncthreads();
-      unsigned long long *tk = ka; ka = kb; kb = tk;
-      unsigned *ti = ia; ia = ib; ib = ti;
     }
-    const unsigned o = moff[h];
-    for (unsigned k = threadIdx.x; k < m; k += blockDim.x) m_index[o + k] = ia[k];
+    for (unsigned k = threadIdx.x; k < m; k += blockDim.x) m_index[o + k] = si[k];
     __syncthreads();
   }
+}
+
+// big[h] = 1 for a halo (output order) claimed unsorted with more than
+// MS_CHUNK members, msz[h] its member count there (0 otherwise); both are
+// scanned in place afterwards
+__global__ void k_big_flags(const unsigned *order, long long nh, const unsigned long long *h_pool,
+                            const long long *h_mass_sorted, unsigned *big, unsigned *msz) {
+  const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= nh) return;
+  const unsigned m = (unsigned)h_mass_sorted[h];
+  const bool b = !(h_pool[order[h]] & POOL_SORTED) && m > (unsigned)MS_CHUNK;
+  big[h] = b ? 1u : 0u;
+  msz[h] = b ? m : 0u;
+}
+
+// the large halos as segments s = 0 .. nbig-1 in output order: their halo,
+// start in the concatenated key array (seg_start[nbig] = total) and pool base
+__global__ void k_big_list(const unsigned *order, long long nh, const unsigned long long *h_pool,
+                           const unsigned *big_scan, const unsigned *msz_scan, unsigned *seg_h, unsigned *seg_start,
+                           unsigned *seg_base) {
+  const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= nh) return;
+  if (h == 0) seg_start[big_scan[nh]] = msz_scan[nh];
+  if (big_scan[h + 1] == big_scan[h]) return;
+  const unsigned s = big_scan[h];
+  seg_h[s] = (unsigned)h;
+  seg_start[s] = msz_scan[h];
+  seg_base[s] = (unsigned)(h_pool[order[h]] & ~POOL_SORTED);
+}
+
+// key j of the concatenated segments: (segment << 32) | d2 bits >> 31 (the
+// top 32 bits below the sign, monotone in d2 >= 0); value = pool position
+__global__ void k_big_keys(const unsigned *seg_start, unsigned nbig, const unsigned *seg_base,
+                           const unsigned long long *pool_key, unsigned ntot, unsigned long long *key,
+                           unsigned *val) {
+  const unsigned j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ntot) return;
+  unsigned lo = 0, hi = nbig;  // seg_start[lo] <= j < seg_start[hi]
+  while (hi - lo > 1) {
+    const unsigned mid = (lo + hi) >> 1;
+    if (seg_start[mid] <= j) lo = mid;
+    else hi = mid;
+  }
+  const unsigned p = seg_base[lo] + (j - seg_start[lo]);
+  key[j] = ((unsigned long long)lo << 32) | (unsigned)(pool_key[p] >> 31);
+  val[j] = p;
+}
+
+// after the radix sort: each run of equal keys (same segment, d2 equal in
+// its top 32 bits) is put in (full d2 bits, input index) order by the thread
+// at its start; runs are short (pairs of members within 2^-21 in d2)
+__global__ void k_big_ties(const unsigned long long *key, unsigned *val, unsigned ntot,
+                           const unsigned long long *pool_key, const unsigned *pool_idx) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i + 1 >= ntot) return;
+  const unsigned long long k = key[i];
+  if (key[i + 1] != k || (i > 0 && key[i - 1] == k)) return;
+  unsigned e = i + 2;
+  while (e < ntot && key[e] == k) e++;
+  for (unsigned a = i + 1; a < e; a++) {
+    const unsigned v = val[a];
+    const unsigned long long fk = pool_key[v];
+    const unsigned fi = pool_idx[v];
+    unsigned b = a;
+    while (b > i && pair_less(fk, fi, pool_key[val[b - 1]], pool_idx[val[b - 1]])) {
+      val[b] = val[b - 1];
+      b--;
+    }
+    val[b] = v;
+  }
+}
+
+__global__ void k_big_out(const unsigned long long *key, const unsigned *val, unsigned ntot, const unsigned *seg_h,
+                          const unsigned *seg_start, const unsigned *moff, const unsigned *pool_idx,
+                          unsigned *m_index) {
+  const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ntot) return;
+  const unsigned s = (unsigned)(key[i] >> 32);
+  m_index[moff[seg_h[s]] + (i - seg_start[s])] = pool_idx[val[i]];
 }
 
 inline unsigned nblk(long long n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -3641,8 +3650,9 @@ enum {
   SC_ST_CENTRE, SC_CAND_POS, SC_CAND_SLOT, SC_CAND_S, SC_ORDER, SC_RKEYS, SC_MASS32, SC_MOFF, SC_TKEY, SC_TIDX,
   SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS, SC_CELLNCH, SC_FEAT, SC_RB0,
   SC_SBEST, SC_CELLGROUPS, SC_GROUPPREF, SC_GU, SC_CANDLIST, SC_CNT2, SC_LMAX, SC_BIG, SC_RESOLVED, SC_BIDXRANK,
-  SC_BIDXCUBE, SC_TOPG, SC_XKEY, SC_XIDX, SC_XPOS, SC_TAIL
+  SC_BIDXCUBE, SC_TOPG, SC_XKEY, SC_XIDX, SC_XPOS, SC_TAIL, SC_BIGSEG
 };
+static_assert((int)SC_BIGSEG < (int)SLOT_CELL_U32, "SOD scratch slots overlap the shared ones");
 
 // Rounds go to the device tail loop once the last host round had no seed
 // for the bound pass, no seed with more than tail_max_cand candidates, at
@@ -4269,8 +4279,33 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     if ((rc = scan_u32(c, mass32, moff, nh, true))) return rc;
     k_widen<<<nblk(nh + 1, 256), 256, 0, c->stream>>>(moff, nh + 1, c->d_m_offset);
     k_member_sort<<<std::min<long long>(nh, 4 * dev_sms), 256, 0, c->stream>>>(
-        order, nh, h_pool, c->d_h_mass, moff, pool_key, pool_idx, tkey, tidx, c->d_m_index);
+        order, nh, h_pool, c->d_h_mass, moff, pool_key, pool_idx, c->d_m_index);
     kernels += 11;
+    // the large halos claimed unsorted: one device-wide sort
+    unsigned *bsc;
+    if ((rc = scratch(c, SC_BIGSEG, 5 * ((size_t)nh + 2), &bsc))) return rc;
+    unsigned *big_scan = bsc, *msz_scan = bsc + (nh + 2), *seg_h = bsc + 2 * (nh + 2),
+             *seg_start = bsc + 3 * (nh + 2), *seg_base = bsc + 4 * (nh + 2);
+    k_big_flags<<<g1, 256, 0, c->stream>>>(order, nh, h_pool, c->d_h_mass, big_scan, msz_scan);
+    kernels++;
+    if ((rc = scan_u32(c, big_scan, big_scan, nh, true)) || (rc = scan_u32(c, msz_scan, msz_scan, nh, true)))
+      return rc;
+    k_big_list<<<g1, 256, 0, c->stream>>>(order, nh, h_pool, big_scan, msz_scan, seg_h, seg_start, seg_base);
+    kernels++;
+    unsigned tot[2] = {0, 0};
+    PSOD_CUDA(c, cudaMemcpyAsync(&tot[0], big_scan + nh, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    PSOD_CUDA(c, cudaMemcpyAsync(&tot[1], msz_scan + nh, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
+    const unsigned nbig = tot[0], ntot = tot[1];
+    if (nbig > 0) {
+      k_big_keys<<<nblk(ntot, 256), 256, 0, c->stream>>>(seg_start, nbig, seg_base, pool_key, ntot, tkey, tidx);
+      kernels++;
+      if ((rc = radix_sort_u64(c, tkey, tidx, ntot, 64))) return rc;
+      k_big_ties<<<nblk(ntot, 256), 256, 0, c->stream>>>(tkey, tidx, ntot, pool_key, pool_idx);
+      k_big_out<<<nblk(ntot, 256), 256, 0, c->stream>>>(tkey, tidx, ntot, seg_h, seg_start, moff, pool_idx,
+                                                        c->d_m_index);
+      kernels += 2;
+    }
   } else {
     PSOD_CUDA(c, cudaMemsetAsync(c->d_m_offset, 0, sizeof(long long), c->stream));
   }
