@@ -34,6 +34,7 @@ namespace {
 constexpr int TPB = 256;          // threads per seed CTA
 constexpr unsigned RN_CHUNK = 2048;  // neighbour records per refinement work item
 constexpr int NWARP = TPB / 32;
+constexpr unsigned SEL_SPLIT_MAX = 4;  // select: contenders summed by the whole CTA
 constexpr int NB = 4096;          // histogram buckets per level
 constexpr int MAXLEV = 4;         // histogram levels kept in shared memory
 constexpr int CAP = 2048;         // elements sorted in shared memory
@@ -202,6 +203,9 @@ struct Smem {
   // last radial_search hit: sorted-buffer index and bucket lower bound
   int res_k;
   unsigned long long res_lo;
+  // select: the contenders of a seed that has few
+  unsigned nsel;
+  unsigned sel[SEL_SPLIT_MAX];
 };
 
 __device__ __forceinline__ int wrapi(int a, int nx) {
@@ -1114,7 +1118,8 @@ __device__ __forceinline__ NbrList nbr_list(const SodConst &K, const SodBufs &B,
 // as one list, 32 records a step.
 template <bool EXACT>
 __device__ __forceinline__ void refine_sum(const SodConst &K, const SodBufs &B, unsigned cp, int ic, int jc, int kc,
-                           unsigned long long &sq_out, double &sf_out, unsigned *visits = nullptr) {
+                           unsigned long long &sq_out, double &sf_out, unsigned *visits = nullptr,
+                           unsigned part = 0, unsigned nparts = 1) {
   const int lane = threadIdx.x & 31;
   const float4 cv = B.cube[cp];
   const float cxg = to_grid(cv.x, K.nxf), cyg = to_grid(cv.y, K.nxf), czg = to_grid(cv.z, K.nxf);
@@ -1126,7 +1131,8 @@ __device__ __forceinline__ void refine_sum(const SodConst &K, const SodBufs &B, 
   double sf = 0.0;
   const NbrList L = nbr_list(K, B, pcx, pcy, pcz, ic, jc, kc);
   if (visits && lane == 0) *visits += L.total;
-  for (unsigned t0 = 0; t0 < L.total; t0 += 32) {
+  // warp `part` of `nparts` takes every nparts-th step of 32 records
+  for (unsigned t0 = 32 * part; t0 < L.total; t0 += 32 * nparts) {
     const unsigned t = t0 + (unsigned)lane;
     const unsigned q = L.at(t < L.total ? t : L.total - 1);
     if (t >= L.total) continue;
@@ -1151,7 +1157,7 @@ __device__ __forceinline__ void refine_sum(const SodConst &K, const SodBufs &B, 
     }
   }
   // the particle the run scan files under another cell
-  if (K.has_quirk && lane == 0) {
+  if (K.has_quirk && lane == 0 && part == 0) {
     const int ax = (int)(K.quirk_listed % K.nx), ay = (int)((K.quirk_listed / K.nx) % K.nx),
               az = (int)(K.quirk_listed / ((unsigned)K.nx * K.nx));
     const bool listed_in_sel2 = in_sel2(K, ax, ay, az, ic, jc, kc);
@@ -1785,13 +1791,39 @@ __device__ __forceinline__ void select_seed(const SodConst &K, const SodBufs &B,
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   unsigned long long best_sq = 0, best_key = ~0ull;
   unsigned best_pos = 0xffffffffu;
-  for (unsigned k = w; k < n; k += NWARP) {
-    if (!(B.cand_s[off + k] >= thr)) continue;  // cannot reach the maximum
-    const unsigned cp = B.cand_pos[off + k];
+  // Contenders (approximate sum within 2*REF_TOL of the maximum) get exact
+  // sums.  Most seeds have one or two: then every warp of the CTA takes a
+  // share of each contender's records (the int64 fixed-point sum is exact,
+  // so the split leaves it unchanged); with more, a warp sums a contender.
+  if (threadIdx.x == 0) S.nsel = 0;
+  __syncthreads();
+  for (unsigned k = threadIdx.x; k < n; k += TPB)
+    if (B.cand_s[off + k] >= thr) {
+      const unsigned j = atomicAdd(&S.nsel, 1u);
+      if (j < SEL_SPLIT_MAX) S.sel[j] = k;
+    }
+  __syncthreads();
+  const unsigned nsel = S.nsel;
+  const bool split = nsel <= SEL_SPLIT_MAX;
+  const unsigned nloop = split ? nsel : n;
+  for (unsigned k = split ? 0u : (unsigned)w; k < nloop; k += split ? 1u : (unsigned)NWARP) {
+    const unsigned ck = split ? S.sel[k] : k;
+    if (!split && !(B.cand_s[off + ck] >= thr)) continue;  // cannot reach the maximum
+    const unsigned cp = B.cand_pos[off + ck];
     unsigned long long sq;
     double sf;
-    refine_sum<true>(K, B, cp, g.ic, g.jc, g.kc, sq, sf);
-    if (lane == 0) {
+    if (split) {
+      refine_sum<true>(K, B, cp, g.ic, g.jc, g.kc, sq, sf, nullptr, (unsigned)w, NWARP);
+      __syncthreads();
+      if (lane == 0) S.red_u64[w] = sq;
+      __syncthreads();
+      sq = 0;
+#pragma unroll
+      for (int q = 0; q < NWARP; q++) sq += S.red_u64[q];
+    } else {
+      refine_sum<true>(K, B, cp, g.ic, g.jc, g.kc, sq, sf);
+    }
+    if (lane == 0 && (!split || w == 0)) {
       const float4 cv = B.cube[cp];
       const unsigned cw = __float_as_uint(cv.w);
       int lx, ly, lz;
