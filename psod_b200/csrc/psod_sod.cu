@@ -121,10 +121,10 @@ struct SodBufs {
   unsigned long long *learn_n, learn_cap;
   unsigned long long *bracket_hits, *bracket_seeds, *cross_balls, *cross_records;
   // refinement bounds: 64-candidate groups per (slot, candidate cell) and
-  // their prefix; per group the upper bounds U of its sub-groups; per slot
-  // the best lower bound of the maximum sum (float bits)
+  // their prefix; per candidate an upper bound U of its sum; per slot the
+  // best lower bound of the maximum sum (float bits)
   unsigned *cell_groups, *group_pref;
-  float *g_u;  // per 64-candidate group, NSUB sub-group bounds
+  float *cand_u;  // per candidate position (as cand_s), bounded seeds only
   unsigned *s_lmax;
   unsigned *work_bound;
   int bound_on;
@@ -1382,27 +1382,24 @@ __device__ __forceinline__ void tile_terms2(const RecTile &tile, unsigned nt, fl
 // reads each one by broadcast; warps never wait on one another.  Partial
 // sums of a candidate's neighbour chunks are added into cand_s.
 //
-// BOUND: the same items, but each record adds only to upper bounds of the
-// group's sixteen sub-groups of 4 candidates (in the cell's candidate
-// order, Morton-compact in dense cells): U(s) = sum over records within
-// reach of k(d to the sub-group's box) for records near the group's box and
-// k(d to the group's box) for the others, so no candidate of s can have a
-// larger S.  Near records are staged in tiles; lane l accumulates sub-group
-// l/2 over the tile's records l%2, l%2+2, ...  U is inflated by 1e-3, far
-// above the FP32 error of the sums.  The second pair pass keeps only candidates whose sub-group
-// bound reaches the seed's lower bound; the others cannot hold the argmax
-// and their sums stay 0, below the select threshold.
+// BOUND: the same items, giving each candidate c an upper bound U(c) of its
+// sum.  Records nearer than sqrt(NEAR2) cells to the group's box are staged
+// in tiles and summed exactly for every candidate (the pair pass's own
+// loop); each farther record within reach adds k(d to the group's box),
+// which no candidate's term exceeds, to every candidate of the group.  U is
+// inflated by 1e-3, far above the FP32 error of the sums.  The second pair
+// pass keeps only candidates whose bound reaches the seed's lower bound;
+// the others cannot hold the argmax and their sums stay 0, below the select
+// threshold.
+//
+// The near field is where a box bound is loose (a record inside the box
+// counts 1/eps = 64 against a true term of a few), so it is summed exactly;
+// the far field varies little across a compact group.  With the fine order
+// of dense cells (a 64-candidate group spans ~0.1-0.3 cells in halo cores)
+// a CPU model of NFW halos of 3e5-1e6 particles (c = 4-12) measured the
+// near sums at 8-10 % of the unpruned pair work and the survivors at 2-15 %,
+// against 37-61 % survivors with box bounds on sub-groups of 4.
 constexpr unsigned ITEM_GRAB = 1;  // refinement items claimed per counter update
-
-
-// Sub-groups of SUBG candidates (16 per 64-candidate group, two lanes each).
-// Records nearer than sqrt(NEAR2) cells to a group's box bound its
-// sub-groups through their own boxes; farther ones through the group's box,
-// where the difference is small.  (Measured on an NFW halo of 3e4
-// particles, with the exact lower bound: the pair work pruned is 26 % with
-// group boxes only, 79 % with every record on boxes of 4 candidates, 74 %
-// with only records within 0.3 cells, which are a small fraction.)
-constexpr unsigned SUBG = 4, NSUB = 64 / SUBG;
 constexpr float NEAR2 = 0.09f;
 
 template <bool BOUND>
@@ -1460,7 +1457,6 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
     const unsigned nch = B.cell_nch[ci];
     const unsigned chunk = rem / nch, nchunk = rem % nch;
     const unsigned slot = ci / 27, o = ci % 27;
-    const unsigned grp = B.group_pref[ci] + chunk;
     const bool bounded = B.bound_on && B.st_cn[slot] >= B.bound_min;
     if (BOUND && !bounded) continue;
     if (!BOUND && lane == 0) s_count[w][3]++;
@@ -1571,54 +1567,14 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
       hiz = fmaxf(hiz, __shfl_xor_sync(0xffffffffu, hiz, o));
     }
     const bool any_active = lox <= hix;
-    // BOUND: the box of sub-group lane/2 (candidates 4s..4s+3 of the group:
-    // first candidates of lanes 4s.. for s < 8, second candidates of lanes
-    // 4(s-8).. for s >= 8)
-    float slx = 3e38f, shx = -3e38f, sly = 3e38f, shy = -3e38f, slz = 3e38f, shz = -3e38f;
-    if (BOUND) {
-      float a[6] = {active ? cx : 3e38f, active ? cx : -3e38f, active ? cy : 3e38f,
-                    active ? cy : -3e38f, active ? cz : 3e38f, active ? cz : -3e38f};
-      float b[6] = {active1 ? bx : 3e38f, active1 ? bx : -3e38f, active1 ? by : 3e38f,
-                    active1 ? by : -3e38f, active1 ? bz : 3e38f, active1 ? bz : -3e38f};
-#pragma unroll
-      for (int o = 2; o > 0; o >>= 1)
-#pragma unroll
-        for (int c = 0; c < 6; c += 2) {
-          a[c] = fminf(a[c], __shfl_xor_sync(0xffffffffu, a[c], o));
-          a[c + 1] = fmaxf(a[c + 1], __shfl_xor_sync(0xffffffffu, a[c + 1], o));
-          b[c] = fminf(b[c], __shfl_xor_sync(0xffffffffu, b[c], o));
-          b[c + 1] = fmaxf(b[c + 1], __shfl_xor_sync(0xffffffffu, b[c + 1], o));
-        }
-      const int sg = lane >> 1, src = (sg & 7) << 2;
-      float m[6];
-#pragma unroll
-      for (int c = 0; c < 6; c++) {
-        const float va = __shfl_sync(0xffffffffu, a[c], src), vb = __shfl_sync(0xffffffffu, b[c], src);
-        m[c] = sg < 8 ? va : vb;
-      }
-      slx = m[0]; shx = m[1]; sly = m[2]; shy = m[3]; slz = m[4]; shz = m[5];
-    }
     const unsigned r0 = nchunk * RN_CHUNK, r1 = any_active ? min(total, r0 + RN_CHUNK) : r0;
     const unsigned lt = (1u << lane) - 1u;
     double sum = 0.0, sum1 = 0.0;
     unsigned visits = 0, slots = 0, loaded = 0;
     // tile of 32 kept records: the pair tests of every candidate lane
-    float ub = 0.f;  // BOUND: this lane's share of its sub-group's near-record bound
     float uf = 0.f;  // BOUND: this lane's far records
     const float e2b = (float)K.eps2;
     auto consume = [&](unsigned nt) {
-      if (BOUND) {
-        __syncwarp();
-        for (unsigned j = (unsigned)lane & 1u; j < nt; j += 2u) {
-          const float4 rec = make_float4(s_tile[w].x[j], s_tile[w].y[j], s_tile[w].z[j], 0.f);
-          const float ex = fmaxf(fmaxf(slx - rec.x, rec.x - shx), 0.f), ey = fmaxf(fmaxf(sly - rec.y, rec.y - shy), 0.f),
-                      ez = fmaxf(fmaxf(slz - rec.z, rec.z - shz), 0.f);
-          const float db2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-          if (db2 <= 1.0001f) ub += rsqrt_pos(db2 + e2b);
-        }
-        __syncwarp();
-        return;
-      }
       // pad to a multiple of 8 with records far from every candidate
       if ((unsigned)lane < ((8u - (nt & 7u)) & 7u)) {
         s_tile[w].x[nt + lane] = 1e18f;
@@ -1654,10 +1610,11 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
       const unsigned run_end = min(s_rp[w][r + 1], r1);
       const unsigned base = s_rb[w][r] - s_rp[w][r];  // cube slot = base + record number
       // SD steps of 32 records per pass: each lane issues its SD loads
-      // before the first is used.  The bound pass has little arithmetic to
-      // hide their latency behind; the pair pass is bound by instruction
-      // issue and runs best with one (measured at 1024^3).
-      constexpr int SD = BOUND ? 4 : 1;
+      // before the first is used.  Both passes run best with one (measured
+      // at 1024^3: with its exact near-field tiles the bound pass needs the
+      // registers more than the loads in flight; four took it from 325 to
+      // 603 ms through spills).
+      constexpr int SD = 1;
       for (unsigned xs0 = pos; xs0 < run_end; xs0 += 32u * SD) {
         float4 vs[SD];
 #pragma unroll
@@ -1713,26 +1670,24 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
       }
       pos = run_end;
     }
-    if (BOUND) {
-      if (fill > 0) consume(fill);
-      for (int sh = 16; sh > 0; sh >>= 1) uf += __shfl_xor_sync(0xffffffffu, uf, sh);
-      ub += __shfl_xor_sync(0xffffffffu, ub, 1);
-      ub += uf;
-      if (!wf) ub = __int_as_float(0x7f800000);
-      if ((lane & 1) == 0 && any_active) {
-        // the particle the run scan files under another cell may add up to
-        // 1/eps = 64 to any candidate's sum outside these runs
-        atomicAdd(&B.g_u[grp * NSUB + (unsigned)(lane >> 1)],
-                  ub * 1.001f + ((K.has_quirk && nchunk == 0) ? 64.f : 0.f));
-      }
-      continue;
-    }
     if (fill > 0) consume(fill);
+    if (BOUND) {
+      for (int sh = 16; sh > 0; sh >>= 1) uf += __shfl_xor_sync(0xffffffffu, uf, sh);
+      // the particle the run scan files under another cell may add up to
+      // 1/eps = 64 to any candidate's sum outside these runs; a candidate
+      // that is the run scan's own quirk particle gets no bound (it always
+      // stays in the exact pass), nor do items near the periodic edge
+      const float extra = (K.has_quirk && nchunk == 0) ? 64.f : 0.f;
+      const float inf = __int_as_float(0x7f800000);
+      if (have) atomicAdd(&B.cand_u[q], (wf && !quirk) ? (float)((sum + (double)uf) * 1.001) + extra : inf);
+      if (have1) atomicAdd(&B.cand_u[q1], (wf && !quirk1) ? (float)((sum1 + (double)uf) * 1.001) + extra : inf);
+    }
     if (lane == 0) {
       s_count[w][0] += visits;
       s_count[w][1] += slots;
       s_count[w][2] += loaded;
     }
+    if (BOUND) continue;
     if (nchunk == 0 && K.has_quirk && (active || active1)) {
       // the particle the run scan files under another cell: counted if that
       // cell is in x_sel2 but outside this candidate cell's 27 neighbours
@@ -2801,7 +2756,7 @@ __global__ void k_seed_lower(SodConst K, SodBufs B) {
   if ((threadIdx.x & 31) == 0) atomicMax(&B.s_lmax[slot], __float_as_uint((float)(sf * 0.999)));
 }
 
-// The group holding the sub-group with the largest finite upper bound, per
+// The group holding the candidate with the largest finite upper bound, per
 // bounded seed (warp per seed).  Its candidates are the likeliest to hold
 // the maximum, so their sums, computed before all others, give a lower bound
 // close to it.  Also the group's item range for the phase-1 pass.
@@ -2812,12 +2767,14 @@ __global__ void k_top_group(SodConst K, SodBufs B) {
   float bu = -1.f;
   unsigned best = 0xffffffffu;
   if (B.bound_on && B.st_cn[slot] >= B.bound_min) {
-    const unsigned g0 = B.group_pref[slot * 27u] * NSUB, g1 = B.group_pref[slot * 27u + 27u] * NSUB;
-    for (unsigned si = g0 + (unsigned)lane; si < g1; si += 32u) {
-      const float u = B.g_u[si];
-      if (u <= 3e38f && u > bu) {  // an infinite bound (item near the periodic edge) says nothing
-        bu = u;
-        best = si / NSUB;
+    for (unsigned ci = slot * 27u; ci < slot * 27u + 27u; ci++) {
+      const unsigned cnt = B.cell_cnt[ci], off = B.cell_off[ci], gp = B.group_pref[ci];
+      for (unsigned k = (unsigned)lane; k < cnt; k += 32u) {
+        const float u = B.cand_u[off + k];
+        if (u <= 3e38f && u > bu) {  // an infinite bound (item near the periodic edge) says nothing
+          bu = u;
+          best = gp + k / 64u;
+        }
       }
     }
   }
@@ -2866,7 +2823,7 @@ __global__ void k_top_lower(SodConst K, SodBufs B) {
 
 // The candidates the second pair pass must still sum (warp per candidate
 // cell, stable): all of an unbounded seed's; of a bounded seed's, those
-// outside the top group whose sub-group bound reaches the seed's lower
+// outside the top group whose own bound reaches the seed's lower
 // bound.  Their positions go to cand_list at the cell's candidate offset;
 // the cell's phase-2 item count follows from their number.
 __global__ void k_survivors(SodConst K, SodBufs B) {
@@ -2883,7 +2840,7 @@ __global__ void k_survivors(SodConst K, SodBufs B) {
     bool keep = k < cnt;
     if (keep && bounded) {
       const unsigned grp = gp + k / 64u;
-      keep = grp != top && B.g_u[grp * NSUB + (k % 64u) / SUBG] >= lmax;
+      keep = grp != top && B.cand_u[off + k] >= lmax;
       gone += (!keep && grp != top) ? 1u : 0u;
     }
     const unsigned m = __ballot_sync(0xffffffffu, keep);
@@ -2898,9 +2855,9 @@ __global__ void k_survivors(SodConst K, SodBufs B) {
   }
 }
 
-// zero the per-sub-group bounds of this round (group count on the device)
-__global__ void k_zero_groups(const unsigned *total, float *u) {
-  const unsigned n = *total * NSUB;
+// zero the per-candidate bounds of this round (candidate count on the device)
+__global__ void k_zero_bounds(const unsigned *used, unsigned long long cap, float *u) {
+  const unsigned n = (unsigned)min((unsigned long long)*used, cap);
   for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) u[i] = 0.f;
 }
 
@@ -3794,13 +3751,12 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     return rc;
   unsigned *cell_nch;
   if ((rc = scratch(c, SC_CELLNCH, (size_t)cap_ready * 27, &cell_nch))) return rc;
-  // refinement bound groups: at most cand_cap/64 + 27 per ready seed
-  const size_t gcap = (size_t)cand_cap / 64 + (size_t)cap_ready * 27 + 1;
+  // refinement bound groups (64 candidates) and the per-candidate bounds
   unsigned *cell_groups, *group_pref, *s_lmax, *cand_list, *cnt2;
-  float *g_u;
+  float *cand_u;
   if ((rc = scratch(c, SC_CELLGROUPS, (size_t)cap_ready * 27, &cell_groups)) ||
       (rc = scratch(c, SC_GROUPPREF, (size_t)cap_ready * 27 + 1, &group_pref)) ||
-      (rc = scratch(c, SC_GU, gcap * NSUB, &g_u)) || (rc = scratch(c, SC_CANDLIST, (size_t)cand_cap, &cand_list)) ||
+      (rc = scratch(c, SC_GU, (size_t)cand_cap, &cand_u)) || (rc = scratch(c, SC_CANDLIST, (size_t)cand_cap, &cand_list)) ||
       (rc = scratch(c, SC_CNT2, (size_t)cap_ready * 27 * 3 + 1, &cnt2)) ||
       (rc = scratch(c, SC_LMAX, (size_t)cap_ready, &s_lmax)))
     return rc;
@@ -3948,7 +3904,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   B.cross_records = u64s + 13;
   B.cell_groups = cell_groups;
   B.group_pref = group_pref;
-  B.g_u = g_u;
+  B.cand_u = cand_u;
   B.s_lmax = s_lmax;
   B.cand_list = cand_list;
   B.cnt2 = cnt2;
@@ -4100,7 +4056,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
     if (B.bound_on) {
       if ((rc = scan_u32(c, cell_groups, group_pref, (long long)B.nitems_cells, true))) return rc;
       t_bound.start(c->stream);
-      k_zero_groups<<<ref_grid, 256, 0, c->stream>>>(group_pref + B.nitems_cells, g_u);
+      k_zero_bounds<<<ref_grid, 256, 0, c->stream>>>(cand_used, (unsigned long long)cand_cap, cand_u);
       PSOD_CUDA(c, cudaMemsetAsync(s_lmax, 0, sizeof(unsigned) * nready, c->stream));
       k_seed_lower<<<nblk((long long)nready * 32, 256), 256, 0, c->stream>>>(K, B);
       k_refine_warp<true><<<ref_grid, 256, 0, c->stream>>>(K, B);

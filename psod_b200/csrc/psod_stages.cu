@@ -243,6 +243,89 @@ __global__ void k_cell_scatter(const float4 *rec, long long n, const unsigned *c
   inv[__float_as_uint(r.w)] = slot;
 }
 
+// Dense sub-cells are then ordered by a finer Morton key inside the
+// sub-cell: 4, 8 or 16 bins per axis for sub-cells of at least 32, 128 or
+// 1024 records, so a bin holds about one record and 64 consecutive records
+// of a dense cell span a box a few bins wide.  This is what lets the
+// refinement's group boxes stay small in halo cores (tens of thousands of
+// particles per cell), where the 4x4x4 order alone leaves a 64-record group
+// spread over a whole sub-cell.  Like the sub-cell order it changes no
+// output.
+constexpr unsigned FINE_MIN = 32, FINE_BINS_MAX = 4096;
+
+__device__ __forceinline__ unsigned fine_axis(float xg, double xs, int bits) {
+  const double d = dsub((double)xg, xs);
+  const int q = (int)(dsub(d, floor(d)) * (double)(4 << bits));
+  return (unsigned)q & ((1u << bits) - 1u);
+}
+
+__device__ __forceinline__ unsigned fine_key(const float4 &p, float nxf, double xs, int bits) {
+  const unsigned a = fine_axis(to_grid(p.x, nxf), xs, bits), b = fine_axis(to_grid(p.y, nxf), xs, bits),
+                 c = fine_axis(to_grid(p.z, nxf), xs, bits);
+  unsigned k = 0;
+  for (int j = 0; j < bits; j++)
+    k |= (((a >> j) & 1u) << (3 * j)) | (((b >> j) & 1u) << (3 * j + 1)) | (((c >> j) & 1u) << (3 * j + 2));
+  return k;
+}
+
+// one CTA per dense cell, its 64 sub-cells in turn: a counting sort of each
+// sub-cell of FINE_MIN or more records by its fine key, through tmp (the
+// same slots of a spare record array), then back into the cube with inv
+// updated.  tab holds the sub-cells' end slots (the scatter's cursors).
+__global__ void __launch_bounds__(256) k_sub_fine(float4 *cube, unsigned *inv, float4 *tmp, const unsigned *tab,
+                                                  const unsigned *bigcell, const unsigned *start, float nxf,
+                                                  double xs) {
+  __shared__ unsigned hist[FINE_BINS_MAX];
+  __shared__ unsigned wtot[8];
+  const unsigned b = blockIdx.x;
+  const unsigned *t = tab + (unsigned long long)b * SUB_N;
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  unsigned a = start[bigcell[b]];
+  for (unsigned s = 0; s < SUB_N; s++) {
+    const unsigned e = t[s], m = e - a;
+    if (m >= FINE_MIN) {
+      const int bits = m >= 1024u ? 4 : (m >= 128u ? 3 : 2);
+      const unsigned nb = 1u << (3 * bits), per = (nb + 255u) / 256u;  // nb <= 4096: per <= 16
+      for (unsigned i = tid; i < nb; i += 256u) hist[i] = 0u;
+      __syncthreads();
+      for (unsigned i = a + tid; i < e; i += 256u) atomicAdd(&hist[fine_key(cube[i], nxf, xs, bits)], 1u);
+      __syncthreads();
+      // exclusive scan: thread tid owns bins [tid*per, tid*per + per)
+      const unsigned lo = min(nb, (unsigned)tid * per), hi = min(nb, lo + per);
+      unsigned own = 0;
+      for (unsigned i = lo; i < hi; i++) own += hist[i];
+      unsigned x = own;
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      if (lane == 31) wtot[wid] = x;
+      __syncthreads();
+      unsigned wbase = 0;
+      for (int q = 0; q < wid; q++) wbase += wtot[q];
+      unsigned run = wbase + x - own;
+      for (unsigned i = lo; i < hi; i++) {
+        const unsigned h = hist[i];
+        hist[i] = run;
+        run += h;
+      }
+      __syncthreads();
+      for (unsigned i = a + tid; i < e; i += 256u) {
+        const float4 v = cube[i];
+        tmp[a + atomicAdd(&hist[fine_key(v, nxf, xs, bits)], 1u)] = v;
+      }
+      __syncthreads();
+      for (unsigned i = a + tid; i < e; i += 256u) {
+        const float4 v = tmp[i];
+        cube[i] = v;
+        inv[__float_as_uint(v.w)] = i;
+      }
+      __syncthreads();
+    }
+    a = e;
+  }
+}
+
 __global__ void k_set_range(unsigned *a, unsigned long long lo, unsigned long long hi, unsigned v) {
   unsigned long long i = lo + (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < hi) a[i] = v;
@@ -664,6 +747,9 @@ int stage_cellsort(psod_ctx *c, const float *dpos) {
     }
     k_cell_scatter<<<nblk(n, 256), 256, 0, c->stream>>>(rec, n, cell, count, tab, (float)nx, xs, c->d_cube,
                                                         c->d_inv);
+    // rec is free once the scatter has read it
+    if (hnbig)
+      k_sub_fine<<<hnbig, 256, 0, c->stream>>>(c->d_cube, c->d_inv, rec, tab, bigcell, c->d_cell_start, (float)nx, xs);
     PSOD_CUDA(c, cudaGetLastError());
     PSOD_CUDA(c, cudaStreamSynchronize(c->stream));
   }
