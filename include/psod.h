@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define PSOD_ABI_VERSION 3
+#define PSOD_ABI_VERSION 4
 #define PSOD_MAX_EXTRA_DELTA 4
 
 typedef enum psod_status {
@@ -82,6 +82,20 @@ typedef struct psod_params {
   double delta_extra[PSOD_MAX_EXTRA_DELTA]; /* N and R for each, same rule */
   int32_t mode;        /* psod_mode */
   int32_t device;      /* CUDA device ordinal */
+  /* Zone decomposition (main:321-441): the box is cut into nxcpu^3 zones
+   * and this context analyses zone nzone (0-based, z fastest: nzone =
+   * iz + nxcpu*(iy + nxcpu*ix), main:344-346) with its buffer of nxbuffer
+   * cells (0 means nxzone/2, nxzone = nx/nxcpu).  The caller loads the
+   * zone's particles with their buffer (main:573-600, or
+   * psod_read_cube_zone); halos are kept only when their centre lies in
+   * the zone (main:2118-2120).  nxcpu = 1 (default) is the one-rank box.
+   * nx must be a multiple of nxcpu, and for nxcpu > 1 the zone with its
+   * buffer must either span at least the box (nxzone + 2*nxbuffer >= nx)
+   * or leave max(ncut, 2) cells outside it: between the two the
+   * reference's linked-list walk would wrap into the far side of its local
+   * grid, which is refused.  0 (left unset) reads as 1. */
+  int32_t nxcpu;
+  int32_t nzone;
 } psod_params;
 
 /* Halo table.  The caller provides the arrays it wants (NULL = skip), sized
@@ -237,6 +251,16 @@ int psod_write_strct(const char *path, const psod_halo_table *t, int64_t nhalo, 
  * malformed file, PSOD_ERR_ARG for bad arguments or a short capacity. */
 int psod_read_cube_zone(const char *root, int32_t ncpu, int32_t nzone, int32_t nx, int32_t nxbuffer, int32_t id_bytes,
                         int64_t capacity, int64_t *npart, float *pos, float *vel, int64_t *id);
+
+/* The driver's selection of one zone's particles with their buffer
+ * (main:573-600, the FP64 test of main:578-584): keep[i] = 1 when particle
+ * i (pos: xyz-interleaved float32, box units) lies in zone nzone of
+ * nxcpu^3 (the numbering of psod_params) or within nxbuffer cells of it
+ * (0 means nxzone/2), periodically; *nkeep gets their count.  Host code,
+ * no device.  The selected particles, in input order, are what a zone
+ * context (psod_params.nxcpu > 1) is loaded with. */
+int psod_select_zone(int32_t nx, int32_t nxcpu, int32_t nzone, int32_t nxbuffer, const float *pos, int64_t n,
+                     uint8_t *keep, int64_t *nkeep);
 
 /* CIC density (cic + cicm1, the same fixed-point arithmetic) for a zone of
  * at most 64 cells per side, without any device allocation.  This entry

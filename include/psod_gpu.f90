@@ -31,6 +31,8 @@ module psod_gpu
      real(c_double)     :: delta_extra(4)
      integer(c_int32_t) :: mode
      integer(c_int32_t) :: device
+     integer(c_int32_t) :: nxcpu
+     integer(c_int32_t) :: nzone
   end type psod_params
 
   type, bind(C) :: psod_halo_table
@@ -208,6 +210,17 @@ module psod_gpu
        integer(c_int64_t), value :: capacity
        integer(c_int64_t), intent(out) :: npart
        type(c_ptr), value :: pos, vel, id
+     end function
+     ! the driver's zone selection (main:573-600): keep(i) = 1 for the
+     ! zone's particles with their buffer
+     integer(c_int) function psod_select_zone(nx, nxcpu, nzone, nxbuffer, pos, n, keep, nkeep) &
+          bind(C, name="psod_select_zone")
+       import :: c_int, c_int32_t, c_int64_t, c_ptr
+       integer(c_int32_t), value :: nx, nxcpu, nzone, nxbuffer
+       type(c_ptr), value :: pos
+       integer(c_int64_t), value :: n
+       type(c_ptr), value :: keep
+       integer(c_int64_t), intent(out) :: nkeep
      end function
      ! friends-of-friends on the loaded particles (replaces fofpara's local
      ! scan, mergehaloes, gatherhaloes, selecthaloes, computecom and

@@ -42,6 +42,8 @@ class _Params(C.Structure):
         ("ndelta_extra", C.c_int32),
         ("delta_extra", C.c_double * MAX_EXTRA),
         ("npart_total", C.c_int64),
+        ("nxcpu", C.c_int32),
+        ("nzone", C.c_int32),
     ]
 
 
@@ -127,6 +129,8 @@ class Params:
     rbin_hi: float = 1.0
     delta_extra: tuple = ()
     npart_total: int = 0
+    nxcpu: int = 1  # zones per axis (nxcpu^3 zones, main:340-342)
+    nzone: int = 0  # zone analysed, z fastest (main:344-346)
 
     def c(self, n: int) -> _Params:
         p = _Params()
@@ -144,6 +148,8 @@ class Params:
         for i, d in enumerate(self.delta_extra):
             p.delta_extra[i] = d
         p.npart_total = self.npart_total if self.npart_total > 0 else n
+        p.nxcpu = self.nxcpu
+        p.nzone = self.nzone
         return p
 
 
@@ -249,8 +255,32 @@ def _collect(res: _Result, params: Params) -> Result:
     return out
 
 
+def zone_select(pos, nx: int, nxcpu: int, nzone: int, nxbuffer: int = 0) -> np.ndarray:
+    """The driver's selection of zone ``nzone``'s particles with their
+    buffer (main:573-600): zone indices as main:344-346, centre as
+    main:428-430, half-widths rxsmall/rxlarge as main:433-439, and on every
+    axis |x - xc| < rxsmall or > rxlarge in FP64 (main:578-584)."""
+    p = np.asarray(pos, dtype=np.float32).reshape(-1, 3).astype(np.float64)
+    ncpu = nxcpu
+    ix = int(nzone / float(ncpu * ncpu))
+    iy = int((nzone - ix * ncpu * ncpu) / float(ncpu))
+    iz = nzone - ix * ncpu * ncpu - iy * ncpu
+    nxzone = nx // ncpu
+    nxb = nxbuffer if nxbuffer != 0 else nxzone // 2
+    keep = np.ones(p.shape[0], dtype=bool)
+    for a, i in enumerate((ix, iy, iz)):
+        lo, hi = i / float(ncpu), (i + 1) / float(ncpu)
+        xc = (lo + hi) / 2.0
+        rs = (0.5 + nxb / float(nxzone)) / float(ncpu)
+        rl = 1.0 - rs
+        d = np.abs(p[:, a] - xc)
+        keep &= (d < rs) | (d > rl)
+    return keep
+
+
 def run(params: Params, pos, ids, mode=REFERENCE) -> Result:
-    """cic -> cicm1 -> tri_cic -> spherover, one rank, one zone."""
+    """cic -> cicm1 -> tri_cic -> spherover for one zone (``params.nxcpu``,
+    ``params.nzone``; the whole box by default) on the particles given."""
     p = _as_pos(pos)
     i = _as_ids(ids)
     cp = params.c(p.shape[0])

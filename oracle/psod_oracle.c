@@ -132,14 +132,16 @@ static void sort_with_order(double *list, int64_t *order, int64_t n, int mode,
 }
 
 /* ------------------------------------------------------------------ */
-/* 1-rank zone geometry (main:321-441, 665-668, 689-698, 738-739).     */
+/* Zone geometry (main:321-441, 665-668, 689-698, 738-739): zone nzone  */
+/* of nxcpu^3, with its buffer.                                        */
 /* ------------------------------------------------------------------ */
 typedef struct {
   int32_t nx;       /* grid cells per side */
-  int32_t nxzone;   /* nx / nxcpu, nxcpu = 1 */
+  int32_t nxcpu;    /* zones per axis */
+  int32_t nxzone;   /* nx / nxcpu */
   int32_t nxbuffer; /* resolved buffer */
-  double xmin, xmax; /* zone + buffer, box units (same on y and z) */
-  double xminzone, xmaxzone; /* utile zone, grid units (after *scale) */
+  double xmin[3], xmax[3]; /* zone + buffer per axis, box units */
+  double xminzone[3], xmaxzone[3]; /* utile zone per axis, grid units (after *scale) */
   int64_t local_nx; /* spherover's local_nx = nxzone + 2*nxbuffer */
   int32_t nxcic;    /* 2*nx */
   double scale;     /* nx */
@@ -151,22 +153,40 @@ static int zone_setup(const psod_oracle_params *p, zone_t *z) {
   if (p->nx < 5 || p->ncut < 1 || 2 * p->ncut + 1 > p->nx || p->nmin < 10 ||
       p->nbins < 1 || p->nsel < 1 || p->npart_total < 1)
     return PSOD_ORACLE_ERR_ARG;
+  const int32_t ncpu = p->nxcpu <= 0 ? 1 : p->nxcpu;
+  if (p->nx % ncpu != 0 || p->nzone < 0 || (int64_t)p->nzone >= (int64_t)ncpu * ncpu * ncpu)
+    return PSOD_ORACLE_ERR_ARG;
   z->nx = p->nx;
-  z->nxzone = p->nx; /* nxzone = nx/nxcpu, main:349 */
+  z->nxcpu = ncpu;
+  z->nxzone = p->nx / ncpu; /* main:349 */
   z->nxbuffer = p->nxbuffer;
   if (z->nxbuffer == 0) z->nxbuffer = z->nxzone / 2; /* main:380-381 */
   if (z->nxbuffer < p->ncut) return PSOD_ORACLE_ERR_ARG;     /* main:386 */
-  /* main:392 allows nxbuffer == nxzone; the CIC indices of the last half
-   * cell then land in the reference's padding past the periodic grid, which
-   * is not restated here */
-  if (z->nxbuffer >= z->nxzone) return PSOD_ORACLE_ERR_ARG;
-  /* main:401-402 with ixzone = 0, nxcpu = 1 */
+  if (ncpu == 1) {
+    /* main:392 allows nxbuffer == nxzone; the CIC indices of the last half
+     * cell then land in the reference's padding past the periodic grid,
+     * which is not restated here */
+    if (z->nxbuffer >= z->nxzone) return PSOD_ORACLE_ERR_ARG;
+  } else {
+    if (z->nxbuffer > z->nxzone) return PSOD_ORACLE_ERR_ARG; /* main:392 */
+    /* a local grid shorter than the box by fewer than max(ncut, 2) cells
+     * would let the wrapped cell walks land on its far side (refused, as
+     * by the library) */
+    const int64_t local = (int64_t)z->nxzone + 2 * (int64_t)z->nxbuffer;
+    const int32_t reach = p->ncut > 2 ? p->ncut : 2;
+    if (local < p->nx && local > p->nx - reach) return PSOD_ORACLE_ERR_ARG;
+  }
+  /* zone indices, main:344-346 */
+  const int32_t iz3[3] = {p->nzone / (ncpu * ncpu), (p->nzone - (p->nzone / (ncpu * ncpu)) * ncpu * ncpu) / ncpu,
+                          p->nzone % ncpu};
   double q = (double)z->nxbuffer / (double)z->nxzone;
-  z->xmin = (0.0 - q) / 1.0;
-  z->xmax = (0.0 + 1.0 + q) / 1.0;
   z->scale = (double)p->nx;                 /* main:689 */
-  z->xminzone = (0.0 / 1.0) * z->scale;     /* main:420, 691 */
-  z->xmaxzone = (1.0 / 1.0) * z->scale;     /* main:421, 692 */
+  for (int a = 0; a < 3; a++) {
+    z->xmin[a] = ((double)iz3[a] - q) / (double)ncpu;       /* main:401 */
+    z->xmax[a] = ((double)iz3[a] + 1.0 + q) / (double)ncpu; /* main:402 */
+    z->xminzone[a] = ((double)iz3[a] / (double)ncpu) * z->scale;         /* main:420, 691 */
+    z->xmaxzone[a] = (((double)iz3[a] + 1.0) / (double)ncpu) * z->scale; /* main:421, 692 */
+  }
   z->local_nx = (int64_t)z->nxzone + 2 * (int64_t)z->nxbuffer; /* main:739 */
   z->nxcic = 2 * p->nx;                     /* main:667 */
   z->mpf = (float)(1.0 / (double)p->npart_total);              /* main:662 */
@@ -212,7 +232,7 @@ int psod_oracle_cic(const psod_oracle_params *p, int64_t n, const float *pos,
   const int64_t nc = z.nxcic;
   const int64_t nnode = nc * nc * nc;
   const double dx = 1.0 / (double)nc; /* main:1126 */
-  const double xxmin = z.xmin;        /* main:665 */
+  const double *xxmin = z.xmin;       /* main:665 */
   int64_t *fix = NULL;
   if (mode == PSOD_ORACLE_CANONICAL) {
     fix = (int64_t *)calloc((size_t)nnode, sizeof(int64_t));
@@ -223,15 +243,15 @@ int psod_oracle_cic(const psod_oracle_params *p, int64_t n, const float *pos,
   const double mpf = (double)z.mpf;
   for (int64_t i = 0; i < n; i++) {
     const float *x = pos + 3 * i;
-    if (!(in_zone_periodic(x[0], z.xmin, z.xmax) &&
-          in_zone_periodic(x[1], z.xmin, z.xmax) &&
-          in_zone_periodic(x[2], z.xmin, z.xmax)))
+    if (!(in_zone_periodic(x[0], z.xmin[0], z.xmax[0]) &&
+          in_zone_periodic(x[1], z.xmin[1], z.xmax[1]) &&
+          in_zone_periodic(x[2], z.xmin[2], z.xmax[2])))
       continue;
     int32_t ix, ixp, iy, iyp, iz, izp;
     double ddx, dex, ddy, dey, ddz, dez;
-    if (!cic_axis(x[0], xxmin, dx, (int32_t)nc, &ix, &ixp, &ddx, &dex) ||
-        !cic_axis(x[1], xxmin, dx, (int32_t)nc, &iy, &iyp, &ddy, &dey) ||
-        !cic_axis(x[2], xxmin, dx, (int32_t)nc, &iz, &izp, &ddz, &dez)) {
+    if (!cic_axis(x[0], xxmin[0], dx, (int32_t)nc, &ix, &ixp, &ddx, &dex) ||
+        !cic_axis(x[1], xxmin[1], dx, (int32_t)nc, &iy, &iyp, &ddy, &dey) ||
+        !cic_axis(x[2], xxmin[2], dx, (int32_t)nc, &iz, &izp, &ddz, &dez)) {
       free(fix);
       return PSOD_ORACLE_ERR_ARG;
     }
@@ -273,19 +293,19 @@ int psod_oracle_cicm1(const psod_oracle_params *p, int64_t n,
   if (st) return st;
   const int64_t nc = z.nxcic;
   const double dx = 1.0 / (double)nc;
-  const double xxmin = z.xmin;
+  const double *xxmin = z.xmin;
   for (int64_t i = 0; i < n; i++) {
     const float *x = pos + 3 * i;
     rho[i] = 0.0;
-    if (!(in_zone_periodic(x[0], z.xmin, z.xmax) &&
-          in_zone_periodic(x[1], z.xmin, z.xmax) &&
-          in_zone_periodic(x[2], z.xmin, z.xmax)))
+    if (!(in_zone_periodic(x[0], z.xmin[0], z.xmax[0]) &&
+          in_zone_periodic(x[1], z.xmin[1], z.xmax[1]) &&
+          in_zone_periodic(x[2], z.xmin[2], z.xmax[2])))
       continue;
     int32_t ix, ixp, iy, iyp, iz, izp;
     double ddx, dex, ddy, dey, ddz, dez;
-    if (!cic_axis(x[0], xxmin, dx, (int32_t)nc, &ix, &ixp, &ddx, &dex) ||
-        !cic_axis(x[1], xxmin, dx, (int32_t)nc, &iy, &iyp, &ddy, &dey) ||
-        !cic_axis(x[2], xxmin, dx, (int32_t)nc, &iz, &izp, &ddz, &dez))
+    if (!cic_axis(x[0], xxmin[0], dx, (int32_t)nc, &ix, &ixp, &ddx, &dex) ||
+        !cic_axis(x[1], xxmin[1], dx, (int32_t)nc, &iy, &iyp, &ddy, &dey) ||
+        !cic_axis(x[2], xxmin[2], dx, (int32_t)nc, &iz, &izp, &ddz, &dez))
       return PSOD_ORACLE_ERR_ARG;
     const int32_t cx[8] = {ix, ixp, ix, ixp, ix, ixp, ix, ixp};
     const int32_t cy[8] = {iy, iy, iyp, iyp, iy, iy, iyp, iyp};
@@ -394,10 +414,10 @@ static double cell_gap(double t0, int t, double nxd) {
   return fmax(d - 0.5, 0.0);
 }
 static int64_t ball_touch(const int64_t *num, int32_t nx, int32_t ncut, const int64_t c0[3], double xc,
-                          double yc, double zc, double xs, double rb) {
+                          double yc, double zc, const double xs[3], double rb) {
   const double nxd = (double)nx;
-  const double tx = cell_rel(xc, c0[0], xs, nxd), ty = cell_rel(yc, c0[1], xs, nxd),
-               tz = cell_rel(zc, c0[2], xs, nxd);
+  const double tx = cell_rel(xc, c0[0], xs[0], nxd), ty = cell_rel(yc, c0[1], xs[1], nxd),
+               tz = cell_rel(zc, c0[2], xs[2], nxd);
   const double rm2 = rb * rb;
   int64_t sum = 0;
   for (int dk = -ncut; dk <= ncut; dk++)
@@ -465,7 +485,8 @@ static int spherover_impl(const psod_oracle_params *p, int64_t n,
   }
   const int32_t nx = z.nx;
   const double scale = z.scale;
-  const double xxmin = z.xmin; /* main:738 */
+  const double *xxmin = z.xmin; /* main:738 */
+  const int64_t local_nx = z.local_nx; /* main:739 */
   const double Mmin = (double)p->nmin;
   const double munit = (double)z.munit;
   const double tx = (double)nx; /* taillex, main:1517 */
@@ -486,7 +507,7 @@ static int spherover_impl(const psod_oracle_params *p, int64_t n,
   for (int64_t i = 0; i < n; i++) {
     int64_t c3[3];
     for (int a = 0; a < 3; a++) {
-      int64_t ia = (int64_t)floor((double)pg[3 * i + a] - xxmin * scale);
+      int64_t ia = (int64_t)floor((double)pg[3 * i + a] - xxmin[a] * scale);
       if (ia < 0) ia = ia + nx;
       if (ia >= nx) ia = ia - nx;
       c3[a] = ia;
@@ -541,7 +562,7 @@ static int spherover_impl(const psod_oracle_params *p, int64_t n,
     {
       double xs[3] = {xc, yc, zc};
       for (int a = 0; a < 3; a++) { /* main:1644-1654 */
-        int64_t ia = (int64_t)floor(xs[a] - xxmin * scale);
+        int64_t ia = (int64_t)floor(xs[a] - xxmin[a] * scale);
         if (ia < 0) ia = ia + nx;
         if (ia >= nx) ia = ia - nx;
         c0[a] = ia;
@@ -554,14 +575,17 @@ static int spherover_impl(const psod_oracle_params *p, int64_t n,
       int64_t ii = di + c0[0];
       if (ii >= nx) ii -= nx;
       if (ii < 0) ii += nx;
+      if (ii >= local_nx) continue; /* outside the local grid */
       for (int dj = -p->ncut; dj <= p->ncut && !status; dj++) {
         int64_t jj = dj + c0[1];
         if (jj >= nx) jj -= nx;
         if (jj < 0) jj += nx;
+        if (jj >= local_nx) continue; /* outside the local grid */
         for (int dk = -p->ncut; dk <= p->ncut && !status; dk++) {
           int64_t kk = dk + c0[2];
           if (kk >= nx) kk -= nx;
           if (kk < 0) kk += nx;
+          if (kk >= local_nx) continue; /* outside the local grid */
           int64_t ind = ii + (int64_t)nx * (jj + (int64_t)nx * kk);
           for (int64_t ip = first[ind]; ip < first[ind] + num[ind]; ip++) {
             int64_t q = isort_ngp[ip];
@@ -586,14 +610,17 @@ static int spherover_impl(const psod_oracle_params *p, int64_t n,
       int64_t ii = di + c0[0];
       if (ii >= nx) ii -= nx;
       if (ii < 0) ii += nx;
+      if (ii >= local_nx) continue; /* outside the local grid */
       for (int dj = -2; dj <= 2; dj++) {
         int64_t jj = dj + c0[1];
         if (jj >= nx) jj -= nx;
         if (jj < 0) jj += nx;
+        if (jj >= local_nx) continue; /* outside the local grid */
         for (int dk = -2; dk <= 2; dk++) {
           int64_t kk = dk + c0[2];
           if (kk >= nx) kk -= nx;
           if (kk < 0) kk += nx;
+          if (kk >= local_nx) continue; /* outside the local grid */
           int64_t ind = ii + (int64_t)nx * (jj + (int64_t)nx * kk);
           for (int64_t ip = first[ind]; ip < first[ind] + num[ind]; ip++) {
             int64_t q = isort_ngp[ip];
@@ -617,14 +644,17 @@ static int spherover_impl(const psod_oracle_params *p, int64_t n,
         int64_t ii = di + c0[0];
         if (ii >= nx) ii -= nx;
         if (ii < 0) ii += nx;
+        if (ii >= local_nx) continue; /* outside the local grid */
         for (int dj = -1; dj <= 1; dj++) {
           int64_t jj = dj + c0[1];
           if (jj >= nx) jj -= nx;
           if (jj < 0) jj += nx;
+          if (jj >= local_nx) continue; /* outside the local grid */
           for (int dk = -1; dk <= 1; dk++) {
             int64_t kk = dk + c0[2];
             if (kk >= nx) kk -= nx;
             if (kk < 0) kk += nx;
+            if (kk >= local_nx) continue; /* outside the local grid */
             int64_t ind = ii + (int64_t)nx * (jj + (int64_t)nx * kk);
             for (int64_t ip = first[ind]; ip < first[ind] + num[ind]; ip++) {
               int64_t q = isort_ngp[ip];
@@ -722,7 +752,10 @@ static int spherover_impl(const psod_oracle_params *p, int64_t n,
     }
     /* algorithmic reads: the cells meeting the ball out to the stopping
      * particle (the i-th, 1-based) */
-    res->cross_touch += ball_touch(num, nx, p->ncut, c0, xc, yc, zc, xxmin * scale, sqrt(dist.v[i - 1]));
+    {
+      const double xs3[3] = {xxmin[0] * scale, xxmin[1] * scale, xxmin[2] * scale};
+      res->cross_touch += ball_touch(num, nx, p->ncut, c0, xc, yc, zc, xs3, sqrt(dist.v[i - 1]));
+    }
     const double amass = (double)masse * munit;
 
     /* profile edges and cumulative counts, main:2103-2115 */
@@ -737,9 +770,9 @@ static int spherover_impl(const psod_oracle_params *p, int64_t n,
     }
 
     /* keep test, main:2118-2120 */
-    const int keep = amass >= Mmin && xc <= z.xmaxzone && xc > z.xminzone &&
-                     yc <= z.xmaxzone && yc > z.xminzone &&
-                     zc <= z.xmaxzone && zc > z.xminzone;
+    const int keep = amass >= Mmin && xc <= z.xmaxzone[0] && xc > z.xminzone[0] &&
+                     yc <= z.xmaxzone[1] && yc > z.xminzone[1] &&
+                     zc <= z.xmaxzone[2] && zc > z.xminzone[2];
     if (keep) {
       vpush(&h_id, iamas);
       vpush(&h_mass, masse);

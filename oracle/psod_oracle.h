@@ -67,6 +67,8 @@ typedef struct psod_oracle_params {
   int32_t ndelta_extra;                          /* extra thresholds */
   double delta_extra[PSOD_ORACLE_MAX_EXTRA_DELTA];
   int64_t npart_total; /* nparttotal (mpf = 1/npart_total) */
+  int32_t nxcpu;     /* zones per axis (nxcpu^3 zones, main:340-342); 0 or 1: one zone */
+  int32_t nzone;     /* the zone analysed, z fastest (main:344-346) */
 } psod_oracle_params;
 
 typedef struct psod_oracle_result {

@@ -49,6 +49,8 @@ class Params(C.Structure):
         ("delta_extra", C.c_double * MAX_EXTRA),
         ("mode", C.c_int32),
         ("device", C.c_int32),
+        ("nxcpu", C.c_int32),
+        ("nzone", C.c_int32),
     ]
 
 
@@ -231,6 +233,7 @@ EXPORTS = [
     "psod_write_masst",
     "psod_write_strct",
     "psod_read_cube_zone",
+    "psod_select_zone",
     "psod_fof",
     "psod_fof_halo_count",
     "psod_fof_get_halos",
@@ -299,6 +302,7 @@ def load(build_if_missing: bool = True):
     L.psod_write_strct.argtypes = [C.c_char_p, P(HaloTable), C.c_int64, C.c_int64, vp, vp, vp, vp, vp]
     L.psod_read_cube_zone.argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int64,
                                       P(C.c_int64), vp, vp, vp]
+    L.psod_select_zone.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, vp, C.c_int64, vp, P(C.c_int64)]
     L.psod_fof.argtypes = [vp, P(FofParams), P(FofStats)]
     L.psod_fof_halo_count.argtypes = [vp, P(C.c_int64), P(C.c_int64)]
     L.psod_fof_get_halos.argtypes = [vp, P(FofTable)]

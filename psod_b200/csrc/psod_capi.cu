@@ -1,4 +1,5 @@
 // psod_capi.cu -- the extern "C" boundary of libpsod.so (include/psod.h).
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -120,6 +121,8 @@ void psod_params_default(psod_params *p) {
   p->ndelta_extra = 0;
   p->mode = PSOD_MODE_PLAIN;
   p->device = 0;
+  p->nxcpu = 1;  // one zone: the one-rank run
+  p->nzone = 0;
 }
 
 int psod_ctx_create(const psod_params *pin, psod_ctx **out) {
@@ -143,11 +146,27 @@ int psod_ctx_create(const psod_params *pin, psod_ctx **out) {
   else if (!(p.rbin_lo > 0.0) || !(p.rbin_hi > 0.0)) why = "profile edge factors must be positive";
   else if (p.ndelta_extra < 0 || p.ndelta_extra > PSOD_MAX_EXTRA_DELTA) why = "at most 4 extra thresholds";
   else if (!(p.delta > 0.0)) why = "delta must be positive";
-  int nxbuffer = p.nxbuffer == 0 ? p.nx / 2 : p.nxbuffer;  // main:380-381, nxzone = nx
+  if (p.nxcpu == 0) p.nxcpu = 1;
+  if (why.empty() && (p.nxcpu < 1 || p.nx % p.nxcpu != 0)) why = "nxcpu must be >= 1 and divide nx";
+  if (why.empty() && (p.nzone < 0 || (long long)p.nzone >= (long long)p.nxcpu * p.nxcpu * p.nxcpu))
+    why = "nzone must lie in [0, nxcpu^3)";
+  const int nxzone = why.empty() ? p.nx / p.nxcpu : 1;          // main:349
+  int nxbuffer = p.nxbuffer == 0 ? nxzone / 2 : p.nxbuffer;     // main:380-381
   if (why.empty() && nxbuffer < p.ncut) why = "nxbuffer must be >= ncut (main:386)";
-  // the reference allows nxbuffer == nx (main:392); its CIC array is then
-  // padded past the periodic grid, which this engine does not keep
-  if (why.empty() && nxbuffer >= p.nx) why = "nxbuffer must be < nx";
+  if (p.nxcpu == 1) {
+    // the reference allows nxbuffer == nx (main:392); its CIC array is then
+    // padded past the periodic grid, which this engine does not keep
+    if (why.empty() && nxbuffer >= p.nx) why = "nxbuffer must be < nx";
+  } else {
+    if (why.empty() && nxbuffer > nxzone) why = "nxbuffer must be <= nxzone (main:392)";
+    // the linked-list walks (main:1657-1675) wrap cell indices modulo nx
+    // and then skip those outside the local grid: unless the local grid
+    // spans the box or leaves max(ncut, 2) cells outside, a wrapped index
+    // lands on the far side of the local grid
+    const int local = nxzone + 2 * nxbuffer, reach = std::max(p.ncut, 2);
+    if (why.empty() && local < p.nx && local > p.nx - reach)
+      why = "the zone with its buffer must span the box or leave max(ncut, 2) cells outside";
+  }
   if (!why.empty()) {
     delete c;
     return PSOD_ERR_ARG;
@@ -156,9 +175,18 @@ int psod_ctx_create(const psod_params *pin, psod_ctx **out) {
   c->nxbuffer = nxbuffer;
   c->ncut = p.ncut;
   c->nsel = p.nsel;
-  // zone with buffer for one rank (main:401-402): (0 - nxb/nxzone)/nxcpu
-  const double q = (double)nxbuffer / (double)p.nx;
-  c->xxmin = (0.0 - q) / 1.0;
+  // zone indices (main:344-346) and the zone with its buffer (main:401-406)
+  // and without (main:420-425), box units
+  c->nxcpu = p.nxcpu;
+  const int ncpu = p.nxcpu;
+  const int izone[3] = {p.nzone / (ncpu * ncpu), (p.nzone / ncpu) % ncpu, p.nzone % ncpu};
+  const double q = (double)nxbuffer / (double)nxzone;
+  for (int a = 0; a < 3; a++) {
+    c->xxmin[a] = ((double)izone[a] - q) / (double)ncpu;
+    c->xxmax[a] = ((double)izone[a] + 1.0 + q) / (double)ncpu;
+    c->zone_lo[a] = (double)izone[a] / (double)ncpu;
+    c->zone_hi[a] = ((double)izone[a] + 1.0) / (double)ncpu;
+  }
   c->scale = (double)p.nx;  // main:689
   // profile edge factors with the host libm, as the reference evaluates
   // exp(log(lo) + (j-1)*(log(hi)-log(lo))/(nbins-1)) (main:2105)

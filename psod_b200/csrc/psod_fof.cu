@@ -860,6 +860,9 @@ extern "C" {
 int psod_fof(psod_ctx *c, const psod_fof_params *p, psod_fof_stats *stats) {
   if (!c || !p) return PSOD_ERR_ARG;
   if (!c->d_cube || c->n <= 0) return set_err(c, PSOD_ERR_STATE, "no particles: call psod_load_particles first");
+  // pFoF's own domain decomposition is not the SOD zones: the finder runs
+  // on a one-zone context (the whole periodic box)
+  if (c->nxcpu != 1) return set_err(c, PSOD_ERR_ARG, "psod_fof needs a one-zone context (nxcpu = 1)");
   cudaSetDevice(c->device);
   c->fof_done = false;
   const long long n = c->n;
@@ -880,7 +883,7 @@ int psod_fof(psod_ctx *c, const psod_fof_params *p, psod_fof_stats *stats) {
   FofGeo G;
   G.nx = c->nx;
   G.nxf = (float)c->nx;
-  G.xs = c->xxmin * c->scale;
+  G.xs = c->xxmin[0] * c->scale;  // one zone: the same on every axis
   G.k = k;
   G.R = R;
   G.reach2 = reach2;

@@ -160,3 +160,32 @@ extern "C" int psod_read_cube_zone(const char *root, int32_t ncpu, int32_t nzone
   *npart = count;
   return PSOD_OK;
 }
+
+// The driver's particle selection for one zone (main:573-600): the zone's
+// particles with their buffer, by the same FP64 test as the cube reader.
+extern "C" int psod_select_zone(int32_t nx, int32_t nxcpu, int32_t nzone, int32_t nxbuffer, const float *pos,
+                                int64_t n, uint8_t *keep, int64_t *nkeep) {
+  if (nx < 1 || nxcpu < 1 || nx % nxcpu != 0 || nzone < 0 || (int64_t)nzone >= (int64_t)nxcpu * nxcpu * nxcpu ||
+      nxbuffer < 0 || n < 0 || (n > 0 && (!pos || !keep)) || !nkeep)
+    return PSOD_ERR_ARG;
+  const int nxzone = nx / nxcpu;                          // main:350
+  const int nxb = nxbuffer == 0 ? nxzone / 2 : nxbuffer;  // main:380-381
+  if (nxb > nxzone) return PSOD_ERR_ARG;                  // main:392-397
+  // zone indices (main:344-346), centre and half-widths with buffer (main:421-439)
+  const int izone[3] = {nzone / (nxcpu * nxcpu), (nzone / nxcpu) % nxcpu, nzone % nxcpu};
+  ZoneSelect z;
+  for (int a = 0; a < 3; a++) {
+    const double lo = (double)izone[a] / (double)nxcpu, hi = (double)(izone[a] + 1) / (double)nxcpu;
+    z.xc[a] = (lo + hi) / 2.0;
+    z.rsmall[a] = (0.5 + (double)nxb / (double)nxzone) / (double)nxcpu;
+    z.rlarge[a] = 1.0 - z.rsmall[a];
+  }
+  int64_t count = 0;
+  for (int64_t i = 0; i < n; i++) {
+    const bool k = z.keep(pos + 3 * i);
+    keep[i] = k ? 1 : 0;
+    count += k ? 1 : 0;
+  }
+  *nkeep = count;
+  return PSOD_OK;
+}

@@ -90,7 +90,7 @@ struct SodConst {
   int nx;
   int ncut;
   float nxf;
-  double xs;        // xxmin*scale (grid units)
+  double xs[3];     // xxmin*scale per axis (grid units)
   double tx;        // taillex = nx (main:1517)
   double scale;     // nx
   double delta;     // seuil
@@ -101,7 +101,7 @@ struct SodConst {
   long long nsel;
   long long n_total;    // records in the zone
   unsigned mmin_count;  // smallest alive count reaching Mmin
-  double zmin, zmax; // utile zone in grid units (main:691-696)
+  double zmin[3], zmax[3]; // utile zone per axis in grid units (main:691-696)
   double eps2;      // (scale/nx/2**6)**2 (main:1527)
   double rmin2;     // (scale/nx)**2 (main:1526)
   int nbins;
@@ -128,7 +128,10 @@ struct psod_ctx {
   psod_params p;  // resolved parameters
   int nx = 0, nxbuffer = 0, ncut = 0;
   long long nsel = 0;
-  double xxmin = 0;  // zone-with-buffer lower edge, box units
+  double xxmin[3] = {0, 0, 0};  // zone-with-buffer lower edge per axis, box units
+  double xxmax[3] = {0, 0, 0};  // its upper edge
+  double zone_lo[3] = {0, 0, 0}, zone_hi[3] = {0, 0, 0};  // utile zone, box units
+  int nxcpu = 1;
   double scale = 0;
   float mpf = 0, munit = 0;
   int device = 0;

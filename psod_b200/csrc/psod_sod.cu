@@ -287,12 +287,12 @@ __device__ __forceinline__ void for_region(const SodConst &K, const SodBufs &B, 
   const unsigned nx = (unsigned)K.nx;
   const double nxd = (double)K.nx;
   // ball centre relative to the seed cell centre (cell i spans [i+xs, i+xs+1))
-  auto rel = [&](double x, int i) {
-    double d = x - ((double)i + K.xs + 0.5);
+  auto rel = [&](double x, int i, int a) {
+    double d = x - ((double)i + K.xs[a] + 0.5);
     d = d - nxd * floor(d / nxd + 0.5);
     return d;
   };
-  const double tx = rel(G.xc, G.ic), ty = rel(G.yc, G.jc), tz = rel(G.zc, G.kc);
+  const double tx = rel(G.xc, G.ic, 0), ty = rel(G.yc, G.jc, 1), tz = rel(G.zc, G.kc, 2);
   const double rm = G.rb + 1e-3;  // margin for rounding at cell edges
   const double rm2 = rm * rm;
   for (int row = w; row < nrow; row += NWARP) {
@@ -329,12 +329,12 @@ __device__ __forceinline__ unsigned region_records(const SodConst &K, const SodB
   const int R = K.ncut, side = 2 * R + 1, nrow = side * side;
   const unsigned nx = (unsigned)K.nx;
   const double nxd = (double)K.nx;
-  auto rel = [&](double x, int i) {
-    double d = x - ((double)i + K.xs + 0.5);
+  auto rel = [&](double x, int i, int a) {
+    double d = x - ((double)i + K.xs[a] + 0.5);
     d = d - nxd * floor(d / nxd + 0.5);
     return d;
   };
-  const double tx = rel(G.xc, G.ic), ty = rel(G.yc, G.jc), tz = rel(G.zc, G.kc);
+  const double tx = rel(G.xc, G.ic, 0), ty = rel(G.yc, G.jc, 1), tz = rel(G.zc, G.kc, 2);
   const double rm2 = G.rb * G.rb;
   unsigned sum = 0;
   for (int row = threadIdx.x; row < nrow; row += TPB) {
@@ -821,9 +821,9 @@ __device__ __forceinline__ SeedGeo seed_geo(const SodConst &K, const SodBufs &B,
   SeedGeo g;
   g.sp = B.inv[B.seed_idx[rank]];
   const float4 v = B.cube[g.sp];
-  g.ic = sod_cell_axis(to_grid(v.x, K.nxf), K.xs, K.nx);
-  g.jc = sod_cell_axis(to_grid(v.y, K.nxf), K.xs, K.nx);
-  g.kc = sod_cell_axis(to_grid(v.z, K.nxf), K.xs, K.nx);
+  g.ic = sod_cell_axis(to_grid(v.x, K.nxf), K.xs[0], K.nx);
+  g.jc = sod_cell_axis(to_grid(v.y, K.nxf), K.xs[1], K.nx);
+  g.kc = sod_cell_axis(to_grid(v.z, K.nxf), K.xs[2], K.nx);
   return g;
 }
 
@@ -1124,8 +1124,8 @@ __device__ __forceinline__ void refine_sum(const SodConst &K, const SodBufs &B, 
   const float4 cv = B.cube[cp];
   const float cxg = to_grid(cv.x, K.nxf), cyg = to_grid(cv.y, K.nxf), czg = to_grid(cv.z, K.nxf);
   const double cx = cxg, cy = cyg, cz = czg;
-  const int pcx = sod_cell_axis(cxg, K.xs, K.nx), pcy = sod_cell_axis(cyg, K.xs, K.nx),
-            pcz = sod_cell_axis(czg, K.xs, K.nx);
+  const int pcx = sod_cell_axis(cxg, K.xs[0], K.nx), pcy = sod_cell_axis(cyg, K.xs[1], K.nx),
+            pcz = sod_cell_axis(czg, K.xs[2], K.nx);
   const float e2f = (float)K.eps2;
   unsigned long long sq = 0;
   double sf = 0.0;
@@ -1533,12 +1533,12 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
       }
       if (lane == 0) {
         // the 3-cell coordinate window of each axis stays clear of the box edge
-        auto clear = [&](int c) {
-          double s0 = (double)(c - 1) + K.xs;
+        auto clear = [&](int c, int a) {
+          double s0 = (double)(c - 1) + K.xs[a];
           s0 -= K.tx * floor(s0 / K.tx);
           return s0 >= 1.0 && s0 + 3.0 <= K.tx - 1.0;
         };
-        s_wf[w] = clear(cxc) && clear(cyc) && clear(czc);
+        s_wf[w] = clear(cxc, 0) && clear(cyc, 1) && clear(czc, 2);
       }
     }
     __syncwarp();
@@ -1787,9 +1787,9 @@ __device__ __forceinline__ void select_seed(const SodConst &K, const SodBufs &B,
         ly = pdiff((int)((K.quirk_listed / K.nx) % K.nx), g.jc, K.nx);
         lz = pdiff((int)(K.quirk_listed / ((unsigned)K.nx * K.nx)), g.kc, K.nx);
       } else {
-        lx = pdiff(sod_cell_axis(to_grid(cv.x, K.nxf), K.xs, K.nx), g.ic, K.nx);
-        ly = pdiff(sod_cell_axis(to_grid(cv.y, K.nxf), K.xs, K.nx), g.jc, K.nx);
-        lz = pdiff(sod_cell_axis(to_grid(cv.z, K.nxf), K.xs, K.nx), g.kc, K.nx);
+        lx = pdiff(sod_cell_axis(to_grid(cv.x, K.nxf), K.xs[0], K.nx), g.ic, K.nx);
+        ly = pdiff(sod_cell_axis(to_grid(cv.y, K.nxf), K.xs[1], K.nx), g.jc, K.nx);
+        lz = pdiff(sod_cell_axis(to_grid(cv.z, K.nxf), K.xs[2], K.nx), g.kc, K.nx);
       }
       const unsigned o = (unsigned)(((lx + 1) * 3 + (ly + 1)) * 3 + (lz + 1));
       const unsigned long long key = ((unsigned long long)o << 32) | (cw & PSOD_IDX_MASK);
@@ -1964,9 +1964,9 @@ __device__ __forceinline__ unsigned count_alive_cube(const SodConst &K, const So
 // listed cell of a record for the alive-count bookkeeping
 __device__ __forceinline__ unsigned listed_cell(const SodConst &K, unsigned p, float4 v) {
   if (K.has_quirk && p == K.quirk_pos) return K.quirk_listed;
-  const unsigned i = (unsigned)sod_cell_axis(to_grid(v.x, K.nxf), K.xs, K.nx);
-  const unsigned j = (unsigned)sod_cell_axis(to_grid(v.y, K.nxf), K.xs, K.nx);
-  const unsigned k = (unsigned)sod_cell_axis(to_grid(v.z, K.nxf), K.xs, K.nx);
+  const unsigned i = (unsigned)sod_cell_axis(to_grid(v.x, K.nxf), K.xs[0], K.nx);
+  const unsigned j = (unsigned)sod_cell_axis(to_grid(v.y, K.nxf), K.xs[1], K.nx);
+  const unsigned k = (unsigned)sod_cell_axis(to_grid(v.z, K.nxf), K.xs[2], K.nx);
   return i + (unsigned)K.nx * (j + (unsigned)K.nx * k);
 }
 
@@ -2247,8 +2247,8 @@ __device__ __forceinline__ void cross_seed(const SodConst &K, const SodBufs &B, 
 
   // keep test (main:2118-2120)
   const double amass = dmul((double)masse, K.munit);
-  const bool keep = amass >= K.mmin && xc <= K.zmax && xc > K.zmin && yc <= K.zmax && yc > K.zmin &&
-                    zc <= K.zmax && zc > K.zmin;
+  const bool keep = amass >= K.mmin && xc <= K.zmax[0] && xc > K.zmin[0] && yc <= K.zmax[1] &&
+                    yc > K.zmin[1] && zc <= K.zmax[2] && zc > K.zmin[2];
 
   // 4a. profile (main:2103-2115): cumulative counts below each edge; the
   // region must hold every particle closer than the last edge
@@ -2459,12 +2459,12 @@ __device__ __forceinline__ int ball_row_ranges(const SodConst &K, const SodBufs 
 __device__ __forceinline__ unsigned warp_load_ball(const SodConst &K, const SodBufs &B, WSlice &W, const Region &G) {
   const int lane = threadIdx.x & 31;
   const double nxd = (double)K.nx;
-  auto rel = [&](double x, int i) {
-    double d = x - ((double)i + K.xs + 0.5);
+  auto rel = [&](double x, int i, int a) {
+    double d = x - ((double)i + K.xs[a] + 0.5);
     d = d - nxd * floor(d / nxd + 0.5);
     return d;
   };
-  const double tx = rel(G.xc, G.ic), ty = rel(G.yc, G.jc), tz = rel(G.zc, G.kc);
+  const double tx = rel(G.xc, G.ic, 0), ty = rel(G.yc, G.jc, 1), tz = rel(G.zc, G.kc, 2);
   const double rm = G.rb + 1e-3, rm2 = rm * rm;
   int jlo, jhi, klo, khi;
   ball_rows(K, ty, tz, rm, jlo, jhi, klo, khi);
@@ -2542,12 +2542,12 @@ __device__ __forceinline__ long long warp_stop(const SodConst &K, const WSlice &
 __device__ __forceinline__ unsigned warp_ball_records(const SodConst &K, const SodBufs &B, const Region &G) {
   const int lane = threadIdx.x & 31;
   const double nxd = (double)K.nx;
-  auto rel = [&](double x, int i) {
-    double d = x - ((double)i + K.xs + 0.5);
+  auto rel = [&](double x, int i, int a) {
+    double d = x - ((double)i + K.xs[a] + 0.5);
     d = d - nxd * floor(d / nxd + 0.5);
     return d;
   };
-  const double tx = rel(G.xc, G.ic), ty = rel(G.yc, G.jc), tz = rel(G.zc, G.kc);
+  const double tx = rel(G.xc, G.ic, 0), ty = rel(G.yc, G.jc, 1), tz = rel(G.zc, G.kc, 2);
   const double rm2 = G.rb * G.rb;
   int jlo, jhi, klo, khi;
   ball_rows(K, ty, tz, G.rb, jlo, jhi, klo, khi);
@@ -2647,8 +2647,8 @@ __global__ void __launch_bounds__(256) k_cross_warp(SodConst K, SodBufs B) {
   }
   // keep test (main:2118-2120)
   const double amass = dmul((double)masse, K.munit);
-  const bool keep = amass >= K.mmin && xc <= K.zmax && xc > K.zmin && yc <= K.zmax && yc > K.zmin &&
-                    zc <= K.zmax && zc > K.zmin;
+  const bool keep = amass >= K.mmin && xc <= K.zmax[0] && xc > K.zmin[0] && yc <= K.zmax[1] &&
+                    yc > K.zmin[1] && zc <= K.zmax[2] && zc > K.zmin[2];
   if (keep) {
     const double emax = dmul(rayon, B.edge_fac[K.nbins - 1]);
     if (!(emax * (1.0 + 1e-9) < G.rb)) {
@@ -2882,9 +2882,9 @@ __global__ void k_seed_blocks(const unsigned *seed_idx, const unsigned *inv, con
   long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= nseed) return;
   const float4 v = cube[inv[seed_idx[r]]];
-  const int ci = sod_cell_axis(to_grid(v.x, K.nxf), K.xs, K.nx) / bs;
-  const int cj = sod_cell_axis(to_grid(v.y, K.nxf), K.xs, K.nx) / bs;
-  const int ck = sod_cell_axis(to_grid(v.z, K.nxf), K.xs, K.nx) / bs;
+  const int ci = sod_cell_axis(to_grid(v.x, K.nxf), K.xs[0], K.nx) / bs;
+  const int cj = sod_cell_axis(to_grid(v.y, K.nxf), K.xs[1], K.nx) / bs;
+  const int ck = sod_cell_axis(to_grid(v.z, K.nxf), K.xs[2], K.nx) / bs;
   block_of[r] = (unsigned)ci + (unsigned)nb * ((unsigned)cj + (unsigned)nb * (unsigned)ck);
   rank[r] = (unsigned)r;
 }
@@ -3087,8 +3087,8 @@ __device__ __forceinline__ void tail_refine_cell(const SodConst &K, const SodBuf
                                                  const SeedGeo &g, RecTile &T) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
-  auto clear = [&](int c) {  // the 3-cell coordinate window stays clear of the box edge
-    double s0 = (double)(c - 1) + K.xs;
+  auto clear = [&](int c, int a) {  // the 3-cell coordinate window stays clear of the box edge
+    double s0 = (double)(c - 1) + K.xs[a];
     s0 -= K.tx * floor(s0 / K.tx);
     return s0 >= 1.0 && s0 + 3.0 <= K.tx - 1.0;
   };
@@ -3099,7 +3099,7 @@ __device__ __forceinline__ void tail_refine_cell(const SodConst &K, const SodBuf
     const unsigned coff = B.cell_off[ci];
     const int cxc = wrapi(g.ic + o / 9 - 1, K.nx), cyc = wrapi(g.jc + (o / 3) % 3 - 1, K.nx),
               czc = wrapi(g.kc + o % 3 - 1, K.nx);
-    const bool wf = clear(cxc) && clear(cyc) && clear(czc);
+    const bool wf = clear(cxc, 0) && clear(cyc, 1) && clear(czc, 2);
     const NbrList L = nbr_list(K, B, cxc, cyc, czc, g.ic, g.jc, g.kc);
     for (unsigned c0 = 0; c0 < cnt; c0 += 32) {
       const unsigned k = c0 + (unsigned)lane;
@@ -3598,7 +3598,7 @@ SodConst make_sod_const(const psod_ctx *c) {
   K.ncut = c->ncut;
   K.nxf = (float)c->nx;
   K.scale = c->scale;
-  K.xs = c->xxmin * c->scale;                 // main:1565
+  for (int a = 0; a < 3; a++) K.xs[a] = c->xxmin[a] * c->scale;  // main:1565
   K.tx = (double)c->nx;                       // main:1517
   K.delta = c->p.delta;
   K.delta2 = c->p.delta2;
@@ -3615,8 +3615,10 @@ SodConst make_sod_const(const psod_ctx *c) {
     while ((double)m * mu < (double)c->p.nmin) m++;
     K.mmin_count = (unsigned)m;
   }
-  K.zmin = 0.0 * c->scale;                    // main:420, 691
-  K.zmax = 1.0 * c->scale;                    // main:421, 692
+  for (int a = 0; a < 3; a++) {
+    K.zmin[a] = c->zone_lo[a] * c->scale;     // main:420, 691
+    K.zmax[a] = c->zone_hi[a] * c->scale;     // main:421, 692
+  }
   const double rmin = c->scale / c->nx;       // main:1526
   K.rmin2 = rmin * rmin;
   const double eps = c->scale / c->nx / 64.0; // main:1527

@@ -134,15 +134,15 @@ __global__ void __launch_bounds__(SLAB_THREADS) k_slab_scatter(const float *pos,
   }
 }
 
-__global__ void k_cell_count(const float4 *rec, long long n, float nxf, double xs, int nx, unsigned *cell,
+__global__ void k_cell_count(const float4 *rec, long long n, float nxf, double3 xs, int nx, unsigned *cell,
                              unsigned *count) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   unsigned c = 0xffffffffu;
   if (i < n) {
     const float4 v = rec[i];
-    const int ci = sod_cell_axis(to_grid(v.x, nxf), xs, nx);
-    const int cj = sod_cell_axis(to_grid(v.y, nxf), xs, nx);
-    const int ck = sod_cell_axis(to_grid(v.z, nxf), xs, nx);
+    const int ci = sod_cell_axis(to_grid(v.x, nxf), xs.x, nx);
+    const int cj = sod_cell_axis(to_grid(v.y, nxf), xs.y, nx);
+    const int ck = sod_cell_axis(to_grid(v.z, nxf), xs.z, nx);
     c = (unsigned)ci + (unsigned)nx * ((unsigned)cj + (unsigned)nx * (unsigned)ck);
     cell[i] = c;
   }
@@ -166,9 +166,9 @@ __device__ __forceinline__ unsigned sub_axis(float xg, double xs) {
   return (unsigned)min(max(s, 0), 3);
 }
 
-__device__ __forceinline__ unsigned sub_key(const float4 &p, float nxf, double xs) {
-  const unsigned a = sub_axis(to_grid(p.x, nxf), xs), b = sub_axis(to_grid(p.y, nxf), xs),
-                 c = sub_axis(to_grid(p.z, nxf), xs);
+__device__ __forceinline__ unsigned sub_key(const float4 &p, float nxf, double3 xs) {
+  const unsigned a = sub_axis(to_grid(p.x, nxf), xs.x), b = sub_axis(to_grid(p.y, nxf), xs.y),
+                 c = sub_axis(to_grid(p.z, nxf), xs.z);
   return (a & 1u) | ((b & 1u) << 1) | ((c & 1u) << 2) | ((a >> 1) << 3) | ((b >> 1) << 4) | ((c >> 1) << 5);
 }
 
@@ -196,7 +196,7 @@ __global__ void k_mark_big(unsigned *count, unsigned long long ncell, unsigned *
 }
 
 __global__ void k_sub_count(const float4 *rec, long long n, const unsigned *cell, const unsigned *count, float nxf,
-                            double xs, unsigned *tab) {
+                            double3 xs, unsigned *tab) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const unsigned v = count[cell[i]];
@@ -221,7 +221,7 @@ __global__ void k_sub_scan(unsigned *tab, const unsigned *bigcell, unsigned nbig
 }
 
 __global__ void k_cell_scatter(const float4 *rec, long long n, const unsigned *cell, unsigned *fill, unsigned *tab,
-                               float nxf, double xs, float4 *cube, unsigned *inv) {
+                               float nxf, double3 xs, float4 *cube, unsigned *inv) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const unsigned c = i < n ? cell[i] : 0xffffffffu;
   const unsigned v = i < n ? fill[c] : 0u;  // the flag bit never changes under the atomics below
@@ -259,9 +259,9 @@ __device__ __forceinline__ unsigned fine_axis(float xg, double xs, int bits) {
   return (unsigned)q & ((1u << bits) - 1u);
 }
 
-__device__ __forceinline__ unsigned fine_key(const float4 &p, float nxf, double xs, int bits) {
-  const unsigned a = fine_axis(to_grid(p.x, nxf), xs, bits), b = fine_axis(to_grid(p.y, nxf), xs, bits),
-                 c = fine_axis(to_grid(p.z, nxf), xs, bits);
+__device__ __forceinline__ unsigned fine_key(const float4 &p, float nxf, double3 xs, int bits) {
+  const unsigned a = fine_axis(to_grid(p.x, nxf), xs.x, bits), b = fine_axis(to_grid(p.y, nxf), xs.y, bits),
+                 c = fine_axis(to_grid(p.z, nxf), xs.z, bits);
   unsigned k = 0;
   for (int j = 0; j < bits; j++)
     k |= (((a >> j) & 1u) << (3 * j)) | (((b >> j) & 1u) << (3 * j + 1)) | (((c >> j) & 1u) << (3 * j + 2));
@@ -274,7 +274,7 @@ __device__ __forceinline__ unsigned fine_key(const float4 &p, float nxf, double 
 // updated.  tab holds the sub-cells' end slots (the scatter's cursors).
 __global__ void __launch_bounds__(256) k_sub_fine(float4 *cube, unsigned *inv, float4 *tmp, const unsigned *tab,
                                                   const unsigned *bigcell, const unsigned *start, float nxf,
-                                                  double xs) {
+                                                  double3 xs) {
   __shared__ unsigned hist[FINE_BINS_MAX];
   __shared__ unsigned wtot[8];
   const unsigned b = blockIdx.x;
@@ -336,16 +336,18 @@ __global__ void k_set_range(unsigned *a, unsigned long long lo, unsigned long lo
 // weights ddx (upper node) and dex (lower node).
 // ---------------------------------------------------------------------------
 struct CicConst {
-  double xxmin, xxmax, dx, kc;
+  double xxmin[3], xxmax[3];  // zone with buffer per axis, box units
+  double dx, kc;
   double inv_dx;  // 1/dx when it is exact (dx a power of two), else 0
   int nc;
+  int zone_test;  // 1: particles outside the zone with buffer are skipped (main:1138-1146)
 };
 
 // CIC along one axis (main:1154-1190): the two node indices and the weights
 // ddx (upper node) and dex (lower node).  (x - xxmin)/dx is formed as a
 // product when 1/dx is exact, which gives the same double.
-__device__ __forceinline__ void cic_axis(float xf, const CicConst &k, int &i0, int &i1, double &dd, double &de) {
-  const double diff = dsub((double)xf, k.xxmin);
+__device__ __forceinline__ void cic_axis(float xf, const CicConst &k, int a, int &i0, int &i1, double &dd, double &de) {
+  const double diff = dsub((double)xf, k.xxmin[a]);
   double d = k.inv_dx != 0.0 ? dmul(diff, k.inv_dx) : ddiv(diff, k.dx);
   int ix = (int)d;  // Fortran int(): truncation
   if (d < 0.0) ix = ix - 1;
@@ -368,19 +370,23 @@ __device__ __forceinline__ bool in_zone_periodic(double x, double lo, double hi)
          (x >= dsub(lo, 1.0) && x <= dsub(hi, 1.0));
 }
 
+// the particle selection of cic and cicm1 (main:1138-1146, 1309-1317)
+__device__ __forceinline__ bool in_cic_zone(const float4 &p, const CicConst &k) {
+  return in_zone_periodic(p.x, k.xxmin[0], k.xxmax[0]) && in_zone_periodic(p.y, k.xxmin[1], k.xxmax[1]) &&
+         in_zone_periodic(p.z, k.xxmin[2], k.xxmax[2]);
+}
+
 // deposit: 8 int64 atomics per particle, weights quantised to 2^-40
 __global__ void k_cic_deposit(const float4 *cube, long long n, CicConst k, unsigned long long *grid) {
   long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   float4 p = cube[i];
-  if (!(in_zone_periodic(p.x, k.xxmin, k.xxmax) && in_zone_periodic(p.y, k.xxmin, k.xxmax) &&
-        in_zone_periodic(p.z, k.xxmin, k.xxmax)))
-    return;
+  if (!in_cic_zone(p, k)) return;
   int ix, ixp, iy, iyp, iz, izp;
   double ddx, dex, ddy, dey, ddz, dez;
-  cic_axis(p.x, k, ix, ixp, ddx, dex);
-  cic_axis(p.y, k, iy, iyp, ddy, dey);
-  cic_axis(p.z, k, iz, izp, ddz, dez);
+  cic_axis(p.x, k, 0, ix, ixp, ddx, dex);
+  cic_axis(p.y, k, 1, iy, iyp, ddy, dey);
+  cic_axis(p.z, k, 2, iz, izp, ddz, dez);
   const long long nc = k.nc;
   const int cx[2] = {ix, ixp}, cy[2] = {iy, iyp}, cz[2] = {iz, izp};
   const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
@@ -401,16 +407,15 @@ __global__ void k_cic_interp(const float4 *cube, long long n, CicConst k, const 
   if (i >= n) return;
   float4 p = cube[i];
   unsigned idx = __float_as_uint(p.w) & PSOD_IDX_MASK;
-  if (!(in_zone_periodic(p.x, k.xxmin, k.xxmax) && in_zone_periodic(p.y, k.xxmin, k.xxmax) &&
-        in_zone_periodic(p.z, k.xxmin, k.xxmax))) {
+  if (!in_cic_zone(p, k)) {
     rho[idx] = 0.0;
     return;
   }
   int ix, ixp, iy, iyp, iz, izp;
   double ddx, dex, ddy, dey, ddz, dez;
-  cic_axis(p.x, k, ix, ixp, ddx, dex);
-  cic_axis(p.y, k, iy, iyp, ddy, dey);
-  cic_axis(p.z, k, iz, izp, ddz, dez);
+  cic_axis(p.x, k, 0, ix, ixp, ddx, dex);
+  cic_axis(p.y, k, 1, iy, iyp, ddy, dey);
+  cic_axis(p.z, k, 2, iz, izp, ddz, dez);
   const long long nc = k.nc;
   const int cx[2] = {ix, ixp}, cy[2] = {iy, iyp}, cz[2] = {iz, izp};
   const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
@@ -459,8 +464,11 @@ __device__ __forceinline__ void range_prefix(const unsigned *s_len, unsigned *s_
   if (lane == 31) s_pre[n] = x;
 }
 
-__global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsigned *cs, int nx, double xs, CicConst k,
-                                                  double *rho, int *bad) {
+// ZONE: particles outside the zone with buffer are skipped (zone contexts;
+// the test costs registers, so one-zone contexts run without it)
+template <bool ZONE>
+__global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsigned *cs, int nx, double3 xs, CicConst k,
+                                                  double *rho, int *bad, unsigned quirk_pos) {
   extern __shared__ __align__(16) unsigned long long win[];
   __shared__ unsigned s_rb[CRNG], s_len[CRNG], s_pre[CRNG + 1];
   const int ntile = nx / CT;
@@ -534,25 +542,31 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
     };
     for (unsigned fb = f0; fb < f1; fb += DEP_BATCH) {
       float4 vb[DEP_BATCH];
+      bool qb[DEP_BATCH];
 #pragma unroll
       for (unsigned u = 0; u < DEP_BATCH; u++) {
         const unsigned f = fb + u;
+        qb[u] = false;
         if (f < f1) {
           while (s_pre[r + 1] <= f) r++;
-          vb[u] = cube[s_rb[r] + (f - s_pre[r])];
+          const unsigned slot = s_rb[r] + (f - s_pre[r]);
+          vb[u] = cube[slot];
+          qb[u] = slot == quirk_pos;
         }
       }
 #pragma unroll
       for (unsigned u = 0; u < DEP_BATCH; u++) {
         if (fb + u >= f1) break;
+        if (qb[u]) continue;  // deposited below from its own cell
         const float4 v = vb[u];
         int ix, ixp, iy, iyp, iz, izp;
         double ddx, dex, ddy, dey, ddz, dez;
-        cic_axis(v.x, k, ix, ixp, ddx, dex);
-        cic_axis(v.y, k, iy, iyp, ddy, dey);
-        cic_axis(v.z, k, iz, izp, ddz, dez);
-        const int sx = sod_cell_axis(to_grid(v.x, nxf), xs, nx), sy = sod_cell_axis(to_grid(v.y, nxf), xs, nx),
-                  sz = sod_cell_axis(to_grid(v.z, nxf), xs, nx);
+        cic_axis(v.x, k, 0, ix, ixp, ddx, dex);
+        cic_axis(v.y, k, 1, iy, iyp, ddy, dey);
+        cic_axis(v.z, k, 2, iz, izp, ddz, dez);
+        if (ZONE && !in_cic_zone(v, k)) continue;
+        const int sx = sod_cell_axis(to_grid(v.x, nxf), xs.x, nx), sy = sod_cell_axis(to_grid(v.y, nxf), xs.y, nx),
+                  sz = sod_cell_axis(to_grid(v.z, nxf), xs.z, nx);
         if ((ix >> 1) != sx || (iy >> 1) != sy || (iz >> 1) != sz) {
           atomicOr(bad, 1);
           continue;
@@ -582,6 +596,45 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
     }
     flush();
   }
+  // The run scan files a single particle of the last cell under the
+  // previous cell's run (the linked-list quirk), which may lie in another
+  // tile.  Its CIC weights belong to its own cell: every tile whose cells
+  // with halo hold that cell deposits it, and the tile owning the cell
+  // interpolates it.
+  auto cell_rel = [&](int c, int c0) {  // periodic offset of cell c from c0 - 1
+    int d = c - (c0 - 1);
+    if (d < 0) d += nx;
+    if (d >= nx) d -= nx;
+    return d;
+  };
+  float4 vq = make_float4(0.f, 0.f, 0.f, 0.f);
+  int qx = 0, qy = 0, qz = 0;
+  const bool has_q = quirk_pos != 0xffffffffu;
+  if (has_q) {
+    vq = cube[quirk_pos];
+    qx = cell_rel(sod_cell_axis(to_grid(vq.x, nxf), xs.x, nx), x0);
+    qy = cell_rel(sod_cell_axis(to_grid(vq.y, nxf), xs.y, nx), y0);
+    qz = cell_rel(sod_cell_axis(to_grid(vq.z, nxf), xs.z, nx), z0);
+  }
+  if (threadIdx.x == 0 && has_q && qx <= CT + 1 && qy <= CT + 1 && qz <= CT + 1 &&
+      !(ZONE && !in_cic_zone(vq, k))) {
+    int ix, ixp, iy, iyp, iz, izp;
+    double ddx, dex, ddy, dey, ddz, dez;
+    cic_axis(vq.x, k, 0, ix, ixp, ddx, dex);
+    cic_axis(vq.y, k, 1, iy, iyp, ddy, dey);
+    cic_axis(vq.z, k, 2, iz, izp, ddz, dez);
+    const int cx[2] = {widx(ix, ox), widx(ixp, ox)}, cy[2] = {widx(iy, oy), widx(iyp, oy)},
+              cz[2] = {widx(iz, oz), widx(izp, oz)};
+    const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const int a = c & 1, bb = (c >> 1) & 1, ee = c >> 2;
+      if (cx[a] < CW && cy[bb] < CW && cz[ee] < CW) {
+        const double wgt = dmul(dmul(wx[a], wy[bb]), wz[ee]);
+        atomicAdd(&win[cx[a] + CW * (cy[bb] + CW * cz[ee])], (unsigned long long)__double2ll_rn(dmul(wgt, FIX_ONE)));
+      }
+    }
+  }
   __syncthreads();
   // own particles: rho in the reference's term order (main:1368-1383)
   for (int row = threadIdx.x; row < CT * CT; row += blockDim.x) {
@@ -597,11 +650,15 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
   const unsigned total = s_pre[CT * CT];
   auto interp = [&](const float4 v) {
     const unsigned idx = __float_as_uint(v.w) & PSOD_IDX_MASK;
+    if (ZONE && !in_cic_zone(v, k)) {  // not selected by cicm1: rho stays 0
+      rho[idx] = 0.0;
+      return;
+    }
     int ix, ixp, iy, iyp, iz, izp;
     double ddx, dex, ddy, dey, ddz, dez;
-    cic_axis(v.x, k, ix, ixp, ddx, dex);
-    cic_axis(v.y, k, iy, iyp, ddy, dey);
-    cic_axis(v.z, k, iz, izp, ddz, dez);
+    cic_axis(v.x, k, 0, ix, ixp, ddx, dex);
+    cic_axis(v.y, k, 1, iy, iyp, ddy, dey);
+    cic_axis(v.z, k, 2, iz, izp, ddz, dez);
     const int cx[2] = {widx(ix, ox), widx(ixp, ox)}, cy[2] = {widx(iy, oy), widx(iyp, oy)},
               cz[2] = {widx(iz, oz), widx(izp, oz)};
     const double wx[2] = {dex, ddx}, wy[2] = {dey, ddy}, wz[2] = {dez, ddz};
@@ -625,15 +682,20 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
   for (unsigned fa = threadIdx.x; fa < total; fa += 2 * blockDim.x) {
     const unsigned fb = fa + blockDim.x;
     while (s_pre[r + 1] <= fa) r++;
-    const float4 va = cube[s_rb[r] + (fa - s_pre[r])];
+    const unsigned sa = s_rb[r] + (fa - s_pre[r]);
+    const float4 va = cube[sa];
     float4 vb = va;
+    unsigned sb = sa;
     if (fb < total) {
       while (s_pre[r + 1] <= fb) r++;
-      vb = cube[s_rb[r] + (fb - s_pre[r])];
+      sb = s_rb[r] + (fb - s_pre[r]);
+      vb = cube[sb];
     }
-    interp(va);
-    if (fb < total) interp(vb);
+    if (sa != quirk_pos) interp(va);
+    if (fb < total && sb != quirk_pos) interp(vb);
   }
+  // the quirk particle, by the tile that owns its cell
+  if (threadIdx.x == 0 && has_q && qx >= 1 && qx <= CT && qy >= 1 && qy <= CT && qz >= 1 && qz <= CT) interp(vq);
 }
 
 __global__ void k_grid_to_double(const unsigned long long *grid, long long nnode, double kc, double *out) {
@@ -713,16 +775,17 @@ int stage_cellsort(psod_ctx *c, const float *dpos) {
   if ((st = ensure(c, &c->d_inv, &c->inv_cap, (size_t)n))) return st;
   PSOD_CUDA(c, cudaMemsetAsync(count, 0, sizeof(unsigned) * (c->ncell + 1), c->stream));
   PSOD_CUDA(c, cudaMemsetAsync(bad, 0, 2 * sizeof(int), c->stream));
-  const double xs = c->xxmin * c->scale;  // main:1565
+  // xxmin*scale per axis (main:1565); slabs follow the z axis
+  const double3 xs = make_double3(c->xxmin[0] * c->scale, c->xxmin[1] * c->scale, c->xxmin[2] * c->scale);
   // records grouped by slab first (see k_slab_scatter)
   const int nslab = std::min(nx, SLAB_MAX);
   PSOD_CUDA(c, cudaMemsetAsync(slabs, 0, sizeof(unsigned) * SLAB_MAX, c->stream));
   const unsigned ntile = nblk(n, SLAB_TILE);
-  k_slab_count<<<ntile, SLAB_THREADS, 0, c->stream>>>(dpos, n, (float)nx, xs, nx, nslab, slabs, bad);
+  k_slab_count<<<ntile, SLAB_THREADS, 0, c->stream>>>(dpos, n, (float)nx, xs.z, nx, nslab, slabs, bad);
   k_slab_scan<<<1, 32, 0, c->stream>>>(slabs, nslab, slabs + SLAB_MAX);
   const int slab_smem = SLAB_TILE * (int)(sizeof(float4) + sizeof(unsigned short));
   PSOD_CUDA(c, cudaFuncSetAttribute(k_slab_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, slab_smem));
-  k_slab_scatter<<<ntile, SLAB_THREADS, slab_smem, c->stream>>>(dpos, n, (float)nx, xs, nx, nslab, slabs + SLAB_MAX,
+  k_slab_scatter<<<ntile, SLAB_THREADS, slab_smem, c->stream>>>(dpos, n, (float)nx, xs.z, nx, nslab, slabs + SLAB_MAX,
                                                                 rec);
   k_cell_count<<<nblk(n, 256), 256, 0, c->stream>>>(rec, n, (float)nx, xs, nx, cell, count);
   if ((st = scan_u32(c, count, c->d_cell_start, (long long)c->ncell, true))) return st;
@@ -769,7 +832,7 @@ int stage_cellsort(psod_ctx *c, const float *dpos) {
       unsigned idx[3];
       for (int a = 0; a < 3; a++) {
         float xg = v[a] * (float)nx;  // exact product rounded once, as on the device
-        int i = (int)std::floor((double)xg - xs);
+        int i = (int)std::floor((double)xg - (a == 0 ? xs.x : a == 1 ? xs.y : xs.z));
         if (i < 0) i += nx;
         if (i >= nx) i -= nx;
         idx[a] = (unsigned)i;
@@ -796,8 +859,12 @@ static CicConst make_cic_const(const psod_ctx *c) {
   k.nc = 2 * c->nx;                                 // main:667
   k.dx = 1.0 / (double)k.nc;                        // main:1126
   k.inv_dx = ((k.nc & (k.nc - 1)) == 0) ? (double)k.nc : 0.0;
-  k.xxmin = c->xxmin;                               // main:665
-  k.xxmax = -c->xxmin + 1.0;                        // zone + buffer upper edge
+  for (int a = 0; a < 3; a++) {
+    k.xxmin[a] = c->xxmin[a];                       // main:665
+    k.xxmax[a] = c->xxmax[a];                       // zone + buffer upper edge
+  }
+  // one zone covers the box: every particle is selected
+  k.zone_test = c->nxcpu > 1 ? 1 : 0;
   const double vol = (k.dx * k.dx) * k.dx;          // main:1263
   k.kc = ((double)c->mpf / FIX_ONE) / vol;
   return k;
@@ -813,15 +880,22 @@ int stage_cic(psod_ctx *c, double *grid_out) {
   }
   // fused tile path (no global grid) when the box tiles evenly
   bool tiled = false;
-  if (c->nx % CT == 0 && c->nx >= 2 * (CT + 2) && c->xxmin <= 0.0 && -c->xxmin + 1.0 >= 1.0) {
+  if (c->nx % CT == 0 && c->nx >= 2 * (CT + 2)) {
     int *bad = nullptr;
     if ((st = scratch(c, SLOT_CIC_FLAG, 1, &bad))) return st;
     PSOD_CUDA(c, cudaMemsetAsync(bad, 0, sizeof(int), c->stream));
     const int smem = CW3 * (int)sizeof(unsigned long long);
-    PSOD_CUDA(c, cudaFuncSetAttribute(k_cic_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    PSOD_CUDA(c, cudaFuncSetAttribute(k_cic_tile<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    PSOD_CUDA(c, cudaFuncSetAttribute(k_cic_tile<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const long long ntiles = (long long)(c->nx / CT) * (c->nx / CT) * (c->nx / CT);
-    k_cic_tile<<<(unsigned)ntiles, 256, smem, c->stream>>>(c->d_cube, c->d_cell_start, c->nx,
-                                                           c->xxmin * c->scale, k, c->d_rho, bad);
+    const double3 xs = make_double3(c->xxmin[0] * c->scale, c->xxmin[1] * c->scale, c->xxmin[2] * c->scale);
+    const unsigned qpos = c->has_quirk ? c->quirk_pos : 0xffffffffu;
+    if (k.zone_test)
+      k_cic_tile<true><<<(unsigned)ntiles, 256, smem, c->stream>>>(c->d_cube, c->d_cell_start, c->nx, xs, k, c->d_rho,
+                                                                   bad, qpos);
+    else
+      k_cic_tile<false><<<(unsigned)ntiles, 256, smem, c->stream>>>(c->d_cube, c->d_cell_start, c->nx, xs, k, c->d_rho,
+                                                                    bad, qpos);
     int hbad = 0;
     PSOD_CUDA(c, cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     PSOD_CUDA(c, cudaStreamSynchronize(c->stream));

@@ -430,3 +430,20 @@ def read_cube_zone(root: str, ncpu: int, nzone: int, nx: int, nxbuffer: int = 0,
     if st != capi.OK:
         raise PsodError(st, f"psod_read_cube_zone({root}, zone {nzone}) failed")
     return pos[: n.value], vel[: n.value], ids[: n.value]
+
+
+def select_zone(pos, nx: int, nxcpu: int, nzone: int, nxbuffer: int = 0) -> np.ndarray:
+    """The driver's selection of one zone's particles with their buffer
+    (main:573-600) through ``psod_select_zone``: a boolean mask over ``pos``
+    ((n, 3) float32, box units) of the particles that a context with
+    ``nxcpu=nxcpu, nzone=nzone`` is loaded with, in input order."""
+    lib = capi.load()
+    pos = np.ascontiguousarray(pos, np.float32)
+    n = pos.shape[0]
+    keep = np.zeros(max(n, 1), np.uint8)
+    nk = C.c_int64(0)
+    st = lib.psod_select_zone(nx, nxcpu, nzone, nxbuffer, _ptr(pos), n, _ptr(keep), C.byref(nk))
+    if st != capi.OK:
+        raise PsodError(st, f"psod_select_zone(nx={nx}, nxcpu={nxcpu}, nzone={nzone}) failed")
+    return keep[:n].astype(bool)
+

@@ -28,7 +28,7 @@ def test_library_exports_header():
 
 def test_abi_version_and_strings():
     lib = capi.load()
-    assert lib.psod_abi_version() == 3
+    assert lib.psod_abi_version() == 4
     assert b"nsel" in lib.psod_status_string(capi.ERR_NSEL)
     assert lib.psod_status_string(capi.OK) == b"ok"
 
