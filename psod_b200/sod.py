@@ -75,7 +75,10 @@ def _ptr(t):
 
 
 class SphericalOverdensity:
-    """One zone of the SOD stage on one GPU (the reference's 1-rank run)."""
+    """One zone of the SOD stage on one GPU: the whole periodic box (the
+    reference's 1-rank run) by default, or zone ``nzone`` of ``nxcpu``^3
+    (``nxcpu=``, ``nzone=`` parameters) loaded with that zone's particles
+    and buffer (``select_zone``)."""
 
     def __init__(self, nx: int, device: int = 0, **params):
         self.lib = capi.load()
