@@ -227,3 +227,26 @@ def test_gpu_zones_match_oracle(oracle, nx, nxcpu, nmax, mode):
             assert np.array_equal(getattr(t, f), getattr(r, f)), (z, f)
         total += t.nhalo
     assert total > 0
+
+
+@pytest.mark.gpu
+def test_gpu_zone_runner_and_count(oracle):
+    """psod_b200.zones on one GPU: every zone of the 32^3 box through the
+    GPU zone runner; the tables (member indices back in the full particle
+    arrays) and the summed count equal the oracle's zone runs."""
+    _gpu_or_skip()
+    from psod_b200 import synth
+    from psod_b200.zones import gpu_zone_runner, run_zones
+
+    b = synth.make_box(32, nmax_halo=2000, seed=11)
+    pos, ids = b.pos.numpy(), b.ids.numpy()
+    n = pos.shape[0]
+    tables, count = run_zones(pos, ids, 2, gpu_zone_runner(32, 2, mode=1))
+    total = 0
+    for z, t in tables.items():
+        sel = np.nonzero(oracle.zone_select(pos, 32, 2, z))[0]
+        r = oracle.run(oracle.Params(nx=32, nxcpu=2, nzone=z, npart_total=n), pos[sel], ids[sel], oracle.CANONICAL)
+        assert np.array_equal(t.halo_id, r.halo_id) and np.array_equal(t.halo_mass, r.halo_mass), z
+        assert np.array_equal(t.member_index, sel[r.member_index]), z
+        total += r.nhalo
+    assert count == total > 0
