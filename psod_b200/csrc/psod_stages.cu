@@ -499,6 +499,9 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
       if (pb[q] >= pa[q]) {
         rb = cs[base + (unsigned)pa[q]];
         len = cs[base + (unsigned)pb[q] + 1] - rb;
+        // the quirk particle (the cube's last record, at the end of its
+        // listed cell's run) is deposited below from its own cell
+        if (len && rb + len - 1u == quirk_pos) len--;
       }
       s_rb[2 * row + q] = rb;
       s_len[2 * row + q] = len;
@@ -542,22 +545,17 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
     };
     for (unsigned fb = f0; fb < f1; fb += DEP_BATCH) {
       float4 vb[DEP_BATCH];
-      bool qb[DEP_BATCH];
 #pragma unroll
       for (unsigned u = 0; u < DEP_BATCH; u++) {
         const unsigned f = fb + u;
-        qb[u] = false;
         if (f < f1) {
           while (s_pre[r + 1] <= f) r++;
-          const unsigned slot = s_rb[r] + (f - s_pre[r]);
-          vb[u] = cube[slot];
-          qb[u] = slot == quirk_pos;
+          vb[u] = cube[s_rb[r] + (f - s_pre[r])];
         }
       }
 #pragma unroll
       for (unsigned u = 0; u < DEP_BATCH; u++) {
         if (fb + u >= f1) break;
-        if (qb[u]) continue;  // deposited below from its own cell
         const float4 v = vb[u];
         int ix, ixp, iy, iyp, iz, izp;
         double ddx, dex, ddy, dey, ddz, dez;
@@ -641,8 +639,10 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
     const int yy = y0 + row % CT, zz = z0 + row / CT;
     const unsigned long long base = (unsigned long long)nx * ((unsigned)yy + (unsigned long long)nx * (unsigned)zz);
     const unsigned rb = cs[base + (unsigned)x0];
+    unsigned len = cs[base + (unsigned)(x0 + CT - 1) + 1] - rb;
+    if (len && rb + len - 1u == quirk_pos) len--;  // interpolated below, by its own cell's tile
     s_rb[row] = rb;
-    s_len[row] = cs[base + (unsigned)(x0 + CT - 1) + 1] - rb;
+    s_len[row] = len;
   }
   __syncthreads();
   range_prefix(s_len, s_pre, CT * CT);
@@ -682,17 +682,14 @@ __global__ void __launch_bounds__(256) k_cic_tile(const float4 *cube, const unsi
   for (unsigned fa = threadIdx.x; fa < total; fa += 2 * blockDim.x) {
     const unsigned fb = fa + blockDim.x;
     while (s_pre[r + 1] <= fa) r++;
-    const unsigned sa = s_rb[r] + (fa - s_pre[r]);
-    const float4 va = cube[sa];
+    const float4 va = cube[s_rb[r] + (fa - s_pre[r])];
     float4 vb = va;
-    unsigned sb = sa;
     if (fb < total) {
       while (s_pre[r + 1] <= fb) r++;
-      sb = s_rb[r] + (fb - s_pre[r]);
-      vb = cube[sb];
+      vb = cube[s_rb[r] + (fb - s_pre[r])];
     }
-    if (sa != quirk_pos) interp(va);
-    if (fb < total && sb != quirk_pos) interp(vb);
+    interp(va);
+    if (fb < total) interp(vb);
   }
   // the quirk particle, by the tile that owns its cell
   if (threadIdx.x == 0 && has_q && qx >= 1 && qx <= CT && qy >= 1 && qy <= CT && qz >= 1 && qz <= CT) interp(vq);
