@@ -1638,8 +1638,8 @@ __global__ void __launch_bounds__(256, 3) k_refine_warp(SodConst K, SodBufs B) {
                           ez = fmaxf(fmaxf(loz - rec.z, rec.z - hiz), 0.f);
               const float db2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
               if (BOUND) {
-                // far records add k(d to the group's box) to every sub-group
-                // here; near ones go to the tile for the sub-group boxes
+                // far records add k(d to the group's box) to every
+                // candidate here; near ones go to the tile for exact sums
                 if (keep && db2 >= NEAR2 && db2 <= 1.0001f) uf += rsqrt_pos(db2 + e2b);
                 keep = keep && db2 < NEAR2;
               } else {
