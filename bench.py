@@ -27,6 +27,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -888,6 +889,87 @@ def relaunch_with_torchrun(args):
     return subprocess.call(cmd)
 
 
+def run_zones(args):
+    """The reference's zone decomposition on one GPU: the workload's box cut
+    into K^3 zones (-npu's buffer, main:211-219), each zone's particles and
+    buffer selected by the FP64 test of psod_select_zone (main:578-584, here
+    on the device over the resident box), and a zone context per zone
+    running the SOD stage (cell sort, CIC, seed order, spherover) on them in
+    turn.  value: kept halos of all zones per second of summed device time
+    of the zone steps (the selection and the context set-up untimed); the
+    zone catalogues together are compared with the one-zone run's halo
+    count.  A report run, not the bench contract's timing."""
+    import torch
+
+    from psod_b200 import synth
+    from psod_b200.sod import SphericalOverdensity
+
+    nx, k = args.nx, args.zones
+    wl = WORKLOADS.get(nx, dict(nmax_halo=20000, box=f"{nx}^3"))
+    thresholds = dict(delta_extra=EXTRA_DELTAS, nbins=EXTRA_BINS) if args.ndelta else {}
+    # the learned mode needs a trained bracket: zones run batched (or plain)
+    params = dict(npu=npu_for(nx), mode=0 if args.mode_id == 0 else 1, **thresholds)
+    torch.cuda.set_device(0)
+    box = synth.make_box(nx, nmax_halo=wl["nmax_halo"], seed=args.seed, device="cuda:0")
+    pos_d, ids_d = box.pos, box.ids
+    del box
+    torch.cuda.empty_cache()
+    n = int(pos_d.shape[0])
+    with SphericalOverdensity(nx, device=0, **params) as one:
+        one.load(pos_d, ids_d)
+        one_st = one.run()
+    torch.cuda.empty_cache()
+    nxzone = nx // k
+    # the buffer -npu derives (main:211-219, as psod_ctx_create does), else half a zone
+    npu = params["npu"]
+    nxb = 4 * math.ceil((npu * 2.0 / 200.0) ** (1.0 / 3.0) / 2.0) if npu > 0 else nxzone // 2
+    rs = (0.5 + nxb / float(nxzone)) / float(k)
+
+    def axis_keep(col, i):
+        xc = ((i / float(k)) + ((i + 1) / float(k))) / 2.0
+        d = (pos_d[:, col].double() - xc).abs()
+        return (d < rs) | (d > 1.0 - rs)
+
+    total_ms, halos, parts = 0.0, 0, 0
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for z in range(k ** 3):
+        ix, iy, iz = z // (k * k), (z // k) % k, z % k
+        keep = axis_keep(0, ix) & axis_keep(1, iy) & axis_keep(2, iz)
+        sel = torch.nonzero(keep).squeeze(1)
+        p, i = pos_d[sel].contiguous(), ids_d[sel].contiguous()
+        del keep, sel
+        with SphericalOverdensity(nx, device=0, nxcpu=k, nzone=z, **params) as s:
+            s.load(p, i, npart_total=n)  # warm-up: sizes the context's buffers
+            s.run()
+            torch.cuda.synchronize()
+            ev0.record()
+            s.load(p, i, npart_total=n)
+            st = s.run()
+            ev1.record()
+            torch.cuda.synchronize()
+        total_ms += ev0.elapsed_time(ev1)
+        halos += st["nhalo"]
+        parts += int(p.shape[0])
+        del p, i
+        torch.cuda.empty_cache()
+    line = {
+        "metric": METRIC + ", zone decomposition",
+        "value": round(halos / (total_ms / 1000.0), 2),
+        "unit": "halos/s",
+        "n_gpus": 1,
+        "zones": k ** 3,
+        "ms_all_zones": round(total_ms, 1),
+        "halos": halos,
+        "one_zone_halos": one_st["nhalo"],
+        "particles_loaded": parts,
+        "particles": n,
+        "nxbuffer": nxb,
+        "config": workload_config(nx, args.ndelta, False),
+        "data": "synthetic NFW-mixture box (seeded); zone particles resident in HBM",
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -907,6 +989,8 @@ def main():
                     help="time the halo-properties stage (psod_halo_properties) on the SOD table; one GPU")
     ap.add_argument("--fof", action="store_true",
                     help="time the friends-of-friends stage (psod_fof) instead of SOD; one GPU")
+    ap.add_argument("--zones", type=int, default=0,
+                    help="report run of the reference's zone decomposition: the box as K^3 zones in turn; one GPU")
     ap.add_argument("--heavy", action="store_true",
                     help="the heavy-tail stress box (1024^3 + 16 clusters of 5e6, -npu 1e7, Delta 200/500, 64 bins)")
     args = ap.parse_args()
@@ -919,6 +1003,8 @@ def main():
         run_fof(args)
     elif args.props:
         run_props(args)
+    elif args.zones > 0:
+        run_zones(args)
     else:
         run_ours(args)
 
