@@ -3640,7 +3640,7 @@ enum {
   SC_HRDELTA, SC_HPOOL, SC_COUNTS, SC_ST_ACTIVE, SC_ST_NA, SC_ST_COFF, SC_ST_CN,
   SC_ST_CENTRE, SC_CAND_POS, SC_CAND_SLOT, SC_CAND_S, SC_ORDER, SC_RKEYS, SC_MASS32, SC_MOFF, SC_TKEY, SC_TIDX,
   SC_CELLCNT, SC_CELLOFF, SC_CELLCHUNK, SC_CHUNKPREF, SC_ACT_A, SC_ACT_B, SC_BPOS, SC_CELLNCH, SC_FEAT, SC_RB0,
-  SC_SBEST, SC_CELLGROUPS, SC_GROUPPREF, SC_GU, SC_CANDLIST, SC_CNT2, SC_LMAX, SC_BIG, SC_RESOLVED, SC_BIDXRANK,
+  SC_SBEST, SC_CELLGROUPS, SC_GROUPPREF, SC_CANDU, SC_CANDLIST, SC_CNT2, SC_LMAX, SC_BIG, SC_RESOLVED, SC_BIDXRANK,
   SC_BIDXCUBE, SC_TOPG, SC_XKEY, SC_XIDX, SC_XPOS, SC_TAIL, SC_BIGSEG
 };
 static_assert((int)SC_BIGSEG < (int)SLOT_CELL_U32, "SOD scratch slots overlap the shared ones");
@@ -3758,7 +3758,7 @@ int stage_spherover(psod_ctx *c, psod_run_stats *out_stats) {
   float *cand_u;
   if ((rc = scratch(c, SC_CELLGROUPS, (size_t)cap_ready * 27, &cell_groups)) ||
       (rc = scratch(c, SC_GROUPPREF, (size_t)cap_ready * 27 + 1, &group_pref)) ||
-      (rc = scratch(c, SC_GU, (size_t)cand_cap, &cand_u)) || (rc = scratch(c, SC_CANDLIST, (size_t)cand_cap, &cand_list)) ||
+      (rc = scratch(c, SC_CANDU, (size_t)cand_cap, &cand_u)) || (rc = scratch(c, SC_CANDLIST, (size_t)cand_cap, &cand_list)) ||
       (rc = scratch(c, SC_CNT2, (size_t)cap_ready * 27 * 3 + 1, &cnt2)) ||
       (rc = scratch(c, SC_LMAX, (size_t)cap_ready, &s_lmax)))
     return rc;
