@@ -250,3 +250,17 @@ def test_gpu_zone_runner_and_count(oracle):
         assert np.array_equal(t.member_index, sel[r.member_index]), z
         total += r.nhalo
     assert count == total > 0
+
+
+def test_oracle_refuses_the_same_zone_parameters(oracle):
+    """The oracle's zone set-up refuses what psod_ctx_create refuses: nx not
+    a multiple of nxcpu, nzone out of range, a buffer wider than the zone,
+    and a local grid just short of the box."""
+    pos = np.random.default_rng(1).random((1000, 3)).astype(np.float32)
+    ids = np.arange(1000, dtype=np.int64)
+    for kw in (dict(nx=32, nxcpu=3), dict(nx=32, nxcpu=2, nzone=8), dict(nx=32, nxcpu=2, nxbuffer=17),
+               dict(nx=48, nxcpu=2, nxbuffer=11, ncut=4)):
+        r = oracle.run(oracle.Params(npart_total=1000, **kw), pos, ids, oracle.CANONICAL)
+        assert r.status != 0, kw
+    r = oracle.run(oracle.Params(nx=48, nxcpu=3, nzone=13, npart_total=1000), pos, ids, oracle.CANONICAL)
+    assert r.status == 0
