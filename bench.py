@@ -915,10 +915,12 @@ def run_zones(args):
     del box
     torch.cuda.empty_cache()
     n = int(pos_d.shape[0])
-    with SphericalOverdensity(nx, device=0, **params) as one:
-        one.load(pos_d, ids_d)
-        one_st = one.run()
-    torch.cuda.empty_cache()
+    one_st = {"nhalo": None}
+    if args.zone_only < 0:  # the one-zone run, for the catalogue comparison
+        with SphericalOverdensity(nx, device=0, **params) as one:
+            one.load(pos_d, ids_d)
+            one_st = one.run()
+        torch.cuda.empty_cache()
     nxzone = nx // k
     # the buffer -npu derives (main:211-219, as psod_ctx_create does), else half a zone
     npu = params["npu"]
@@ -932,7 +934,7 @@ def run_zones(args):
 
     total_ms, halos, parts = 0.0, 0, 0
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for z in range(k ** 3):
+    for z in (range(k ** 3) if args.zone_only < 0 else [args.zone_only]):
         ix, iy, iz = z // (k * k), (z // k) % k, z % k
         keep = axis_keep(0, ix) & axis_keep(1, iy) & axis_keep(2, iz)
         sel = torch.nonzero(keep).squeeze(1)
@@ -957,7 +959,7 @@ def run_zones(args):
         "value": round(halos / (total_ms / 1000.0), 2),
         "unit": "halos/s",
         "n_gpus": 1,
-        "zones": k ** 3,
+        "zones": k ** 3 if args.zone_only < 0 else 1,
         "ms_all_zones": round(total_ms, 1),
         "halos": halos,
         "one_zone_halos": one_st["nhalo"],
@@ -991,6 +993,8 @@ def main():
                     help="time the friends-of-friends stage (psod_fof) instead of SOD; one GPU")
     ap.add_argument("--zones", type=int, default=0,
                     help="report run of the reference's zone decomposition: the box as K^3 zones in turn; one GPU")
+    ap.add_argument("--zone-only", dest="zone_only", type=int, default=-1,
+                    help="with --zones: run only this zone (no one-zone comparison)")
     ap.add_argument("--heavy", action="store_true",
                     help="the heavy-tail stress box (1024^3 + 16 clusters of 5e6, -npu 1e7, Delta 200/500, 64 bins)")
     args = ap.parse_args()
